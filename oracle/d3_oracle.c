@@ -1,0 +1,803 @@
+/* FP64 CPU oracle for the D3 dispersion hot path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
+ * this file, as the checker.  It is a loop-for-loop restatement of the
+ * reference Fortran (s-dftd3 v1.6.0); every function names the file:line it
+ * follows.  Loop orders, expression orders and the OpenMP thread-private
+ * accumulation follow the reference so the results agree to rounding.
+ *
+ * Parity pins: the tests compare this oracle with the reference's golden
+ * vectors (the JSON files in tests/golden, generated from the reference's test files by
+ * tests/golden/make_golden.py). */
+#include "d3_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../simple-dftd3_b200/csrc/d3_tables.h"
+
+#define EPS DBL_EPSILON
+#define KCN 16.0                 /* ncoord.f90:31 */
+#define WF 4.0                   /* model.f90:80 */
+#define RS9 (4.0 / 3.0)          /* rational.f90:73, zero.f90:77 */
+
+/* ---------------------------------------------------------------- model -- */
+
+typedef struct {
+    int nid, mref;
+    int *id;          /* [nat] species index */
+    int *num;         /* [nid] atomic number */
+    int *ref;         /* [nid] */
+    double *rcov;     /* [nid] */
+    double *r4r2;     /* [nid] */
+    double *rvdw;     /* [nid][nid] */
+    double *cn;       /* [nid][mref], cn[isp*mref + iref] */
+    double *c6;       /* c6(iref, jref, isp, jsp) at ((isp*nid + jsp)*mref + iref)*mref + jref */
+    int *ghost;       /* [nat] */
+} model_t;
+
+double oracle_covalent_radius(int z)
+{
+    /* mctc-lib get_covalent_rad: 4/3 scaled D3 covalent radius in Bohr */
+    if (z < 1 || z > D3_MAX_ELEM_R4R2) return 0.0;
+    return 4.0 / 3.0 * (D3_AATOAU * d3_rcov_aa[z - 1]);
+}
+
+double oracle_r4r2(int z)
+{
+    /* data/r4r2.f90:69-70, 91-105 */
+    if (z < 1 || z > D3_MAX_ELEM_R4R2) return 0.0;
+    return sqrt(0.5 * (d3_r4_over_r2[z - 1] * sqrt((double)z)));
+}
+
+static double get_vdw_rad(int z1, int z2)
+{
+    /* data/vdwrad.f90:1163-1197 (both inside the table for Z <= 103) */
+    int ic = z1 > z2 ? (z2 - 1) + z1 * (z1 - 1) / 2 : (z1 - 1) + z2 * (z2 - 1) / 2;
+    return D3_AATOAU * d3_vdwrad_aa[ic];
+}
+
+static double get_c6(int iref, int jref, int ati, int atj)
+{
+    /* reference.f90:160-171, 0-based reference indices, 1-based Z */
+    int ic;
+    if (ati > atj) {
+        ic = (atj - 1) + ati * (ati - 1) / 2;
+        return d3_c6ab[ic * 49 + jref * 7 + iref];
+    }
+    ic = (ati - 1) + atj * (atj - 1) / 2;
+    return d3_c6ab[ic * 49 + iref * 7 + jref];
+}
+
+static void model_free(model_t *m)
+{
+    free(m->id); free(m->num); free(m->ref); free(m->rcov); free(m->r4r2);
+    free(m->rvdw); free(m->cn); free(m->c6); free(m->ghost);
+}
+
+static int model_new(model_t *m, int nat, const int *numbers, const int *ghost)
+{
+    /* species by first occurrence (mctc-lib structure constructor), then
+     * new_d3_model (model.f90:87-181) */
+    memset(m, 0, sizeof(*m));
+    m->id = malloc(sizeof(int) * (nat > 0 ? nat : 1));
+    m->num = malloc(sizeof(int) * (nat > 0 ? nat : 1));
+    for (int i = 0; i < nat; i++) {
+        int z = numbers[i], s;
+        if (z < 1 || z > D3_MAX_ELEM) { free(m->id); free(m->num); return 1; }
+        for (s = 0; s < m->nid; s++) if (m->num[s] == z) break;
+        if (s == m->nid) m->num[m->nid++] = z;
+        m->id[i] = s;
+    }
+    int nid = m->nid;
+    m->ref = malloc(sizeof(int) * nid);
+    m->mref = 0;
+    for (int s = 0; s < nid; s++) {
+        m->ref[s] = d3_nref[m->num[s] - 1];
+        if (m->ref[s] > m->mref) m->mref = m->ref[s];
+    }
+    int mref = m->mref;
+    m->rcov = malloc(sizeof(double) * nid);
+    m->r4r2 = malloc(sizeof(double) * nid);
+    for (int s = 0; s < nid; s++) {
+        m->rcov[s] = oracle_covalent_radius(m->num[s]);
+        m->r4r2[s] = oracle_r4r2(m->num[s]);
+    }
+    m->rvdw = malloc(sizeof(double) * nid * nid);
+    for (int is = 0; is < nid; is++)
+        for (int js = 0; js <= is; js++) {
+            double r = get_vdw_rad(m->num[js], m->num[is]);
+            m->rvdw[js * nid + is] = r;
+            m->rvdw[is * nid + js] = r;
+        }
+    m->cn = calloc((size_t)mref * nid, sizeof(double));
+    for (int s = 0; s < nid; s++)
+        for (int r = 0; r < m->ref[s]; r++)
+            m->cn[s * mref + r] = d3_refcn[(m->num[s] - 1) * 7 + r];
+    m->c6 = calloc((size_t)mref * mref * nid * nid, sizeof(double));
+#define MC6(ir, jr, is, js) m->c6[(((size_t)(is) * nid + (js)) * mref + (ir)) * mref + (jr)]
+    for (int is = 0; is < nid; is++)
+        for (int js = 0; js <= is; js++)
+            for (int ir = 0; ir < m->ref[is]; ir++)
+                for (int jr = 0; jr < m->ref[js]; jr++) {
+                    MC6(jr, ir, js, is) = get_c6(jr, ir, m->num[js], m->num[is]);
+                    MC6(ir, jr, is, js) = MC6(jr, ir, js, is);
+                }
+    m->ghost = calloc(nat > 0 ? nat : 1, sizeof(int));
+    if (ghost)
+        for (int i = 0; i < nat; i++) m->ghost[i] = ghost[i] != 0;
+    return 0;
+}
+
+/* --------------------------------------------------------------- cutoff -- */
+
+static void crossproduct(const double *a, const double *b, double *c)
+{
+    /* cutoff.f90:229-238 */
+    double x = a[1] * b[2] - b[1] * a[2];
+    double y = a[2] * b[0] - b[2] * a[0];
+    double z = a[0] * b[1] - b[0] * a[1];
+    c[0] = x; c[1] = y; c[2] = z;
+}
+
+/* lat[k][c]: column k of the Fortran lat(3,3), i.e. vector k */
+static void get_translations(const double lat[3][3], double rthr, int rep[3])
+{
+    /* cutoff.f90:204-227 */
+    double norm[3][3];
+    crossproduct(lat[1], lat[2], norm[0]);
+    crossproduct(lat[2], lat[0], norm[1]);
+    crossproduct(lat[0], lat[1], norm[2]);
+    for (int k = 0; k < 3; k++) {
+        double n2 = sqrt(norm[k][0] * norm[k][0] + norm[k][1] * norm[k][1] + norm[k][2] * norm[k][2]);
+        for (int c = 0; c < 3; c++) norm[k][c] = norm[k][c] / n2;
+    }
+    for (int k = 0; k < 3; k++) {
+        double cs = norm[k][0] * lat[k][0] + norm[k][1] * lat[k][1] + norm[k][2] * lat[k][2];
+        rep[k] = (int)ceil(fabs(rthr / cs));
+    }
+}
+
+int oracle_lattice_points(const double *lattice, const int *periodic, double rthr,
+                          double *trans, int cap)
+{
+    /* get_lattice_points, cutoff.f90:140-186 */
+    int np = (periodic[0] != 0) + (periodic[1] != 0) + (periodic[2] != 0);
+    double lat[3][3];
+    int rep[3] = {0, 0, 0};
+    if (np == 0) {
+        if (trans && cap >= 1) trans[0] = trans[1] = trans[2] = 0.0;
+        return 1;
+    }
+    for (int k = 0; k < 3; k++)
+        for (int c = 0; c < 3; c++) lat[k][c] = lattice[k * 3 + c];
+    if (np == 3) {
+        get_translations(lat, rthr, rep);
+    } else if (np == 1) {
+        for (int k = 0; k < 3; k++) {
+            double v = sqrt(lat[k][0] * lat[k][0] + lat[k][1] * lat[k][1] + lat[k][2] * lat[k][2]);
+            rep[k] = periodic[k] ? (int)ceil(rthr / v) : 0;
+        }
+    } else {
+        /* get_normals, then norms(i, :) = lat(i, :) where periodic(i) */
+        double norms[3][3];
+        for (int k = 0; k < 3; k++)
+            crossproduct(lat[(k + 1) % 3], lat[(k + 2) % 3], norms[k]);
+        for (int k = 0; k < 3; k++)
+            for (int c = 0; c < 3; c++)
+                if (periodic[c]) norms[k][c] = lat[k][c];
+        get_translations(norms, rthr, rep);
+        for (int k = 0; k < 3; k++) if (!periodic[k]) rep[k] = 0;
+    }
+    int n = (2 * rep[0] + 1) * (2 * rep[1] + 1) * (2 * rep[2] + 1);
+    if (trans && cap >= n) {
+        int itr = 0;
+        for (int ix = -rep[0]; ix <= rep[0]; ix++)
+            for (int iy = -rep[1]; iy <= rep[1]; iy++)
+                for (int iz = -rep[2]; iz <= rep[2]; iz++, itr++)
+                    for (int c = 0; c < 3; c++)
+                        trans[itr * 3 + c] = lat[0][c] * ix + lat[1][c] * iy + lat[2][c] * iz;
+    }
+    return n;
+}
+
+static double *lattice_points(const double *lattice, const int *periodic, double rthr, int *ntr)
+{
+    int n = oracle_lattice_points(lattice, periodic, rthr, NULL, 0);
+    double *t = malloc(sizeof(double) * 3 * n);
+    oracle_lattice_points(lattice, periodic, rthr, t, n);
+    *ntr = n;
+    return t;
+}
+
+static void smooth_cutoff(double r, double cutoff, double width, double *sw, double *dswdr)
+{
+    /* cutoff.f90:73-99 */
+    if (width <= 0.0 || width >= cutoff) {
+        *sw = 1.0; *dswdr = 0.0;
+    } else {
+        double inner = cutoff - width;
+        if (r <= inner) { *sw = 1.0; *dswdr = 0.0; }
+        else if (r >= cutoff) { *sw = 0.0; *dswdr = 0.0; }
+        else {
+            double x = (cutoff - r) / width;
+            *sw = x * x * x * (10.0 + x * (-15.0 + 6.0 * x));
+            *dswdr = -30.0 * x * x * (1.0 - x) * (1.0 - x) / width;
+        }
+    }
+}
+
+/* ------------------------------------------------------------ partition -- */
+
+static int owns_pair(int part, int nparts, int i, int j)
+{
+    /* partition.f90:127-147 with 0-based i >= j */
+    if (nparts <= 1) return 1;
+    long long idx = (long long)i * (i + 1) / 2 + j;
+    return idx % nparts == part;
+}
+
+/* ------------------------------------------------------------------ wrap -- */
+
+static void matinv_3x3(const double a[3][3], double inv[3][3])
+{
+    /* inverse by cofactors (mctc-lib matinv_3x3); a[r][c] is row r, col c */
+    double det = a[0][0] * a[1][1] * a[2][2] - a[0][0] * a[1][2] * a[2][1]
+               - a[0][1] * a[1][0] * a[2][2] + a[0][1] * a[1][2] * a[2][0]
+               + a[0][2] * a[1][0] * a[2][1] - a[0][2] * a[1][1] * a[2][0];
+    double d = 1.0 / det;
+    inv[0][0] = +d * (a[1][1] * a[2][2] - a[1][2] * a[2][1]);
+    inv[1][0] = -d * (a[1][0] * a[2][2] - a[1][2] * a[2][0]);
+    inv[2][0] = +d * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+    inv[0][1] = -d * (a[0][1] * a[2][2] - a[0][2] * a[2][1]);
+    inv[1][1] = +d * (a[0][0] * a[2][2] - a[0][2] * a[2][0]);
+    inv[2][1] = -d * (a[0][0] * a[2][1] - a[0][1] * a[2][0]);
+    inv[0][2] = +d * (a[0][1] * a[1][2] - a[0][2] * a[1][1]);
+    inv[1][2] = -d * (a[0][0] * a[1][2] - a[0][2] * a[1][0]);
+    inv[2][2] = +d * (a[0][0] * a[1][1] - a[0][1] * a[1][0]);
+}
+
+static double shift_back_abc(double in)
+{
+    /* utils.f90:48-64 */
+    const double eps = 1.0e-14;
+    double out = in;
+    if (in < (0.0 - eps)) out = in + ceil(-in);
+    if (in > (1.0 + eps)) out = in - floor(in);
+    if (fabs(in - 1.0) < eps) out = in - 1.0;
+    return out;
+}
+
+void oracle_wrap_to_central_cell(int nat, double *xyz, const double *lattice, const int *periodic)
+{
+    /* utils.f90:29-44: matrix M has the lattice vectors as columns */
+    if (!(periodic[0] || periodic[1] || periodic[2])) return;
+    double m[3][3], inv[3][3];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) m[r][c] = lattice[c * 3 + r];
+    matinv_3x3(m, inv);
+    for (int i = 0; i < nat; i++) {
+        double *x = xyz + 3 * i, f[3];
+        for (int r = 0; r < 3; r++)
+            f[r] = shift_back_abc(inv[r][0] * x[0] + inv[r][1] * x[1] + inv[r][2] * x[2]);
+        for (int r = 0; r < 3; r++)
+            x[r] = m[r][0] * f[0] + m[r][1] * f[1] + m[r][2] * f[2];
+    }
+}
+
+/* --------------------------------------------------------------- ncoord -- */
+
+static void partitioned_cn(int nat, const double *xyz, const int *id, const double *rcov,
+                           const double *trans, int ntr, double cutoff, double *cn)
+{
+    /* get_partitioned_coordination_number, ncoord.f90:86-144 (complete work) */
+    double cutoff2 = cutoff * cutoff;
+    for (int i = 0; i < nat; i++) cn[i] = 0.0;
+#pragma omp parallel
+    {
+        double *loc = calloc(nat, sizeof(double));
+#pragma omp for schedule(dynamic, 1)
+        for (int i = 0; i < nat; i++) {
+            int izp = id[i];
+            for (int j = 0; j <= i; j++) {
+                int jzp = id[j];
+                double rc = rcov[izp] + rcov[jzp];
+                for (int t = 0; t < ntr; t++) {
+                    double v0 = xyz[3 * i + 0] - (xyz[3 * j + 0] + trans[3 * t + 0]);
+                    double v1 = xyz[3 * i + 1] - (xyz[3 * j + 1] + trans[3 * t + 1]);
+                    double v2 = xyz[3 * i + 2] - (xyz[3 * j + 2] + trans[3 * t + 2]);
+                    double r2 = v0 * v0 + v1 * v1 + v2 * v2;
+                    if (r2 > cutoff2 || r2 < 1.0e-12) continue;
+                    double r1 = sqrt(r2);
+                    double countf = 1.0 / (1.0 + exp(-KCN * (rc / r1 - 1.0)));
+                    loc[i] += countf;
+                    if (i != j) loc[j] += countf;
+                }
+            }
+        }
+#pragma omp critical(oracle_cn)
+        for (int i = 0; i < nat; i++) cn[i] += loc[i];
+        free(loc);
+    }
+}
+
+static void add_cn_derivs(int nat, const double *xyz, const int *id, const double *rcov,
+                          const double *trans, int ntr, double cutoff, const double *dEdcn,
+                          double *gradient, double *sigma)
+{
+    /* add_coordination_number_derivs, ncoord.f90:152-228 (complete work) */
+    double cutoff2 = cutoff * cutoff;
+#pragma omp parallel
+    {
+        double *gl = calloc(3 * (size_t)nat, sizeof(double));
+        double sl[9] = {0};
+#pragma omp for schedule(dynamic, 1)
+        for (int i = 0; i < nat; i++) {
+            int izp = id[i];
+            for (int j = 0; j <= i; j++) {
+                int jzp = id[j];
+                double rc = rcov[izp] + rcov[jzp];
+                for (int t = 0; t < ntr; t++) {
+                    double v[3];
+                    for (int c = 0; c < 3; c++)
+                        v[c] = xyz[3 * i + c] - (xyz[3 * j + c] + trans[3 * t + c]);
+                    double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+                    if (r2 > cutoff2 || r2 < 1.0e-12) continue;
+                    double r1 = sqrt(r2);
+                    double expterm = exp(-KCN * (rc / r1 - 1.0));
+                    double cf = 1.0 / (1.0 + expterm);
+                    double dcf = -cf * (1.0 - cf) * KCN * rc / r2;
+                    double cd[3];
+                    for (int c = 0; c < 3; c++) cd[c] = dcf * v[c] / r1;
+                    double de = dEdcn[i] + dEdcn[j];
+                    for (int c = 0; c < 3; c++) {
+                        gl[3 * i + c] += cd[c] * de;
+                        gl[3 * j + c] -= cd[c] * de;
+                    }
+                    double w = dEdcn[i] + (j != i ? dEdcn[j] : 0.0);
+                    for (int a = 0; a < 3; a++)
+                        for (int b = 0; b < 3; b++) sl[a + 3 * b] += cd[a] * v[b] * w;
+                }
+            }
+        }
+#pragma omp critical(oracle_cnd)
+        {
+            for (int k = 0; k < 3 * nat; k++) gradient[k] += gl[k];
+            for (int k = 0; k < 9; k++) sigma[k] += sl[k];
+        }
+        free(gl);
+    }
+}
+
+int oracle_coordination_number(int nat, const int *numbers, const double *xyz,
+                               const double *lattice, const int *periodic, double cutoff, double *cn)
+{
+    model_t m;
+    if (model_new(&m, nat, numbers, NULL)) return 1;
+    int ntr;
+    double zero[9] = {0};
+    double *trans = lattice_points(lattice ? lattice : zero, periodic, cutoff, &ntr);
+    partitioned_cn(nat, xyz, m.id, m.rcov, trans, ntr, cutoff, cn);
+    free(trans);
+    model_free(&m);
+    return 0;
+}
+
+/* ---------------------------------------------------------------- model -- */
+
+static int is_exceptional(double v) { return isnan(v) || fabs(v) > DBL_MAX; }
+
+static void weight_references(const model_t *m, int nat, const double *cn,
+                              double *gwvec, double *gwdcn)
+{
+    /* model.f90:201-324 (first-derivative and energy-only branches), with
+     * gwvec(iref, iat) at [iat*mref + iref] */
+    int mref = m->mref;
+    double wf2 = 2 * WF;
+    for (int k = 0; k < nat * mref; k++) {
+        gwvec[k] = 0.0;
+        if (gwdcn) gwdcn[k] = 0.0;
+    }
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nat; i++) {
+        int izp = m->id[i];
+        int nref = m->ref[izp];
+        const double *cnref = m->cn + izp * mref;
+        double gwt[D3_MAX_REF];
+        double norm = 0.0, dnorm = 0.0;
+        for (int r = 0; r < nref; r++) {
+            double gw = exp(-WF * (cn[i] - cnref[r]) * (cn[i] - cnref[r]));
+            gwt[r] = gw;
+            double dcn = cnref[r] - cn[i];
+            norm = norm + gw;
+            dnorm = dnorm + wf2 * dcn * gw;
+        }
+        norm = 1.0 / norm;
+        double maxcn = cnref[0];
+        for (int r = 1; r < nref; r++) if (cnref[r] > maxcn) maxcn = cnref[r];
+        for (int r = 0; r < nref; r++) {
+            double expw = gwt[r];
+            double dcn = cnref[r] - cn[i];
+            double expd = wf2 * dcn * expw;
+            double gwk = expw * norm;
+            if (is_exceptional(gwk)) gwk = (maxcn == cnref[r]) ? 1.0 : 0.0;
+            gwvec[i * mref + r] = gwk;
+            if (gwdcn) {
+                double dgwk = expd * norm - expw * dnorm * (norm * norm);
+                if (is_exceptional(dgwk)) dgwk = 0.0;
+                gwdcn[i * mref + r] = dgwk;
+            }
+        }
+    }
+}
+
+int oracle_weight_references(int nat, const int *numbers, const double *cn,
+                             int *mref_out, double *gwvec, double *gwdcn)
+{
+    model_t m;
+    if (model_new(&m, nat, numbers, NULL)) return 1;
+    *mref_out = m.mref;
+    if (gwvec) weight_references(&m, nat, cn, gwvec, gwdcn);
+    model_free(&m);
+    return 0;
+}
+
+static void get_atomic_c6(const model_t *m, int nat, const double *gwvec, const double *gwdcn,
+                          double *c6, double *dc6dcn, int part, int nparts)
+{
+    /* model.f90:340-491 (first-derivative and energy-only branches);
+     * c6(iat, jat) at [iat*nat + jat], dc6dcn(iat, jat) = dC6_ij/dCN_i */
+    int mref = m->mref, nid = m->nid;
+    memset(c6, 0, sizeof(double) * (size_t)nat * nat);
+    if (dc6dcn) memset(dc6dcn, 0, sizeof(double) * (size_t)nat * nat);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i = 0; i < nat; i++) {
+        if (m->ghost[i]) continue;
+        int izp = m->id[i];
+        for (int j = 0; j <= i; j++) {
+            if (m->ghost[j]) continue;
+            if (!owns_pair(part, nparts, i, j)) continue;
+            int jzp = m->id[j];
+            double dc6 = 0.0, dci = 0.0, dcj = 0.0;
+            for (int ir = 0; ir < m->ref[izp]; ir++)
+                for (int jr = 0; jr < m->ref[jzp]; jr++) {
+                    double refc6 = m->c6[(((size_t)izp * nid + jzp) * mref + ir) * mref + jr];
+                    dc6 = dc6 + gwvec[i * mref + ir] * gwvec[j * mref + jr] * refc6;
+                    if (dc6dcn) {
+                        dci = dci + gwdcn[i * mref + ir] * gwvec[j * mref + jr] * refc6;
+                        dcj = dcj + gwvec[i * mref + ir] * gwdcn[j * mref + jr] * refc6;
+                    }
+                }
+            c6[(size_t)i * nat + j] = dc6;
+            c6[(size_t)j * nat + i] = dc6;
+            if (dc6dcn) {
+                dc6dcn[(size_t)i * nat + j] = dci;
+                dc6dcn[(size_t)j * nat + i] = dcj;
+            }
+        }
+    }
+}
+
+/* -------------------------------------------------------------- two-body -- */
+
+static void dispersion2(const model_t *m, const oracle_param *p, int nat, const double *xyz,
+                        const double *trans, int ntr, double cutoff, double width,
+                        const double *c6, const double *dc6dcn, double *energy,
+                        double *dEdcn, double *gradient, double *sigma, int part, int nparts)
+{
+    /* rational.f90:220-514 and zero.f90:306-553; derivatives when dEdcn != NULL */
+    if (fabs(p->s6) < EPS && fabs(p->s8) < EPS) return;
+    double cutoff2 = cutoff * cutoff;
+    int grad = dEdcn != NULL;
+    double alp6 = p->alp, alp8 = p->alp + 2.0;
+#pragma omp parallel
+    {
+        double *el = calloc(nat, sizeof(double));
+        double *dl = grad ? calloc(nat, sizeof(double)) : NULL;
+        double *gl = grad ? calloc(3 * (size_t)nat, sizeof(double)) : NULL;
+        double sl[9] = {0};
+#pragma omp for schedule(dynamic, 1)
+        for (int i = 0; i < nat; i++) {
+            int izp = m->id[i];
+            for (int j = 0; j <= i; j++) {
+                if (!owns_pair(part, nparts, i, j)) continue;
+                int jzp = m->id[j];
+                double rrij = 3 * m->r4r2[izp] * m->r4r2[jzp];
+                double c6ij = c6[(size_t)j * nat + i];
+                double r0ij = 0, r0ij6 = 0, r0ij8 = 0, rs6r0 = 0, rs8r0 = 0;
+                if (p->damping == ORACLE_RATIONAL) {
+                    r0ij = p->a1 * sqrt(rrij) + p->a2;
+                    double r0ij2 = r0ij * r0ij;
+                    r0ij6 = r0ij2 * r0ij2 * r0ij2;
+                    r0ij8 = r0ij6 * r0ij2;
+                } else {
+                    r0ij = m->rvdw[jzp * m->nid + izp];
+                    rs6r0 = p->rs6 * r0ij;
+                    rs8r0 = p->rs8 * r0ij;
+                }
+                for (int t = 0; t < ntr; t++) {
+                    double v[3];
+                    for (int c = 0; c < 3; c++)
+                        v[c] = xyz[3 * i + c] - (xyz[3 * j + c] + trans[3 * t + c]);
+                    double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+                    if (r2 > cutoff2 || r2 < EPS) continue;
+                    double r1 = sqrt(r2);
+                    double sw, dswdr;
+                    smooth_cutoff(r1, cutoff, width, &sw, &dswdr);
+                    double edisp0, gdisp0;
+                    if (p->damping == ORACLE_RATIONAL) {
+                        double r4 = r2 * r2;
+                        double t6 = 1.0 / (r4 * r2 + r0ij6);
+                        double t8 = 1.0 / (r4 * r4 + r0ij8);
+                        double d6 = -6 * r4 * t6 * t6;
+                        double d8 = -8 * r4 * r2 * t8 * t8;
+                        edisp0 = p->s6 * t6 + p->s8 * rrij * t8;
+                        gdisp0 = p->s6 * d6 + p->s8 * rrij * d8;
+                    } else {
+                        double r6 = r2 * r2 * r2;
+                        double r8 = r6 * r2;
+                        double t6 = pow(rs6r0 / r1, alp6);
+                        double t8 = pow(rs8r0 / r1, alp8);
+                        double f6 = 1.0 / (1.0 + 6.0 * t6);
+                        double f8 = 1.0 / (1.0 + 6.0 * t8);
+                        double d6 = -6.0 * f6 / r2 + 6.0 * alp6 * t6 * (f6 * f6) / r2;
+                        double d8 = -8.0 * f8 / r2 + 6.0 * alp8 * t8 * (f8 * f8) / r2;
+                        edisp0 = p->s6 * f6 / r6 + p->s8 * rrij * f8 / r8;
+                        gdisp0 = p->s6 * d6 / r6 + p->s8 * rrij * d8 / r8;
+                    }
+                    double edisp = sw * edisp0;
+                    double dE = -c6ij * edisp * 0.5;
+                    el[i] += dE;
+                    if (i != j) el[j] += dE;
+                    if (!grad) continue;
+                    double gdisp = sw * gdisp0 + dswdr * edisp0 / r1;
+                    double dG[3];
+                    for (int c = 0; c < 3; c++) dG[c] = -c6ij * gdisp * v[c];
+                    double dS[9];
+                    for (int a = 0; a < 3; a++)
+                        for (int b = 0; b < 3; b++) dS[a + 3 * b] = dG[a] * v[b] * 0.5;
+                    dl[i] -= dc6dcn[(size_t)i * nat + j] * edisp;
+                    for (int k = 0; k < 9; k++) sl[k] += dS[k];
+                    if (i != j) {
+                        dl[j] -= dc6dcn[(size_t)j * nat + i] * edisp;
+                        for (int c = 0; c < 3; c++) {
+                            gl[3 * i + c] += dG[c];
+                            gl[3 * j + c] -= dG[c];
+                        }
+                        for (int k = 0; k < 9; k++) sl[k] += dS[k];
+                    }
+                }
+            }
+        }
+#pragma omp critical(oracle_disp2)
+        {
+            for (int i = 0; i < nat; i++) energy[i] += el[i];
+            if (grad) {
+                for (int i = 0; i < nat; i++) dEdcn[i] += dl[i];
+                for (int k = 0; k < 3 * nat; k++) gradient[k] += gl[k];
+                for (int k = 0; k < 9; k++) sigma[k] += sl[k];
+            }
+        }
+        free(el); free(dl); free(gl);
+    }
+}
+
+/* ------------------------------------------------------------ three-body -- */
+
+static double triple_scale(int ii, int jj, int kk)
+{
+    /* atm.f90:954-980 */
+    if (ii == jj) return ii == kk ? 1.0 / 6.0 : 0.5;
+    return (ii != kk && jj != kk) ? 1.0 : 0.5;
+}
+
+static void dispersion3(const model_t *m, const oracle_param *p, int nat, const double *xyz,
+                        const double *trans, int ntr, double cutoff, double width,
+                        const double *c6, const double *dc6dcn, double *energy,
+                        double *dEdcn, double *gradient, double *sigma, int part, int nparts)
+{
+    /* get_atm_dispersion, atm.f90:433-825, called with rs9 = 4/3 and
+     * alp + 2 (rational.f90:563, zero.f90:602) */
+    double s9 = p->s9;
+    if (fabs(s9) < EPS) return;
+    double alp = p->alp + 2.0;
+    double cutoff2 = cutoff * cutoff;
+    double alp3 = alp / 3.0;
+    int grad = dEdcn != NULL;
+    int nid = m->nid;
+#pragma omp parallel
+    {
+        double *el = calloc(nat, sizeof(double));
+        double *dl = grad ? calloc(nat, sizeof(double)) : NULL;
+        double *gl = grad ? calloc(3 * (size_t)nat, sizeof(double)) : NULL;
+        double sl[9] = {0};
+#pragma omp for schedule(dynamic, 1)
+        for (int i = 0; i < nat; i++) {
+            int izp = m->id[i];
+            for (int j = 0; j <= i; j++) {
+                if (!owns_pair(part, nparts, i, j)) continue;
+                int jzp = m->id[j];
+                double c6ij = c6[(size_t)j * nat + i];
+                double r0ij = RS9 * m->rvdw[jzp * nid + izp];
+                for (int jt = 0; jt < ntr; jt++) {
+                    double vij[3];
+                    for (int c = 0; c < 3; c++)
+                        vij[c] = xyz[3 * j + c] + trans[3 * jt + c] - xyz[3 * i + c];
+                    double r2ij = vij[0] * vij[0] + vij[1] * vij[1] + vij[2] * vij[2];
+                    if (r2ij > cutoff2 || r2ij < EPS) continue;
+                    double rij = sqrt(r2ij);
+                    double swij, dswijdr;
+                    smooth_cutoff(rij, cutoff, width, &swij, &dswijdr);
+                    for (int k = 0; k <= j; k++) {
+                        int kzp = m->id[k];
+                        double c6ik = c6[(size_t)k * nat + i];
+                        double c6jk = c6[(size_t)k * nat + j];
+                        if (grad && (fabs(c6ij) < EPS || fabs(c6ik) < EPS || fabs(c6jk) < EPS))
+                            continue;
+                        double c9 = -s9 * sqrt(fabs(c6ij * c6ik * c6jk));
+                        double r0ik = RS9 * m->rvdw[kzp * nid + izp];
+                        double r0jk = RS9 * m->rvdw[kzp * nid + jzp];
+                        double r0 = r0ij * r0ik * r0jk;
+                        double triple = triple_scale(i, j, k);
+                        for (int kt = 0; kt < ntr; kt++) {
+                            double vik[3], vjk[3];
+                            for (int c = 0; c < 3; c++)
+                                vik[c] = xyz[3 * k + c] + trans[3 * kt + c] - xyz[3 * i + c];
+                            double r2ik = vik[0] * vik[0] + vik[1] * vik[1] + vik[2] * vik[2];
+                            if (r2ik > cutoff2 || r2ik < EPS) continue;
+                            double rik = sqrt(r2ik);
+                            double swik, dswikdr;
+                            smooth_cutoff(rik, cutoff, width, &swik, &dswikdr);
+                            for (int c = 0; c < 3; c++) vjk[c] = vik[c] - vij[c];
+                            double r2jk = vjk[0] * vjk[0] + vjk[1] * vjk[1] + vjk[2] * vjk[2];
+                            if (r2jk > cutoff2 || r2jk < EPS) continue;
+                            double rjk = sqrt(r2jk);
+                            double swjk, dswjkdr;
+                            smooth_cutoff(rjk, cutoff, width, &swjk, &dswjkdr);
+                            double sw = swij * swik * swjk;
+                            double r2 = r2ij * r2ik * r2jk;
+                            double r1 = sqrt(r2);
+                            double r3 = r2 * r1;
+                            double r5 = r3 * r2;
+                            double fdmp = 1.0 / (1.0 + 6.0 * pow(r0 / r1, alp3));
+                            double ang = 0.375 * (r2ij + r2jk - r2ik) * (r2ij - r2jk + r2ik)
+                                       * (-r2ij + r2jk + r2ik) / r5 + 1.0 / r3;
+                            double rr = ang * fdmp;
+                            if (!grad) {
+                                double dE = rr * c9 * triple * sw / 3.0;
+                                el[i] -= dE; el[j] -= dE; el[k] -= dE;
+                                continue;
+                            }
+                            double r0r1alp3 = pow(r0 / r1, alp3);
+                            double dfdmp = -2.0 * alp * r0r1alp3 * (fdmp * fdmp);
+                            double dang, dGij[3], dGik[3], dGjk[3];
+                            dang = -0.375 * (r2ij * r2ij * r2ij + r2ij * r2ij * (r2jk + r2ik)
+                                   + r2ij * (3.0 * r2jk * r2jk + 2.0 * r2jk * r2ik + 3.0 * r2ik * r2ik)
+                                   - 5.0 * (r2jk - r2ik) * (r2jk - r2ik) * (r2jk + r2ik)) / r5;
+                            double dE0 = rr * c9;
+                            for (int c = 0; c < 3; c++)
+                                dGij[c] = sw * c9 * (-dang * fdmp + ang * dfdmp) / r2ij * vij[c]
+                                        - dE0 * dswijdr / rij * swik * swjk * vij[c];
+                            dang = -0.375 * (r2ik * r2ik * r2ik + r2ik * r2ik * (r2jk + r2ij)
+                                   + r2ik * (3.0 * r2jk * r2jk + 2.0 * r2jk * r2ij + 3.0 * r2ij * r2ij)
+                                   - 5.0 * (r2jk - r2ij) * (r2jk - r2ij) * (r2jk + r2ij)) / r5;
+                            for (int c = 0; c < 3; c++)
+                                dGik[c] = sw * c9 * (-dang * fdmp + ang * dfdmp) / r2ik * vik[c]
+                                        - dE0 * dswikdr / rik * swij * swjk * vik[c];
+                            dang = -0.375 * (r2jk * r2jk * r2jk + r2jk * r2jk * (r2ik + r2ij)
+                                   + r2jk * (3.0 * r2ik * r2ik + 2.0 * r2ik * r2ij + 3.0 * r2ij * r2ij)
+                                   - 5.0 * (r2ik - r2ij) * (r2ik - r2ij) * (r2ik + r2ij)) / r5;
+                            for (int c = 0; c < 3; c++)
+                                dGjk[c] = sw * c9 * (-dang * fdmp + ang * dfdmp) / r2jk * vjk[c]
+                                        - dE0 * dswjkdr / rjk * swij * swik * vjk[c];
+                            double dE = dE0 * triple * sw;
+                            el[i] -= dE / 3.0; el[j] -= dE / 3.0; el[k] -= dE / 3.0;
+                            for (int c = 0; c < 3; c++) {
+                                gl[3 * i + c] -= (dGij[c] + dGik[c]) * triple;
+                                gl[3 * j + c] += (dGij[c] - dGjk[c]) * triple;
+                                gl[3 * k + c] += (dGik[c] + dGjk[c]) * triple;
+                            }
+                            for (int a = 0; a < 3; a++)
+                                for (int b = 0; b < 3; b++)
+                                    sl[a + 3 * b] += (dGij[a] * vij[b] + dGik[a] * vik[b]
+                                                      + dGjk[a] * vjk[b]) * triple;
+                            dl[i] -= dE * 0.5 * (dc6dcn[(size_t)i * nat + j] / c6ij
+                                                 + dc6dcn[(size_t)i * nat + k] / c6ik);
+                            dl[j] -= dE * 0.5 * (dc6dcn[(size_t)j * nat + i] / c6ij
+                                                 + dc6dcn[(size_t)j * nat + k] / c6jk);
+                            dl[k] -= dE * 0.5 * (dc6dcn[(size_t)k * nat + i] / c6ik
+                                                 + dc6dcn[(size_t)k * nat + j] / c6jk);
+                        }
+                    }
+                }
+            }
+        }
+#pragma omp critical(oracle_disp3)
+        {
+            for (int i = 0; i < nat; i++) energy[i] += el[i];
+            if (grad) {
+                for (int i = 0; i < nat; i++) dEdcn[i] += dl[i];
+                for (int k = 0; k < 3 * nat; k++) gradient[k] += gl[k];
+                for (int k = 0; k < 9; k++) sigma[k] += sl[k];
+            }
+        }
+        free(el); free(dl); free(gl);
+    }
+}
+
+/* ------------------------------------------------------------- pipeline -- */
+
+int oracle_get_dispersion(int nat, const int *numbers, const double *xyz,
+                          const double *lattice, const int *periodic, const int *ghost,
+                          const oracle_param *param, const oracle_cutoff *cutoff,
+                          int part, int nparts, double *energy, double *energies,
+                          double *gradient, double *sigma, double *cn_out, double *dEdcn_out)
+{
+    /* get_dispersion_atomic_v2, disp.f90:56-185, and the scalar sum at :397 */
+    model_t m;
+    if (model_new(&m, nat, numbers, ghost)) return 1;
+    double zero[9] = {0};
+    int per0[3] = {0, 0, 0};
+    const double *lat = lattice ? lattice : zero;
+    const int *per = periodic ? periodic : per0;
+    int grad = gradient != NULL || sigma != NULL;
+    int mref = m.mref;
+    int threebody = fabs(param->s9) >= EPS;
+    int ntr;
+
+    double *cn = malloc(sizeof(double) * (nat > 0 ? nat : 1));
+    double *trans = lattice_points(lat, per, cutoff->cn, &ntr);
+    partitioned_cn(nat, xyz, m.id, m.rcov, trans, ntr, cutoff->cn, cn);
+    free(trans);
+
+    double *gwvec = malloc(sizeof(double) * (size_t)(nat > 0 ? nat : 1) * mref);
+    double *gwdcn = grad ? malloc(sizeof(double) * (size_t)(nat > 0 ? nat : 1) * mref) : NULL;
+    weight_references(&m, nat, cn, gwvec, gwdcn);
+
+    size_t nn = (size_t)nat * nat;
+    double *c6 = malloc(sizeof(double) * (nn > 0 ? nn : 1));
+    double *dc6dcn = grad ? malloc(sizeof(double) * (nn > 0 ? nn : 1)) : NULL;
+    if (threebody)
+        get_atomic_c6(&m, nat, gwvec, gwdcn, c6, dc6dcn, 0, 1);
+    else
+        get_atomic_c6(&m, nat, gwvec, gwdcn, c6, dc6dcn, part, nparts);
+
+    double *en = calloc(nat > 0 ? nat : 1, sizeof(double));
+    double *dEdcn = grad ? calloc(nat > 0 ? nat : 1, sizeof(double)) : NULL;
+    double *gl = grad ? calloc(3 * (size_t)(nat > 0 ? nat : 1), sizeof(double)) : NULL;
+    double sl[9] = {0};
+
+    trans = lattice_points(lat, per, cutoff->disp2, &ntr);
+    dispersion2(&m, param, nat, xyz, trans, ntr, cutoff->disp2, cutoff->width2, c6, dc6dcn,
+                en, dEdcn, gl, sl, part, nparts);
+    free(trans);
+    trans = lattice_points(lat, per, cutoff->disp3, &ntr);
+    dispersion3(&m, param, nat, xyz, trans, ntr, cutoff->disp3, cutoff->width3, c6, dc6dcn,
+                en, dEdcn, gl, sl, part, nparts);
+    free(trans);
+    if (dEdcn_out && grad)
+        for (int i = 0; i < nat; i++) dEdcn_out[i] = dEdcn[i];
+    if (grad) {
+        trans = lattice_points(lat, per, cutoff->cn, &ntr);
+        add_cn_derivs(nat, xyz, m.id, m.rcov, trans, ntr, cutoff->cn, dEdcn, gl, sl);
+        free(trans);
+        if (gradient) memcpy(gradient, gl, sizeof(double) * 3 * nat);
+        if (sigma) memcpy(sigma, sl, sizeof(double) * 9);
+    }
+    double e = 0.0;
+    for (int i = 0; i < nat; i++) e += en[i];
+    if (energy) *energy = e;
+    if (energies) memcpy(energies, en, sizeof(double) * nat);
+    if (cn_out) memcpy(cn_out, cn, sizeof(double) * nat);
+
+    free(cn); free(gwvec); free(gwdcn); free(c6); free(dc6dcn);
+    free(en); free(dEdcn); free(gl);
+    model_free(&m);
+    return 0;
+}

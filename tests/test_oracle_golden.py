@@ -1,0 +1,114 @@
+"""Pin the FP64 oracle against the reference's own golden vectors.
+
+Each fixture in tests/golden was extracted from the reference's test files by
+tests/golden/make_golden.py; the tolerances are the reference tests' own.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle_ref as O
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def _load(name):
+    return json.loads((GOLDEN / name).read_text())
+
+
+def _positions(case):
+    p = np.array(case["positions"], dtype=float)
+    return p * O.AATOAU if case["unit"] == "angstrom" else p
+
+
+@pytest.mark.parametrize("case", _load("validation.json"), ids=lambda c: c["name"])
+def test_validation_fixture(case):
+    """test/validation/*.json through the CLI path, abs 1e-6 (tester.py:61)."""
+    res = O.dispersion(case["numbers"], _positions(case), case["param"], grad="gradient" in case)
+    assert abs(res["energy"] - case["energy"]) < case["tol_abs"]
+    if "gradient" in case:
+        np.testing.assert_allclose(res["gradient"].ravel(), case["gradient"], rtol=0, atol=case["tol_abs"])
+        # the CLI prints the virial in Fortran (column-major) order
+        np.testing.assert_allclose(res["virial"].ravel(), case["virial"], rtol=0, atol=case["tol_abs"])
+
+
+@pytest.mark.parametrize("case", _load("python.json"), ids=lambda c: c["name"])
+def test_python_api_fixture(case):
+    for sub in case["cases"]:
+        res = O.dispersion(case["numbers"], _positions(case), sub["param"], grad="gradient" in sub)
+        if "energy" in sub:
+            if "tol_rel" in case:
+                assert res["energy"] == pytest.approx(sub["energy"], rel=case["tol_rel"])
+            else:
+                assert abs(res["energy"] - sub["energy"]) < case["tol_abs"]
+        if "gradient" in sub:
+            np.testing.assert_allclose(res["gradient"], sub["gradient"], rtol=0, atol=case["tol_abs"])
+
+
+def test_periodic_regression_ta():
+    """test_regression.f90:49-75: 90-atom Ta cell, energy and |gradient| at 100 eps."""
+    case = _load("unit.json")[0]
+    res = O.dispersion(case["numbers"], _positions(case), case["param"], lattice=case["lattice"],
+                       periodic=case["periodic"], wrap=False)
+    assert abs(res["energy"] - case["energy"]) < case["tol_abs"]
+    assert abs(np.linalg.norm(res["gradient"]) - case["gradient_norm"]) < case["tol_abs"]
+
+
+def test_gaussian_weights_amf3():
+    """test_model.f90:279-310: reference weights of AmF3 with a 30 Bohr CN cutoff."""
+    case = _load("unit.json")[1]
+    cn = O.coordination_number(case["numbers"], _positions(case), case["cn_cutoff"])
+    gw, _ = O.weight_references(case["numbers"], cn)
+    ref = np.array(case["weights"])
+    assert gw.shape[1] <= ref.shape[1]
+    assert np.abs(gw - ref[:, :gw.shape[1]]).max() < case["tol_abs"]
+    assert not np.any(ref[:, gw.shape[1]:])
+
+
+def _small_periodic():
+    case = _load("python.json")[0]
+    nums = np.array(case["numbers"])[:8]
+    pos = _positions(case)[:8]
+    lat = np.array([[9.0, 0.3, -0.2], [0.1, 8.5, 0.4], [-0.3, 0.2, 10.0]])
+    return nums, pos, lat
+
+
+@pytest.mark.parametrize("damping", ["rational", "zero"])
+def test_oracle_numerical_gradient(damping):
+    """Central finite differences, as test_dftd3.f90:124-168 (step 1e-6)."""
+    case = _load("python.json")[0]
+    nums = case["numbers"]
+    pos = _positions(case)
+    par = next(c["param"] for c in case["cases"] if c["param"]["damping"] == damping and c["param"]["s9"] == 1.0)
+    res = O.dispersion(nums, pos, par)
+    step = 1.0e-6
+    num = np.zeros_like(pos)
+    for i in range(0, len(nums), 3):
+        for c in range(3):
+            p = pos.copy(); p[i, c] += step
+            er = O.dispersion(nums, p, par, grad=False)["energy"]
+            p[i, c] -= 2 * step
+            el = O.dispersion(nums, p, par, grad=False)["energy"]
+            num[i, c] = 0.5 * (er - el) / step
+    np.testing.assert_allclose(res["gradient"][::3], num[::3], atol=1.0e-8, rtol=0)
+
+
+def test_oracle_numerical_sigma():
+    """Strain finite differences of a periodic cell, as test_dftd3.f90:191-236."""
+    nums, pos, lat = _small_periodic()
+    par = {"damping": "rational", "s6": 1.0, "s8": 1.2177, "a1": 0.4145, "a2": 4.8593, "s9": 1.0, "alp": 14.0}
+    cut = (30.0, 15.0, 20.0, 0.0, 0.0)
+    res = O.dispersion(nums, pos, par, lattice=lat, cutoff=cut, wrap=False)
+    step = 1.0e-6
+    num = np.zeros((3, 3))
+    for a in range(3):
+        for b in range(3):
+            eps = np.eye(3); eps[a, b] += step
+            er = O.dispersion(nums, pos @ eps.T, par, lattice=lat @ eps.T, cutoff=cut, grad=False, wrap=False)["energy"]
+            eps[a, b] -= 2 * step
+            el = O.dispersion(nums, pos @ eps.T, par, lattice=lat @ eps.T, cutoff=cut, grad=False, wrap=False)["energy"]
+            num[a, b] = 0.5 * (er - el) / step
+    # the returned array is the Fortran sigma(3,3) in column-major order
+    np.testing.assert_allclose(res["virial"].T, num, atol=1.0e-7, rtol=0)
