@@ -1,0 +1,119 @@
+/* Extensions of the B200 DFT-D3 library beyond the reference C API.
+ *
+ * None of these has a counterpart in the reference (s-dftd3 v1.6.0); they add
+ * precision selection, ragged batches of independent systems in one
+ * evaluation, and an entry point on device buffers for framework callers
+ * (the torch autograd wrapper).  Handles and the error convention are those of
+ * s-dftd3.h. */
+#pragma once
+
+#include "s-dftd3.h"
+
+/* Arithmetic of the hot path: FP64 everywhere (the default, parity form), or
+ * FP32 pair/triple arithmetic with FP64 accumulation, weights and reductions. */
+#define DFTD3_B200_PRECISION_FP64 0
+#define DFTD3_B200_PRECISION_MIXED 1
+
+typedef struct _dftd3_b200_batch* dftd3_b200_batch;
+
+/* Select the arithmetic of a model created by dftd3_new_d3_model. */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_set_model_precision(dftd3_error /* error */,
+                               dftd3_model /* model */,
+                               int /* precision */);
+
+/* Create a batch of nsys independent systems.  Atoms are concatenated:
+ * natoms[nsys], numbers[sum natoms].  lattices[nsys][3][3] and
+ * periodic[nsys][3] may be NULL for molecules.  The batch keeps device
+ * workspace and the captured launch sequence between evaluations. */
+SDFTD3_API_ENTRY dftd3_b200_batch SDFTD3_API_CALL
+dftd3_b200_new_batch(dftd3_error /* error */,
+                     int /* nsys */,
+                     const int* /* natoms [nsys] */,
+                     const int* /* numbers [sum natoms] */,
+                     const double* /* lattices [nsys][3][3] or NULL */,
+                     const bool* /* periodic [nsys][3] or NULL */);
+
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_set_batch_realspace_cutoff(dftd3_error /* error */,
+                                      dftd3_b200_batch /* batch */,
+                                      double /* disp2 */,
+                                      double /* disp3 */,
+                                      double /* cn */,
+                                      double /* width2 */,
+                                      double /* width3 */);
+
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_set_batch_precision(dftd3_error /* error */,
+                               dftd3_b200_batch /* batch */,
+                               int /* precision */);
+
+/* Evaluate all systems from host buffers.  positions[sum natoms][3] (Bohr) are
+ * wrapped per system like dftd3_new_structure; lattices may be NULL to keep
+ * the batch's lattices.  energies[nsys]; gradient[sum natoms][3] and
+ * sigma[nsys][3][3] may be NULL (then only energies are evaluated). */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_get_dispersion_batched(dftd3_error /* error */,
+                                  dftd3_b200_batch /* batch */,
+                                  dftd3_param /* param */,
+                                  const double* /* positions */,
+                                  const double* /* lattices or NULL */,
+                                  double* /* energies [nsys] */,
+                                  double* /* gradient [sum natoms][3] or NULL */,
+                                  double* /* sigma [nsys][3][3] or NULL */);
+
+/* Evaluate all systems from device buffers on the caller's stream (a
+ * cudaStream_t used as given; NULL is the legacy default stream).  Positions are used as
+ * given (no wrapping); the lattices, which decide the image lists, are read
+ * from host memory (NULL keeps the current ones).  param_grad[nsys][5], if
+ * non-NULL, receives
+ * dE/d(s6, s8, a1, a2, s9) (rational) or dE/d(s6, s8, rs6, rs8, s9) (zero).
+ * The call is asynchronous with respect to the host. */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_get_dispersion_device(dftd3_error /* error */,
+                                 dftd3_b200_batch /* batch */,
+                                 dftd3_param /* param */,
+                                 const double* /* d_positions [sum natoms][3] */,
+                                 const double* /* lattices [nsys][3][3] (host) or NULL */,
+                                 double* /* d_energies [nsys] */,
+                                 double* /* d_gradient or NULL */,
+                                 double* /* d_sigma or NULL */,
+                                 double* /* d_param_grad or NULL */,
+                                 void* /* stream */);
+
+/* Work counters of the last evaluation: accepted pair terms of the two-body
+ * sum, accepted ATM triples and CN terms (counted on request, see
+ * dftd3_b200_set_batch_counting). */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_set_batch_counting(dftd3_error /* error */,
+                              dftd3_b200_batch /* batch */,
+                              int /* enable */);
+
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_get_batch_counts(dftd3_error /* error */,
+                            dftd3_b200_batch /* batch */,
+                            long long* /* counts[3]: pair, triple, cn */);
+
+/* Device time of each pipeline stage of the last evaluation in ms, recorded
+ * with CUDA events while profiling is enabled: [0] position split, [1]
+ * coordination number, [2] reference weights, [3] two-body, [4] three-body,
+ * [5] CN chain rule, [6] per-system reductions. */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_set_batch_profiling(dftd3_error /* error */,
+                               dftd3_b200_batch /* batch */,
+                               int /* enable */);
+
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_get_batch_stage_times(dftd3_error /* error */,
+                                 dftd3_b200_batch /* batch */,
+                                 double* /* ms[7] */);
+
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_delete_batch(dftd3_b200_batch* /* batch */);
+
+/* Measured fused-multiply-add throughput of the current device in TFLOP/s
+ * (precision DFTD3_B200_PRECISION_FP64: FP64 pipe, _MIXED: FP32 pipe); the
+ * denominator of the roofline fraction the benchmark reports. */
+SDFTD3_API_ENTRY double SDFTD3_API_CALL
+dftd3_b200_fma_peak(dftd3_error /* error */,
+                    int /* precision */);

@@ -1,0 +1,113 @@
+// Device-side data layout of the D3 pipeline and the kernel entry points.
+//
+// One evaluation covers a ragged batch of independent systems.  Atoms of all
+// systems are concatenated; every per-atom array below is indexed by the
+// batch atom index.  A single structure is a batch of one.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace d3 {
+
+constexpr int kMaxRef = 7;          // references per element (reference.f90:28)
+constexpr int kImageKinds = 3;      // lattice point sets: CN, two-body, three-body
+constexpr int kImgCN = 0, kImgDisp2 = 1, kImgDisp3 = 2;
+constexpr int kSigma = 6;           // packed symmetric virial: xx yy zz xy xz yz
+constexpr int kParamGrad = 5;       // dE/d(s6, s8, a1|rs6, a2|rs8, s9)
+constexpr int kPairSlots = 6;       // per species pair: rrij, q1..q4, pad
+
+enum Damping : int { kRational = 0, kZero = 1 };
+
+// Per-batch geometry and bookkeeping.
+struct Batch {
+    int nsys = 0, natoms = 0, nid = 0;
+    const int* sys_of_atom = nullptr;    // [natoms]
+    const int* atom_off = nullptr;       // [nsys + 1]
+    const int* local = nullptr;          // [natoms] index inside its system
+    const int* sp = nullptr;             // [natoms] batch species index
+    const uint8_t* ghost = nullptr;      // [natoms] or null
+    const int* img_off = nullptr;        // [kImageKinds][nsys + 1]
+    const double* img = nullptr;         // [nimg][3]
+    const double* x = nullptr;           // [natoms] SoA positions (Bohr)
+    const double* y = nullptr;
+    const double* z = nullptr;
+    const float4* xhi = nullptr;         // [natoms] float head of x,y,z (mixed form)
+    const float4* xlo = nullptr;         // [natoms] float tail x - head
+};
+
+// Per-species model tables (new_d3_model, model.f90:87-181) for the batch's
+// species set, and the per-pair damping constants of the current parameters.
+struct Species {
+    const double* rcov = nullptr;        // [nid]
+    const int* nref = nullptr;           // [nid]
+    const double* refcn = nullptr;       // [nid][kMaxRef]
+    const double* c6ref = nullptr;       // [nid][nid][kMaxRef][kMaxRef] = c6(ir, jr, is, js)
+    const float* c6ref_f = nullptr;      // same in FP32 (mixed form)
+    const double* pair = nullptr;        // [nid][nid][kPairSlots] damping constants, see engine
+    const double* atm_r0 = nullptr;      // [nid][nid] rs9 * rvdw
+};
+
+struct Damp {
+    int kind = kRational;
+    double s6 = 1, s8 = 1, s9 = 0, a1 = 0.4, a2 = 5, rs6 = 1, rs8 = 1, alp = 14;
+};
+
+struct Partition {
+    int part = 0, nparts = 1;
+};
+
+// Work arrays of one evaluation.
+struct Work {
+    double* cn = nullptr;        // [natoms]
+    double* gw = nullptr;        // [natoms][kMaxRef]
+    double* dgw = nullptr;       // [natoms][kMaxRef]
+    float* gwf = nullptr;        // [natoms][kMaxRef] (mixed form)
+    float* dgwf = nullptr;       // [natoms][kMaxRef] (mixed form)
+    double* dEdcn = nullptr;     // [natoms]
+    double* e_atom = nullptr;    // [natoms]
+    double* grad = nullptr;      // [natoms][3]
+    double* sig_atom = nullptr;  // [natoms][kSigma]
+    double* pg_atom = nullptr;   // [natoms][kParamGrad] or null
+    unsigned long long* counts = nullptr;  // [3] pair, triple, cn terms or null
+    // three-body
+    double* c6mat = nullptr;     // per system dense [n][n][3]: c6, dc6/dcn_row, dc6/dcn_col
+    const long long* c6mat_off = nullptr;   // [nsys] offsets (in elements of 3 doubles)
+    int* nbr_count = nullptr;    // [natoms]
+    long long* nbr_off = nullptr;// [natoms + 1]
+    int4* nbr = nullptr;         // [total] (j, image, -, -)
+    double* nbr_vec = nullptr;   // [total][4] vector x_j + T - x_i and r2
+    double* atm_acc = nullptr;   // dense per-system [n][n][4] triangular accumulator
+    double* e3_atom = nullptr;   // [natoms] three-body energy per root atom
+};
+
+struct Config {
+    double cut_cn = 40, cut2 = 60, cut3 = 40, width2 = 0, width3 = 0;
+    bool grad = true;
+    bool mixed = false;
+    bool param_grad = false;
+    bool cn_partitioned = false;   // partition the CN and chain-rule loops too
+};
+
+// FMA throughput of the FP64 (fp64=true) or FP32 pipe in TFLOP/s (blocking).
+double measure_fma_peak(bool fp64);
+
+// Launchers (d3_kernels.cu); all asynchronous on `stream`.
+void launch_split_positions(const double* pos, int natoms, double* x, double* y, double* z,
+                            float4* xhi, float4* xlo, bool mixed, cudaStream_t stream);
+void launch_coordination_number(const Batch& b, const Species& s, const Config& c,
+                                const Partition& p, const Work& w, cudaStream_t stream);
+void launch_weights(const Batch& b, const Species& s, const Config& c, const Work& w,
+                    cudaStream_t stream);
+void launch_two_body(const Batch& b, const Species& s, const Damp& d, const Config& c,
+                     const Partition& p, const Work& w, cudaStream_t stream);
+void launch_three_body(const Batch& b, const Species& s, const Damp& d, const Config& c,
+                       const Partition& p, const Work& w, long long nbr_capacity,
+                       int max_sys_atoms, cudaStream_t stream);
+void launch_cn_chain_rule(const Batch& b, const Species& s, const Config& c, const Partition& p,
+                          const Work& w, cudaStream_t stream);
+void launch_reduce_systems(const Batch& b, const Config& c, const Work& w, double* energies,
+                           double* sigma9, double* param_grad, double* grad_out,
+                           cudaStream_t stream);
+
+}  // namespace d3

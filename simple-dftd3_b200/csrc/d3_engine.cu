@@ -1,0 +1,561 @@
+// Host-side driver of the D3 pipeline (see d3_engine.h).
+#include "d3_engine.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "d3_tables.h"
+
+namespace d3 {
+
+namespace {
+
+void check(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess)
+        throw Error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+void cross(const double* a, const double* b, double* c)
+{
+    // cutoff.f90:229-238
+    const double x = a[1] * b[2] - b[1] * a[2];
+    const double y = a[2] * b[0] - b[2] * a[0];
+    const double z = a[0] * b[1] - b[0] * a[1];
+    c[0] = x; c[1] = y; c[2] = z;
+}
+
+void translations(const double lat[3][3], double rthr, int rep[3])
+{
+    // get_translations, cutoff.f90:204-227 (lat[k] is lattice vector k)
+    double nrm[3][3];
+    cross(lat[1], lat[2], nrm[0]);
+    cross(lat[2], lat[0], nrm[1]);
+    cross(lat[0], lat[1], nrm[2]);
+    for (int k = 0; k < 3; k++) {
+        const double n = std::sqrt(nrm[k][0] * nrm[k][0] + nrm[k][1] * nrm[k][1] + nrm[k][2] * nrm[k][2]);
+        for (int c = 0; c < 3; c++) nrm[k][c] /= n;
+    }
+    for (int k = 0; k < 3; k++) {
+        const double cs = nrm[k][0] * lat[k][0] + nrm[k][1] * lat[k][1] + nrm[k][2] * lat[k][2];
+        rep[k] = (int)std::ceil(std::fabs(rthr / cs));
+    }
+}
+
+double shift_back_abc(double in)
+{
+    // utils.f90:48-64
+    const double eps = 1.0e-14;
+    double out = in;
+    if (in < -eps) out = in + std::ceil(-in);
+    if (in > 1.0 + eps) out = in - std::floor(in);
+    if (std::fabs(in - 1.0) < eps) out = in - 1.0;
+    return out;
+}
+
+double covalent_radius(int z)
+{
+    // D3 covalent radius in Bohr, 4/3 of the tabulated radius (see d3_tables.h)
+    return 4.0 / 3.0 * (D3_AATOAU * d3_rcov_aa[z - 1]);
+}
+
+double r4r2_value(int z)
+{
+    // data/r4r2.f90:69-70
+    return std::sqrt(0.5 * (d3_r4_over_r2[z - 1] * std::sqrt((double)z)));
+}
+
+double vdw_rad(int z1, int z2)
+{
+    // data/vdwrad.f90:1163-1197, both elements inside the table
+    const int ic = z1 > z2 ? (z2 - 1) + z1 * (z1 - 1) / 2 : (z1 - 1) + z2 * (z2 - 1) / 2;
+    return D3_AATOAU * d3_vdwrad_aa[ic];
+}
+
+double ref_c6(int iref, int jref, int ati, int atj)
+{
+    // get_c6, reference.f90:160-171
+    if (ati > atj) {
+        const int ic = (atj - 1) + ati * (ati - 1) / 2;
+        return d3_c6ab[ic * 49 + jref * 7 + iref];
+    }
+    const int ic = (ati - 1) + atj * (atj - 1) / 2;
+    return d3_c6ab[ic * 49 + iref * 7 + jref];
+}
+
+}  // namespace
+
+std::vector<double> lattice_points(const double* lattice, const bool* periodic, double rthr)
+{
+    const int np = (int)periodic[0] + (int)periodic[1] + (int)periodic[2];
+    if (np == 0) return {0.0, 0.0, 0.0};
+    double lat[3][3];
+    for (int k = 0; k < 3; k++)
+        for (int c = 0; c < 3; c++) lat[k][c] = lattice[3 * k + c];
+    int rep[3] = {0, 0, 0};
+    if (np == 3) {
+        translations(lat, rthr, rep);
+    } else if (np == 1) {
+        for (int k = 0; k < 3; k++) {
+            const double v = std::sqrt(lat[k][0] * lat[k][0] + lat[k][1] * lat[k][1] + lat[k][2] * lat[k][2]);
+            rep[k] = periodic[k] ? (int)std::ceil(rthr / v) : 0;
+        }
+    } else {
+        // get_normals, then component c of every vector is taken from the
+        // lattice where periodic(c) holds (cutoff.f90:168-176)
+        double nrm[3][3];
+        for (int k = 0; k < 3; k++) cross(lat[(k + 1) % 3], lat[(k + 2) % 3], nrm[k]);
+        for (int k = 0; k < 3; k++)
+            for (int c = 0; c < 3; c++)
+                if (periodic[c]) nrm[k][c] = lat[k][c];
+        translations(nrm, rthr, rep);
+        for (int k = 0; k < 3; k++)
+            if (!periodic[k]) rep[k] = 0;
+    }
+    std::vector<double> t;
+    t.reserve(3 * (2 * rep[0] + 1) * (2 * rep[1] + 1) * (2 * rep[2] + 1));
+    for (int ix = -rep[0]; ix <= rep[0]; ix++)
+        for (int iy = -rep[1]; iy <= rep[1]; iy++)
+            for (int iz = -rep[2]; iz <= rep[2]; iz++)
+                for (int c = 0; c < 3; c++) t.push_back(lat[0][c] * ix + lat[1][c] * iy + lat[2][c] * iz);
+    return t;
+}
+
+void wrap_to_central_cell(int nat, double* xyz, const double* lattice, const bool* periodic)
+{
+    if (!(periodic[0] || periodic[1] || periodic[2])) return;
+    // M has the lattice vectors as columns; f = M^-1 x by cofactors
+    double a[3][3];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) a[r][c] = lattice[3 * c + r];
+    const double det = a[0][0] * a[1][1] * a[2][2] - a[0][0] * a[1][2] * a[2][1]
+                     - a[0][1] * a[1][0] * a[2][2] + a[0][1] * a[1][2] * a[2][0]
+                     + a[0][2] * a[1][0] * a[2][1] - a[0][2] * a[1][1] * a[2][0];
+    const double d = 1.0 / det;
+    double inv[3][3];
+    inv[0][0] = +d * (a[1][1] * a[2][2] - a[1][2] * a[2][1]);
+    inv[1][0] = -d * (a[1][0] * a[2][2] - a[1][2] * a[2][0]);
+    inv[2][0] = +d * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+    inv[0][1] = -d * (a[0][1] * a[2][2] - a[0][2] * a[2][1]);
+    inv[1][1] = +d * (a[0][0] * a[2][2] - a[0][2] * a[2][0]);
+    inv[2][1] = -d * (a[0][0] * a[2][1] - a[0][1] * a[2][0]);
+    inv[0][2] = +d * (a[0][1] * a[1][2] - a[0][2] * a[1][1]);
+    inv[1][2] = -d * (a[0][0] * a[1][2] - a[0][2] * a[1][0]);
+    inv[2][2] = +d * (a[0][0] * a[1][1] - a[0][1] * a[1][0]);
+    for (int i = 0; i < nat; i++) {
+        double* x = xyz + 3 * i;
+        double f[3];
+        for (int r = 0; r < 3; r++) f[r] = shift_back_abc(inv[r][0] * x[0] + inv[r][1] * x[1] + inv[r][2] * x[2]);
+        for (int r = 0; r < 3; r++) x[r] = a[r][0] * f[0] + a[r][1] * f[1] + a[r][2] * f[2];
+    }
+}
+
+bool has_overlapping_atoms(int nat, const double* xyz)
+{
+    // Sort by x and compare within a 1e-9 window: the same pairs as the
+    // reference's O(N^2) scan report.
+    std::vector<int> idx(nat);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::sort(idx.begin(), idx.end(), [&](int a, int b) { return xyz[3 * a] < xyz[3 * b]; });
+    for (int a = 0; a < nat; a++) {
+        const double* p = xyz + 3 * idx[a];
+        for (int b = a + 1; b < nat; b++) {
+            const double* q = xyz + 3 * idx[b];
+            if (q[0] - p[0] >= 1.0e-9) break;
+            const double dx = q[0] - p[0], dy = q[1] - p[1], dz = q[2] - p[2];
+            if (std::sqrt(dx * dx + dy * dy + dz * dz) < 1.0e-9) return true;
+        }
+    }
+    return false;
+}
+
+template <class T>
+T* Engine::dev_alloc(size_t n)
+{
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    check(cudaMalloc(&p, n * sizeof(T)), "cudaMalloc");
+    allocations_.push_back(p);
+    return static_cast<T*>(p);
+}
+
+Engine::Engine(int nsys, const int* natoms, const int* numbers, const double* lattices,
+               const bool* periodic, int device)
+{
+    if (nsys <= 0) throw Error("Invalid number of systems");
+    if (device < 0) check(cudaGetDevice(&device_), "cudaGetDevice");
+    else device_ = device;
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    nsys_ = nsys;
+    atom_off_.assign(nsys + 1, 0);
+    for (int s = 0; s < nsys; s++) {
+        if (natoms[s] < 0) throw Error("Invalid number of atoms");
+        atom_off_[s + 1] = atom_off_[s] + natoms[s];
+        max_sys_atoms_ = std::max(max_sys_atoms_, natoms[s]);
+    }
+    natoms_ = atom_off_[nsys];
+    sys_of_atom_.resize(natoms_);
+    local_.resize(natoms_);
+    for (int s = 0; s < nsys; s++)
+        for (int a = atom_off_[s]; a < atom_off_[s + 1]; a++) {
+            sys_of_atom_[a] = s;
+            local_[a] = a - atom_off_[s];
+        }
+    lat_.assign(9 * (size_t)nsys, 0.0);
+    per_.reset(new bool[3 * (size_t)nsys]);
+    for (int s = 0; s < nsys; s++)
+        for (int k = 0; k < 3; k++) per_[3 * s + k] = periodic ? periodic[3 * s + k] : (lattices != nullptr);
+    if (lattices) std::copy(lattices, lattices + 9 * (size_t)nsys, lat_.begin());
+    build_tables(numbers);
+    ghost_.assign(natoms_, 0);
+
+    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    const int nid = tab_.nid();
+    d_sys_of_atom_ = dev_alloc<int>(natoms_);
+    d_atom_off_ = dev_alloc<int>(nsys + 1);
+    d_local_ = dev_alloc<int>(natoms_);
+    d_sp_ = dev_alloc<int>(natoms_);
+    d_ghost_ = dev_alloc<uint8_t>(natoms_);
+    d_img_off_ = dev_alloc<int>(kImageKinds * (nsys + 1));
+    d_rcov_ = dev_alloc<double>(nid);
+    d_nref_ = dev_alloc<int>(nid);
+    d_refcn_ = dev_alloc<double>(nid * kMaxRef);
+    d_c6ref_ = dev_alloc<double>((size_t)nid * nid * kMaxRef * kMaxRef);
+    d_c6ref_f_ = dev_alloc<float>((size_t)nid * nid * kMaxRef * kMaxRef);
+    d_pair_ = dev_alloc<double>((size_t)nid * nid * kPairSlots);
+    d_atm_r0_ = dev_alloc<double>((size_t)nid * nid);
+    d_counts_ = dev_alloc<unsigned long long>(3);
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes) check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_), "upload");
+    };
+    up(d_sys_of_atom_, sys_of_atom_.data(), sizeof(int) * natoms_);
+    up(d_atom_off_, atom_off_.data(), sizeof(int) * (nsys + 1));
+    up(d_local_, local_.data(), sizeof(int) * natoms_);
+    up(d_sp_, sp_.data(), sizeof(int) * natoms_);
+    up(d_ghost_, ghost_.data(), natoms_);
+    up(d_rcov_, tab_.rcov.data(), sizeof(double) * nid);
+    up(d_nref_, tab_.nref.data(), sizeof(int) * nid);
+    up(d_refcn_, tab_.refcn.data(), sizeof(double) * nid * kMaxRef);
+    up(d_c6ref_, tab_.c6ref.data(), sizeof(double) * tab_.c6ref.size());
+    up(d_c6ref_f_, tab_.c6ref_f.data(), sizeof(float) * tab_.c6ref_f.size());
+    std::vector<double> r0((size_t)nid * nid);
+    for (int a = 0; a < nid; a++)
+        for (int b = 0; b < nid; b++) r0[a * nid + b] = 4.0 / 3.0 * tab_.rvdw[a * nid + b];
+    up(d_atm_r0_, r0.data(), sizeof(double) * r0.size());
+    // three-body dense blocks per system
+    c6mat_off_.assign(nsys, 0);
+    long long off = 0;
+    for (int s = 0; s < nsys; s++) {
+        c6mat_off_[s] = off;
+        off += (long long)natoms[s] * natoms[s];
+    }
+    c6mat_total_ = off;
+    check(cudaStreamSynchronize(stream_), "upload sync");
+}
+
+Engine::~Engine()
+{
+    cudaSetDevice(device_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (auto& e : ev_)
+        if (e) cudaEventDestroy(e);
+    for (void* p : allocations_) cudaFree(p);
+    if (h_stage_) cudaFreeHost(h_stage_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::build_tables(const int* numbers)
+{
+    // species by first occurrence over the batch
+    sp_.resize(natoms_);
+    for (int a = 0; a < natoms_; a++) {
+        const int z = numbers[a];
+        if (z < 1 || z > D3_MAX_ELEM) throw Error("Unsupported element with atomic number " + std::to_string(z));
+        auto it = std::find(tab_.num.begin(), tab_.num.end(), z);
+        if (it == tab_.num.end()) {
+            tab_.num.push_back(z);
+            sp_[a] = tab_.nid() - 1;
+        } else {
+            sp_[a] = (int)(it - tab_.num.begin());
+        }
+    }
+    const int nid = tab_.nid();
+    tab_.rcov.resize(nid);
+    tab_.r4r2.resize(nid);
+    tab_.nref.resize(nid);
+    tab_.refcn.assign((size_t)nid * kMaxRef, 0.0);
+    for (int s = 0; s < nid; s++) {
+        const int z = tab_.num[s];
+        tab_.rcov[s] = covalent_radius(z);
+        tab_.r4r2[s] = r4r2_value(z);
+        tab_.nref[s] = d3_nref[z - 1];
+        for (int r = 0; r < tab_.nref[s]; r++) tab_.refcn[s * kMaxRef + r] = d3_refcn[(z - 1) * 7 + r];
+    }
+    tab_.rvdw.assign((size_t)nid * nid, 0.0);
+    for (int is = 0; is < nid; is++)
+        for (int js = 0; js <= is; js++) {
+            const double r = vdw_rad(tab_.num[js], tab_.num[is]);
+            tab_.rvdw[js * nid + is] = r;
+            tab_.rvdw[is * nid + js] = r;
+        }
+    // c6(ir, jr, is, js) as filled by new_d3_model (model.f90:150-163)
+    tab_.c6ref.assign((size_t)nid * nid * kMaxRef * kMaxRef, 0.0);
+    auto at = [&](int ir, int jr, int is, int js) -> double& {
+        return tab_.c6ref[(((size_t)is * nid + js) * kMaxRef + ir) * kMaxRef + jr];
+    };
+    for (int is = 0; is < nid; is++)
+        for (int js = 0; js <= is; js++)
+            for (int ir = 0; ir < tab_.nref[is]; ir++)
+                for (int jr = 0; jr < tab_.nref[js]; jr++) {
+                    at(jr, ir, js, is) = ref_c6(jr, ir, tab_.num[js], tab_.num[is]);
+                    at(ir, jr, is, js) = at(jr, ir, js, is);
+                }
+    tab_.c6ref_f.assign(tab_.c6ref.begin(), tab_.c6ref.end());
+}
+
+bool Engine::periodic_any(int sys) const
+{
+    return per_[3 * sys] || per_[3 * sys + 1] || per_[3 * sys + 2];
+}
+
+void Engine::set_ghost(const std::vector<uint8_t>& ghost)
+{
+    ghost_ = ghost;
+    ghost_.resize(natoms_, 0);
+    check(cudaMemcpyAsync(d_ghost_, ghost_.data(), natoms_, cudaMemcpyHostToDevice, stream_), "ghost");
+    check(cudaStreamSynchronize(stream_), "ghost sync");
+}
+
+void Engine::set_partition(int part, int nparts, bool cn_partitioned)
+{
+    part_.part = part;
+    part_.nparts = nparts;
+    cn_partitioned_ = cn_partitioned;
+}
+
+void Engine::set_lattices(const double* lattices)
+{
+    if (!lattices) return;
+    if (!std::equal(lattices, lattices + 9 * (size_t)nsys_, lat_.begin())) {
+        std::copy(lattices, lattices + 9 * (size_t)nsys_, lat_.begin());
+        images_valid_ = false;
+    }
+}
+
+void Engine::counts(long long out[3]) const
+{
+    unsigned long long h[3] = {0, 0, 0};
+    check(cudaMemcpy(h, d_counts_, sizeof(h), cudaMemcpyDeviceToHost), "counts");
+    for (int k = 0; k < 3; k++) out[k] = (long long)h[k];
+}
+
+void Engine::ensure_images(cudaStream_t stream)
+{
+    if (images_valid_) return;
+    const double rthr[kImageKinds] = {cut_.cn, cut_.disp2, cut_.disp3};
+    std::vector<int> off(kImageKinds * (nsys_ + 1), 0);
+    std::vector<double> all;
+    for (int k = 0; k < kImageKinds; k++) {
+        for (int s = 0; s < nsys_; s++) {
+            off[k * (nsys_ + 1) + s] = (int)(all.size() / 3);
+            std::vector<double> t = lattice_points(&lat_[9 * s], &per_[3 * s], rthr[k]);
+            all.insert(all.end(), t.begin(), t.end());
+        }
+        off[k * (nsys_ + 1) + nsys_] = (int)(all.size() / 3);
+    }
+    if (all.size() > img_capacity_) {
+        if (d_img_) {
+            check(cudaStreamSynchronize(stream), "images sync");
+            auto it = std::find(allocations_.begin(), allocations_.end(), (void*)d_img_);
+            if (it != allocations_.end()) allocations_.erase(it);
+            check(cudaFree(d_img_), "cudaFree");
+        }
+        img_capacity_ = all.size() + all.size() / 4 + 3;
+        d_img_ = dev_alloc<double>(img_capacity_);
+    }
+    check(cudaMemcpyAsync(d_img_, all.data(), sizeof(double) * all.size(), cudaMemcpyHostToDevice, stream), "images");
+    check(cudaMemcpyAsync(d_img_off_, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, stream), "img_off");
+    // the host vectors go out of scope: make the copies complete first
+    check(cudaStreamSynchronize(stream), "images sync");
+    images_valid_ = true;
+}
+
+void Engine::ensure_workspace(bool grad, bool param_grad, bool threebody)
+{
+    if (!ws_ready_) {
+        const size_t n = natoms_;
+        d_x_ = dev_alloc<double>(n); d_y_ = dev_alloc<double>(n); d_z_ = dev_alloc<double>(n);
+        d_xhi_ = dev_alloc<float4>(n); d_xlo_ = dev_alloc<float4>(n);
+        work_.cn = dev_alloc<double>(n);
+        work_.gw = dev_alloc<double>(n * kMaxRef);
+        work_.dgw = dev_alloc<double>(n * kMaxRef);
+        work_.gwf = dev_alloc<float>(n * kMaxRef);
+        work_.dgwf = dev_alloc<float>(n * kMaxRef);
+        work_.dEdcn = dev_alloc<double>(n);
+        work_.e_atom = dev_alloc<double>(n);
+        work_.grad = dev_alloc<double>(3 * n);
+        work_.sig_atom = dev_alloc<double>(kSigma * n);
+        d_pos_in_ = dev_alloc<double>(3 * n);
+        d_energies_ = dev_alloc<double>(nsys_);
+        d_grad_out_ = dev_alloc<double>(3 * n);
+        d_sigma_ = dev_alloc<double>(9 * (size_t)nsys_);
+        ws_ready_ = true;
+    }
+    if (param_grad && !ws_pg_) {
+        work_.pg_atom = dev_alloc<double>(kParamGrad * (size_t)natoms_);
+        ws_pg_ = true;
+    }
+    if (threebody && !ws_3b_) {
+        throw Error("three-body workspace requested before it is available");
+    }
+    (void)grad;
+}
+
+void Engine::upload_pair_table(const Damp& d, cudaStream_t stream)
+{
+    if (pair_valid_ && std::memcmp(&d, &last_damp_, sizeof(Damp)) == 0) return;
+    const int nid = tab_.nid();
+    std::vector<double> t((size_t)nid * nid * kPairSlots, 0.0);
+    for (int a = 0; a < nid; a++)
+        for (int b = 0; b < nid; b++) {
+            double* p = &t[kPairSlots * (a * nid + b)];
+            // rrij = 3 r4r2_i r4r2_j (rational.f90:458, zero.f90:475)
+            const double rrij = 3 * tab_.r4r2[a] * tab_.r4r2[b];
+            p[0] = rrij;
+            if (d.kind == kRational) {
+                const double r0 = d.a1 * std::sqrt(rrij) + d.a2;
+                const double r02 = r0 * r0;
+                const double r06 = r02 * r02 * r02;
+                p[1] = r06;
+                p[2] = r06 * r02;
+                p[3] = r0;
+                p[4] = std::sqrt(rrij);
+            } else {
+                const double r0 = tab_.rvdw[b * nid + a];
+                p[1] = d.rs6 * r0;
+                p[2] = d.rs8 * r0;
+                p[3] = r0;
+            }
+        }
+    check(cudaMemcpyAsync(d_pair_, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice, stream), "pair table");
+    check(cudaStreamSynchronize(stream), "pair table sync");
+    last_damp_ = d;
+    pair_valid_ = true;
+}
+
+void Engine::run(const Damp& d, const double* d_positions, double* d_energies, double* d_gradient,
+                 double* d_sigma9, double* d_param_grad, bool grad, cudaStream_t stream)
+{
+    const bool pg = d_param_grad != nullptr;
+    const bool threebody = std::fabs(d.s9) >= DBL_EPSILON || (pg && false);
+    if (threebody) throw Error("three-body term is not available in this build");
+    ensure_images(stream);
+    ensure_workspace(grad, pg, threebody);
+    upload_pair_table(d, stream);
+
+    Batch b;
+    b.nsys = nsys_; b.natoms = natoms_; b.nid = tab_.nid();
+    b.sys_of_atom = d_sys_of_atom_; b.atom_off = d_atom_off_; b.local = d_local_; b.sp = d_sp_;
+    b.ghost = d_ghost_; b.img_off = d_img_off_; b.img = d_img_;
+    b.x = d_x_; b.y = d_y_; b.z = d_z_; b.xhi = d_xhi_; b.xlo = d_xlo_;
+    Species s;
+    s.rcov = d_rcov_; s.nref = d_nref_; s.refcn = d_refcn_; s.c6ref = d_c6ref_;
+    s.c6ref_f = d_c6ref_f_; s.pair = d_pair_; s.atm_r0 = d_atm_r0_;
+    Config c;
+    c.cut_cn = cut_.cn; c.cut2 = cut_.disp2; c.cut3 = cut_.disp3;
+    c.width2 = cut_.width2; c.width3 = cut_.width3;
+    c.grad = grad; c.mixed = mixed_; c.param_grad = pg; c.cn_partitioned = cn_partitioned_;
+    Work w = work_;
+    w.counts = counting_ ? d_counts_ : nullptr;
+    w.e3_atom = nullptr;
+    if (!pg) w.pg_atom = nullptr;
+    if (counting_) check(cudaMemsetAsync(d_counts_, 0, 3 * sizeof(unsigned long long), stream), "counts");
+
+    auto mark = [&](int k) {
+        if (profiling_) check(cudaEventRecord(ev_[k], stream), "cudaEventRecord");
+    };
+    if (profiling_ && !ev_[0])
+        for (auto& e : ev_) check(cudaEventCreate(&e), "cudaEventCreate");
+    mark(0);
+    launch_split_positions(d_positions, natoms_, d_x_, d_y_, d_z_, d_xhi_, d_xlo_, mixed_, stream);
+    mark(1);
+    launch_coordination_number(b, s, c, part_, w, stream);
+    mark(2);
+    launch_weights(b, s, c, w, stream);
+    mark(3);
+    if (std::fabs(d.s6) >= DBL_EPSILON || std::fabs(d.s8) >= DBL_EPSILON || pg) {
+        launch_two_body(b, s, d, c, part_, w, stream);
+    } else {
+        check(cudaMemsetAsync(w.e_atom, 0, sizeof(double) * natoms_, stream), "memset");
+        if (grad) {
+            check(cudaMemsetAsync(w.dEdcn, 0, sizeof(double) * natoms_, stream), "memset");
+            check(cudaMemsetAsync(w.grad, 0, sizeof(double) * 3 * natoms_, stream), "memset");
+            check(cudaMemsetAsync(w.sig_atom, 0, sizeof(double) * kSigma * natoms_, stream), "memset");
+        }
+    }
+    mark(4);
+    mark(5);
+    if (grad) launch_cn_chain_rule(b, s, c, part_, w, stream);
+    mark(6);
+    launch_reduce_systems(b, c, w, d_energies, d_sigma9, d_param_grad, d_gradient, stream);
+    mark(7);
+    ev_recorded_ = profiling_;
+    check(cudaGetLastError(), "kernel launch");
+}
+
+void Engine::stage_times(double out[kStages])
+{
+    for (int k = 0; k < kStages; k++) out[k] = 0.0;
+    if (!ev_recorded_) return;
+    check(cudaEventSynchronize(ev_[kStages]), "cudaEventSynchronize");
+    for (int k = 0; k < kStages; k++) {
+        float ms = 0.f;
+        check(cudaEventElapsedTime(&ms, ev_[k], ev_[k + 1]), "cudaEventElapsedTime");
+        out[k] = ms;
+    }
+}
+
+void Engine::evaluate_host(const Damp& d, const double* positions, double* energies, double* gradient,
+                           double* sigma9)
+{
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    const bool grad = gradient != nullptr || sigma9 != nullptr;
+    ensure_workspace(grad, false, false);
+    const size_t nin = 3 * (size_t)natoms_;
+    const size_t nout = nsys_ + 3 * (size_t)natoms_ + 9 * (size_t)nsys_;
+    if (h_stage_len_ < nin + nout) {
+        if (h_stage_) cudaFreeHost(h_stage_);
+        h_stage_len_ = nin + nout;
+        check(cudaMallocHost(&h_stage_, sizeof(double) * h_stage_len_), "cudaMallocHost");
+    }
+    double* hin = h_stage_;
+    double* he = h_stage_ + nin;
+    double* hg = he + nsys_;
+    double* hs = hg + 3 * (size_t)natoms_;
+    std::memcpy(hin, positions, sizeof(double) * nin);
+    check(cudaMemcpyAsync(d_pos_in_, hin, sizeof(double) * nin, cudaMemcpyHostToDevice, stream_), "positions");
+    run(d, d_pos_in_, d_energies_, grad ? d_grad_out_ : nullptr, grad ? d_sigma_ : nullptr, nullptr, grad, stream_);
+    check(cudaMemcpyAsync(he, d_energies_, sizeof(double) * nsys_, cudaMemcpyDeviceToHost, stream_), "energies");
+    if (grad) {
+        check(cudaMemcpyAsync(hg, d_grad_out_, sizeof(double) * 3 * natoms_, cudaMemcpyDeviceToHost, stream_), "gradient");
+        check(cudaMemcpyAsync(hs, d_sigma_, sizeof(double) * 9 * nsys_, cudaMemcpyDeviceToHost, stream_), "sigma");
+    }
+    check(cudaStreamSynchronize(stream_), "evaluate");
+    std::memcpy(energies, he, sizeof(double) * nsys_);
+    if (gradient) std::memcpy(gradient, hg, sizeof(double) * 3 * natoms_);
+    if (sigma9) std::memcpy(sigma9, hs, sizeof(double) * 9 * nsys_);
+}
+
+void Engine::evaluate_device(const Damp& d, const double* d_positions, double* d_energies,
+                             double* d_gradient, double* d_sigma9, double* d_param_grad,
+                             cudaStream_t stream)
+{
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    const bool grad = d_gradient != nullptr || d_sigma9 != nullptr;
+    run(d, d_positions, d_energies, d_gradient, d_sigma9, d_param_grad, grad, stream);
+}
+
+}  // namespace d3

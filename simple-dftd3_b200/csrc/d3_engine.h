@@ -1,0 +1,148 @@
+// Host-side driver of the D3 pipeline: model tables, lattice images, device
+// workspace and the launch sequence of one evaluation.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "d3_device.cuh"
+
+namespace d3 {
+
+struct Cutoffs {
+    // realspace_cutoff defaults (cutoff.f90:26-38)
+    double disp2 = 60.0, disp3 = 40.0, cn = 40.0, width2 = 0.0, width3 = 0.0;
+};
+
+struct Error : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+// Lattice translations within rthr (get_lattice_points, cutoff.f90:140-227).
+// lattice[3][3] holds one vector per row; periodic[3].
+std::vector<double> lattice_points(const double* lattice, const bool* periodic, double rthr);
+
+// Wrap positions into the central cell (wrap_to_central_cell, utils.f90:29-64).
+void wrap_to_central_cell(int nat, double* xyz, const double* lattice, const bool* periodic);
+
+// True if two atoms are closer than 1e-9 Bohr (verify_structure, api.f90:1517-1530).
+bool has_overlapping_atoms(int nat, const double* xyz);
+
+// Species set and the per-species D3 model tables (new_d3_model, model.f90:87-181).
+struct ModelTables {
+    std::vector<int> num;            // atomic number per species
+    std::vector<double> rcov, r4r2, refcn, c6ref, rvdw;
+    std::vector<float> c6ref_f;
+    std::vector<int> nref;
+    int nid() const { return (int)num.size(); }
+};
+
+class Engine {
+public:
+    // nsys systems with natoms[s] atoms each; numbers concatenated.
+    // lattices[nsys][9] and periodic[nsys][3] may be null (molecules).
+    Engine(int nsys, const int* natoms, const int* numbers, const double* lattices,
+           const bool* periodic, int device = -1);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    int nsys() const { return nsys_; }
+    int natoms() const { return natoms_; }
+    const ModelTables& tables() const { return tab_; }
+    const std::vector<int>& atom_off() const { return atom_off_; }
+    bool periodic_any(int sys) const;
+    const double* lattice(int sys) const { return &lat_[9 * sys]; }
+    const bool* periodic(int sys) const { return &per_[3 * sys]; }
+
+    void set_cutoffs(const Cutoffs& c) { cut_ = c; images_valid_ = false; }
+    const Cutoffs& cutoffs() const { return cut_; }
+    void set_ghost(const std::vector<uint8_t>& ghost);
+    void set_partition(int part, int nparts, bool cn_partitioned);
+    void set_precision(int mixed) { mixed_ = mixed != 0; }
+    bool mixed() const { return mixed_; }
+    void set_counting(bool on) { counting_ = on; }
+    void counts(long long out[3]) const;
+    // Replace the lattices (host, [nsys][9]); images are rebuilt lazily.
+    void set_lattices(const double* lattices);
+
+    // Evaluate from host buffers (positions already wrapped).  Blocking.
+    void evaluate_host(const Damp& d, const double* positions, double* energies, double* gradient,
+                       double* sigma9);
+    // Evaluate from device buffers on `stream` (the caller's stream, used as
+    // given: 0 is the legacy default stream).  Asynchronous.
+    void evaluate_device(const Damp& d, const double* d_positions, double* d_energies,
+                         double* d_gradient, double* d_sigma9, double* d_param_grad,
+                         cudaStream_t stream);
+
+    cudaStream_t stream() const { return stream_; }
+
+    // Per-stage device times of the last evaluation (ms), recorded with CUDA
+    // events when profiling is on.  Stages: see kStageNames.
+    static constexpr int kStages = 7;
+    void set_profiling(bool on) { profiling_ = on; }
+    void stage_times(double out[kStages]);
+
+private:
+    void build_tables(const int* numbers);
+    void ensure_images(cudaStream_t stream);
+    void ensure_workspace(bool grad, bool param_grad, bool threebody);
+    void upload_pair_table(const Damp& d, cudaStream_t stream);
+    void run(const Damp& d, const double* d_positions, double* d_energies, double* d_gradient,
+             double* d_sigma9, double* d_param_grad, bool grad, cudaStream_t stream);
+    template <class T> T* dev_alloc(size_t n);
+
+    int device_ = 0;
+    int nsys_ = 0, natoms_ = 0, max_sys_atoms_ = 0;
+    std::vector<int> atom_off_, sys_of_atom_, local_, sp_;
+    std::vector<double> lat_;
+    std::vector<bool> per_storage_;
+    std::unique_ptr<bool[]> per_;
+    std::vector<uint8_t> ghost_;
+    ModelTables tab_;
+    Cutoffs cut_;
+    Partition part_;
+    bool cn_partitioned_ = false;
+    bool mixed_ = false;
+    bool counting_ = false;
+    bool profiling_ = false;
+    cudaEvent_t ev_[kStages + 1] = {};
+    bool ev_recorded_ = false;
+    bool images_valid_ = false;
+    Damp last_damp_{};
+    bool pair_valid_ = false;
+
+    cudaStream_t stream_ = nullptr;
+    std::vector<void*> allocations_;
+    // static device data
+    int *d_sys_of_atom_ = nullptr, *d_atom_off_ = nullptr, *d_local_ = nullptr, *d_sp_ = nullptr;
+    uint8_t* d_ghost_ = nullptr;
+    int* d_img_off_ = nullptr;
+    double* d_img_ = nullptr;
+    size_t img_capacity_ = 0;
+    double *d_rcov_ = nullptr, *d_refcn_ = nullptr, *d_c6ref_ = nullptr, *d_pair_ = nullptr,
+           *d_atm_r0_ = nullptr;
+    float* d_c6ref_f_ = nullptr;
+    int* d_nref_ = nullptr;
+    // workspace
+    double *d_x_ = nullptr, *d_y_ = nullptr, *d_z_ = nullptr;
+    float4 *d_xhi_ = nullptr, *d_xlo_ = nullptr;
+    Work work_{};
+    bool ws_grad_ = false, ws_pg_ = false, ws_3b_ = false, ws_ready_ = false;
+    double* d_pos_in_ = nullptr;
+    double *d_energies_ = nullptr, *d_grad_out_ = nullptr, *d_sigma_ = nullptr;
+    double *h_stage_ = nullptr;   // pinned staging: positions in, results out
+    size_t h_stage_len_ = 0;
+    unsigned long long* d_counts_ = nullptr;
+    // three-body
+    std::vector<long long> c6mat_off_;
+    long long c6mat_total_ = 0, acc_total_ = 0, nbr_capacity_ = 0;
+    long long* d_c6mat_off_ = nullptr;
+};
+
+}  // namespace d3
