@@ -111,6 +111,39 @@ dftd3_b200_get_batch_stage_times(dftd3_error /* error */,
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_b200_delete_batch(dftd3_b200_batch* /* batch */);
 
+/* Energy, gradient and virial of one system (two-body term, s9 = 0) without
+ * allocating memory.  This entry point has no counterpart in the reference.
+ * It serves callers that cannot allocate device memory while they run --
+ * code executing under another framework's stream capture, integrators that
+ * hand out all device memory from their own pool, latency-critical loops in
+ * which cudaMalloc/cudaFree (which can synchronise the device) are not
+ * allowed.  All work arrays come from a fixed __device__ array inside
+ * the library (4 MiB), held by every GPU that loads it until exit.
+ *   numbers[natoms], lattice[3][3], periodic[3] and cutoffs[5] (disp2, disp3,
+ *   cn, width2, width3; NULL for the defaults) are host memory;
+ *   d_positions[natoms][3], d_energy[1], d_gradient[natoms][3] and
+ *   d_sigma[9] are device memory (gradient and sigma may be NULL); positions
+ *   are used as given (no wrapping).  Work is enqueued on `stream`.
+ * Limits: 4096 atoms, 16 elements, 8192 lattice translations per cutoff;
+ * larger inputs are rejected with an error.  All calls on a device share the
+ * array, so calls that overlap on the GPU race and must be serialised by the
+ * caller.  The first call on a device looks up the array's device address
+ * with that device current; make it before any stream capture. */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_get_dispersion_noalloc(dftd3_error /* error */,
+                                  dftd3_param /* param */,
+                                  int /* natoms */,
+                                  const int* /* numbers [natoms] (host) */,
+                                  const double* /* d_positions [natoms][3] */,
+                                  const double* /* lattice [3][3] (host) or NULL */,
+                                  const bool* /* periodic [3] (host) or NULL */,
+                                  const double* /* cutoffs [5] (host) or NULL */,
+                                  int /* precision */,
+                                  double* /* d_energy [1] */,
+                                  double* /* d_gradient [natoms][3] or NULL */,
+                                  double* /* d_sigma [9] or NULL */,
+                                  void* /* stream */);
+
 /* Measured fused-multiply-add throughput of the current device in TFLOP/s
  * (precision DFTD3_B200_PRECISION_FP64: FP64 pipe, _MIXED: FP32 pipe); the
  * denominator of the roofline fraction the benchmark reports. */

@@ -17,6 +17,12 @@
 #include "d3_engine.h"
 #include "d3_tables.h"
 
+namespace d3 {
+bool noalloc_dispersion(const Damp& damp, int natoms, const int* numbers, const double* d_positions,
+                        const double* lattice, const bool* periodic, const double* cutoffs, int precision,
+                        double* d_energy, double* d_gradient, double* d_sigma, cudaStream_t stream, char* msg);
+}
+
 struct _dftd3_error {
     bool set = false;
     std::string message;
@@ -608,6 +614,22 @@ void dftd3_b200_get_batch_stage_times(dftd3_error error, dftd3_b200_batch batch,
         return;
     }
     guarded(error, [&] { batch->engine->stage_times(ms); });
+}
+
+void dftd3_b200_get_dispersion_noalloc(dftd3_error error, dftd3_param param, int natoms, const int* numbers,
+                                       const double* d_positions, const double* lattice, const bool* periodic,
+                                       const double* cutoffs, int precision, double* d_energy,
+                                       double* d_gradient, double* d_sigma, void* stream)
+{
+    if (!error) return;
+    if (!param) {
+        fail(error, "Damping parameters are missing");
+        return;
+    }
+    char msg[256];
+    if (!d3::noalloc_dispersion(param->damp, natoms, numbers, d_positions, lattice, periodic, cutoffs, precision,
+                                d_energy, d_gradient, d_sigma, static_cast<cudaStream_t>(stream), msg))
+        fail(error, msg);
 }
 
 double dftd3_b200_fma_peak(dftd3_error error, int precision)
