@@ -70,15 +70,9 @@ struct Work {
     double* sig_atom = nullptr;  // [natoms][kSigma]
     double* pg_atom = nullptr;   // [natoms][kParamGrad] or null
     unsigned long long* counts = nullptr;  // [3] pair, triple, cn terms or null
-    // three-body
-    double* c6mat = nullptr;     // per system dense [n][n][3]: c6, dc6/dcn_row, dc6/dcn_col
-    const long long* c6mat_off = nullptr;   // [nsys] offsets (in elements of 3 doubles)
-    int* nbr_count = nullptr;    // [natoms]
-    long long* nbr_off = nullptr;// [natoms + 1]
-    int4* nbr = nullptr;         // [total] (j, image, -, -)
-    double* nbr_vec = nullptr;   // [total][4] vector x_j + T - x_i and r2
-    double* atm_acc = nullptr;   // dense per-system [n][n][4] triangular accumulator
-    double* e3_atom = nullptr;   // [natoms] three-body energy per root atom
+    // three-body results per root atom (summed by the per-system reduction)
+    double* e3_atom = nullptr;   // [natoms] three-body energy of the root's triples
+    double* sig3_atom = nullptr; // [natoms][kSigma] three-body virial of the root's triples
 };
 
 struct Config {
@@ -101,9 +95,22 @@ void launch_weights(const Batch& b, const Species& s, const Config& c, const Wor
                     cudaStream_t stream);
 void launch_two_body(const Batch& b, const Species& s, const Damp& d, const Config& c,
                      const Partition& p, const Work& w, cudaStream_t stream);
-void launch_three_body(const Batch& b, const Species& s, const Damp& d, const Config& c,
-                       const Partition& p, const Work& w, long long nbr_capacity,
-                       int max_sys_atoms, cudaStream_t stream);
+// Three-body term (d3_atm.cu): C6 table, neighbour lists, triple sum.
+size_t atm_c6_entry_bytes(bool mixed);
+void launch_c6_matrix(const Batch& b, const Species& s, const Work& w, const long long* d_mat_off,
+                      void* mat, long long total, bool mixed, cudaStream_t stream);
+void launch_nbr_count(const Batch& b, const Config& c, int* cnt, int* max_cnt, cudaStream_t stream);
+size_t scan_temp_bytes(int n);
+void launch_scan(void* temp, size_t temp_bytes, const int* cnt_ext, long long* off, int n,
+                 cudaStream_t stream);
+void launch_nbr_fill(const Batch& b, const Config& c, const long long* off, int* nbr_j, int* nbr_gend,
+                     double4* nbr_v, cudaStream_t stream);
+int atm_blocks_per_sm(bool mixed, bool grad);
+void launch_triples(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
+                    const Work& w, const void* mat, const long long* mat_off, const long long* off,
+                    const int* cnt, const int* nbr_j, const int* nbr_gend, const double4* nbr_v,
+                    unsigned int* queue, double* slot_acc, int slot_stride, int blocks, double* e3,
+                    double* sig3, cudaStream_t stream);
 void launch_cn_chain_rule(const Batch& b, const Species& s, const Config& c, const Partition& p,
                           const Work& w, cudaStream_t stream);
 void launch_reduce_systems(const Batch& b, const Config& c, const Work& w, double* energies,

@@ -264,6 +264,7 @@ Engine::~Engine()
         if (e) cudaEventDestroy(e);
     for (void* p : allocations_) cudaFree(p);
     if (h_stage_) cudaFreeHost(h_stage_);
+    if (h_atm_counts_) cudaFreeHost(h_atm_counts_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -408,10 +409,8 @@ void Engine::ensure_workspace(bool grad, bool param_grad, bool threebody)
         work_.pg_atom = dev_alloc<double>(kParamGrad * (size_t)natoms_);
         ws_pg_ = true;
     }
-    if (threebody && !ws_3b_) {
-        throw Error("three-body workspace requested before it is available");
-    }
     (void)grad;
+    (void)threebody;
 }
 
 void Engine::upload_pair_table(const Damp& d, cudaStream_t stream)
@@ -450,8 +449,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
                  double* d_sigma9, double* d_param_grad, bool grad, cudaStream_t stream)
 {
     const bool pg = d_param_grad != nullptr;
-    const bool threebody = std::fabs(d.s9) >= DBL_EPSILON || (pg && false);
-    if (threebody) throw Error("three-body term is not available in this build");
+    const bool threebody = std::fabs(d.s9) >= DBL_EPSILON;
     ensure_images(stream);
     ensure_workspace(grad, pg, threebody);
     upload_pair_table(d, stream);
@@ -471,6 +469,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     Work w = work_;
     w.counts = counting_ ? d_counts_ : nullptr;
     w.e3_atom = nullptr;
+    w.sig3_atom = nullptr;
     if (!pg) w.pg_atom = nullptr;
     if (counting_) check(cudaMemsetAsync(d_counts_, 0, 3 * sizeof(unsigned long long), stream), "counts");
 
@@ -497,6 +496,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
         }
     }
     mark(4);
+    if (threebody) run_three_body(b, s, d, c, w, stream);
     mark(5);
     if (grad) launch_cn_chain_rule(b, s, c, part_, w, stream);
     mark(6);
@@ -504,6 +504,75 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     mark(7);
     ev_recorded_ = profiling_;
     check(cudaGetLastError(), "kernel launch");
+}
+
+void Engine::free_block(void*& p)
+{
+    if (!p) return;
+    auto it = std::find(allocations_.begin(), allocations_.end(), p);
+    if (it != allocations_.end()) allocations_.erase(it);
+    check(cudaFree(p), "cudaFree");
+    p = nullptr;
+}
+
+void Engine::run_three_body(const Batch& b, const Species& s, const Damp& d, const Config& c, Work& w,
+                            cudaStream_t stream)
+{
+    const int n = natoms_;
+    if (!atm_ready_) {
+        d_c6mat_off_ = dev_alloc<long long>(nsys_);
+        check(cudaMemcpy(d_c6mat_off_, c6mat_off_.data(), sizeof(long long) * nsys_, cudaMemcpyHostToDevice),
+              "c6 offsets");
+        // sized for the FP64 entries, which also hold the FP32 ones
+        d_c6mat_ = dev_alloc<unsigned char>(atm_c6_entry_bytes(false) * (size_t)std::max<long long>(c6mat_total_, 1));
+        d_cnt_ = dev_alloc<int>(n + 1);
+        d_off_ = dev_alloc<long long>(n + 1);
+        d_maxcnt_ = dev_alloc<int>(1);
+        d_queue_ = dev_alloc<unsigned int>(1);
+        d_e3_ = dev_alloc<double>(n);
+        d_sig3_ = dev_alloc<double>((size_t)kSigma * n);
+        scan_bytes_ = scan_temp_bytes(n);
+        d_scan_temp_ = dev_alloc<unsigned char>(scan_bytes_);
+        check(cudaMallocHost(&h_atm_counts_, 2 * sizeof(long long)), "cudaMallocHost");
+        atm_ready_ = true;
+    }
+    launch_c6_matrix(b, s, w, d_c6mat_off_, d_c6mat_, c6mat_total_, c.mixed, stream);
+    check(cudaMemsetAsync(d_maxcnt_, 0, sizeof(int), stream), "memset");
+    check(cudaMemsetAsync(d_cnt_ + n, 0, sizeof(int), stream), "memset");
+    launch_nbr_count(b, c, d_cnt_, d_maxcnt_, stream);
+    launch_scan(d_scan_temp_, scan_bytes_, d_cnt_, d_off_, n, stream);
+    check(cudaMemcpyAsync(h_atm_counts_, d_off_ + n, sizeof(long long), cudaMemcpyDeviceToHost, stream), "total");
+    check(cudaMemcpyAsync(h_atm_counts_ + 1, d_maxcnt_, sizeof(int), cudaMemcpyDeviceToHost, stream), "max");
+    check(cudaStreamSynchronize(stream), "neighbour count");
+    const long long total = h_atm_counts_[0];
+    const int maxcnt = (int)(reinterpret_cast<int*>(h_atm_counts_ + 1)[0]);
+    last_triples_entries_ = total;
+    if (total > nbr_cap_) {
+        void* pj = d_nbr_j_; void* pg = d_nbr_gend_; void* pv = d_nbr_v_;
+        free_block(pj); free_block(pg); free_block(pv);
+        nbr_cap_ = total + total / 4 + 1024;
+        d_nbr_j_ = dev_alloc<int>(nbr_cap_);
+        d_nbr_gend_ = dev_alloc<int>(nbr_cap_);
+        d_nbr_v_ = dev_alloc<double4>(nbr_cap_);
+    }
+    int dev = 0, sms = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
+    const int blocks = std::max(1, std::min(n, sms * atm_blocks_per_sm(c.mixed, c.grad)));
+    const int stride = std::max(maxcnt, 1);
+    const long long need = (long long)blocks * stride * 6;
+    if (c.grad && need > slot_cap_) {
+        void* p = d_slot_acc_;
+        free_block(p);
+        slot_cap_ = need + need / 4;
+        d_slot_acc_ = dev_alloc<double>(slot_cap_);
+    }
+    launch_nbr_fill(b, c, d_off_, d_nbr_j_, d_nbr_gend_, d_nbr_v_, stream);
+    check(cudaMemsetAsync(d_queue_, 0, sizeof(unsigned int), stream), "memset");
+    launch_triples(b, s, d, c, part_, w, d_c6mat_, d_c6mat_off_, d_off_, d_cnt_, d_nbr_j_, d_nbr_gend_, d_nbr_v_,
+                   d_queue_, d_slot_acc_, stride, blocks, d_e3_, d_sig3_, stream);
+    w.e3_atom = d_e3_;
+    w.sig3_atom = c.grad ? d_sig3_ : nullptr;
 }
 
 void Engine::stage_times(double out[kStages])

@@ -140,9 +140,30 @@ private:
     size_t h_stage_len_ = 0;
     unsigned long long* d_counts_ = nullptr;
     // three-body
+    void run_three_body(const Batch& b, const Species& s, const Damp& d, const Config& c, Work& w,
+                        cudaStream_t stream);
+    void free_block(void*& p);
     std::vector<long long> c6mat_off_;
-    long long c6mat_total_ = 0, acc_total_ = 0, nbr_capacity_ = 0;
+    long long c6mat_total_ = 0;
     long long* d_c6mat_off_ = nullptr;
+    void* d_c6mat_ = nullptr;
+    int* d_cnt_ = nullptr;
+    long long* d_off_ = nullptr;
+    int* d_maxcnt_ = nullptr;
+    unsigned int* d_queue_ = nullptr;
+    void* d_scan_temp_ = nullptr;
+    size_t scan_bytes_ = 0;
+    int* d_nbr_j_ = nullptr;
+    int* d_nbr_gend_ = nullptr;
+    double4* d_nbr_v_ = nullptr;
+    long long nbr_cap_ = 0;
+    double* d_slot_acc_ = nullptr;
+    long long slot_cap_ = 0;
+    double* d_e3_ = nullptr;
+    double* d_sig3_ = nullptr;
+    long long* h_atm_counts_ = nullptr;   // pinned: total entries, largest list
+    bool atm_ready_ = false;
+    long long last_triples_entries_ = 0;
 };
 
 }  // namespace d3

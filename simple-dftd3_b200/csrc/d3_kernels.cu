@@ -488,7 +488,8 @@ __global__ void k_reduce_systems(Batch b, Config c, Work w, double* energies, do
     for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
         v[0] += w.e_atom[a] + (w.e3_atom ? w.e3_atom[a] : 0.0);
         if (c.grad)
-            for (int k = 0; k < kSigma; k++) v[1 + k] += w.sig_atom[kSigma * a + k];
+            for (int k = 0; k < kSigma; k++)
+                v[1 + k] += w.sig_atom[kSigma * a + k] + (w.sig3_atom ? w.sig3_atom[kSigma * a + k] : 0.0);
         if (c.param_grad && w.pg_atom)
             for (int k = 0; k < kParamGrad; k++) v[1 + kSigma + k] += w.pg_atom[kParamGrad * a + k];
         if (c.grad && grad_out)
