@@ -1,20 +1,25 @@
 #!/usr/bin/env python3
 """Benchmark of the D3 dispersion hot path on B200.
 
-Workload (one step): energy, gradient and virial of the periodic 2000-atom
-triclinic cell (edges 40-45 Bohr, angles 85-95 deg, H/C/N/O/Si/Al, d_min 2.0,
-seeded), D3(BJ) two-body over all lattice images within 60 Bohr with the CN
-chain rule (PBE parameters s6=1, s8=0.7875, a1=0.4289, a2=4.4407).
-The headline `value` is pair-terms/s of the mixed FP32/FP64 form with inputs
-resident in HBM; the plain FP64 form is reported beside it, and `e2e` is the
-same metric through the C ABI with host buffers (positions H2D and
-energy/gradient/virial D2H inside the timed region).  A pair-term is one
-accepted (i, j <= i, T) of the reference's two-body loop.
+Headline workload (one step): energy, gradient and virial of the periodic
+2000-atom triclinic cell (edges 40-45 Bohr, angles 85-95 deg, H/C/N/O/Si/Al,
+d_min 2.0, seeded), D3(BJ) two-body over all lattice images within 60 Bohr with
+the CN chain rule (PBE parameters s6=1, s8=0.7875, a1=0.4289, a2=4.4407).
+`value` is pair-terms/s of the mixed FP32/FP64 form with inputs resident in
+HBM; the plain FP64 form is reported beside it, and `e2e` is the same metric
+through the C ABI with host buffers (positions H2D and energy/gradient/virial
+D2H inside the timed region).  A pair-term is one accepted (i, j <= i, T) of
+the reference's two-body loop; a triple-term one accepted ATM triple.
 
-Multi-GPU: one process per GPU (torchrun); every rank evaluates its own cell
-(seed = rank), no collective on the data path ("scaling": "weak").
+The three-body workloads (ATM, s9 = 1) are measured beside the headline in
+`extra_workloads`: the 5000-atom cluster (triple-terms/s), the batch of 4096
+molecules (molecules/s) and a subset of the 256 periodic frames.  Any of them
+can be the only workload with --workload (used for profiling small cases with
+--natoms / --nsys).
 
---impl reference times the FP64 CPU restatement of the reference (the
+Multi-GPU: one process per GPU (torchrun); every rank evaluates its own copy
+of the workload (seed = rank), no collective on the data path ("scaling":
+"weak").  --impl reference times the FP64 CPU restatement of the reference (the
 reference is Fortran and cannot be built here) on the host cores.
 """
 import argparse
@@ -33,8 +38,13 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "simple-dftd3_b200"))
 
 L2_FLUSH_BYTES = 256 << 20     # larger than the 126 MB L2
-FLOPS_PER_PAIR = 65            # two-body BJ term, E+G+sigma+dEdcn (flop counting: FMA = 2)
+# algorithmic flops per unit of work (FMA = 2); fixed between the two forms
+FLOPS_PER_PAIR = 65            # two-body BJ term with gradient, virial and dE/dCN
+FLOPS_PER_TRIPLE = 220         # ATM term with gradient, virial and dE/dCN
 METRIC = "pair-terms/s, D3(BJ) two-body E+grad+virial (mixed FP32/FP64, <=1e-7 rel. E error)"
+# DRAM bytes (read + write) of one k_two_body_tiled<float> launch on cell2000, from the
+# ncu capture summarised in profiles/k_two_body_tiled_cell2000_mixed.md
+TWO_BODY_TRAFFIC_BYTES = 325632
 
 
 def parse_args():
@@ -43,18 +53,47 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cell2000",
+                    choices=["cell2000", "molecule100", "cluster5000", "batch4096", "frames256"])
+    ap.add_argument("--natoms", type=int, default=None, help="atoms per system (smaller cases for profiling)")
+    ap.add_argument("--nsys", type=int, default=None, help="systems of the batched workloads")
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true")
     return ap.parse_args()
 
 
-def workload(seed):
-    from dftd3 import synthetic
-    d = synthetic.cell2000(seed=seed)
-    par = dict(synthetic.PBE_BJ, damping="rational", s9=0.0)
-    return d, par
+def make_workload(name, seed=0, natoms=None, nsys=None):
+    """(systems, parameters): systems is a list of (numbers, positions, lattice, periodic)."""
+    from dftd3 import synthetic as S
+    if name == "cell2000":
+        d = S.cell2000(seed=seed, natoms=natoms or 2000)
+        systems = [(d["numbers"], d["positions"], d["lattice"], d["periodic"])]
+        s9 = 0.0
+    elif name == "molecule100":
+        d = S.molecule100(seed=seed)
+        systems = [(d["numbers"], d["positions"], None, None)]
+        s9 = 0.0
+    elif name == "cluster5000":
+        d = S.cluster5000(seed=seed, natoms=natoms or 5000)
+        systems = [(d["numbers"], d["positions"], None, None)]
+        s9 = 1.0
+    elif name == "batch4096":
+        d = S.batch4096(seed=seed, nmol=nsys or 4096)
+        systems = [(n, p, None, None) for n, p in zip(d["numbers"], d["positions"])]
+        s9 = 1.0
+    else:
+        d = S.frames256(seed=seed, nframes=nsys or 256, natoms=natoms or 512)
+        systems = [(n, p, l, per) for n, p, l, per in zip(d["numbers"], d["positions"], d["lattices"],
+                                                          d["periodic"])]
+        s9 = 1.0
+    par = dict(S.PBE_BJ, damping="rational", s9=s9)
+    return systems, par
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled while the GPU work runs."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -65,22 +104,20 @@ class ClockSampler:
         self.proc = None
         self.lines = []
 
-    def __enter__(self):
+    def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except (OSError, FileNotFoundError):
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
             self.proc = None
-        return self
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
-    def __exit__(self, *exc):
+    def stop(self):
         if self.proc:
             self.proc.terminate()
             try:
@@ -109,28 +146,93 @@ class ClockSampler:
                 "samples": len(mhz)}
 
 
-def cpu_reference_time(d, par, repeats=3):
-    """Wall time of the FP64 CPU restatement of one evaluation (all host threads)."""
+class Runner:
+    """One workload on the device: batch handle, device buffers, timed steps."""
+
+    def __init__(self, systems, par):
+        import torch
+        from dftd3 import library as lib
+        self.torch, self.lib = torch, lib
+        self.systems = systems
+        self.natoms = np.array([len(s[0]) for s in systems], dtype=np.int32)
+        numbers = np.ascontiguousarray(np.concatenate([np.asarray(s[0]) for s in systems]), dtype=np.int32)
+        pos = np.ascontiguousarray(np.concatenate([np.asarray(s[1], dtype=float).reshape(-1, 3) for s in systems]))
+        periodic = systems[0][2] is not None
+        lat = np.ascontiguousarray([s[2] for s in systems], dtype=float) if periodic else None
+        per = np.ascontiguousarray([s[3] for s in systems], dtype=bool) if periodic else None
+        self.batch = lib.new_batch(self.natoms, numbers, lat, per)
+        self.param = lib.new_rational_damping(par["s6"], par["s8"], par["s9"], par["a1"], par["a2"], par["alp"])
+        self.pos = torch.tensor(pos, dtype=torch.float64, device="cuda")
+        nsys = len(systems)
+        self.e = torch.zeros(nsys, dtype=torch.float64, device="cuda")
+        self.g = torch.zeros_like(self.pos)
+        self.s = torch.zeros(9 * nsys, dtype=torch.float64, device="cuda")
+        self.stream = torch.cuda.current_stream()
+
+    def step(self):
+        self.lib.get_dispersion_device(self.batch, self.param, self.pos.data_ptr(), None, self.e.data_ptr(),
+                                       self.g.data_ptr(), self.s.data_ptr(), 0, self.stream.cuda_stream)
+
+    def counts(self):
+        self.lib.set_batch_counting(self.batch, True)
+        self.step()
+        self.torch.cuda.synchronize()
+        c = self.lib.get_batch_counts(self.batch)
+        self.lib.set_batch_counting(self.batch, False)
+        return {"pair_terms": int(c[0]), "triple_terms": int(c[1]), "cn_terms": int(c[2])}
+
+    def time(self, precision, steps, warmup, flush, dist=None):
+        torch, lib = self.torch, self.lib
+        lib.set_batch_precision(self.batch, lib.PRECISION_FP64 if precision == "fp64" else lib.PRECISION_MIXED)
+        for _ in range(warmup):
+            self.step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        for k in range(steps):
+            flush.zero_()
+            starts[k].record(self.stream)
+            self.step()
+            ends[k].record(self.stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / steps
+        # per-stage device times of a few more steps (CUDA events inside the engine)
+        lib.set_batch_profiling(self.batch, True)
+        stages = {}
+        for _ in range(3):
+            flush.zero_()
+            self.step()
+            torch.cuda.synchronize()
+            for kk, vv in lib.get_batch_stage_times(self.batch).items():
+                stages[kk] = stages.get(kk, 0.0) + vv / 3
+        lib.set_batch_profiling(self.batch, False)
+        return {"ms_per_step": ms, "stage_ms": stages, "energy": self.e.double().sum().item()}
+
+
+def roofline(units, flops_per_unit, stage_ms, peak, kernel, bound):
+    t = stage_ms * 1e-3
+    achieved = units * flops_per_unit / t / 1e12 if t > 0 else None
+    return {"bound": bound, "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak if achieved else None}
+
+
+def cpu_reference_seconds(systems, par, repeats=3):
+    """Wall time of the FP64 CPU restatement for the given systems (all host threads)."""
     sys.path.insert(0, str(ROOT / "tests"))
     import oracle_ref
     times = []
     for _ in range(repeats):
         t0 = time.perf_counter()
-        oracle_ref.dispersion(d["numbers"], d["positions"], par, lattice=d["lattice"], periodic=d["periodic"])
+        for num, pos, lat, per in systems:
+            oracle_ref.dispersion(num, pos, par, lattice=lat, periodic=per)
         times.append(time.perf_counter() - t0)
     return statistics.median(times)
-
-
-def count_pair_terms(lib, batch, param, pos, tensors, torch):
-    lib.set_batch_counting(batch, True)
-    e, g, s = tensors
-    lib.get_dispersion_device(batch, param, pos.data_ptr(), None, e.data_ptr(), g.data_ptr(), s.data_ptr(), 0,
-                              torch.cuda.current_stream().cuda_stream)
-
-    torch.cuda.synchronize()
-    counts = lib.get_batch_counts(batch)
-    lib.set_batch_counting(batch, False)
-    return int(counts[0]), int(counts[2])
 
 
 def run_ours(args, rank, world, dist):
@@ -140,197 +242,203 @@ def run_ours(args, rank, world, dist):
 
     local = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(local)
-    d, par = workload(seed=rank)
-    nat = len(d["numbers"])
-    param = lib.new_rational_damping(par["s6"], par["s8"], par["s9"], par["a1"], par["a2"], par["alp"])
-    natoms = np.array([nat], dtype=np.int32)
-    batch = lib.new_batch(natoms, np.ascontiguousarray(d["numbers"], dtype=np.int32),
-                          np.ascontiguousarray(d["lattice"]), np.ascontiguousarray(d["periodic"]))
-    # wrapped positions resident on the device
-    pos_h = np.ascontiguousarray(d["positions"], dtype=float)
-    from dftd3.interface import Structure  # wrapping as the API does
-    mol = DispersionModel(d["numbers"], pos_h, d["lattice"], d["periodic"])
-    pos = torch.tensor(pos_h, dtype=torch.float64, device="cuda")
-    e = torch.zeros(1, dtype=torch.float64, device="cuda")
-    g = torch.zeros((nat, 3), dtype=torch.float64, device="cuda")
-    s = torch.zeros(9, dtype=torch.float64, device="cuda")
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-
-    pair_terms, cn_terms = count_pair_terms(lib, batch, param, pos, (e, g, s), torch)
-
-    def step():
-        lib.get_dispersion_device(batch, param, pos.data_ptr(), None, e.data_ptr(), g.data_ptr(), s.data_ptr(),
-                                  0, stream.cuda_stream)
-
-    results = {}
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    systems, par = make_workload(args.workload, seed=rank, natoms=args.natoms, nsys=args.nsys)
+    run = Runner(systems, par)
+    counts = run.counts()
+    precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     sampler = ClockSampler(local)
-    sampler.__enter__()
-    for prec_name, prec in (("fp64", lib.PRECISION_FP64), ("mixed", lib.PRECISION_MIXED)):
-        lib.set_batch_precision(batch, prec)
-        for _ in range(args.warmup):
-            step()
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        for k in range(args.steps):
-            flush.zero_()
-            starts[k].record(stream)
-            step()
-            ends[k].record(stream)
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
-        # dominant kernel time from the engine's stage events (one profiled step)
-        lib.set_batch_profiling(batch, True)
-        stage = {}
-        for _ in range(3):
-            flush.zero_()
-            step()
-            torch.cuda.synchronize()
-            st = lib.get_batch_stage_times(batch)
-            for kk, vv in st.items():
-                stage[kk] = stage.get(kk, 0.0) + vv / 3
-        lib.set_batch_profiling(batch, False)
-        results[prec_name] = dict(ms=ms, stages=stage, energy=float(e.item()))
-
-    sampler.__exit__(None, None, None)
+    sampler.start()
+    res = {p: run.time(p, args.steps, args.warmup, flush, dist) for p in precs}
+    extra = {}
+    if not args.no_extra and args.workload == "cell2000":
+        for name, steps in (("cluster5000", 3), ("batch4096", 3), ("frames256", 1)):
+            nsys = 16 if name == "frames256" else None
+            sy, pr = make_workload(name, seed=rank, nsys=nsys)
+            rx = Runner(sy, pr)
+            cx = rx.counts()
+            tx = {p: rx.time(p, steps, 1, flush, dist) for p in ("fp64", "mixed")}
+            units = cx["triple_terms"]
+            entry = {"systems": len(sy), "atoms": int(rx.natoms.sum()), **cx}
+            for p in tx:
+                entry[p] = {"ms_per_step": tx[p]["ms_per_step"], "stage_ms": tx[p]["stage_ms"],
+                            "triple_terms_per_s": units / (tx[p]["ms_per_step"] * 1e-3),
+                            "systems_per_s": len(sy) / (tx[p]["ms_per_step"] * 1e-3)}
+            entry["mixed_speedup_vs_fp64"] = tx["fp64"]["ms_per_step"] / tx["mixed"]["ms_per_step"]
+            entry["mixed_vs_fp64_rel_energy_error"] = (abs(tx["mixed"]["energy"] - tx["fp64"]["energy"])
+                                                       / abs(tx["fp64"]["energy"]))
+            if name == "frames256":
+                entry["note"] = "16 of the 256 frames per step"
+            extra[name] = entry
+            del rx
+    sampler.stop()
     clocks = sampler.summary()
-    # end to end through the C ABI with host buffers (dftd3_get_dispersion)
-    rp = RationalDampingParam(s6=par["s6"], s8=par["s8"], s9=par["s9"], a1=par["a1"], a2=par["a2"], alp=par["alp"])
-    mol.set_precision("mixed")
-    for _ in range(args.warmup):
-        r = mol.get_dispersion(rp, grad=True)
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        r = mol.get_dispersion(rp, grad=True)
-    e2e_s = time.perf_counter() - t0
-    e2e_energy = float(r["energy"])
 
-    # mixed-vs-FP64 error on this workload
-    rel_err = abs(results["mixed"]["energy"] - results["fp64"]["energy"]) / abs(results["fp64"]["energy"])
+    e2e_ms = None
+    if not args.no_e2e and len(systems) == 1:
+        num, pos, lat, per = systems[0]
+        mol = DispersionModel(np.asarray(num), np.asarray(pos, dtype=float), lat, per)
+        mol.set_precision("mixed" if "mixed" in precs else "fp64")
+        rp = RationalDampingParam(s6=par["s6"], s8=par["s8"], s9=par["s9"], a1=par["a1"], a2=par["a2"], alp=par["alp"])
+        for _ in range(args.warmup):
+            mol.get_dispersion(rp, grad=True)
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            mol.get_dispersion(rp, grad=True)
+        e2e_ms = 1e3 * (time.perf_counter() - t0) / args.steps
 
-    ms_mixed = results["mixed"]["ms"] / args.steps
-    ms_fp64 = results["fp64"]["ms"] / args.steps
-    e2e_ms = 1e3 * e2e_s / args.steps
+    head = "mixed" if "mixed" in res else "fp64"
+    ms = res[head]["ms_per_step"]
     if dist:
         import torch.distributed as tdist
-        t = torch.tensor([ms_mixed, ms_fp64, e2e_ms], dtype=torch.float64, device="cuda")
+        t = torch.tensor([res[p]["ms_per_step"] for p in precs] + [e2e_ms or 0.0], dtype=torch.float64,
+                         device="cuda")
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms_mixed, ms_fp64, e2e_ms = (float(x) for x in t.tolist())
+        vals = t.tolist()
+        for k, p in enumerate(precs):
+            res[p]["ms_per_step"] = vals[k]
+        e2e_ms = vals[-1] if e2e_ms else None
+        ms = res[head]["ms_per_step"]
     if rank != 0:
         return
-    total_terms = pair_terms * world
+
+    atm = par["s9"] != 0.0
+    unit_key = "triple_terms" if atm else "pair_terms"
+    unit = "triple-terms/s" if atm else "pair-terms/s"
+    units = counts[unit_key]
     peak64 = lib.fma_peak(lib.PRECISION_FP64)
     peak32 = lib.fma_peak(lib.PRECISION_MIXED)
-    t2b = results["mixed"]["stages"]["two_body"] * 1e-3
-    achieved = pair_terms * FLOPS_PER_PAIR / t2b / 1e12 if t2b > 0 else None
-    t2b64 = results["fp64"]["stages"]["two_body"] * 1e-3
-    achieved64 = pair_terms * FLOPS_PER_PAIR / t2b64 / 1e12 if t2b64 > 0 else None
+    stage = "three_body" if atm else "two_body"
+    flops = FLOPS_PER_TRIPLE if atm else FLOPS_PER_PAIR
+    kern = "k_triples" if atm else "k_two_body_tiled"
     line = {
-        "metric": METRIC,
-        "value": total_terms / (ms_mixed * 1e-3),
-        "unit": "pair-terms/s",
+        "metric": METRIC if args.workload == "cell2000" else f"{unit} ({args.workload})",
+        "value": world * units / (ms * 1e-3),
+        "unit": unit,
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": ms_mixed,
+        "ms_per_step": ms,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 (pair terms) + f64 (accumulation, weights, reductions)",
-        "data": "synthetic (seeded generator, dftd3/synthetic.py cell2000)",
-        "config": {"workload": "cell2000: periodic triclinic 2000 atoms, D3(BJ) two-body + CN chain rule, "
-                               "E+grad+virial, disp2 60 / CN 40 Bohr",
-                   "pair_terms_per_step": pair_terms, "cn_terms_per_step": cn_terms,
+        "dtype": "f32 pair/triple terms, f64 accumulation, weights and reductions" if head == "mixed" else "f64",
+        "data": f"synthetic (seeded generator dftd3/synthetic.py, {args.workload})",
+        "config": {"workload": {"cell2000": "cell2000: periodic triclinic 2000 atoms, D3(BJ) two-body + CN chain "
+                                            "rule, E+grad+virial, disp2 60 / CN 40 Bohr"}.get(args.workload, args.workload),
+                   "systems": len(systems), "atoms": int(run.natoms.sum()), **counts,
                    "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}"},
-        "fp64": {"value": total_terms / (ms_fp64 * 1e-3), "ms_per_step": ms_fp64,
-                 "stage_ms": results["fp64"]["stages"]},
-        "mixed_stage_ms": results["mixed"]["stages"],
-        "mixed_vs_fp64_rel_energy_error": rel_err,
-        "e2e": {"value": total_terms / (e2e_ms * 1e-3), "unit": "pair-terms/s", "ms_per_step": e2e_ms,
-                "h2d_bytes_per_step": 3 * 8 * pair_terms * 0 + 3 * 8 * len(d["numbers"]),
-                "d2h_bytes_per_step": 8 + 3 * 8 * len(d["numbers"]) + 9 * 8, "energy": e2e_energy},
-        "gpu_launches": 6 * args.steps * 2,
-        "roofline": {"bound": "fp32", "kernel": "k_two_body<float, rational>", "achieved": achieved,
-                     "peak": peak32, "unit": "TFLOP/s", "frac": (achieved / peak32) if achieved else None,
-                     "traffic": None,
-                     "peak_source": "measured in-run FMA throughput (MEASURED_PEAKS.json has no FP32/FP64 figure)",
-                     "fp64": {"achieved": achieved64, "peak": peak64,
-                              "frac": (achieved64 / peak64) if achieved64 else None}},
+        "precision_results": {p: {"value": world * units / (res[p]["ms_per_step"] * 1e-3), **res[p]} for p in precs},
+        "gpu_launches": None,
+        "roofline": None,
         "clocks": clocks,
     }
-    if world == 1:
-        cpu_s = cpu_reference_time(d, par, repeats=3)
-        line["cpu_baseline"] = {"value": pair_terms / cpu_s, "unit": "pair-terms/s",
-                                "cores": os.cpu_count(), "kind": "port",
-                                "sample": "one full cell2000 evaluation (E+grad+virial), median of 3, "
-                                          "FP64 C/OpenMP restatement of the reference"}
+    if "mixed" in res and "fp64" in res:
+        line["mixed_speedup_vs_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
+        line["mixed_vs_fp64_rel_energy_error"] = abs(res["mixed"]["energy"] - res["fp64"]["energy"]) / abs(
+            res["fp64"]["energy"])
+    # kernels launched per step: sort (key kernel + radix-sort passes), gather, tile
+    # bounds, CN, weights, two-body, chain rule, reduction; ATM adds C6 table,
+    # neighbour count, scan, fill and the triple kernel
+    per_step = 9 + 8 + (5 if atm else 0)
+    line["gpu_launches"] = per_step * args.steps * len(precs)
+    rl = roofline(units, flops, res[head]["stage_ms"][stage], peak32 if head == "mixed" else peak64,
+                  kern + ("<float>" if head == "mixed" else "<double>"), "fp32" if head == "mixed" else "fp64")
+    rl["traffic"] = TWO_BODY_TRAFFIC_BYTES if (args.workload == "cell2000" and head == "mixed") else None
+    if rl["traffic"] is not None:
+        rl["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch (profiles/)"
+    rl["peak_source"] = "measured in-run FMA throughput (MEASURED_PEAKS.json has no FP32/FP64 pipe figure)"
+    if "fp64" in res:
+        rl["fp64"] = roofline(units, flops, res["fp64"]["stage_ms"][stage], peak64, kern + "<double>", "fp64")
+    line["roofline"] = rl
+    if e2e_ms:
+        line["e2e"] = {"value": world * units / (e2e_ms * 1e-3), "unit": unit, "ms_per_step": e2e_ms,
+                       "h2d_bytes_per_step": 24 * int(run.natoms.sum()),
+                       "d2h_bytes_per_step": 8 + 24 * int(run.natoms.sum()) + 72}
+    if extra:
+        line["extra_workloads"] = extra
+        for name, entry in extra.items():
+            entry["roofline_mixed"] = roofline(entry["triple_terms"], FLOPS_PER_TRIPLE,
+                                               entry["mixed"]["stage_ms"]["three_body"], peak32, "k_triples<float>",
+                                               "fp32")
+    if world == 1 and not args.no_cpu:
+        sample = systems if len(systems) == 1 else systems[:64]
+        cpu_s = cpu_reference_seconds(sample, par, repeats=3)
+        sample_units = units if len(sample) == len(systems) else None
+        line["cpu_baseline"] = {
+            "value": (sample_units / cpu_s) if sample_units else len(sample) / cpu_s,
+            "unit": unit if sample_units else "systems/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{len(sample)} system(s) of {args.workload} (E+grad+virial), median of 3 runs, "
+                      "FP64 C/OpenMP restatement of the reference"}
     print(json.dumps(line), flush=True)
+
+
+def count_pairs_cpu(systems, cutoff=60.0):
+    """Accepted (i, j <= i, T) two-body terms (numpy, for the reference arm)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_ref
+    total = 0
+    for num, pos, lat, per in systems:
+        trans = oracle_ref.lattice_points(lat, per, cutoff) if lat is not None else np.zeros((1, 3))
+        pos = np.asarray(pos)
+        for i in range(len(pos)):
+            v = pos[i][None, None, :] - (pos[: i + 1][:, None, :] + trans[None, :, :])
+            r2 = np.einsum("ijk,ijk->ij", v, v)
+            total += int(np.count_nonzero((r2 <= cutoff * cutoff) & (r2 >= np.finfo(float).eps)))
+    return total
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    d, par = workload(seed=0)
+    systems, par = make_workload(args.workload, seed=0, natoms=args.natoms, nsys=args.nsys)
     sys.path.insert(0, str(ROOT / "tests"))
     import oracle_ref
-    # pair-term count of the workload from a cheap energy-free pass is not
-    # available on the CPU; use the GPU-independent analytic count instead
-    times = []
+    sample = systems if len(systems) == 1 else systems[:64]
+
+    def one():
+        for num, pos, lat, per in sample:
+            oracle_ref.dispersion(num, pos, par, lattice=lat, periodic=per)
+
     for _ in range(args.warmup):
-        oracle_ref.dispersion(d["numbers"], d["positions"], par, lattice=d["lattice"], periodic=d["periodic"])
+        one()
+    times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        oracle_ref.dispersion(d["numbers"], d["positions"], par, lattice=d["lattice"], periodic=d["periodic"])
+        one()
         times.append(time.perf_counter() - t0)
-    terms = count_pairs_cpu(d)
     ms = 1e3 * sum(times) / len(times)
-    value = terms / (ms * 1e-3)
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pair-terms/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "cell2000", "pair_terms_per_step": terms},
-            "cpu_baseline": {"value": value, "unit": "pair-terms/s", "cores": os.cpu_count(), "kind": "port",
-                             "sample": "one full cell2000 evaluation per step (FP64 C/OpenMP restatement; "
-                                       "the Fortran reference cannot be built here)"},
-            "e2e": {"value": value, "unit": "pair-terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if par["s9"] == 0.0 and len(sample) == len(systems):
+        units = count_pairs_cpu(sample)
+        unit = "pair-terms/s"
+        value = units / (ms * 1e-3)
+    else:
+        unit = "systems/s"
+        value = len(sample) / (ms * 1e-3)
+    line = {"impl": "reference", "metric": METRIC if args.workload == "cell2000" else f"{unit} ({args.workload})",
+            "value": value, "unit": unit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": f"synthetic (seeded generator dftd3/synthetic.py, {args.workload})",
+            "config": {"workload": args.workload, "systems_per_step": len(sample)},
+            "cpu_baseline": {"value": value, "unit": unit, "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"{len(sample)} system(s) of {args.workload} per step (FP64 C/OpenMP "
+                                       "restatement; the Fortran reference cannot be built here)"},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
-
-def count_pairs_cpu(d):
-    """Accepted (i, j <= i, T) pair-terms of the two-body loop (numpy)."""
-    from dftd3.synthetic import triclinic  # noqa: F401
-    sys.path.insert(0, str(ROOT / "tests"))
-    import oracle_ref
-    trans = oracle_ref.lattice_points(d["lattice"], d["periodic"], 60.0)
-    pos = np.asarray(d["positions"])
-    n = len(pos)
-    total = 0
-    c2 = 60.0 * 60.0
-    for i in range(n):
-        v = pos[i][None, None, :] - (pos[: i + 1][:, None, :] + trans[None, :, :])
-        r2 = np.einsum("ijk,ijk->ij", v, v)
-        total += int(np.count_nonzero((r2 <= c2) & (r2 >= np.finfo(float).eps)))
-    return total
 
 
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    dist = None
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
+    dist = None
     if world > 1:
         import datetime
         import torch

@@ -36,7 +36,7 @@ namespace {
 constexpr int kTA = 32;          // j-entries per tile
 constexpr int kTB = 64;          // k-entries per tile
 constexpr int kThreadsAtm = 256; // 16 x 16
-constexpr int kAcc = 6;          // per-entry accumulators: S, D, Gx, Gy, Gz, Q
+constexpr int kAcc = 5;          // per-entry accumulators: S, Gx, Gy, Gz, dE/dCN of the partner
 constexpr double kRs9 = 4.0 / 3.0;
 
 // ------------------------------------------------------------ C6 matrix ----
@@ -168,7 +168,12 @@ __global__ void k_nbr_fill(Batch b, Config c, const long long* off, int* nbr_j, 
 // ------------------------------------------------------------ triple sum ----
 
 template <class R>
-__device__ __forceinline__ R rsqrt_r(R x) { if constexpr (sizeof(R) == 8) return sqrt(x); else return sqrtf(x); }
+__device__ __forceinline__ R rsqrt_r(R x) { if constexpr (sizeof(R) == 8) return rsqrt(x); else return rsqrtf(x); }
+
+// Reciprocal of the triple arithmetic: IEEE in the FP64 form, the hardware
+// approximation (a few ulp) in the FP32 part of the mixed form.
+template <class R>
+__device__ __forceinline__ R rcp_r(R x) { if constexpr (sizeof(R) == 8) return R(1) / x; else return __fdividef(1.0f, x); }
 
 // log and exp in the precision of the form (natural base for FP64, base 2
 // with the hardware units for FP32; only their composition matters).
@@ -192,16 +197,18 @@ __device__ __forceinline__ void smooth(R r, R cutoff, R width, R& sw, R& dsw)
     }
 }
 
-// One neighbour entry staged in shared memory.
+template <class R> struct Vec4;
+template <> struct Vec4<double> { using type = double4; };
+template <> struct Vec4<float> { using type = float4; };
+
+// One neighbour entry of the current root, precomputed once per root.
 template <class R>
 struct Slot {
-    R vx, vy, vz, r2;        // head of x_j + T - x_i and r^2
-    float lx, ly, lz;        // tail of the vector (mixed form)
-    R lr2;                   // log r^2 (base of rlog)
-    R sc6, qij, qji;         // sqrt(C6_ij), dC6_ij/dCN_i / C6, dC6_ij/dCN_j / C6
-    R lr0;                   // log(rs9 * rvdw_ij)
-    R sw, dswr;              // switch and dsw/dr / r
-    int atom, gend, sp, orig;
+    typename Vec4<R>::type v;   // head of x_j + T - x_i, r^2
+    typename Vec4<R>::type l;   // tail of the vector (mixed form), 1/r^2
+    typename Vec4<R>::type c;   // sqrt(C6_ij), dC6_ij/dCN_i / C6, dC6_ij/dCN_j / C6, alp3 log(r0_ij / r_ij)
+    typename Vec4<R>::type s;   // 1/r, switch, dsw/dr / r, -
+    int4 meta;                  // atom, group end, species, input index
 };
 
 __device__ __forceinline__ bool owns_pair_atm(const Partition& p, int i, int j)
@@ -210,68 +217,49 @@ __device__ __forceinline__ bool owns_pair_atm(const Partition& p, int i, int j)
     return (hi * (hi + 1) / 2 + lo) % p.nparts == p.part;
 }
 
+// P(x; y, z) = x^3 + x^2 (y + z) + x (3 y^2 + 2 y z + 3 z^2) - 5 (y - z)^2 (y + z),
+// the numerator of the angular derivative along x (atm.f90:751-776), with
+// s1 = x + y + z.
 template <class R>
-__device__ __forceinline__ void load_slot(Slot<R>& s, int root, int k, long long base, const Batch& b,
-                                          const Species& sp, const Config& c, const int* nbr_j,
-                                          const int* nbr_gend, const double4* nbr_v, const C6Entry<R>* mat,
-                                          long long mrow, int nsys_n, int a0)
+__device__ __forceinline__ R ang_deriv(R x, R y, R z, R s1)
 {
-    const int j = nbr_j[base + k];
-    const double4 v = nbr_v[base + k];
-    s.atom = j;
-    s.gend = nbr_gend[base + k];
-    s.sp = b.sp[j];
-    s.orig = b.local[j];
-    if constexpr (sizeof(R) == 8) {
-        s.vx = v.x; s.vy = v.y; s.vz = v.z;
-        s.lx = s.ly = s.lz = 0.f;
-    } else {
-        s.vx = __double2float_rn(v.x); s.vy = __double2float_rn(v.y); s.vz = __double2float_rn(v.z);
-        s.lx = __double2float_rn(v.x - (double)s.vx);
-        s.ly = __double2float_rn(v.y - (double)s.vy);
-        s.lz = __double2float_rn(v.z - (double)s.vz);
-    }
-    s.r2 = R(v.w);
-    s.lr2 = rlog<R>(R(v.w));
-    const C6Entry<R> e = mat[mrow + (j - a0)];
-    s.sc6 = e.sc6; s.qij = e.qrc; s.qji = e.qcr;
-    const double r0 = __ldg(sp.atm_r0 + b.sp[root] * b.nid + s.sp);
-    s.lr0 = rlog<R>(R(r0));
-    if (c.width3 > 0.0 && c.width3 < c.cut3) {
-        R sw, dsw;
-        const R r = rsqrt_r<R>(R(v.w));
-        smooth<R>(r, R(c.cut3), R(c.width3), sw, dsw);
-        s.sw = sw; s.dswr = dsw / r;
-    } else {
-        s.sw = R(1); s.dswr = R(0);
-    }
-    (void)nsys_n;
+    const R u = y + z, d = y - z;
+    const R w = d * d;
+    return x * (x * s1 + w + R(2) * u * u) - R(5) * u * w;
 }
 
 template <class R, bool GRAD>
-__global__ void __launch_bounds__(kThreadsAtm) k_triples(Batch b, Species sp, Damp d, Config c, Partition part,
+__global__ void __launch_bounds__(kThreadsAtm, sizeof(R) == 4 ? 3 : 1) k_triples(Batch b, Species sp, Damp d, Config c, Partition part,
                                                          Work w, const C6Entry<R>* mat, const long long* mat_off,
                                                          const long long* off, const int* cnt, const int* nbr_j,
                                                          const int* nbr_gend, const double4* nbr_v,
-                                                         unsigned int* queue, double* slot_acc, int slot_stride,
-                                                         double* e3, double* sig3)
+                                                         unsigned int* queue, double* slot_acc, Slot<R>* slot_scr,
+                                                         int slot_stride, double* e3, double* sig3)
 {
-    __shared__ Slot<R> sa[kTA];
-    __shared__ Slot<R> sb[kTB];
-    __shared__ R kred[16][kTB / 2][kAcc];
+    // dynamic shared memory: entry tiles, C6 of the tile's (j, k) pairs, k-role reduction
+    extern __shared__ __align__(16) unsigned char smem[];
+    Slot<R>* sa = reinterpret_cast<Slot<R>*>(smem);
+    Slot<R>* sb = sa + kTA;
+    auto sjk = reinterpret_cast<C6Entry<R>(*)[kTB]>(sb + kTB);
+    auto kred = reinterpret_cast<R(*)[kTB / 2][kAcc]>(sjk + kTA);
     __shared__ int s_root;
+    __shared__ R slr0[kMaxSpeciesFast * kMaxSpeciesFast];
+    __shared__ double wsum[kThreadsAtm / 32][13];
     const int tid = threadIdx.x;
     const int tx = tid & 15, ty = tid >> 4;
     const int lane = tid & 31;
     double* acc = slot_acc + (size_t)blockIdx.x * slot_stride * kAcc;
+    Slot<R>* scr = slot_scr + (size_t)blockIdx.x * slot_stride;
     const R s9 = R(d.s9);
     const R alp = R(d.alp + 2.0);        // ATM exponent alp + 2 (rational.f90:563)
     const R alp3 = alp / R(3);
     const R cut2 = R(c.cut3 * c.cut3);
     const bool smooth_on = c.width3 > 0.0 && c.width3 < c.cut3;
     const R cutoff = R(c.cut3), width = R(c.width3);
-    // log-base conversion: rlog/rexp use base e (FP64) or base 2 (FP32)
-    const R half = R(0.5);
+    const bool table_r0 = b.nid <= kMaxSpeciesFast;
+    if (table_r0)
+        for (int k = tid; k < b.nid * b.nid; k += kThreadsAtm) slr0[k] = rlog<R>(R(__ldg(sp.atm_r0 + k)));
+    __syncthreads();
 
     for (;;) {
         if (tid == 0) {
@@ -287,22 +275,58 @@ __global__ void __launch_bounds__(kThreadsAtm) k_triples(Batch b, Species sp, Da
         const int sys = b.sys_of_atom[i];
         const int a0 = b.atom_off[sys];
         const int nsys_n = b.atom_off[sys + 1] - a0;
-        const long long mrow_i = mat_off[sys] + (long long)(i - a0) * nsys_n;
+        const long long mbase = mat_off[sys];
+        const long long mrow_i = mbase + (long long)(i - a0) * nsys_n;
         const int orig_i = b.local[i];
-        double e_root = 0.0;
+        const int si = b.sp[i];
+        double e_root = 0.0, dei = 0.0;
         double sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+        int ntrip = 0;
         if (m > 0) {
-            if (GRAD)
-                for (int k = tid; k < m * kAcc; k += kThreadsAtm) acc[k] = 0.0;
+            // entry records of this root (all threads)
+            for (int k = tid; k < m; k += kThreadsAtm) {
+                const int j = nbr_j[base + k];
+                const double4 v = nbr_v[base + k];
+                Slot<R> r;
+                const int sj = b.sp[j];
+                const C6Entry<R> e = mat[mrow_i + (j - a0)];
+                const double r0 = __ldg(sp.atm_r0 + si * b.nid + sj);
+                if constexpr (sizeof(R) == 8) {
+                    r.v = make_double4(v.x, v.y, v.z, v.w);
+                    r.l = make_double4(0.0, 0.0, 0.0, 1.0 / v.w);
+                    const double rs = rsqrt(v.w);
+                    r.c = make_double4(e.sc6, e.qrc, e.qcr, alp3 * (log(r0) - 0.5 * log(v.w)));
+                    r.s = make_double4(rs, 1.0, 0.0, 0.0);
+                } else {
+                    const float hx = __double2float_rn(v.x), hy = __double2float_rn(v.y), hz = __double2float_rn(v.z);
+                    r.v = make_float4(hx, hy, hz, __double2float_rn(v.w));
+                    r.l = make_float4(__double2float_rn(v.x - (double)hx), __double2float_rn(v.y - (double)hy),
+                                      __double2float_rn(v.z - (double)hz), __double2float_rn(1.0 / v.w));
+                    r.c = make_float4(e.sc6, e.qrc, e.qcr,
+                                      __double2float_rn(double(alp3) * (log2(r0) - 0.5 * log2(v.w))));
+                    r.s = make_float4(__double2float_rn(rsqrt(v.w)), 1.f, 0.f, 0.f);
+                }
+                if (smooth_on) {
+                    R sw, dsw;
+                    const R rr = R(sqrt(v.w));
+                    smooth<R>(rr, cutoff, width, sw, dsw);
+                    r.s.y = sw;
+                    r.s.z = dsw / rr;
+                }
+                r.meta = make_int4(j, nbr_gend[base + k], sj, b.local[j]);
+                scr[k] = r;
+                if (GRAD)
+                    for (int v2 = 0; v2 < kAcc; v2++) acc[k * kAcc + v2] = 0.0;
+            }
+            __syncthreads();
             for (int B0 = 0; B0 < m; B0 += kTB) {
                 __syncthreads();
                 for (int k = tid; k < kTB; k += kThreadsAtm)
-                    if (B0 + k < m)
-                        load_slot<R>(sb[k], i, B0 + k, base, b, sp, c, nbr_j, nbr_gend, nbr_v, mat, mrow_i, nsys_n, a0);
+                    if (B0 + k < m) sb[k] = scr[B0 + k];
                 __syncthreads();
-                // first j-entry whose group reaches this k-tile
+                // first j-entry whose atom group reaches this k-tile
                 int astart = B0;
-                while (astart > 0 && nbr_j[base + astart - 1] == nbr_j[base + B0]) astart--;
+                while (astart > 0 && sb[0].meta.x == scr[astart - 1].meta.x) astart--;
                 R kacc[4][kAcc];
 #pragma unroll
                 for (int q = 0; q < 4; q++)
@@ -311,14 +335,21 @@ __global__ void __launch_bounds__(kThreadsAtm) k_triples(Batch b, Species sp, Da
                 for (int A0 = (astart / kTA) * kTA; A0 < m; A0 += kTA) {
                     __syncthreads();
                     for (int k = tid; k < kTA; k += kThreadsAtm)
-                        if (A0 + k < m)
-                            load_slot<R>(sa[k], i, A0 + k, base, b, sp, c, nbr_j, nbr_gend, nbr_v, mat, mrow_i, nsys_n, a0);
+                        if (A0 + k < m) sa[k] = scr[A0 + k];
+                    __syncthreads();
+                    // C6 table of the tile's (j, k) atom pairs
+                    for (int k = tid; k < kTA * kTB; k += kThreadsAtm) {
+                        const int ia = k / kTB, ib = k % kTB;
+                        if (A0 + ia < m && B0 + ib < m && B0 + ib < sa[ia].meta.y)
+                            sjk[ia][ib] = mat[mbase + (long long)(sa[ia].meta.x - a0) * nsys_n + (sb[ib].meta.x - a0)];
+                    }
                     __syncthreads();
                     R jacc[2][kAcc];
 #pragma unroll
                     for (int p = 0; p < 2; p++)
 #pragma unroll
                         for (int v = 0; v < kAcc; v++) jacc[p][v] = R(0);
+                    R te = R(0), tde = R(0), txx = R(0), tyy = R(0), tzz = R(0), txy = R(0), txz = R(0), tyz = R(0);
 #pragma unroll
                     for (int p = 0; p < 2; p++) {
                         const int ia = ty + 16 * p;
@@ -328,100 +359,91 @@ __global__ void __launch_bounds__(kThreadsAtm) k_triples(Batch b, Species sp, Da
                         for (int q = 0; q < 4; q++) {
                             const int ib = tx + 16 * q;
                             const int kb = B0 + ib;
-                            if (kb >= m || kb >= A.gend) continue;
+                            if (kb >= m || kb >= A.meta.y) continue;
                             const Slot<R>& Bs = sb[ib];
                             // j-k vector: (x_k + T_k - x_i) - (x_j + T_j - x_i)
                             R vx, vy, vz;
                             if constexpr (sizeof(R) == 8) {
-                                vx = Bs.vx - A.vx; vy = Bs.vy - A.vy; vz = Bs.vz - A.vz;
+                                vx = Bs.v.x - A.v.x; vy = Bs.v.y - A.v.y; vz = Bs.v.z - A.v.z;
                             } else {
-                                vx = (Bs.vx - A.vx) + (Bs.lx - A.lx);
-                                vy = (Bs.vy - A.vy) + (Bs.ly - A.ly);
-                                vz = (Bs.vz - A.vz) + (Bs.lz - A.lz);
+                                vx = (Bs.v.x - A.v.x) + (Bs.l.x - A.l.x);
+                                vy = (Bs.v.y - A.v.y) + (Bs.l.y - A.l.y);
+                                vz = (Bs.v.z - A.v.z) + (Bs.l.z - A.l.z);
                             }
-                            const R r2jk = vx * vx + vy * vy + vz * vz;
-                            if (r2jk > cut2 || r2jk < R(DBL_EPSILON)) continue;
-                            // C6 of the j-k pair
-                            const int ja = A.atom, kb_atom = Bs.atom;
-                            const C6Entry<R> ejk = mat[mat_off[sys] + (long long)(ja - a0) * nsys_n + (kb_atom - a0)];
-                            if (GRAD && (A.sc6 == R(0) || Bs.sc6 == R(0) || ejk.sc6 == R(0))) continue;
+                            const R rc = vx * vx + vy * vy + vz * vz;   // r_jk^2
+                            if (rc > cut2 || rc < R(DBL_EPSILON)) continue;
+                            const C6Entry<R> ejk = sjk[ia][ib];
+                            if (GRAD && (A.c.x == R(0) || Bs.c.x == R(0) || ejk.sc6 == R(0))) continue;
                             if (part.nparts > 1) {
-                                // owner of the triple: the pair of its two largest original indices
-                                int o1 = orig_i, o2 = A.orig, o3 = Bs.orig, t;
+                                // owner of the triple: the pair of its two largest input indices
+                                int o1 = orig_i, o2 = A.meta.w, o3 = Bs.meta.w, t;
                                 if (o2 > o1) { t = o1; o1 = o2; o2 = t; }
                                 if (o3 > o2) { t = o2; o2 = o3; o3 = t; }
                                 if (o2 > o1) { t = o1; o1 = o2; o2 = t; }
                                 if (!owns_pair_atm(part, o1, o2)) continue;
                             }
-                            const R c9 = -s9 * A.sc6 * Bs.sc6 * ejk.sc6;
-                            const R lr0jk = rlog<R>(R(__ldg(sp.atm_r0 + A.sp * b.nid + Bs.sp)));
-                            const R r2ij = A.r2, r2ik = Bs.r2;
-                            const R lr2jk = rlog<R>(r2jk);
-                            // (r0/r1)^alp3 with r0 = r0ij r0ik r0jk, r1 = sqrt(r2ij r2ik r2jk)
-                            const R r0r1 = rexp<R>(alp3 * ((A.lr0 + Bs.lr0 + lr0jk) - half * (A.lr2 + Bs.lr2 + lr2jk)));
-                            const R r2 = r2ij * r2ik * r2jk;
-                            const R r1 = rsqrt_r<R>(r2);
-                            const R r3 = r2 * r1;
-                            const R ir5 = R(1) / (r3 * r2);
-                            const R fdmp = R(1) / (R(1) + R(6) * r0r1);
-                            const R ang = R(0.375) * (r2ij + r2jk - r2ik) * (r2ij - r2jk + r2ik)
-                                        * (-r2ij + r2jk + r2ik) * ir5 + r2 * ir5;
-                            const R rr = ang * fdmp;
-                            const int jat = A.atom, kat = Bs.atom;
+                            const R ra = A.v.w, rb = Bs.v.w;            // r_ij^2, r_ik^2
+                            const R rsc = rsqrt_r<R>(rc);
+                            const R irc = rsc * rsc;
+                            const R ir1 = A.s.x * Bs.s.x * rsc;         // 1 / (r_ij r_ik r_jk)
+                            const R ir2 = ir1 * ir1;
+                            const R ir3 = ir2 * ir1;
+                            const R ir5 = ir3 * ir2;
+                            const R lr0jk = table_r0 ? slr0[A.meta.z * b.nid + Bs.meta.z]
+                                                     : rlog<R>(R(__ldg(sp.atm_r0 + A.meta.z * b.nid + Bs.meta.z)));
+                            // (r0/r1)^alp3, r0 = r0ij r0ik r0jk, r1 = r_ij r_ik r_jk
+                            const R t = rexp<R>(A.c.w + Bs.c.w + alp3 * (lr0jk - R(0.5) * rlog<R>(rc)));
+                            const R fdmp = rcp_r<R>(R(1) + R(6) * t);
+                            const R s1 = ra + rb + rc;
+                            const R ang = R(0.375) * (s1 - R(2) * rb) * (s1 - R(2) * rc) * (s1 - R(2) * ra) * ir5 + ir3;
+                            const R c9 = -s9 * A.c.x * Bs.c.x * ejk.sc6;
+                            const int jat = A.meta.x, kat = Bs.meta.x;
                             R triple;
                             if (i == jat) triple = (i == kat) ? R(1.0 / 6.0) : R(0.5);
                             else triple = (i != kat && jat != kat) ? R(1) : R(0.5);
-                            R sw = R(1);
-                            R swjk = R(1), dswjkr = R(0);
+                            R sw = R(1), swjk = R(1), dswjkr = R(0);
                             if (smooth_on) {
                                 R dsw;
-                                const R rjk = rsqrt_r<R>(r2jk);
+                                const R rjk = rc * rsc;
                                 smooth<R>(rjk, cutoff, width, swjk, dsw);
-                                dswjkr = dsw / rjk;
-                                sw = A.sw * Bs.sw * swjk;
+                                dswjkr = dsw * rsc;
+                                sw = A.s.y * Bs.s.y * swjk;
                             }
-                            const R dE0 = rr * c9;
+                            const R dE0 = ang * fdmp * c9;
                             const R dE = dE0 * triple * sw;
-                            e_root -= double(dE);
+                            te -= dE;
+                            ntrip++;
                             if (!GRAD) continue;
-                            const R dfdmp = R(-2) * alp * r0r1 * (fdmp * fdmp);
-                            const R base_ = c9 * ang * dfdmp;
-                            // d/d r_ij, d/d r_ik, d/d r_jk of the angular term (atm.f90:751-776)
-                            const R dang_ij = R(-0.375) * (r2ij * r2ij * r2ij + r2ij * r2ij * (r2jk + r2ik)
-                                + r2ij * (R(3) * r2jk * r2jk + R(2) * r2jk * r2ik + R(3) * r2ik * r2ik)
-                                - R(5) * (r2jk - r2ik) * (r2jk - r2ik) * (r2jk + r2ik)) * ir5;
-                            const R dang_ik = R(-0.375) * (r2ik * r2ik * r2ik + r2ik * r2ik * (r2jk + r2ij)
-                                + r2ik * (R(3) * r2jk * r2jk + R(2) * r2jk * r2ij + R(3) * r2ij * r2ij)
-                                - R(5) * (r2jk - r2ij) * (r2jk - r2ij) * (r2jk + r2ij)) * ir5;
-                            const R dang_jk = R(-0.375) * (r2jk * r2jk * r2jk + r2jk * r2jk * (r2ik + r2ij)
-                                + r2jk * (R(3) * r2ik * r2ik + R(2) * r2ik * r2ij + R(3) * r2ij * r2ij)
-                                - R(5) * (r2ik - r2ij) * (r2ik - r2ij) * (r2ik + r2ij)) * ir5;
-                            R sij = sw * (base_ - c9 * dang_ij * fdmp) / r2ij;
-                            R sik = sw * (base_ - c9 * dang_ik * fdmp) / r2ik;
-                            R sjk = sw * (base_ - c9 * dang_jk * fdmp) / r2jk;
+                            // ds/dr2 pieces: common damping part and the angular parts
+                            const R common = c9 * ang * (R(-2) * alp * t * (fdmp * fdmp));
+                            const R kfac = R(0.375) * c9 * fdmp * ir5;
+                            R sij = sw * (common + kfac * ang_deriv<R>(ra, rc, rb, s1)) * A.l.w;
+                            R sik = sw * (common + kfac * ang_deriv<R>(rb, rc, ra, s1)) * Bs.l.w;
+                            R sjk = sw * (common + kfac * ang_deriv<R>(rc, rb, ra, s1)) * irc;
                             if (smooth_on) {
-                                sij -= dE0 * A.dswr * Bs.sw * swjk;
-                                sik -= dE0 * Bs.dswr * A.sw * swjk;
-                                sjk -= dE0 * dswjkr * A.sw * Bs.sw;
+                                sij -= dE0 * A.s.z * Bs.s.y * swjk;
+                                sik -= dE0 * Bs.s.z * A.s.y * swjk;
+                                sjk -= dE0 * dswjkr * A.s.y * Bs.s.y;
                             }
                             const R tij = triple * sij, tik = triple * sik, tjk = triple * sjk;
                             const R gx = tjk * vx, gy = tjk * vy, gz = tjk * vz;
-                            // j-role entry
+                            // dE/dCN: root share here, partner shares through the entries
+                            tde -= R(0.5) * dE * (A.c.y + Bs.c.y);
                             jacc[p][0] += tij;
-                            jacc[p][1] += dE;
-                            jacc[p][2] -= gx; jacc[p][3] -= gy; jacc[p][4] -= gz;
-                            jacc[p][5] += dE * ejk.qrc;
-                            // k-role entry
+                            jacc[p][1] -= gx; jacc[p][2] -= gy; jacc[p][3] -= gz;
+                            jacc[p][4] -= R(0.5) * dE * (A.c.z + ejk.qrc);
                             kacc[q][0] += tik;
-                            kacc[q][1] += dE;
-                            kacc[q][2] += gx; kacc[q][3] += gy; kacc[q][4] += gz;
-                            kacc[q][5] += dE * ejk.qcr;
-                            // jk part of the virial
-                            sxx += double(gx * vx); syy += double(gy * vy); szz += double(gz * vz);
-                            sxy += double(gx * vy); sxz += double(gx * vz); syz += double(gy * vz);
+                            kacc[q][1] += gx; kacc[q][2] += gy; kacc[q][3] += gz;
+                            kacc[q][4] -= R(0.5) * dE * (Bs.c.z + ejk.qcr);
+                            txx += gx * vx; tyy += gy * vy; tzz += gz * vz;
+                            txy += gx * vy; txz += gx * vz; tyz += gy * vz;
                         }
                     }
+                    e_root += double(te);
                     if (GRAD) {
+                        dei += double(tde);
+                        sxx += double(txx); syy += double(tyy); szz += double(tzz);
+                        sxy += double(txy); sxz += double(txz); syz += double(tyz);
                         // reduce the j-role sums over the 16 k-columns (half warp)
 #pragma unroll
                         for (int p = 0; p < 2; p++)
@@ -444,8 +466,7 @@ __global__ void __launch_bounds__(kThreadsAtm) k_triples(Batch b, Species sp, Da
                     }
                 }
                 if (GRAD) {
-                    // reduce the k-role sums over the 16 j-rows of the block,
-                    // half a k-tile at a time
+                    // reduce the k-role sums over the 16 j-rows, half a k-tile at a time
 #pragma unroll
                     for (int h = 0; h < 2; h++) {
                         __syncthreads();
@@ -467,40 +488,38 @@ __global__ void __launch_bounds__(kThreadsAtm) k_triples(Batch b, Species sp, Da
             }
             __syncthreads();
         }
-        // per-entry scatter (fixed order per entry; atomics into partner atoms)
-        double gix = 0, giy = 0, giz = 0, dei = 0;
+        // per-entry scatter: root share in registers, partner shares by FP64 atomics
+        double gix = 0, giy = 0, giz = 0;
         if (GRAD && m > 0) {
             for (int k = tid; k < m; k += kThreadsAtm) {
-                const double S = acc[k * kAcc + 0], D = acc[k * kAcc + 1];
-                const double Gx = acc[k * kAcc + 2], Gy = acc[k * kAcc + 3], Gz = acc[k * kAcc + 4];
-                const double Q = acc[k * kAcc + 5];
-                if (S == 0.0 && D == 0.0 && Gx == 0.0 && Gy == 0.0 && Gz == 0.0 && Q == 0.0) continue;
+                const double S = acc[k * kAcc + 0];
+                const double Gx = acc[k * kAcc + 1], Gy = acc[k * kAcc + 2], Gz = acc[k * kAcc + 3];
+                const double Dx = acc[k * kAcc + 4];
+                if (S == 0.0 && Gx == 0.0 && Gy == 0.0 && Gz == 0.0 && Dx == 0.0) continue;
                 const double4 v = nbr_v[base + k];
                 const int x = nbr_j[base + k];
-                const C6Entry<R> e = mat[mrow_i + (x - a0)];
                 gix -= S * v.x; giy -= S * v.y; giz -= S * v.z;
                 atomicAdd(w.grad + 3 * x + 0, S * v.x + Gx);
                 atomicAdd(w.grad + 3 * x + 1, S * v.y + Gy);
                 atomicAdd(w.grad + 3 * x + 2, S * v.z + Gz);
                 sxx += S * v.x * v.x; syy += S * v.y * v.y; szz += S * v.z * v.z;
                 sxy += S * v.x * v.y; sxz += S * v.x * v.z; syz += S * v.y * v.z;
-                dei -= 0.5 * D * double(e.qrc);
-                atomicAdd(w.dEdcn + x, -0.5 * (D * double(e.qcr) + Q));
+                atomicAdd(w.dEdcn + x, Dx);
             }
         }
         // block reduction of the root's sums in a fixed order
-        double r[11] = {e_root, gix, giy, giz, dei, sxx, syy, szz, sxy, sxz, syz};
-        for (int v = 0; v < 11; v++)
+        double r[12] = {e_root, gix, giy, giz, dei, sxx, syy, szz, sxy, sxz, syz, double(ntrip)};
+        for (int v = 0; v < 12; v++)
             for (int o = 16; o > 0; o >>= 1) r[v] += __shfl_xor_sync(0xffffffffu, r[v], o);
-        __shared__ double wsum[8][11];
         if (lane == 0)
-            for (int v = 0; v < 11; v++) wsum[tid >> 5][v] = r[v];
+            for (int v = 0; v < 12; v++) wsum[tid >> 5][v] = r[v];
         __syncthreads();
         if (tid == 0) {
-            double t[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+            double t[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
             for (int wq = 0; wq < kThreadsAtm / 32; wq++)
-                for (int v = 0; v < 11; v++) t[v] += wsum[wq][v];
+                for (int v = 0; v < 12; v++) t[v] += wsum[wq][v];
             e3[i] = t[0];
+            if (w.counts) atomicAdd(w.counts + 1, (unsigned long long)t[11]);
             if (GRAD) {
                 atomicAdd(w.grad + 3 * i + 0, t[1]);
                 atomicAdd(w.grad + 3 * i + 1, t[2]);
@@ -552,41 +571,59 @@ void launch_nbr_fill(const Batch& b, const Config& c, const long long* off, int*
     k_nbr_fill<<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, c, off, nbr_j, nbr_gend, nbr_v);
 }
 
-int atm_blocks_per_sm(bool mixed, bool grad)
+template <class R>
+size_t triple_smem()
 {
-    int n = 0;
-    if (mixed) {
-        if (grad) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_triples<float, true>, kThreadsAtm, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_triples<float, false>, kThreadsAtm, 0);
-    } else {
-        if (grad) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_triples<double, true>, kThreadsAtm, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_triples<double, false>, kThreadsAtm, 0);
+    return sizeof(Slot<R>) * (kTA + kTB) + sizeof(C6Entry<R>) * kTA * kTB + sizeof(R) * 16 * (kTB / 2) * kAcc;
+}
+
+template <class R, bool GRAD>
+int triple_occupancy()
+{
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_triples<R, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)triple_smem<R>());
+        configured = true;
     }
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_triples<R, GRAD>, kThreadsAtm, triple_smem<R>());
     return n > 0 ? n : 1;
 }
+
+int atm_blocks_per_sm(bool mixed, bool grad)
+{
+    if (mixed) return grad ? triple_occupancy<float, true>() : triple_occupancy<float, false>();
+    return grad ? triple_occupancy<double, true>() : triple_occupancy<double, false>();
+}
+
+size_t atm_slot_bytes(bool mixed) { return mixed ? sizeof(Slot<float>) : sizeof(Slot<double>); }
 
 void launch_triples(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
                     const Work& w, const void* mat, const long long* mat_off, const long long* off, const int* cnt,
                     const int* nbr_j, const int* nbr_gend, const double4* nbr_v, unsigned int* queue,
-                    double* slot_acc, int slot_stride, int blocks, double* e3, double* sig3, cudaStream_t stream)
+                    double* slot_acc, void* slot_scr, int slot_stride, int blocks, double* e3, double* sig3,
+                    cudaStream_t stream)
 {
     if (b.natoms <= 0) return;
     if (c.mixed) {
+        auto* m = (const C6Entry<float>*)mat;
+        auto* sc = (Slot<float>*)slot_scr;
         if (c.grad)
-            k_triples<float, true><<<blocks, kThreadsAtm, 0, stream>>>(b, s, d, c, p, w, (const C6Entry<float>*)mat, mat_off,
-                off, cnt, nbr_j, nbr_gend, nbr_v, queue, slot_acc, slot_stride, e3, sig3);
+            k_triples<float, true><<<blocks, kThreadsAtm, triple_smem<float>(), stream>>>(b, s, d, c, p, w, m, mat_off, off, cnt, nbr_j,
+                nbr_gend, nbr_v, queue, slot_acc, sc, slot_stride, e3, sig3);
         else
-            k_triples<float, false><<<blocks, kThreadsAtm, 0, stream>>>(b, s, d, c, p, w, (const C6Entry<float>*)mat, mat_off,
-                off, cnt, nbr_j, nbr_gend, nbr_v, queue, slot_acc, slot_stride, e3, sig3);
+            k_triples<float, false><<<blocks, kThreadsAtm, triple_smem<float>(), stream>>>(b, s, d, c, p, w, m, mat_off, off, cnt, nbr_j,
+                nbr_gend, nbr_v, queue, slot_acc, sc, slot_stride, e3, sig3);
     } else {
+        auto* m = (const C6Entry<double>*)mat;
+        auto* sc = (Slot<double>*)slot_scr;
         if (c.grad)
-            k_triples<double, true><<<blocks, kThreadsAtm, 0, stream>>>(b, s, d, c, p, w, (const C6Entry<double>*)mat, mat_off,
-                off, cnt, nbr_j, nbr_gend, nbr_v, queue, slot_acc, slot_stride, e3, sig3);
+            k_triples<double, true><<<blocks, kThreadsAtm, triple_smem<double>(), stream>>>(b, s, d, c, p, w, m, mat_off, off, cnt, nbr_j,
+                nbr_gend, nbr_v, queue, slot_acc, sc, slot_stride, e3, sig3);
         else
-            k_triples<double, false><<<blocks, kThreadsAtm, 0, stream>>>(b, s, d, c, p, w, (const C6Entry<double>*)mat, mat_off,
-                off, cnt, nbr_j, nbr_gend, nbr_v, queue, slot_acc, slot_stride, e3, sig3);
+            k_triples<double, false><<<blocks, kThreadsAtm, triple_smem<double>(), stream>>>(b, s, d, c, p, w, m, mat_off, off, cnt,
+                nbr_j, nbr_gend, nbr_v, queue, slot_acc, sc, slot_stride, e3, sig3);
     }
 }
-
 
 }  // namespace d3

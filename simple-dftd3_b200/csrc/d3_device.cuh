@@ -34,7 +34,15 @@ struct Batch {
     const double* z = nullptr;
     const float4* xhi = nullptr;         // [natoms] float head of x,y,z (mixed form)
     const float4* xlo = nullptr;         // [natoms] float tail x - head
+    // spatial order (optional): atom slot a holds the input atom perm[a]; the
+    // per-atom arrays above are then in slot order
+    const int* perm = nullptr;           // [natoms] or null (input order)
+    const double4* tiles = nullptr;      // [ntiles] bounding sphere (centre, radius) of 32 slots, or null
+    const int* tile_off = nullptr;       // [nsys + 1] first tile of each system
 };
+
+constexpr int kTile = 32;               // atoms per tile (one warp)
+constexpr int kMaxSpeciesFast = 16;     // species handled by the culled pair kernels
 
 // Per-species model tables (new_d3_model, model.f90:87-181) for the batch's
 // species set, and the per-pair damping constants of the current parameters.
@@ -95,6 +103,25 @@ void launch_weights(const Batch& b, const Species& s, const Config& c, const Wor
                     cudaStream_t stream);
 void launch_two_body(const Batch& b, const Species& s, const Damp& d, const Config& c,
                      const Partition& p, const Work& w, cudaStream_t stream);
+// Spatial ordering and tile bounds (d3_pair.cu).
+size_t sort_temp_bytes(int natoms);
+void launch_spatial_sort(const double* pos, int natoms, const int* sys_of_atom, unsigned long long* keys_in,
+                         unsigned long long* keys_out, int* idx_in, int* perm, void* temp, size_t temp_bytes,
+                         cudaStream_t stream);
+void launch_gather_sorted(const double* pos, const int* perm, const int* sp_in, const uint8_t* ghost_in,
+                          const int* sys_of_atom, const int* atom_off, int natoms, double* x, double* y,
+                          double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost, int* local, bool mixed,
+                          cudaStream_t stream);
+void launch_tile_bounds(const Batch& b, const int* tile_sys, int ntiles, double4* tiles, cudaStream_t stream);
+// Culled pair sweeps over sorted atoms and tiles (d3_pair.cu); used by the
+// launchers below when b.tiles is set and nid <= kMaxSpeciesFast.
+void launch_coordination_number_tiled(const Batch& b, const Species& s, const Config& c, const Partition& p,
+                                      const Work& w, cudaStream_t stream);
+void launch_two_body_tiled(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
+                           const Work& w, cudaStream_t stream);
+void launch_cn_chain_rule_tiled(const Batch& b, const Species& s, const Config& c, const Partition& p,
+                                const Work& w, cudaStream_t stream);
+
 // Three-body term (d3_atm.cu): C6 table, neighbour lists, triple sum.
 size_t atm_c6_entry_bytes(bool mixed);
 void launch_c6_matrix(const Batch& b, const Species& s, const Work& w, const long long* d_mat_off,
@@ -106,11 +133,12 @@ void launch_scan(void* temp, size_t temp_bytes, const int* cnt_ext, long long* o
 void launch_nbr_fill(const Batch& b, const Config& c, const long long* off, int* nbr_j, int* nbr_gend,
                      double4* nbr_v, cudaStream_t stream);
 int atm_blocks_per_sm(bool mixed, bool grad);
+size_t atm_slot_bytes(bool mixed);
 void launch_triples(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
                     const Work& w, const void* mat, const long long* mat_off, const long long* off,
                     const int* cnt, const int* nbr_j, const int* nbr_gend, const double4* nbr_v,
-                    unsigned int* queue, double* slot_acc, int slot_stride, int blocks, double* e3,
-                    double* sig3, cudaStream_t stream);
+                    unsigned int* queue, double* slot_acc, void* slot_scr, int slot_stride, int blocks,
+                    double* e3, double* sig3, cudaStream_t stream);
 void launch_cn_chain_rule(const Batch& b, const Species& s, const Config& c, const Partition& p,
                           const Work& w, cudaStream_t stream);
 void launch_reduce_systems(const Batch& b, const Config& c, const Work& w, double* energies,

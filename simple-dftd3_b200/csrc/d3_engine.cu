@@ -245,6 +245,18 @@ Engine::Engine(int nsys, const int* natoms, const int* numbers, const double* la
     for (int a = 0; a < nid; a++)
         for (int b = 0; b < nid; b++) r0[a * nid + b] = 4.0 / 3.0 * tab_.rvdw[a * nid + b];
     up(d_atm_r0_, r0.data(), sizeof(double) * r0.size());
+    // tiles of 32 consecutive atoms of a system
+    std::vector<int> tile_off(nsys + 1, 0), tile_sys;
+    for (int sy = 0; sy < nsys; sy++) {
+        const int nt = (natoms[sy] + kTile - 1) / kTile;
+        tile_off[sy + 1] = tile_off[sy] + nt;
+        for (int t = 0; t < nt; t++) tile_sys.push_back(sy);
+    }
+    ntiles_ = tile_off[nsys];
+    d_tile_off_ = dev_alloc<int>(nsys + 1);
+    d_tile_sys_ = dev_alloc<int>(std::max(ntiles_, 1));
+    up(d_tile_off_, tile_off.data(), sizeof(int) * (nsys + 1));
+    up(d_tile_sys_, tile_sys.data(), sizeof(int) * ntiles_);
     // three-body dense blocks per system
     c6mat_off_.assign(nsys, 0);
     long long off = 0;
@@ -389,6 +401,16 @@ void Engine::ensure_workspace(bool grad, bool param_grad, bool threebody)
     if (!ws_ready_) {
         const size_t n = natoms_;
         d_x_ = dev_alloc<double>(n); d_y_ = dev_alloc<double>(n); d_z_ = dev_alloc<double>(n);
+        d_keys_in_ = dev_alloc<unsigned long long>(n);
+        d_keys_out_ = dev_alloc<unsigned long long>(n);
+        d_idx_in_ = dev_alloc<int>(n);
+        d_perm_ = dev_alloc<int>(n);
+        d_sp_sorted_ = dev_alloc<int>(n);
+        d_local_sorted_ = dev_alloc<int>(n);
+        d_ghost_sorted_ = dev_alloc<uint8_t>(n);
+        d_tiles_ = dev_alloc<double4>(std::max(ntiles_, 1));
+        sort_bytes_ = sort_temp_bytes(natoms_);
+        d_sort_temp_ = dev_alloc<unsigned char>(sort_bytes_);
         d_xhi_ = dev_alloc<float4>(n); d_xlo_ = dev_alloc<float4>(n);
         work_.cn = dev_alloc<double>(n);
         work_.gw = dev_alloc<double>(n * kMaxRef);
@@ -456,9 +478,10 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
 
     Batch b;
     b.nsys = nsys_; b.natoms = natoms_; b.nid = tab_.nid();
-    b.sys_of_atom = d_sys_of_atom_; b.atom_off = d_atom_off_; b.local = d_local_; b.sp = d_sp_;
-    b.ghost = d_ghost_; b.img_off = d_img_off_; b.img = d_img_;
+    b.sys_of_atom = d_sys_of_atom_; b.atom_off = d_atom_off_; b.local = d_local_sorted_; b.sp = d_sp_sorted_;
+    b.ghost = d_ghost_sorted_; b.img_off = d_img_off_; b.img = d_img_;
     b.x = d_x_; b.y = d_y_; b.z = d_z_; b.xhi = d_xhi_; b.xlo = d_xlo_;
+    b.perm = d_perm_; b.tiles = d_tiles_; b.tile_off = d_tile_off_;
     Species s;
     s.rcov = d_rcov_; s.nref = d_nref_; s.refcn = d_refcn_; s.c6ref = d_c6ref_;
     s.c6ref_f = d_c6ref_f_; s.pair = d_pair_; s.atm_r0 = d_atm_r0_;
@@ -479,7 +502,11 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     if (profiling_ && !ev_[0])
         for (auto& e : ev_) check(cudaEventCreate(&e), "cudaEventCreate");
     mark(0);
-    launch_split_positions(d_positions, natoms_, d_x_, d_y_, d_z_, d_xhi_, d_xlo_, mixed_, stream);
+    launch_spatial_sort(d_positions, natoms_, d_sys_of_atom_, d_keys_in_, d_keys_out_, d_idx_in_, d_perm_,
+                        d_sort_temp_, sort_bytes_, stream);
+    launch_gather_sorted(d_positions, d_perm_, d_sp_, d_ghost_, d_sys_of_atom_, d_atom_off_, natoms_, d_x_, d_y_,
+                         d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed_, stream);
+    launch_tile_bounds(b, d_tile_sys_, ntiles_, d_tiles_, stream);
     mark(1);
     launch_coordination_number(b, s, c, part_, w, stream);
     mark(2);
@@ -560,17 +587,24 @@ void Engine::run_three_body(const Batch& b, const Species& s, const Damp& d, con
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
     const int blocks = std::max(1, std::min(n, sms * atm_blocks_per_sm(c.mixed, c.grad)));
     const int stride = std::max(maxcnt, 1);
-    const long long need = (long long)blocks * stride * 6;
-    if (c.grad && need > slot_cap_) {
+    const long long need = (long long)blocks * stride * 8;   // per-entry accumulators (up to 8 doubles)
+    if (need > slot_cap_) {
         void* p = d_slot_acc_;
         free_block(p);
         slot_cap_ = need + need / 4;
         d_slot_acc_ = dev_alloc<double>(slot_cap_);
     }
+    const long long scr_need = (long long)blocks * stride * (long long)atm_slot_bytes(false);
+    if (scr_need > slot_scr_cap_) {
+        void* p = d_slot_scr_;
+        free_block(p);
+        slot_scr_cap_ = scr_need + scr_need / 4;
+        d_slot_scr_ = dev_alloc<unsigned char>(slot_scr_cap_);
+    }
     launch_nbr_fill(b, c, d_off_, d_nbr_j_, d_nbr_gend_, d_nbr_v_, stream);
     check(cudaMemsetAsync(d_queue_, 0, sizeof(unsigned int), stream), "memset");
     launch_triples(b, s, d, c, part_, w, d_c6mat_, d_c6mat_off_, d_off_, d_cnt_, d_nbr_j_, d_nbr_gend_, d_nbr_v_,
-                   d_queue_, d_slot_acc_, stride, blocks, d_e3_, d_sig3_, stream);
+                   d_queue_, d_slot_acc_, d_slot_scr_, stride, blocks, d_e3_, d_sig3_, stream);
     w.e3_atom = d_e3_;
     w.sig3_atom = c.grad ? d_sig3_ : nullptr;
 }

@@ -129,6 +129,17 @@ private:
            *d_atm_r0_ = nullptr;
     float* d_c6ref_f_ = nullptr;
     int* d_nref_ = nullptr;
+    // spatial order and tiles
+    int ntiles_ = 0;
+    int* d_tile_sys_ = nullptr;
+    int* d_tile_off_ = nullptr;
+    unsigned long long *d_keys_in_ = nullptr, *d_keys_out_ = nullptr;
+    int *d_idx_in_ = nullptr, *d_perm_ = nullptr;
+    int *d_sp_sorted_ = nullptr, *d_local_sorted_ = nullptr;
+    uint8_t* d_ghost_sorted_ = nullptr;
+    double4* d_tiles_ = nullptr;
+    void* d_sort_temp_ = nullptr;
+    size_t sort_bytes_ = 0;
     // workspace
     double *d_x_ = nullptr, *d_y_ = nullptr, *d_z_ = nullptr;
     float4 *d_xhi_ = nullptr, *d_xlo_ = nullptr;
@@ -159,6 +170,8 @@ private:
     long long nbr_cap_ = 0;
     double* d_slot_acc_ = nullptr;
     long long slot_cap_ = 0;
+    void* d_slot_scr_ = nullptr;
+    long long slot_scr_cap_ = 0;
     double* d_e3_ = nullptr;
     double* d_sig3_ = nullptr;
     long long* h_atm_counts_ = nullptr;   // pinned: total entries, largest list

@@ -492,8 +492,10 @@ __global__ void k_reduce_systems(Batch b, Config c, Work w, double* energies, do
                 v[1 + k] += w.sig_atom[kSigma * a + k] + (w.sig3_atom ? w.sig3_atom[kSigma * a + k] : 0.0);
         if (c.param_grad && w.pg_atom)
             for (int k = 0; k < kParamGrad; k++) v[1 + kSigma + k] += w.pg_atom[kParamGrad * a + k];
-        if (c.grad && grad_out)
-            for (int k = 0; k < 3; k++) grad_out[3 * a + k] = w.grad[3 * a + k];
+        if (c.grad && grad_out) {
+            const int o = b.perm ? b.perm[a] : a;
+            for (int k = 0; k < 3; k++) grad_out[3 * o + k] = w.grad[3 * a + k];
+        }
     }
     for (int k = 0; k < kVals; k++) red[k][threadIdx.x] = v[k];
     __syncthreads();
@@ -581,6 +583,10 @@ void launch_coordination_number(const Batch& b, const Species& s, const Config& 
                                 const Partition& p, const Work& w, cudaStream_t stream)
 {
     if (b.natoms <= 0) return;
+    if (b.tiles && b.nid <= kMaxSpeciesFast) {
+        launch_coordination_number_tiled(b, s, c, p, w, stream);
+        return;
+    }
     if (c.mixed)
         k_coordination_number<float><<<blocks_for_atoms(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
     else
@@ -597,6 +603,10 @@ void launch_two_body(const Batch& b, const Species& s, const Damp& d, const Conf
                      const Partition& p, const Work& w, cudaStream_t stream)
 {
     if (b.natoms <= 0) return;
+    if (b.tiles && b.nid <= kMaxSpeciesFast) {
+        launch_two_body_tiled(b, s, d, c, p, w, stream);
+        return;
+    }
     const int nb = blocks_for_atoms(b.natoms);
     if (d.kind == kRational) {
         if (c.mixed) k_two_body<float, kRational><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
@@ -611,6 +621,10 @@ void launch_cn_chain_rule(const Batch& b, const Species& s, const Config& c, con
                           const Work& w, cudaStream_t stream)
 {
     if (b.natoms <= 0) return;
+    if (b.tiles && b.nid <= kMaxSpeciesFast) {
+        launch_cn_chain_rule_tiled(b, s, c, p, w, stream);
+        return;
+    }
     if (c.mixed)
         k_cn_chain<float><<<blocks_for_atoms(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
     else

@@ -1,0 +1,645 @@
+// Spatially ordered, tile-culled pair sweeps: coordination number, two-body
+// dispersion and CN chain rule.
+//
+// Atoms of every system are put in Morton order (cub radix sort of quantised
+// positions), and each run of 32 consecutive atoms of a system forms a tile
+// with a bounding sphere.  A warp owns one atom i: it stages y(T) = x_i - T for
+// a chunk of lattice translations in shared memory, tests all 32 atoms of a
+// tile against 32 translations at once with the tile's bounding sphere (one
+// ballot per 32 translations), and evaluates the pair terms only for the
+// translations that can reach the tile, one j per lane.  The work per pair
+// term is the same as in the unsorted kernels; the candidate tests that the
+// cutoff rejects anyway are skipped in blocks of 32.
+//
+// C6 interpolation uses per-warp species vectors: for the warp's atom i and
+// every species s, u_s = sum_r gw_i[r] C6ref(r, ., si, s) and the same with
+// dgw_i, so C6_ij and its two CN derivatives cost 3 short dot products per j
+// (get_atomic_c6, model.f90:432-461).
+#include <cub/cub.cuh>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "d3_device.cuh"
+
+namespace d3 {
+
+namespace {
+
+constexpr int kWarps = 8;
+constexpr int kThreads = 32 * kWarps;
+constexpr int kChunk = 128;            // translations staged per pass (4 ballot words)
+constexpr double kKcn = 16.0;          // ncoord.f90:31
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+__device__ __forceinline__ bool owns_pair(const Partition& p, int i, int j)
+{
+    // partition.f90:127-147 on zero-based system-local input indices
+    if (p.nparts <= 1) return true;
+    long long hi = i > j ? i : j, lo = i > j ? j : i;
+    return (hi * (hi + 1) / 2 + lo) % p.nparts == p.part;
+}
+
+struct Sh64 { double x, y, z; };
+struct Sh32 { float4 hi, lo; };
+template <class R> struct ShOf;
+template <> struct ShOf<double> { using type = Sh64; };
+template <> struct ShOf<float> { using type = Sh32; };
+
+__device__ __forceinline__ Sh32 split3(double x, double y, double z)
+{
+    Sh32 s;
+    s.hi = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z), 0.f);
+    s.lo = make_float4(__double2float_rn(x - (double)s.hi.x), __double2float_rn(y - (double)s.hi.y),
+                       __double2float_rn(z - (double)s.hi.z), 0.f);
+    return s;
+}
+
+__device__ __forceinline__ void pos_of(const Sh64& s, double& x, double& y, double& z) { x = s.x; y = s.y; z = s.z; }
+__device__ __forceinline__ void pos_of(const Sh32& s, double& x, double& y, double& z)
+{
+    x = (double)s.hi.x + (double)s.lo.x;
+    y = (double)s.hi.y + (double)s.lo.y;
+    z = (double)s.hi.z + (double)s.lo.z;
+}
+
+__device__ __forceinline__ void disp(const Sh64& s, double xj, double yj, double zj, float4, float4,
+                                     double& vx, double& vy, double& vz)
+{
+    vx = s.x - xj; vy = s.y - yj; vz = s.z - zj;
+}
+
+__device__ __forceinline__ void disp(const Sh32& s, double, double, double, float4 hj, float4 lj,
+                                     float& vx, float& vy, float& vz)
+{
+    vx = (s.hi.x - hj.x) + (s.lo.x - lj.x);
+    vy = (s.hi.y - hj.y) + (s.lo.y - lj.y);
+    vz = (s.hi.z - hj.z) + (s.lo.z - lj.z);
+}
+
+template <class R>
+__device__ __forceinline__ void stage(typename ShOf<R>::type* buf, const double* img, int t0, int nt, double xi,
+                                      double yi, double zi, int lane)
+{
+    for (int k = lane; k < nt; k += 32) {
+        const double tx = __ldg(img + 3 * (t0 + k)), ty = __ldg(img + 3 * (t0 + k) + 1), tz = __ldg(img + 3 * (t0 + k) + 2);
+        if constexpr (sizeof(R) == 8) buf[k] = Sh64{xi - tx, yi - ty, zi - tz};
+        else buf[k] = split3(xi - tx, yi - ty, zi - tz);
+    }
+    __syncwarp();
+}
+
+// Ballot of the staged translations [32 w, 32 w + 32) that can reach a tile.
+template <class R>
+__device__ __forceinline__ unsigned reach(const typename ShOf<R>::type* buf, int nt, int w, int lane, double4 tb,
+                                          double cutoff)
+{
+    const int k = 32 * w + lane;
+    bool ok = false;
+    if (k < nt) {
+        double yx, yy, yz;
+        pos_of(buf[k], yx, yy, yz);
+        const double dx = yx - tb.x, dy = yy - tb.y, dz = yz - tb.z;
+        const double lim = cutoff + tb.w + 1.0e-6 * cutoff + 1.0e-6;
+        ok = dx * dx + dy * dy + dz * dz <= lim * lim;
+    }
+    return __ballot_sync(0xffffffffu, ok);
+}
+
+template <class R> __device__ __forceinline__ R r_sqrt(R x) { if constexpr (sizeof(R) == 8) return sqrt(x); else return sqrtf(x); }
+template <class R> __device__ __forceinline__ R r_exp(R x) { if constexpr (sizeof(R) == 8) return exp(x); else return expf(x); }
+template <class R> __device__ __forceinline__ R r_pow(R x, R a) { if constexpr (sizeof(R) == 8) return pow(x, a); else return powf(x, a); }
+
+template <class R>
+__device__ __forceinline__ void smooth(R r, R cutoff, R width, R& sw, R& dswdr)
+{
+    // cutoff.f90:73-99
+    if (width <= R(0) || width >= cutoff) { sw = R(1); dswdr = R(0); return; }
+    const R inner = cutoff - width;
+    if (r <= inner) { sw = R(1); dswdr = R(0); }
+    else if (r >= cutoff) { sw = R(0); dswdr = R(0); }
+    else {
+        const R x = (cutoff - r) / width;
+        sw = x * x * x * (R(10) + x * (R(-15) + R(6) * x));
+        dswdr = R(-30) * x * x * (R(1) - x) * (R(1) - x) / width;
+    }
+}
+
+struct Range {
+    int j0, j1, t0, t1, tile0;
+};
+
+__device__ __forceinline__ Range range_of(const Batch& b, int i, int kind)
+{
+    const int sys = b.sys_of_atom[i];
+    Range r;
+    r.j0 = b.atom_off[sys];
+    r.j1 = b.atom_off[sys + 1];
+    r.t0 = b.img_off[kind * (b.nsys + 1) + sys];
+    r.t1 = b.img_off[kind * (b.nsys + 1) + sys + 1];
+    r.tile0 = b.tile_off[sys];
+    return r;
+}
+
+// ----------------------------------------------------- coordination number --
+
+template <class R>
+__global__ void __launch_bounds__(kThreads) k_cn_tiled(Batch b, Species s, Config c, Partition p, Work w)
+{
+    using Sh = typename ShOf<R>::type;
+    __shared__ Sh sbuf[kWarps][kChunk];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int i = blockIdx.x * kWarps + wib;
+    if (i >= b.natoms) return;
+    const Range rg = range_of(b, i, kImgCN);
+    const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
+    const double rci = s.rcov[b.sp[i]];
+    const int li = b.local[i];
+    const R cut2 = R(c.cut_cn * c.cut_cn);
+    double acc = 0.0;
+    R tacc = R(0);
+    unsigned long long nterm = 0;
+    for (int tc = rg.t0; tc < rg.t1; tc += kChunk) {
+        const int nt = min(kChunk, rg.t1 - tc);
+        stage<R>(sbuf[wib], b.img, tc, nt, xi, yi, zi, lane);
+        const int nw = (nt + 31) / 32;
+        for (int jb = rg.j0, tile = rg.tile0; jb < rg.j1; jb += kTile, tile++) {
+            const double4 tb = b.tiles[tile];
+            unsigned mk[4] = {0u, 0u, 0u, 0u};
+            unsigned any = 0u;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (q < nw) { mk[q] = reach<R>(sbuf[wib], nt, q, lane, tb, c.cut_cn); any |= mk[q]; }
+            if (!any) continue;
+            const int j = jb + lane;
+            const bool valid = j < rg.j1 && (!c.cn_partitioned || owns_pair(p, li, b.local[j < rg.j1 ? j : rg.j0]));
+            const int jj = j < rg.j1 ? j : rg.j0;
+            const double xj = b.x[jj], yj = b.y[jj], zj = b.z[jj];
+            float4 hj = make_float4(0, 0, 0, 0), lj = hj;
+            if constexpr (sizeof(R) == 4) { hj = b.xhi[jj]; lj = b.xlo[jj]; }
+            const R rc = R(rci + s.rcov[b.sp[jj]]);
+            if constexpr (sizeof(R) == 4) tacc = R(0);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                unsigned m = mk[q];
+                while (m) {
+                    const int k = 32 * q + __ffs(m) - 1;
+                    m &= m - 1;
+                    R vx, vy, vz;
+                    disp(sbuf[wib][k], xj, yj, zj, hj, lj, vx, vy, vz);
+                    const R r2 = vx * vx + vy * vy + vz * vz;
+                    if (!valid || r2 > cut2 || r2 < R(1.0e-12)) continue;
+                    const R r1 = r_sqrt<R>(r2);
+                    tacc += R(1) / (R(1) + r_exp<R>(-R(kKcn) * (rc / r1 - R(1))));
+                    nterm += (jj <= i);
+                }
+            }
+            if constexpr (sizeof(R) == 4) acc += double(tacc);
+        }
+        __syncwarp();
+    }
+    if constexpr (sizeof(R) == 8) acc = tacc;
+    acc = warp_sum(acc);
+    if (lane == 0) w.cn[i] = acc;
+    if (w.counts) {
+        for (int off = 16; off > 0; off >>= 1) nterm += __shfl_xor_sync(0xffffffffu, nterm, off);
+        if (lane == 0) atomicAdd(w.counts + 2, nterm);
+    }
+}
+
+// ---------------------------------------------------------------- two-body --
+
+template <class R, int DAMP>
+__global__ void __launch_bounds__(kThreads) k_two_body_tiled(Batch b, Species s, Damp d, Config c, Partition p,
+                                                             Work w)
+{
+    using Sh = typename ShOf<R>::type;
+    __shared__ Sh sbuf[kWarps][kChunk];
+    __shared__ R su[kWarps][kMaxSpeciesFast][kMaxRef];
+    __shared__ R sdu[kWarps][kMaxSpeciesFast][kMaxRef];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int i = blockIdx.x * kWarps + wib;
+    if (i >= b.natoms) return;
+    const Range rg = range_of(b, i, kImgDisp2);
+    const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
+    const int si = b.sp[i], nid = b.nid;
+    const int nri = s.nref[si];
+    const int li = b.local[i];
+    const bool gi = b.ghost && b.ghost[i];
+    // species vectors of atom i: u[sj][jr] = sum_ir gw_i[ir] c6(ir, jr, si, sj)
+    for (int idx = lane; idx < nid * kMaxRef; idx += 32) {
+        const int sj = idx / kMaxRef, jr = idx % kMaxRef;
+        R u = R(0), du = R(0);
+        if (!gi && jr < s.nref[sj]) {
+            const int base = (si * nid + sj) * kMaxRef * kMaxRef;
+            for (int ir = 0; ir < nri; ir++) {
+                R ref, g, dg;
+                if constexpr (sizeof(R) == 8) {
+                    ref = __ldg(s.c6ref + base + ir * kMaxRef + jr);
+                    g = w.gw[i * kMaxRef + ir]; dg = w.dgw[i * kMaxRef + ir];
+                } else {
+                    ref = __ldg(s.c6ref_f + base + ir * kMaxRef + jr);
+                    g = w.gwf[i * kMaxRef + ir]; dg = w.dgwf[i * kMaxRef + ir];
+                }
+                u += g * ref;
+                du += dg * ref;
+            }
+        }
+        su[wib][sj][jr] = u;
+        sdu[wib][sj][jr] = du;
+    }
+    __syncwarp();
+    const R cutoff = R(c.cut2), cut2 = R(c.cut2 * c.cut2), width = R(c.width2);
+    const bool smooth_on = c.width2 > 0.0 && c.width2 < c.cut2;
+    const R s6 = R(d.s6), s8 = R(d.s8);
+    const R alp6 = R(d.alp), alp8 = R(d.alp + 2.0);
+    double e = 0, de = 0, gx = 0, gy = 0, gz = 0;
+    double sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+    double pg0 = 0, pg1 = 0, pg2 = 0, pg3 = 0;
+    R te = R(0), tde = R(0), tgx = R(0), tgy = R(0), tgz = R(0);
+    R txx = R(0), tyy = R(0), tzz = R(0), txy = R(0), txz = R(0), tyz = R(0);
+    R tp0 = R(0), tp1 = R(0), tp2 = R(0), tp3 = R(0);
+    unsigned long long nterm = 0;
+    for (int tc = rg.t0; tc < rg.t1; tc += kChunk) {
+        const int nt = min(kChunk, rg.t1 - tc);
+        stage<R>(sbuf[wib], b.img, tc, nt, xi, yi, zi, lane);
+        const int nw = (nt + 31) / 32;
+        for (int jb = rg.j0, tile = rg.tile0; jb < rg.j1; jb += kTile, tile++) {
+            const double4 tb = b.tiles[tile];
+            unsigned mk[4] = {0u, 0u, 0u, 0u};
+            unsigned any = 0u;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (q < nw) { mk[q] = reach<R>(sbuf[wib], nt, q, lane, tb, c.cut2); any |= mk[q]; }
+            if (!any) continue;
+            const int j = jb + lane;
+            const int jj = j < rg.j1 ? j : rg.j0;
+            const bool valid = j < rg.j1 && owns_pair(p, li, b.local[jj]);
+            const double xj = b.x[jj], yj = b.y[jj], zj = b.z[jj];
+            float4 hj = make_float4(0, 0, 0, 0), lj = hj;
+            if constexpr (sizeof(R) == 4) { hj = b.xhi[jj]; lj = b.xlo[jj]; }
+            const int sj = b.sp[jj];
+            R c6 = R(0), dc6i = R(0), dc6j = R(0);
+            if (valid && !(b.ghost && b.ghost[jj])) {
+                const int nrj = s.nref[sj];
+                for (int jr = 0; jr < nrj; jr++) {
+                    R g, dg;
+                    if constexpr (sizeof(R) == 8) { g = w.gw[jj * kMaxRef + jr]; dg = w.dgw[jj * kMaxRef + jr]; }
+                    else { g = w.gwf[jj * kMaxRef + jr]; dg = w.dgwf[jj * kMaxRef + jr]; }
+                    const R u = su[wib][sj][jr], du = sdu[wib][sj][jr];
+                    c6 += u * g;
+                    dc6i += du * g;
+                    dc6j += u * dg;
+                }
+            }
+            const double* pr = s.pair + kPairSlots * (si * nid + sj);
+            const R rrij = R(__ldg(pr + 0));
+            const R q1 = R(__ldg(pr + 1)), q2 = R(__ldg(pr + 2)), q3 = R(__ldg(pr + 3)), q4 = R(__ldg(pr + 4));
+            // mixed form: FP32 partial sums over the translations of this tile,
+            // added to the FP64 accumulators once per tile
+            if constexpr (sizeof(R) == 4) {
+                te = tde = tgx = tgy = tgz = R(0);
+                txx = tyy = tzz = txy = txz = tyz = R(0);
+                tp0 = tp1 = tp2 = tp3 = R(0);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                unsigned m = mk[q];
+                while (m) {
+                    const int k = 32 * q + __ffs(m) - 1;
+                    m &= m - 1;
+                    R vx, vy, vz;
+                    disp(sbuf[wib][k], xj, yj, zj, hj, lj, vx, vy, vz);
+                    const R r2 = vx * vx + vy * vy + vz * vz;
+                    if (!valid || r2 > cut2 || r2 < R(DBL_EPSILON)) continue;
+                    nterm += (jj <= i);   // the reference's (i, j <= i, T) count
+                    R sw = R(1), dswdr = R(0), r1 = R(0);
+                    if (smooth_on) { r1 = r_sqrt<R>(r2); smooth<R>(r1, cutoff, width, sw, dswdr); }
+                    R edisp0, gdisp0, e6, e8, dpa = R(0), dpb = R(0);
+                    if constexpr (DAMP == kRational) {
+                        // rational.f90:462-497: q1 = R0^6, q2 = R0^8, q3 = R0, q4 = sqrt(rrij)
+                        const R r4 = r2 * r2;
+                        const R a6 = r4 * r2 + q1, a8 = r4 * r4 + q2;
+                        const R inv = R(1) / (a6 * a8);
+                        const R t6 = a8 * inv;
+                        const R t8 = a6 * inv;
+                        const R d6 = R(-6) * r4 * t6 * t6;
+                        const R d8 = R(-8) * r4 * r2 * t8 * t8;
+                        e6 = t6; e8 = rrij * t8;
+                        edisp0 = s6 * t6 + s8 * rrij * t8;
+                        gdisp0 = s6 * d6 + s8 * rrij * d8;
+                        if (c.param_grad) {
+                            const R dedr0 = s6 * R(-6) * (q1 / q3) * t6 * t6 + s8 * rrij * R(-8) * (q2 / q3) * t8 * t8;
+                            dpa = dedr0 * q4;
+                            dpb = dedr0;
+                        }
+                    } else {
+                        // zero.f90:490-536: q1 = rs6 R0, q2 = rs8 R0
+                        if (!smooth_on) r1 = r_sqrt<R>(r2);
+                        const R r6 = r2 * r2 * r2;
+                        const R r8 = r6 * r2;
+                        const R t6 = r_pow<R>(q1 / r1, alp6);
+                        const R t8 = r_pow<R>(q2 / r1, alp8);
+                        const R f6 = R(1) / (R(1) + R(6) * t6);
+                        const R f8 = R(1) / (R(1) + R(6) * t8);
+                        const R d6 = R(-6) * f6 / r2 + R(6) * alp6 * t6 * (f6 * f6) / r2;
+                        const R d8 = R(-8) * f8 / r2 + R(6) * alp8 * t8 * (f8 * f8) / r2;
+                        e6 = f6 / r6; e8 = rrij * f8 / r8;
+                        edisp0 = s6 * f6 / r6 + s8 * rrij * f8 / r8;
+                        gdisp0 = s6 * d6 / r6 + s8 * rrij * d8 / r8;
+                        if (c.param_grad) {
+                            dpa = d.rs6 != 0.0 ? s6 / r6 * R(-6) * f6 * f6 * alp6 * t6 / R(d.rs6) : R(0);
+                            dpb = d.rs8 != 0.0 ? s8 * rrij / r8 * R(-6) * f8 * f8 * alp8 * t8 / R(d.rs8) : R(0);
+                        }
+                    }
+                    const R edisp = sw * edisp0;
+                    te += -c6 * edisp * R(0.5);
+                    tde -= dc6i * edisp;
+                    if (c.param_grad) {
+                        const R hc = R(-0.5) * c6 * sw;
+                        tp0 += hc * e6; tp1 += hc * e8;
+                        tp2 += hc * dpa; tp3 += hc * dpb;
+                    }
+                    if (!c.grad) continue;
+                    R gdisp = sw * gdisp0;
+                    if (smooth_on) gdisp += dswdr * edisp0 / r1;
+                    const R f = -c6 * gdisp;
+                    const R dgx = f * vx, dgy = f * vy, dgz = f * vz;
+                    if (jj != i) { tgx += dgx; tgy += dgy; tgz += dgz; }
+                    txx += dgx * vx; tyy += dgy * vy; tzz += dgz * vz;
+                    txy += dgx * vy; txz += dgx * vz; tyz += dgy * vz;
+                }
+            }
+            if constexpr (sizeof(R) == 4) {
+                e += double(te);
+                de += double(tde);
+                if (c.param_grad) { pg0 += double(tp0); pg1 += double(tp1); pg2 += double(tp2); pg3 += double(tp3); }
+                if (c.grad) {
+                    gx += double(tgx); gy += double(tgy); gz += double(tgz);
+                    sxx += double(txx); syy += double(tyy); szz += double(tzz);
+                    sxy += double(txy); sxz += double(txz); syz += double(tyz);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if constexpr (sizeof(R) == 8) {
+        // the FP64 form accumulates directly in the tile sums
+        e = te; de = tde; pg0 = tp0; pg1 = tp1; pg2 = tp2; pg3 = tp3;
+        gx = tgx; gy = tgy; gz = tgz;
+        sxx = txx; syy = tyy; szz = tzz; sxy = txy; sxz = txz; syz = tyz;
+    }
+    sxx *= 0.5; syy *= 0.5; szz *= 0.5; sxy *= 0.5; sxz *= 0.5; syz *= 0.5;
+    e = warp_sum(e);
+    if (lane == 0) w.e_atom[i] = e;
+    if (c.grad) {
+        de = warp_sum(de); gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz);
+        sxx = warp_sum(sxx); syy = warp_sum(syy); szz = warp_sum(szz);
+        sxy = warp_sum(sxy); sxz = warp_sum(sxz); syz = warp_sum(syz);
+        if (lane == 0) {
+            w.dEdcn[i] = de;
+            w.grad[3 * i + 0] = gx; w.grad[3 * i + 1] = gy; w.grad[3 * i + 2] = gz;
+            double* sg = w.sig_atom + kSigma * i;
+            sg[0] = sxx; sg[1] = syy; sg[2] = szz; sg[3] = sxy; sg[4] = sxz; sg[5] = syz;
+        }
+    }
+    if (c.param_grad) {
+        pg0 = warp_sum(pg0); pg1 = warp_sum(pg1); pg2 = warp_sum(pg2); pg3 = warp_sum(pg3);
+        if (lane == 0) {
+            double* pg = w.pg_atom + kParamGrad * i;
+            pg[0] = pg0; pg[1] = pg1; pg[2] = pg2; pg[3] = pg3;
+        }
+    }
+    if (w.counts) {
+        for (int off = 16; off > 0; off >>= 1) nterm += __shfl_xor_sync(0xffffffffu, nterm, off);
+        if (lane == 0) atomicAdd(w.counts + 0, nterm);
+    }
+}
+
+// ------------------------------------------------------------- chain rule --
+
+template <class R>
+__global__ void __launch_bounds__(kThreads) k_chain_tiled(Batch b, Species s, Config c, Partition p, Work w)
+{
+    using Sh = typename ShOf<R>::type;
+    __shared__ Sh sbuf[kWarps][kChunk];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int i = blockIdx.x * kWarps + wib;
+    if (i >= b.natoms) return;
+    const Range rg = range_of(b, i, kImgCN);
+    const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
+    const double rci = s.rcov[b.sp[i]];
+    const double dei = w.dEdcn[i];
+    const int li = b.local[i];
+    const R cut2 = R(c.cut_cn * c.cut_cn);
+    double gx = 0, gy = 0, gz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+    R tgx = R(0), tgy = R(0), tgz = R(0), txx = R(0), tyy = R(0), tzz = R(0);
+    R txy = R(0), txz = R(0), tyz = R(0);
+    for (int tc = rg.t0; tc < rg.t1; tc += kChunk) {
+        const int nt = min(kChunk, rg.t1 - tc);
+        stage<R>(sbuf[wib], b.img, tc, nt, xi, yi, zi, lane);
+        const int nw = (nt + 31) / 32;
+        for (int jb = rg.j0, tile = rg.tile0; jb < rg.j1; jb += kTile, tile++) {
+            const double4 tb = b.tiles[tile];
+            unsigned mk[4] = {0u, 0u, 0u, 0u};
+            unsigned any = 0u;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (q < nw) { mk[q] = reach<R>(sbuf[wib], nt, q, lane, tb, c.cut_cn); any |= mk[q]; }
+            if (!any) continue;
+            const int j = jb + lane;
+            const int jj = j < rg.j1 ? j : rg.j0;
+            const bool valid = j < rg.j1 && (!c.cn_partitioned || owns_pair(p, li, b.local[jj]));
+            const double xj = b.x[jj], yj = b.y[jj], zj = b.z[jj];
+            float4 hj = make_float4(0, 0, 0, 0), lj = hj;
+            if constexpr (sizeof(R) == 4) { hj = b.xhi[jj]; lj = b.xlo[jj]; }
+            const R rc = R(rci + s.rcov[b.sp[jj]]);
+            // 0.5 (dEdcn_i + dEdcn_j) is this atom's virial share of the pair
+            const R dsum = R(dei + w.dEdcn[jj]);
+            if constexpr (sizeof(R) == 4) {
+                tgx = tgy = tgz = txx = tyy = tzz = txy = txz = tyz = R(0);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                unsigned m = mk[q];
+                while (m) {
+                    const int k = 32 * q + __ffs(m) - 1;
+                    m &= m - 1;
+                    R vx, vy, vz;
+                    disp(sbuf[wib][k], xj, yj, zj, hj, lj, vx, vy, vz);
+                    const R r2 = vx * vx + vy * vy + vz * vz;
+                    if (!valid || r2 > cut2 || r2 < R(1.0e-12)) continue;
+                    const R r1 = r_sqrt<R>(r2);
+                    const R expterm = r_exp<R>(-R(kKcn) * (rc / r1 - R(1)));
+                    const R cf = R(1) / (R(1) + expterm);
+                    const R dcf = -cf * (R(1) - cf) * R(kKcn) * rc / r2;
+                    const R f = dcf / r1 * dsum;
+                    const R cx = f * vx, cy = f * vy, cz = f * vz;
+                    if (jj != i) { tgx += cx; tgy += cy; tgz += cz; }
+                    txx += cx * vx; tyy += cy * vy; tzz += cz * vz;
+                    txy += cx * vy; txz += cx * vz; tyz += cy * vz;
+                }
+            }
+            if constexpr (sizeof(R) == 4) {
+                gx += double(tgx); gy += double(tgy); gz += double(tgz);
+                sxx += double(txx); syy += double(tyy); szz += double(tzz);
+                sxy += double(txy); sxz += double(txz); syz += double(tyz);
+            }
+        }
+        __syncwarp();
+    }
+    if constexpr (sizeof(R) == 8) {
+        gx = tgx; gy = tgy; gz = tgz;
+        sxx = txx; syy = tyy; szz = tzz; sxy = txy; sxz = txz; syz = tyz;
+    }
+    sxx *= 0.5; syy *= 0.5; szz *= 0.5; sxy *= 0.5; sxz *= 0.5; syz *= 0.5;
+    gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz);
+    sxx = warp_sum(sxx); syy = warp_sum(syy); szz = warp_sum(szz);
+    sxy = warp_sum(sxy); sxz = warp_sum(sxz); syz = warp_sum(syz);
+    if (lane == 0) {
+        w.grad[3 * i + 0] += gx; w.grad[3 * i + 1] += gy; w.grad[3 * i + 2] += gz;
+        double* sg = w.sig_atom + kSigma * i;
+        sg[0] += sxx; sg[1] += syy; sg[2] += szz; sg[3] += sxy; sg[4] += sxz; sg[5] += syz;
+    }
+}
+
+// ------------------------------------------------------- ordering, tiles ----
+
+__device__ __forceinline__ unsigned long long spread3(unsigned v)
+{
+    unsigned long long x = v & 0x3ffu;
+    x = (x | (x << 16)) & 0x030000FFull;
+    x = (x | (x << 8)) & 0x0300F00Full;
+    x = (x | (x << 4)) & 0x030C30C3ull;
+    x = (x | (x << 2)) & 0x09249249ull;
+    return x;
+}
+
+// Sort key: system index above a 30-bit Morton code of the position
+// quantised to 3 Bohr cells.
+__global__ void k_morton(const double* __restrict__ pos, int n, const int* sys_of_atom,
+                         unsigned long long* keys, int* idx)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    unsigned q[3];
+    for (int c = 0; c < 3; c++) {
+        double f = floor(pos[3 * a + c] / 3.0) + 512.0;
+        f = fmin(fmax(f, 0.0), 1023.0);
+        q[c] = (unsigned)f;
+    }
+    const unsigned long long m = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+    keys[a] = ((unsigned long long)sys_of_atom[a] << 30) | m;
+    idx[a] = a;
+}
+
+__global__ void k_gather_sorted(const double* __restrict__ pos, const int* perm, const int* sp_in,
+                                const uint8_t* ghost_in, const int* sys_of_atom, const int* atom_off, int n,
+                                double* x, double* y, double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost,
+                                int* local, bool mixed)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    const int o = perm[a];
+    const double px = pos[3 * o], py = pos[3 * o + 1], pz = pos[3 * o + 2];
+    x[a] = px; y[a] = py; z[a] = pz;
+    if (mixed) {
+        const Sh32 s = split3(px, py, pz);
+        xhi[a] = s.hi;
+        xlo[a] = s.lo;
+    }
+    sp[a] = sp_in[o];
+    ghost[a] = ghost_in ? ghost_in[o] : 0;
+    local[a] = o - atom_off[sys_of_atom[o]];
+}
+
+// Bounding sphere (centroid, largest distance) of each tile; one warp per tile.
+__global__ void k_tile_bounds(Batch b, const int* tile_sys, int ntiles, double4* tiles)
+{
+    const int lane = threadIdx.x & 31;
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (t >= ntiles) return;
+    const int sys = tile_sys[t];
+    const int a0 = b.atom_off[sys] + kTile * (t - b.tile_off[sys]);
+    const int a1 = min(a0 + kTile, b.atom_off[sys + 1]);
+    const int a = a0 + lane;
+    const bool valid = a < a1;
+    const double x = valid ? b.x[a] : 0.0, y = valid ? b.y[a] : 0.0, z = valid ? b.z[a] : 0.0;
+    const double inv = 1.0 / double(a1 - a0);
+    const double cx = warp_sum(x) * inv, cy = warp_sum(y) * inv, cz = warp_sum(z) * inv;
+    double r = valid ? sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy) + (z - cz) * (z - cz)) : 0.0;
+    for (int off = 16; off > 0; off >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, off));
+    if (lane == 0) tiles[t] = make_double4(cx, cy, cz, r * (1.0 + 1.0e-12) + 1.0e-12);
+}
+
+int blocks_for(int n) { return (n + kWarps - 1) / kWarps; }
+
+}  // namespace
+
+size_t sort_temp_bytes(int natoms)
+{
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                    (const int*)nullptr, (int*)nullptr, natoms);
+    return bytes;
+}
+
+void launch_spatial_sort(const double* pos, int natoms, const int* sys_of_atom, unsigned long long* keys_in,
+                         unsigned long long* keys_out, int* idx_in, int* perm, void* temp, size_t temp_bytes,
+                         cudaStream_t stream)
+{
+    if (natoms <= 0) return;
+    k_morton<<<(natoms + 255) / 256, 256, 0, stream>>>(pos, natoms, sys_of_atom, keys_in, idx_in);
+    cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, idx_in, perm, natoms, 0, 64, stream);
+}
+
+void launch_gather_sorted(const double* pos, const int* perm, const int* sp_in, const uint8_t* ghost_in,
+                          const int* sys_of_atom, const int* atom_off, int natoms, double* x, double* y, double* z,
+                          float4* xhi, float4* xlo, int* sp, uint8_t* ghost, int* local, bool mixed,
+                          cudaStream_t stream)
+{
+    if (natoms <= 0) return;
+    k_gather_sorted<<<(natoms + 255) / 256, 256, 0, stream>>>(pos, perm, sp_in, ghost_in, sys_of_atom, atom_off,
+                                                              natoms, x, y, z, xhi, xlo, sp, ghost, local, mixed);
+}
+
+void launch_tile_bounds(const Batch& b, const int* tile_sys, int ntiles, double4* tiles, cudaStream_t stream)
+{
+    if (ntiles <= 0) return;
+    k_tile_bounds<<<(ntiles + 7) / 8, 256, 0, stream>>>(b, tile_sys, ntiles, tiles);
+}
+
+void launch_coordination_number_tiled(const Batch& b, const Species& s, const Config& c, const Partition& p,
+                                      const Work& w, cudaStream_t stream)
+{
+    if (c.mixed) k_cn_tiled<float><<<blocks_for(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
+    else k_cn_tiled<double><<<blocks_for(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
+}
+
+void launch_two_body_tiled(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
+                           const Work& w, cudaStream_t stream)
+{
+    const int nb = blocks_for(b.natoms);
+    if (d.kind == kRational) {
+        if (c.mixed) k_two_body_tiled<float, kRational><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
+        else k_two_body_tiled<double, kRational><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
+    } else {
+        if (c.mixed) k_two_body_tiled<float, kZero><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
+        else k_two_body_tiled<double, kZero><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
+    }
+}
+
+void launch_cn_chain_rule_tiled(const Batch& b, const Species& s, const Config& c, const Partition& p,
+                                const Work& w, cudaStream_t stream)
+{
+    if (c.mixed) k_chain_tiled<float><<<blocks_for(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
+    else k_chain_tiled<double><<<blocks_for(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
+}
+
+}  // namespace d3
