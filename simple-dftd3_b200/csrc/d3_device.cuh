@@ -81,6 +81,10 @@ struct Work {
     // three-body results per root atom (summed by the per-system reduction)
     double* e3_atom = nullptr;   // [natoms] three-body energy of the root's triples
     double* sig3_atom = nullptr; // [natoms][kSigma] three-body virial of the root's triples
+    // dE/ds9 of the parameter derivatives: pg_s9_scale * sum of e3_pg (the
+    // three-body energy at the current s9, or at s9 = 1 when s9 vanishes)
+    const double* e3_pg = nullptr;
+    double pg_s9_scale = 0.0;
 };
 
 struct Config {

@@ -523,7 +523,23 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
         }
     }
     mark(4);
-    if (threebody) run_three_body(b, s, d, c, w, stream);
+    if (threebody) {
+        run_three_body(b, s, d, c, w, stream);
+        if (pg) {
+            w.e3_pg = w.e3_atom;
+            w.pg_s9_scale = 1.0 / d.s9;
+        }
+    } else if (pg) {
+        // dE/ds9 at s9 = 0: the three-body energy at unit s9, not added to the energy
+        Damp d1 = d;
+        d1.s9 = 1.0;
+        Config c1 = c;
+        c1.grad = false;
+        Work w1 = w;
+        run_three_body(b, s, d1, c1, w1, stream);
+        w.e3_pg = w1.e3_atom;
+        w.pg_s9_scale = 1.0;
+    }
     mark(5);
     if (grad) launch_cn_chain_rule(b, s, c, part_, w, stream);
     mark(6);

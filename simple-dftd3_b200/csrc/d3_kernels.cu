@@ -491,7 +491,8 @@ __global__ void k_reduce_systems(Batch b, Config c, Work w, double* energies, do
             for (int k = 0; k < kSigma; k++)
                 v[1 + k] += w.sig_atom[kSigma * a + k] + (w.sig3_atom ? w.sig3_atom[kSigma * a + k] : 0.0);
         if (c.param_grad && w.pg_atom)
-            for (int k = 0; k < kParamGrad; k++) v[1 + kSigma + k] += w.pg_atom[kParamGrad * a + k];
+            for (int k = 0; k < kParamGrad - 1; k++) v[1 + kSigma + k] += w.pg_atom[kParamGrad * a + k];
+        if (c.param_grad && w.e3_pg) v[kSigma + kParamGrad] += w.e3_pg[a] * w.pg_s9_scale;
         if (c.grad && grad_out) {
             const int o = b.perm ? b.perm[a] : a;
             for (int k = 0; k < 3; k++) grad_out[3 * o + k] = w.grad[3 * a + k];
