@@ -181,7 +181,7 @@ class Runner:
         self.lib.set_batch_counting(self.batch, False)
         return {"pair_terms": int(c[0]), "triple_terms": int(c[1]), "cn_terms": int(c[2])}
 
-    def time(self, precision, steps, warmup, flush, dist=None):
+    def time(self, precision, steps, warmup, flush, dist=None, stages=True):
         torch, lib = self.torch, self.lib
         lib.set_batch_precision(self.batch, lib.PRECISION_FP64 if precision == "fp64" else lib.PRECISION_MIXED)
         for _ in range(warmup):
@@ -202,6 +202,8 @@ class Runner:
             dist.barrier()
         torch.cuda.synchronize()
         ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / steps
+        if not stages:
+            return {"ms_per_step": ms, "energy": self.e.double().sum().item()}
         # per-stage device times of a few more steps (CUDA events inside the engine)
         lib.set_batch_profiling(self.batch, True)
         stages = {}
@@ -213,6 +215,42 @@ class Runner:
                 stages[kk] = stages.get(kk, 0.0) + vv / 3
         lib.set_batch_profiling(self.batch, False)
         return {"ms_per_step": ms, "stage_ms": stages, "energy": self.e.double().sum().item()}
+
+
+def batched_launch_modes(run, systems, par, flush, dist, sample=256):
+    """Batch of molecules: the whole batch as one captured graph (autotuned
+    launch shapes) against one evaluation per molecule (a sample of them)."""
+    import torch
+    lib = run.lib
+    lib.set_batch_precision(run.batch, lib.PRECISION_MIXED)
+    pos_host = run.pos.cpu().numpy()
+    tuned_ms = lib.autotune_batch(run.batch, run.param, pos_host, True)
+    out = {"autotune": dict(lib.get_batch_tuning(run.batch), best_ms=tuned_ms)}
+    lib.set_batch_graph(run.batch, True)
+    graph = {p: run.time(p, 3, 2, flush, dist, stages=False) for p in ("fp64", "mixed")}
+    lib.set_batch_graph(run.batch, False)
+    out["graph"] = {p: {"ms_per_step": graph[p]["ms_per_step"],
+                        "systems_per_s": len(systems) / (graph[p]["ms_per_step"] * 1e-3)} for p in graph}
+    out["graph"]["mixed_speedup_vs_fp64"] = graph["fp64"]["ms_per_step"] / graph["mixed"]["ms_per_step"]
+    # one batch (own engine and launch sequence) per molecule, same precision and stream
+    singles = [Runner([sy], par) for sy in systems[:sample]]
+    for r in singles:
+        lib.set_batch_precision(r.batch, lib.PRECISION_MIXED)
+        r.step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush.zero_()
+    t0.record(stream)
+    for r in singles:
+        r.step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    out["per_molecule_launches"] = {"molecules": len(singles), "ms": ms,
+                                    "systems_per_s": len(singles) / (ms * 1e-3), "precision": "mixed"}
+    del singles
+    return out
 
 
 def roofline(units, flops_per_unit, stage_ms, peak, kernel, bound):
@@ -271,6 +309,8 @@ def run_ours(args, rank, world, dist):
                                                        / abs(tx["fp64"]["energy"]))
             if name == "frames256":
                 entry["note"] = "16 of the 256 frames per step"
+            if name == "batch4096":
+                entry.update(batched_launch_modes(rx, sy, pr, flush, dist))
             extra[name] = entry
             del rx
     sampler.stop()

@@ -68,7 +68,10 @@ dftd3_b200_get_dispersion_batched(dftd3_error /* error */,
  * from host memory (NULL keeps the current ones).  param_grad[nsys][5], if
  * non-NULL, receives
  * dE/d(s6, s8, a1, a2, s9) (rational) or dE/d(s6, s8, rs6, rs8, s9) (zero).
- * The call is asynchronous with respect to the host. */
+ * Two-body evaluations are asynchronous with respect to the host.  With the
+ * three-body term the call waits for the device once: for the neighbour
+ * list sizes (ordinary sequence) or for the list capacity check at the end
+ * (captured sequence, dftd3_b200_set_batch_graph). */
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_b200_get_dispersion_device(dftd3_error /* error */,
                                  dftd3_b200_batch /* batch */,
@@ -107,6 +110,41 @@ SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_b200_get_batch_stage_times(dftd3_error /* error */,
                                  dftd3_b200_batch /* batch */,
                                  double* /* ms[7] */);
+
+/* Replay the whole pipeline of an evaluation as one captured CUDA graph
+ * (enable != 0).  The first evaluation for a parameter set, derivative set
+ * and launch shape runs the ordinary launch sequence and then captures it;
+ * later evaluations launch the graph on the caller's stream.  Inputs and
+ * outputs are staged through buffers the batch owns.  Per-stage times are
+ * not recorded for graph replays.  A replay whose three-body lists outgrow
+ * the captured buffers is detected and evaluated again without the graph. */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_set_batch_graph(dftd3_error /* error */,
+                           dftd3_b200_batch /* batch */,
+                           int /* enable */);
+
+/* Launch shapes of a batch: tuning[0] the cell of the spatial sort key
+ * (Bohr, > 0), tuning[1] atoms per block of the pair sweeps (4 or 8),
+ * tuning[2] resident three-body blocks per SM (0 = occupancy limit). */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_set_batch_tuning(dftd3_error /* error */,
+                            dftd3_b200_batch /* batch */,
+                            const double* /* tuning[3] */);
+
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_get_batch_tuning(dftd3_error /* error */,
+                            dftd3_b200_batch /* batch */,
+                            double* /* tuning[3] */);
+
+/* Autotuner: time the candidate launch shapes on these positions (host,
+ * [sum natoms][3], wrapped like dftd3_b200_get_dispersion_batched) with the
+ * gradient on or off, keep the fastest shape and return its time in ms. */
+SDFTD3_API_ENTRY double SDFTD3_API_CALL
+dftd3_b200_autotune_batch(dftd3_error /* error */,
+                          dftd3_b200_batch /* batch */,
+                          dftd3_param /* param */,
+                          const double* /* positions */,
+                          int /* gradient */);
 
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_b200_delete_batch(dftd3_b200_batch* /* batch */);

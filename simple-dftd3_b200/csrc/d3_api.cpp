@@ -640,6 +640,83 @@ double dftd3_b200_fma_peak(dftd3_error error, int precision)
     return v;
 }
 
+void dftd3_b200_set_batch_graph(dftd3_error error, dftd3_b200_batch batch, int enable)
+{
+    if (!error) return;
+    if (!batch) {
+        fail(error, "Batch is missing");
+        return;
+    }
+    guarded(error, [&] { batch->engine->set_graph(enable != 0); });
+}
+
+void dftd3_b200_set_batch_tuning(dftd3_error error, dftd3_b200_batch batch, const double* tuning)
+{
+    if (!error) return;
+    if (!batch || !tuning) {
+        fail(error, "Batch is missing");
+        return;
+    }
+    guarded(error, [&] {
+        d3::Tuning t;
+        t.morton_cell = tuning[0];
+        t.pair_warps = (int)tuning[1];
+        t.atm_blocks_per_sm = (int)tuning[2];
+        if ((double)t.pair_warps != tuning[1] || (double)t.atm_blocks_per_sm != tuning[2])
+            throw d3::Error("Launch shape counts must be integers");
+        batch->engine->set_tuning(t);
+    });
+}
+
+void dftd3_b200_get_batch_tuning(dftd3_error error, dftd3_b200_batch batch, double* tuning)
+{
+    if (!error) return;
+    if (!batch || !tuning) {
+        fail(error, "Batch is missing");
+        return;
+    }
+    const d3::Tuning& t = batch->engine->tuning();
+    tuning[0] = t.morton_cell;
+    tuning[1] = t.pair_warps;
+    tuning[2] = t.atm_blocks_per_sm;
+}
+
+double dftd3_b200_autotune_batch(dftd3_error error, dftd3_b200_batch batch, dftd3_param param,
+                                 const double* positions, int gradient)
+{
+    if (!error) return 0.0;
+    if (!batch) {
+        fail(error, "Batch is missing");
+        return 0.0;
+    }
+    if (!param) {
+        fail(error, "Damping parameters are missing");
+        return 0.0;
+    }
+    if (!positions) {
+        fail(error, "Invalid batch buffers");
+        return 0.0;
+    }
+    double ms = 0.0;
+    guarded(error, [&] {
+        d3::Engine& eng = *batch->engine;
+        const int n = eng.natoms();
+        batch->wrapped.assign(positions, positions + 3 * (size_t)n);
+        if (!finite_all(batch->wrapped.data(), batch->wrapped.size())) throw d3::Error("Non-finite atomic positions");
+        for (int s = 0; s < eng.nsys(); s++) {
+            const int a0 = eng.atom_off()[s], a1 = eng.atom_off()[s + 1];
+            d3::wrap_to_central_cell(a1 - a0, batch->wrapped.data() + 3 * a0, eng.lattice(s), eng.periodic(s));
+        }
+        double* d_pos = eng.input_buffer();
+        cudaStream_t st = eng.stream();
+        if (cudaMemcpyAsync(d_pos, batch->wrapped.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess)
+            throw d3::Error("CUDA error in autotune upload");
+        ms = eng.autotune(param->damp, d_pos, gradient != 0, st);
+    });
+    return ms;
+}
+
 void dftd3_b200_delete_batch(dftd3_b200_batch* batch)
 {
     if (batch && *batch) {

@@ -37,7 +37,6 @@ constexpr int kTA = 32;          // j-entries per tile
 constexpr int kTB = 64;          // k-entries per tile
 constexpr int kThreadsAtm = 256; // 16 x 16
 constexpr int kAcc = 5;          // per-entry accumulators: S, Gx, Gy, Gz, dE/dCN of the partner
-constexpr double kRs9 = 4.0 / 3.0;
 
 // ------------------------------------------------------------ C6 matrix ----
 
@@ -117,13 +116,18 @@ __global__ void k_nbr_count(Batch b, Config c, int* cnt, int* max_cnt)
     }
 }
 
+__global__ void k_atm_guard(const long long* total, const int* max_cnt, long long cap, int stride, int* guard)
+{
+    *guard = (*total > cap || *max_cnt > stride) ? 1 : 0;
+}
+
 // Entries of root i in (j, T) order.  vec = (x_j + T) - x_i as in atm.f90:718.
 __global__ void k_nbr_fill(Batch b, Config c, const long long* off, int* nbr_j, int* nbr_gend,
-                           double4* nbr_v)
+                           double4* nbr_v, const int* guard)
 {
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= b.natoms) return;
+    if (i >= b.natoms || *guard) return;
     const int sys = b.sys_of_atom[i];
     const int j0 = b.atom_off[sys];
     const int t0 = b.img_off[kImgDisp3 * (b.nsys + 1) + sys], t1 = b.img_off[kImgDisp3 * (b.nsys + 1) + sys + 1];
@@ -256,6 +260,7 @@ __global__ void __launch_bounds__(kThreadsAtm, sizeof(R) == 4 ? 3 : 1) k_triples
     const R cut2 = R(c.cut3 * c.cut3);
     const bool smooth_on = c.width3 > 0.0 && c.width3 < c.cut3;
     const R cutoff = R(c.cut3), width = R(c.width3);
+    if (w.atm_guard && *w.atm_guard) return;   // lists did not fit the reserved buffers
     const bool table_r0 = b.nid <= kMaxSpeciesFast;
     if (table_r0)
         for (int k = tid; k < b.nid * b.nid; k += kThreadsAtm) slr0[k] = rlog<R>(R(__ldg(sp.atm_r0 + k)));
@@ -564,11 +569,17 @@ void launch_scan(void* temp, size_t temp_bytes, const int* cnt_ext, long long* o
     cub::DeviceScan::ExclusiveSum(temp, temp_bytes, cnt_ext, off, n + 1, stream);
 }
 
+void launch_atm_guard(const long long* total, const int* max_cnt, long long cap, int stride, int* guard,
+                      cudaStream_t stream)
+{
+    k_atm_guard<<<1, 1, 0, stream>>>(total, max_cnt, cap, stride, guard);
+}
+
 void launch_nbr_fill(const Batch& b, const Config& c, const long long* off, int* nbr_j, int* nbr_gend,
-                     double4* nbr_v, cudaStream_t stream)
+                     double4* nbr_v, const int* guard, cudaStream_t stream)
 {
     if (b.natoms <= 0) return;
-    k_nbr_fill<<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, c, off, nbr_j, nbr_gend, nbr_v);
+    k_nbr_fill<<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, c, off, nbr_j, nbr_gend, nbr_v, guard);
 }
 
 template <class R>

@@ -85,6 +85,10 @@ struct Work {
     // three-body energy at the current s9, or at s9 = 1 when s9 vanishes)
     const double* e3_pg = nullptr;
     double pg_s9_scale = 0.0;
+    // capacity guard of the three-body lists: set when the neighbour entries
+    // exceed the reserved buffers (captured launch sequences); the list fill
+    // and the triple sum then skip their work
+    int* atm_guard = nullptr;
 };
 
 struct Config {
@@ -93,6 +97,14 @@ struct Config {
     bool mixed = false;
     bool param_grad = false;
     bool cn_partitioned = false;   // partition the CN and chain-rule loops too
+    int pair_warps = 8;            // atoms (warps) per block of the culled pair sweeps: 4 or 8
+};
+
+// Launch-shape choices of one batch, picked by the autotuner or set by hand.
+struct Tuning {
+    double morton_cell = 3.0;      // Bohr; quantisation of the spatial sort key
+    int pair_warps = 8;            // atoms per block of the pair sweeps (4 or 8)
+    int atm_blocks_per_sm = 0;     // resident triple-sum blocks per SM; 0 = occupancy limit
 };
 
 // FMA throughput of the FP64 (fp64=true) or FP32 pipe in TFLOP/s (blocking).
@@ -109,9 +121,9 @@ void launch_two_body(const Batch& b, const Species& s, const Damp& d, const Conf
                      const Partition& p, const Work& w, cudaStream_t stream);
 // Spatial ordering and tile bounds (d3_pair.cu).
 size_t sort_temp_bytes(int natoms);
-void launch_spatial_sort(const double* pos, int natoms, const int* sys_of_atom, unsigned long long* keys_in,
-                         unsigned long long* keys_out, int* idx_in, int* perm, void* temp, size_t temp_bytes,
-                         cudaStream_t stream);
+void launch_spatial_sort(const double* pos, int natoms, const int* sys_of_atom, double cell,
+                         unsigned long long* keys_in, unsigned long long* keys_out, int* idx_in, int* perm,
+                         void* temp, size_t temp_bytes, cudaStream_t stream);
 void launch_gather_sorted(const double* pos, const int* perm, const int* sp_in, const uint8_t* ghost_in,
                           const int* sys_of_atom, const int* atom_off, int natoms, double* x, double* y,
                           double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost, int* local, bool mixed,
@@ -134,8 +146,12 @@ void launch_nbr_count(const Batch& b, const Config& c, int* cnt, int* max_cnt, c
 size_t scan_temp_bytes(int n);
 void launch_scan(void* temp, size_t temp_bytes, const int* cnt_ext, long long* off, int n,
                  cudaStream_t stream);
+// Sets *guard when off[natoms] (the entry total) exceeds cap or the longest
+// list exceeds stride; the fill and triple kernels then return at once.
+void launch_atm_guard(const long long* total, const int* max_cnt, long long cap, int stride, int* guard,
+                      cudaStream_t stream);
 void launch_nbr_fill(const Batch& b, const Config& c, const long long* off, int* nbr_j, int* nbr_gend,
-                     double4* nbr_v, cudaStream_t stream);
+                     double4* nbr_v, const int* guard, cudaStream_t stream);
 int atm_blocks_per_sm(bool mixed, bool grad);
 size_t atm_slot_bytes(bool mixed);
 void launch_triples(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,

@@ -179,6 +179,7 @@ T* Engine::dev_alloc(size_t n)
     if (n == 0) n = 1;
     check(cudaMalloc(&p, n * sizeof(T)), "cudaMalloc");
     allocations_.push_back(p);
+    alloc_epoch_++;   // captured graphs hold device pointers
     return static_cast<T*>(p);
 }
 
@@ -213,6 +214,7 @@ Engine::Engine(int nsys, const int* natoms, const int* numbers, const double* la
     ghost_.assign(natoms_, 0);
 
     check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_), "attribute");
     const int nid = tab_.nid();
     d_sys_of_atom_ = dev_alloc<int>(natoms_);
     d_atom_off_ = dev_alloc<int>(nsys + 1);
@@ -274,9 +276,11 @@ Engine::~Engine()
     if (stream_) cudaStreamSynchronize(stream_);
     for (auto& e : ev_)
         if (e) cudaEventDestroy(e);
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     for (void* p : allocations_) cudaFree(p);
     if (h_stage_) cudaFreeHost(h_stage_);
     if (h_atm_counts_) cudaFreeHost(h_atm_counts_);
+    if (h_guard_) cudaFreeHost(h_guard_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -385,6 +389,7 @@ void Engine::ensure_images(cudaStream_t stream)
             auto it = std::find(allocations_.begin(), allocations_.end(), (void*)d_img_);
             if (it != allocations_.end()) allocations_.erase(it);
             check(cudaFree(d_img_), "cudaFree");
+            alloc_epoch_++;
         }
         img_capacity_ = all.size() + all.size() / 4 + 3;
         d_img_ = dev_alloc<double>(img_capacity_);
@@ -429,7 +434,12 @@ void Engine::ensure_workspace(bool grad, bool param_grad, bool threebody)
     }
     if (param_grad && !ws_pg_) {
         work_.pg_atom = dev_alloc<double>(kParamGrad * (size_t)natoms_);
+        d_pg_out_ = dev_alloc<double>(kParamGrad * (size_t)nsys_);
         ws_pg_ = true;
+    }
+    if (!h_guard_) {
+        check(cudaMallocHost(&h_guard_, sizeof(int)), "cudaMallocHost");
+        *h_guard_ = 0;
     }
     (void)grad;
     (void)threebody;
@@ -489,6 +499,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     c.cut_cn = cut_.cn; c.cut2 = cut_.disp2; c.cut3 = cut_.disp3;
     c.width2 = cut_.width2; c.width3 = cut_.width3;
     c.grad = grad; c.mixed = mixed_; c.param_grad = pg; c.cn_partitioned = cn_partitioned_;
+    c.pair_warps = tune_.pair_warps;
     Work w = work_;
     w.counts = counting_ ? d_counts_ : nullptr;
     w.e3_atom = nullptr;
@@ -496,14 +507,15 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     if (!pg) w.pg_atom = nullptr;
     if (counting_) check(cudaMemsetAsync(d_counts_, 0, 3 * sizeof(unsigned long long), stream), "counts");
 
+    const bool timed = profiling_ && !capturing_;
     auto mark = [&](int k) {
-        if (profiling_) check(cudaEventRecord(ev_[k], stream), "cudaEventRecord");
+        if (timed) check(cudaEventRecord(ev_[k], stream), "cudaEventRecord");
     };
-    if (profiling_ && !ev_[0])
+    if (timed && !ev_[0])
         for (auto& e : ev_) check(cudaEventCreate(&e), "cudaEventCreate");
     mark(0);
-    launch_spatial_sort(d_positions, natoms_, d_sys_of_atom_, d_keys_in_, d_keys_out_, d_idx_in_, d_perm_,
-                        d_sort_temp_, sort_bytes_, stream);
+    launch_spatial_sort(d_positions, natoms_, d_sys_of_atom_, tune_.morton_cell, d_keys_in_, d_keys_out_, d_idx_in_,
+                        d_perm_, d_sort_temp_, sort_bytes_, stream);
     launch_gather_sorted(d_positions, d_perm_, d_sp_, d_ghost_, d_sys_of_atom_, d_atom_off_, natoms_, d_x_, d_y_,
                          d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed_, stream);
     launch_tile_bounds(b, d_tile_sys_, ntiles_, d_tiles_, stream);
@@ -545,7 +557,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     mark(6);
     launch_reduce_systems(b, c, w, d_energies, d_sigma9, d_param_grad, d_gradient, stream);
     mark(7);
-    ev_recorded_ = profiling_;
+    if (!capturing_) ev_recorded_ = profiling_;
     check(cudaGetLastError(), "kernel launch");
 }
 
@@ -555,6 +567,7 @@ void Engine::free_block(void*& p)
     auto it = std::find(allocations_.begin(), allocations_.end(), p);
     if (it != allocations_.end()) allocations_.erase(it);
     check(cudaFree(p), "cudaFree");
+    alloc_epoch_++;
     p = nullptr;
 }
 
@@ -577,6 +590,8 @@ void Engine::run_three_body(const Batch& b, const Species& s, const Damp& d, con
         scan_bytes_ = scan_temp_bytes(n);
         d_scan_temp_ = dev_alloc<unsigned char>(scan_bytes_);
         check(cudaMallocHost(&h_atm_counts_, 2 * sizeof(long long)), "cudaMallocHost");
+        d_guard_ = dev_alloc<int>(1);
+        check(cudaMemsetAsync(d_guard_, 0, sizeof(int), stream), "memset");
         atm_ready_ = true;
     }
     launch_c6_matrix(b, s, w, d_c6mat_off_, d_c6mat_, c6mat_total_, c.mixed, stream);
@@ -584,41 +599,50 @@ void Engine::run_three_body(const Batch& b, const Species& s, const Damp& d, con
     check(cudaMemsetAsync(d_cnt_ + n, 0, sizeof(int), stream), "memset");
     launch_nbr_count(b, c, d_cnt_, d_maxcnt_, stream);
     launch_scan(d_scan_temp_, scan_bytes_, d_cnt_, d_off_, n, stream);
-    check(cudaMemcpyAsync(h_atm_counts_, d_off_ + n, sizeof(long long), cudaMemcpyDeviceToHost, stream), "total");
-    check(cudaMemcpyAsync(h_atm_counts_ + 1, d_maxcnt_, sizeof(int), cudaMemcpyDeviceToHost, stream), "max");
-    check(cudaStreamSynchronize(stream), "neighbour count");
-    const long long total = h_atm_counts_[0];
-    const int maxcnt = (int)(reinterpret_cast<int*>(h_atm_counts_ + 1)[0]);
-    last_triples_entries_ = total;
-    if (total > nbr_cap_) {
-        void* pj = d_nbr_j_; void* pg = d_nbr_gend_; void* pv = d_nbr_v_;
-        free_block(pj); free_block(pg); free_block(pv);
-        nbr_cap_ = total + total / 4 + 1024;
-        d_nbr_j_ = dev_alloc<int>(nbr_cap_);
-        d_nbr_gend_ = dev_alloc<int>(nbr_cap_);
-        d_nbr_v_ = dev_alloc<double4>(nbr_cap_);
+    const int blocks = std::max(1, std::min(n, sms_ * atm_blocks(c.mixed, c.grad)));
+    int stride = atm_stride_;
+    if (!capturing_) {
+        check(cudaMemcpyAsync(h_atm_counts_, d_off_ + n, sizeof(long long), cudaMemcpyDeviceToHost, stream), "total");
+        check(cudaMemcpyAsync(h_atm_counts_ + 1, d_maxcnt_, sizeof(int), cudaMemcpyDeviceToHost, stream), "max");
+        check(cudaStreamSynchronize(stream), "neighbour count");
+        const long long total = h_atm_counts_[0];
+        const int maxcnt = (int)(reinterpret_cast<int*>(h_atm_counts_ + 1)[0]);
+        last_triples_entries_ = total;
+        if (total > nbr_cap_) {
+            void* pj = d_nbr_j_; void* pgd = d_nbr_gend_; void* pv = d_nbr_v_;
+            free_block(pj); free_block(pgd); free_block(pv);
+            nbr_cap_ = total + total / 4 + 1024;
+            d_nbr_j_ = dev_alloc<int>(nbr_cap_);
+            d_nbr_gend_ = dev_alloc<int>(nbr_cap_);
+            d_nbr_v_ = dev_alloc<double4>(nbr_cap_);
+        }
+        // a captured sequence keeps the list length it was captured with: reserve headroom
+        stride = std::max(maxcnt, 1);
+        if (graph_on_) {
+            if (maxcnt > atm_stride_) atm_stride_ = maxcnt + maxcnt / 4 + 32;
+            stride = atm_stride_;
+        }
+        // the slot buffers are sized for the largest resident grid (one block per SM and unit of occupancy)
+        const long long grid = (long long)sms_ * std::max(atm_occupancy(c.mixed, true), atm_occupancy(c.mixed, false));
+        const long long need = grid * stride * 8;   // per-entry accumulators (up to 8 doubles)
+        if (need > slot_cap_) {
+            void* p = d_slot_acc_;
+            free_block(p);
+            slot_cap_ = need + need / 4;
+            d_slot_acc_ = dev_alloc<double>(slot_cap_);
+        }
+        const long long scr_need = grid * stride * (long long)atm_slot_bytes(false);
+        if (scr_need > slot_scr_cap_) {
+            void* p = d_slot_scr_;
+            free_block(p);
+            slot_scr_cap_ = scr_need + scr_need / 4;
+            d_slot_scr_ = dev_alloc<unsigned char>(slot_scr_cap_);
+        }
     }
-    int dev = 0, sms = 0;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
-    const int blocks = std::max(1, std::min(n, sms * atm_blocks_per_sm(c.mixed, c.grad)));
-    const int stride = std::max(maxcnt, 1);
-    const long long need = (long long)blocks * stride * 8;   // per-entry accumulators (up to 8 doubles)
-    if (need > slot_cap_) {
-        void* p = d_slot_acc_;
-        free_block(p);
-        slot_cap_ = need + need / 4;
-        d_slot_acc_ = dev_alloc<double>(slot_cap_);
-    }
-    const long long scr_need = (long long)blocks * stride * (long long)atm_slot_bytes(false);
-    if (scr_need > slot_scr_cap_) {
-        void* p = d_slot_scr_;
-        free_block(p);
-        slot_scr_cap_ = scr_need + scr_need / 4;
-        d_slot_scr_ = dev_alloc<unsigned char>(slot_scr_cap_);
-    }
-    launch_nbr_fill(b, c, d_off_, d_nbr_j_, d_nbr_gend_, d_nbr_v_, stream);
+    launch_atm_guard(d_off_ + n, d_maxcnt_, nbr_cap_, stride, d_guard_, stream);
+    launch_nbr_fill(b, c, d_off_, d_nbr_j_, d_nbr_gend_, d_nbr_v_, d_guard_, stream);
     check(cudaMemsetAsync(d_queue_, 0, sizeof(unsigned int), stream), "memset");
+    w.atm_guard = d_guard_;
     launch_triples(b, s, d, c, part_, w, d_c6mat_, d_c6mat_off_, d_off_, d_cnt_, d_nbr_j_, d_nbr_gend_, d_nbr_v_,
                    d_queue_, d_slot_acc_, d_slot_scr_, stride, blocks, d_e3_, d_sig3_, stream);
     w.e3_atom = d_e3_;
@@ -635,6 +659,184 @@ void Engine::stage_times(double out[kStages])
         check(cudaEventElapsedTime(&ms, ev_[k], ev_[k + 1]), "cudaEventElapsedTime");
         out[k] = ms;
     }
+}
+
+int Engine::atm_occupancy(bool mixed, bool grad)
+{
+    int& occ = atm_occ_[mixed ? 1 : 0][grad ? 1 : 0];
+    if (occ == 0) occ = atm_blocks_per_sm(mixed, grad);
+    return occ;
+}
+
+int Engine::atm_blocks(bool mixed, bool grad)
+{
+    const int occ = atm_occupancy(mixed, grad);
+    return tune_.atm_blocks_per_sm > 0 ? std::min(tune_.atm_blocks_per_sm, occ) : occ;
+}
+
+// ------------------------------------------------------------------ graph --
+
+void Engine::drop_graph()
+{
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    graph_exec_ = nullptr;
+    graph_valid_ = false;
+}
+
+void Engine::set_graph(bool on)
+{
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    if (!on) drop_graph();
+    graph_on_ = on;
+}
+
+void Engine::set_tuning(const Tuning& t)
+{
+    if (t.pair_warps != 4 && t.pair_warps != 8) throw Error("Atoms per pair block must be 4 or 8");
+    if (!(t.morton_cell > 0.0) || !std::isfinite(t.morton_cell)) throw Error("Sort cell must be positive");
+    if (t.atm_blocks_per_sm < 0) throw Error("Three-body blocks per SM must not be negative");
+    tune_ = t;
+    graph_valid_ = false;
+}
+
+Engine::GraphKey Engine::make_key(const Damp& d, bool grad, bool pg) const
+{
+    GraphKey k;
+    std::memset(&k, 0, sizeof(k));   // the key is compared bytewise
+    k.damp = d;
+    k.cut = cut_;
+    k.part = part_;
+    k.tune = tune_;
+    k.grad = grad; k.pg = pg; k.counting = counting_; k.mixed = mixed_; k.cn_part = cn_partitioned_;
+    return k;
+}
+
+void Engine::capture(const Damp& d, const GraphKey& key, bool grad, bool pg)
+{
+    cudaGraph_t g = nullptr;
+    capturing_ = true;
+    check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    try {
+        run(d, d_pos_in_, d_energies_, grad ? d_grad_out_ : nullptr, grad ? d_sigma_ : nullptr,
+            pg ? d_pg_out_ : nullptr, grad, stream_);
+    } catch (...) {
+        cudaStreamEndCapture(stream_, &g);
+        if (g) cudaGraphDestroy(g);
+        capturing_ = false;
+        throw;
+    }
+    capturing_ = false;
+    check(cudaStreamEndCapture(stream_, &g), "cudaStreamEndCapture");
+    bool updated = false;
+    if (graph_exec_) {
+        cudaGraphExecUpdateResultInfo info;
+        updated = cudaGraphExecUpdate(graph_exec_, g, &info) == cudaSuccess;
+        if (!updated) {
+            (void)cudaGetLastError();
+            drop_graph();
+        }
+    }
+    if (!updated) {
+        const cudaError_t e = cudaGraphInstantiate(&graph_exec_, g, 0);
+        cudaGraphDestroy(g);
+        check(e, "cudaGraphInstantiate");
+    } else {
+        cudaGraphDestroy(g);
+    }
+    graph_key_ = key;
+    graph_epoch_ = alloc_epoch_;
+    graph_valid_ = true;
+}
+
+void Engine::run_graphed(const Damp& d, bool grad, bool pg, cudaStream_t stream)
+{
+    ensure_images(stream);
+    ensure_workspace(grad, pg, false);
+    upload_pair_table(d, stream);
+    const GraphKey key = make_key(d, grad, pg);
+    const bool threebody = std::fabs(d.s9) >= DBL_EPSILON || pg;
+    if (graph_valid_ && graph_epoch_ == alloc_epoch_ && std::memcmp(&key, &graph_key_, sizeof(key)) == 0) {
+        check(cudaGraphLaunch(graph_exec_, stream), "cudaGraphLaunch");
+        if (!threebody) return;
+        // the three-body lists must have fitted the buffers the graph was captured with
+        check(cudaMemcpyAsync(h_guard_, d_guard_, sizeof(int), cudaMemcpyDeviceToHost, stream), "guard");
+        check(cudaStreamSynchronize(stream), "graph");
+        if (*h_guard_ == 0) return;
+        graph_valid_ = false;
+    }
+    // ordinary evaluation: this call's results, and the list sizes for the capture
+    run(d, d_pos_in_, d_energies_, grad ? d_grad_out_ : nullptr, grad ? d_sigma_ : nullptr, pg ? d_pg_out_ : nullptr,
+        grad, stream);
+    // the capture records work on the engine stream; it must not overlap buffers still in use
+    check(cudaStreamSynchronize(stream), "evaluation");
+    capture(d, key, grad, pg);
+}
+
+double* Engine::input_buffer()
+{
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    ensure_workspace(true, false, false);
+    return d_pos_in_;
+}
+
+double Engine::autotune(const Damp& d, const double* d_positions, bool grad, cudaStream_t stream)
+{
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    ensure_workspace(grad, false, false);
+    const bool threebody = std::fabs(d.s9) >= DBL_EPSILON;
+    cudaEvent_t e0, e1;
+    check(cudaEventCreate(&e0), "cudaEventCreate");
+    check(cudaEventCreate(&e1), "cudaEventCreate");
+    const bool prof = profiling_;
+    profiling_ = false;
+    auto time_once = [&]() {
+        // one run to size the buffers of this shape, then the faster of two timed runs
+        double best = 1e30;
+        for (int rep = 0; rep < 3; rep++) {
+            check(cudaEventRecord(e0, stream), "cudaEventRecord");
+            run(d, d_positions, d_energies_, grad ? d_grad_out_ : nullptr, grad ? d_sigma_ : nullptr, nullptr, grad,
+                stream);
+            check(cudaEventRecord(e1, stream), "cudaEventRecord");
+            check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+            float ms = 0.f;
+            check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+            if (rep > 0) best = std::min(best, (double)ms);
+        }
+        return best;
+    };
+    Tuning best = tune_;
+    double best_ms = 0.0;
+    try {
+        best_ms = time_once();
+        auto consider = [&](Tuning t) {
+            tune_ = t;
+            const double ms = time_once();
+            if (ms < best_ms) { best_ms = ms; best = t; }
+            tune_ = best;
+        };
+        for (double cell : {2.0, 3.0, 4.5, 6.0})
+            if (cell != best.morton_cell) { Tuning t = best; t.morton_cell = cell; consider(t); }
+        for (int pw : {4, 8})
+            if (pw != best.pair_warps) { Tuning t = best; t.pair_warps = pw; consider(t); }
+        if (threebody) {
+            const int occ = atm_occupancy(mixed_, grad);
+            const int cur = best.atm_blocks_per_sm > 0 ? std::min(best.atm_blocks_per_sm, occ) : occ;
+            for (int bps = 1; bps <= occ; bps++)
+                if (bps != cur) { Tuning t = best; t.atm_blocks_per_sm = bps; consider(t); }
+        }
+    } catch (...) {
+        tune_ = best;
+        profiling_ = prof;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    tune_ = best;
+    profiling_ = prof;
+    graph_valid_ = false;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best_ms;
 }
 
 void Engine::evaluate_host(const Damp& d, const double* positions, double* energies, double* gradient,
@@ -656,7 +858,8 @@ void Engine::evaluate_host(const Damp& d, const double* positions, double* energ
     double* hs = hg + 3 * (size_t)natoms_;
     std::memcpy(hin, positions, sizeof(double) * nin);
     check(cudaMemcpyAsync(d_pos_in_, hin, sizeof(double) * nin, cudaMemcpyHostToDevice, stream_), "positions");
-    run(d, d_pos_in_, d_energies_, grad ? d_grad_out_ : nullptr, grad ? d_sigma_ : nullptr, nullptr, grad, stream_);
+    if (graph_on_) run_graphed(d, grad, false, stream_);
+    else run(d, d_pos_in_, d_energies_, grad ? d_grad_out_ : nullptr, grad ? d_sigma_ : nullptr, nullptr, grad, stream_);
     check(cudaMemcpyAsync(he, d_energies_, sizeof(double) * nsys_, cudaMemcpyDeviceToHost, stream_), "energies");
     if (grad) {
         check(cudaMemcpyAsync(hg, d_grad_out_, sizeof(double) * 3 * natoms_, cudaMemcpyDeviceToHost, stream_), "gradient");
@@ -674,7 +877,24 @@ void Engine::evaluate_device(const Damp& d, const double* d_positions, double* d
 {
     check(cudaSetDevice(device_), "cudaSetDevice");
     const bool grad = d_gradient != nullptr || d_sigma9 != nullptr;
-    run(d, d_positions, d_energies, d_gradient, d_sigma9, d_param_grad, grad, stream);
+    if (!graph_on_) {
+        run(d, d_positions, d_energies, d_gradient, d_sigma9, d_param_grad, grad, stream);
+        return;
+    }
+    // the graph reads and writes engine-owned buffers
+    const bool pg = d_param_grad != nullptr;
+    ensure_workspace(grad, pg, false);
+    const size_t n3 = 3 * (size_t)natoms_;
+    check(cudaMemcpyAsync(d_pos_in_, d_positions, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream), "positions");
+    run_graphed(d, grad, pg, stream);
+    check(cudaMemcpyAsync(d_energies, d_energies_, sizeof(double) * nsys_, cudaMemcpyDeviceToDevice, stream), "energies");
+    if (d_gradient)
+        check(cudaMemcpyAsync(d_gradient, d_grad_out_, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream), "gradient");
+    if (d_sigma9)
+        check(cudaMemcpyAsync(d_sigma9, d_sigma_, sizeof(double) * 9 * nsys_, cudaMemcpyDeviceToDevice, stream), "sigma");
+    if (pg)
+        check(cudaMemcpyAsync(d_param_grad, d_pg_out_, sizeof(double) * kParamGrad * nsys_, cudaMemcpyDeviceToDevice,
+                              stream), "parameter derivatives");
 }
 
 }  // namespace d3

@@ -82,6 +82,26 @@ public:
 
     cudaStream_t stream() const { return stream_; }
 
+    // Captured launch sequence.  With the graph on, an evaluation replays one
+    // CUDA graph of the whole pipeline (sort, CN, weights, two-body, three-body
+    // lists and sum, chain rule, reductions) from engine-owned input/output
+    // buffers.  The first evaluation of a (parameters, derivatives, tuning)
+    // key runs the ordinary sequence, which sizes the three-body lists, and
+    // then captures the graph with 25% headroom on those buffers; a replay
+    // whose lists outgrow them is detected by a device flag and evaluated
+    // again without the graph, and the graph is captured anew.
+    void set_graph(bool on);
+    bool graph() const { return graph_on_; }
+
+    // Launch shapes (spatial sort cell, atoms per pair block, resident triple
+    // blocks per SM).  autotune() times the candidates on the given device
+    // positions and keeps the fastest; it returns that time in ms.
+    void set_tuning(const Tuning& t);
+    const Tuning& tuning() const { return tune_; }
+    double autotune(const Damp& d, const double* d_positions, bool grad, cudaStream_t stream);
+    // Device buffer of natoms x 3 positions owned by the engine (autotune input).
+    double* input_buffer();
+
     // Per-stage device times of the last evaluation (ms), recorded with CUDA
     // events when profiling is on.  Stages: see kStageNames.
     static constexpr int kStages = 7;
@@ -96,6 +116,32 @@ private:
     void run(const Damp& d, const double* d_positions, double* d_energies, double* d_gradient,
              double* d_sigma9, double* d_param_grad, bool grad, cudaStream_t stream);
     template <class T> T* dev_alloc(size_t n);
+
+    // graph state
+    struct GraphKey {
+        Damp damp;
+        Cutoffs cut;
+        Partition part;
+        Tuning tune;
+        int grad, pg, counting, mixed, cn_part;
+    };
+    GraphKey make_key(const Damp& d, bool grad, bool pg) const;
+    void run_graphed(const Damp& d, bool grad, bool pg, cudaStream_t stream);
+    void capture(const Damp& d, const GraphKey& key, bool grad, bool pg);
+    void drop_graph();
+    int atm_blocks(bool mixed, bool grad);      // resident triple blocks per SM (tuned)
+    int atm_occupancy(bool mixed, bool grad);   // occupancy limit
+    bool graph_on_ = false, capturing_ = false, graph_valid_ = false;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    GraphKey graph_key_{};
+    unsigned long long alloc_epoch_ = 0, graph_epoch_ = 0;
+    int* d_guard_ = nullptr;
+    int* h_guard_ = nullptr;     // pinned
+    int atm_stride_ = 0;         // reserved per-root list length of captured three-body sums
+    double* d_pg_out_ = nullptr;
+    Tuning tune_;
+    int sms_ = 0;
+    int atm_occ_[2][2] = {{0, 0}, {0, 0}};
 
     int device_ = 0;
     int nsys_ = 0, natoms_ = 0, max_sys_atoms_ = 0;

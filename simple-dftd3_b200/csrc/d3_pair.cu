@@ -26,8 +26,6 @@ namespace d3 {
 
 namespace {
 
-constexpr int kWarps = 8;
-constexpr int kThreads = 32 * kWarps;
 constexpr int kChunk = 128;            // translations staged per pass (4 ballot words)
 constexpr double kKcn = 16.0;          // ncoord.f90:31
 
@@ -149,13 +147,13 @@ __device__ __forceinline__ Range range_of(const Batch& b, int i, int kind)
 
 // ----------------------------------------------------- coordination number --
 
-template <class R>
-__global__ void __launch_bounds__(kThreads) k_cn_tiled(Batch b, Species s, Config c, Partition p, Work w)
+template <int W, class R>
+__global__ void __launch_bounds__(32 * W, 16 / W) k_cn_tiled(Batch b, Species s, Config c, Partition p, Work w)
 {
     using Sh = typename ShOf<R>::type;
-    __shared__ Sh sbuf[kWarps][kChunk];
+    __shared__ Sh sbuf[W][kChunk];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int i = blockIdx.x * kWarps + wib;
+    const int i = blockIdx.x * W + wib;
     if (i >= b.natoms) return;
     const Range rg = range_of(b, i, kImgCN);
     const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
@@ -215,16 +213,16 @@ __global__ void __launch_bounds__(kThreads) k_cn_tiled(Batch b, Species s, Confi
 
 // ---------------------------------------------------------------- two-body --
 
-template <class R, int DAMP>
-__global__ void __launch_bounds__(kThreads) k_two_body_tiled(Batch b, Species s, Damp d, Config c, Partition p,
+template <int W, class R, int DAMP>
+__global__ void __launch_bounds__(32 * W, 16 / W) k_two_body_tiled(Batch b, Species s, Damp d, Config c, Partition p,
                                                              Work w)
 {
     using Sh = typename ShOf<R>::type;
-    __shared__ Sh sbuf[kWarps][kChunk];
-    __shared__ R su[kWarps][kMaxSpeciesFast][kMaxRef];
-    __shared__ R sdu[kWarps][kMaxSpeciesFast][kMaxRef];
+    __shared__ Sh sbuf[W][kChunk];
+    __shared__ R su[W][kMaxSpeciesFast][kMaxRef];
+    __shared__ R sdu[W][kMaxSpeciesFast][kMaxRef];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int i = blockIdx.x * kWarps + wib;
+    const int i = blockIdx.x * W + wib;
     if (i >= b.natoms) return;
     const Range rg = range_of(b, i, kImgDisp2);
     const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
@@ -424,13 +422,13 @@ __global__ void __launch_bounds__(kThreads) k_two_body_tiled(Batch b, Species s,
 
 // ------------------------------------------------------------- chain rule --
 
-template <class R>
-__global__ void __launch_bounds__(kThreads) k_chain_tiled(Batch b, Species s, Config c, Partition p, Work w)
+template <int W, class R>
+__global__ void __launch_bounds__(32 * W, 16 / W) k_chain_tiled(Batch b, Species s, Config c, Partition p, Work w)
 {
     using Sh = typename ShOf<R>::type;
-    __shared__ Sh sbuf[kWarps][kChunk];
+    __shared__ Sh sbuf[W][kChunk];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int i = blockIdx.x * kWarps + wib;
+    const int i = blockIdx.x * W + wib;
     if (i >= b.natoms) return;
     const Range rg = range_of(b, i, kImgCN);
     const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
@@ -522,15 +520,15 @@ __device__ __forceinline__ unsigned long long spread3(unsigned v)
 }
 
 // Sort key: system index above a 30-bit Morton code of the position
-// quantised to 3 Bohr cells.
-__global__ void k_morton(const double* __restrict__ pos, int n, const int* sys_of_atom,
+// quantised to cells of `cell` Bohr.
+__global__ void k_morton(const double* __restrict__ pos, int n, const int* sys_of_atom, double inv_cell,
                          unsigned long long* keys, int* idx)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= n) return;
     unsigned q[3];
     for (int c = 0; c < 3; c++) {
-        double f = floor(pos[3 * a + c] / 3.0) + 512.0;
+        double f = floor(pos[3 * a + c] * inv_cell) + 512.0;
         f = fmin(fmax(f, 0.0), 1023.0);
         q[c] = (unsigned)f;
     }
@@ -578,7 +576,7 @@ __global__ void k_tile_bounds(Batch b, const int* tile_sys, int ntiles, double4*
     if (lane == 0) tiles[t] = make_double4(cx, cy, cz, r * (1.0 + 1.0e-12) + 1.0e-12);
 }
 
-int blocks_for(int n) { return (n + kWarps - 1) / kWarps; }
+int blocks_for(int n, int warps) { return (n + warps - 1) / warps; }
 
 }  // namespace
 
@@ -590,12 +588,12 @@ size_t sort_temp_bytes(int natoms)
     return bytes;
 }
 
-void launch_spatial_sort(const double* pos, int natoms, const int* sys_of_atom, unsigned long long* keys_in,
-                         unsigned long long* keys_out, int* idx_in, int* perm, void* temp, size_t temp_bytes,
-                         cudaStream_t stream)
+void launch_spatial_sort(const double* pos, int natoms, const int* sys_of_atom, double cell,
+                         unsigned long long* keys_in, unsigned long long* keys_out, int* idx_in, int* perm,
+                         void* temp, size_t temp_bytes, cudaStream_t stream)
 {
     if (natoms <= 0) return;
-    k_morton<<<(natoms + 255) / 256, 256, 0, stream>>>(pos, natoms, sys_of_atom, keys_in, idx_in);
+    k_morton<<<(natoms + 255) / 256, 256, 0, stream>>>(pos, natoms, sys_of_atom, 1.0 / cell, keys_in, idx_in);
     cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, idx_in, perm, natoms, 0, 64, stream);
 }
 
@@ -615,31 +613,45 @@ void launch_tile_bounds(const Batch& b, const int* tile_sys, int ntiles, double4
     k_tile_bounds<<<(ntiles + 7) / 8, 256, 0, stream>>>(b, tile_sys, ntiles, tiles);
 }
 
+// Atoms per block of the pair sweeps: 4 or 8 warps (one atom per warp).
+#define D3_PAIR_LAUNCH(KERNEL, ...)                                                                   \
+    do {                                                                                             \
+        if (c.pair_warps == 4) KERNEL<4, __VA_ARGS__><<<blocks_for(b.natoms, 4), 128, 0, stream>>>ARGS; \
+        else KERNEL<8, __VA_ARGS__><<<blocks_for(b.natoms, 8), 256, 0, stream>>>ARGS;                  \
+    } while (0)
+
 void launch_coordination_number_tiled(const Batch& b, const Species& s, const Config& c, const Partition& p,
                                       const Work& w, cudaStream_t stream)
 {
-    if (c.mixed) k_cn_tiled<float><<<blocks_for(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
-    else k_cn_tiled<double><<<blocks_for(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
+#define ARGS (b, s, c, p, w)
+    if (c.mixed) D3_PAIR_LAUNCH(k_cn_tiled, float);
+    else D3_PAIR_LAUNCH(k_cn_tiled, double);
+#undef ARGS
 }
 
 void launch_two_body_tiled(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
                            const Work& w, cudaStream_t stream)
 {
-    const int nb = blocks_for(b.natoms);
+#define ARGS (b, s, d, c, p, w)
     if (d.kind == kRational) {
-        if (c.mixed) k_two_body_tiled<float, kRational><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
-        else k_two_body_tiled<double, kRational><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
+        if (c.mixed) D3_PAIR_LAUNCH(k_two_body_tiled, float, kRational);
+        else D3_PAIR_LAUNCH(k_two_body_tiled, double, kRational);
     } else {
-        if (c.mixed) k_two_body_tiled<float, kZero><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
-        else k_two_body_tiled<double, kZero><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
+        if (c.mixed) D3_PAIR_LAUNCH(k_two_body_tiled, float, kZero);
+        else D3_PAIR_LAUNCH(k_two_body_tiled, double, kZero);
     }
+#undef ARGS
 }
 
 void launch_cn_chain_rule_tiled(const Batch& b, const Species& s, const Config& c, const Partition& p,
                                 const Work& w, cudaStream_t stream)
 {
-    if (c.mixed) k_chain_tiled<float><<<blocks_for(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
-    else k_chain_tiled<double><<<blocks_for(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
+#define ARGS (b, s, c, p, w)
+    if (c.mixed) D3_PAIR_LAUNCH(k_chain_tiled, float);
+    else D3_PAIR_LAUNCH(k_chain_tiled, double);
+#undef ARGS
 }
+
+#undef D3_PAIR_LAUNCH
 
 }  // namespace d3

@@ -351,6 +351,18 @@ class BatchedDispersion:
             raise ValueError(f"Unknown precision '{precision}', expected one of {sorted(modes)}")
         library.set_batch_precision(self._batch, modes[precision])
 
+    def set_graph(self, enable: bool = True) -> None:
+        """Replay the pipeline as one captured CUDA graph after the first evaluation."""
+        library.set_batch_graph(self._batch, enable)
+
+    def autotune(self, param: DampingParam, grad: bool = True) -> dict:
+        """Time the candidate launch shapes on the current positions and keep the fastest."""
+        ms = library.autotune_batch(self._batch, param._param, self._positions, grad)
+        return dict(library.get_batch_tuning(self._batch), ms=ms)
+
+    def set_tuning(self, morton_cell: float, atoms_per_block: int, atm_blocks_per_sm: int = 0) -> None:
+        library.set_batch_tuning(self._batch, morton_cell, atoms_per_block, atm_blocks_per_sm)
+
     def update(self, positions, lattices: Optional[np.ndarray] = None) -> None:
         self._positions = self._flatten(positions)
         if lattices is not None:

@@ -325,6 +325,30 @@ def get_batch_stage_times(batch: BatchHandle) -> dict:
     return dict(zip(STAGES, ms))
 
 
+def set_batch_graph(batch: BatchHandle, enable: bool) -> None:
+    error_check(lib.dftd3_b200_set_batch_graph)(batch.handle, 1 if enable else 0)
+
+
+TUNING = ("morton_cell", "atoms_per_block", "atm_blocks_per_sm")
+
+
+def set_batch_tuning(batch: BatchHandle, morton_cell: float, atoms_per_block: int, atm_blocks_per_sm: int) -> None:
+    t = np.array([morton_cell, atoms_per_block, atm_blocks_per_sm], dtype=float)
+    error_check(lib.dftd3_b200_set_batch_tuning)(batch.handle, _cast("double*", t))
+
+
+def get_batch_tuning(batch: BatchHandle) -> dict:
+    t = np.zeros(3)
+    error_check(lib.dftd3_b200_get_batch_tuning)(batch.handle, _cast("double*", t))
+    return {"morton_cell": float(t[0]), "atoms_per_block": int(t[1]), "atm_blocks_per_sm": int(t[2])}
+
+
+def autotune_batch(batch: BatchHandle, param: ParamHandle, positions: np.ndarray, grad: bool) -> float:
+    """Pick the fastest launch shape on these positions; returns its time in ms."""
+    return float(error_check(lib.dftd3_b200_autotune_batch)(
+        batch.handle, param.handle, _cast("double*", positions), 1 if grad else 0))
+
+
 def fma_peak(precision: int) -> float:
     """Measured FMA throughput (TFLOP/s) of the FP64 or FP32 pipe."""
     return float(error_check(lib.dftd3_b200_fma_peak)(precision))
