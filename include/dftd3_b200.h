@@ -146,6 +146,37 @@ dftd3_b200_autotune_batch(dftd3_error /* error */,
                           const double* /* positions */,
                           int /* gradient */);
 
+/* Reducer of a partitioned evaluation: sums `count` doubles of a device
+ * buffer in place over all parts (an all-reduce over the processes of a
+ * job).  Called on the host between kernel launches with the stream of the
+ * evaluation; it must order its work on that stream (for example a NCCL
+ * all-reduce enqueued there, or a stream synchronisation before a host
+ * exchange) and return 0 on success. */
+typedef int (*dftd3_b200_reducer)(double* /* buffer */,
+                                  int /* count */,
+                                  void* /* stream */,
+                                  void* /* user data */);
+
+/* Distribute the evaluation of a batch over nparts processes, this one
+ * being part `part` (0-based): the stand-in for dftd3_set_model_mpi_comm
+ * (reference api.f90:483-506) for callers that own their communicator (NCCL
+ * through torch.distributed, MPI, ...).  Every pair and triple loop,
+ * including the coordination number and its chain rule, is split by the
+ * reference's pair ownership (partition.f90:127-147); the coordination
+ * numbers and dE/dCN are summed over the parts before they are used
+ * (disp.f90:120-126,166-171) and the results once at the end
+ * (get_dispersion_mpi_atomic, mpi.f90), so every part returns the complete
+ * energies, gradient and virials.  All parts must evaluate the same
+ * positions, parameters and launch shapes.  reducer = NULL ends the
+ * partition.  Not combinable with dftd3_b200_set_batch_graph. */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_set_batch_reducer(dftd3_error /* error */,
+                             dftd3_b200_batch /* batch */,
+                             dftd3_b200_reducer /* reducer or NULL */,
+                             void* /* user data */,
+                             int /* part */,
+                             int /* nparts */);
+
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_b200_delete_batch(dftd3_b200_batch* /* batch */);
 

@@ -294,9 +294,10 @@ void oracle_wrap_to_central_cell(int nat, double *xyz, const double *lattice, co
 /* --------------------------------------------------------------- ncoord -- */
 
 static void partitioned_cn(int nat, const double *xyz, const int *id, const double *rcov,
-                           const double *trans, int ntr, double cutoff, double *cn)
+                           const double *trans, int ntr, double cutoff, double *cn, int part, int nparts)
 {
-    /* get_partitioned_coordination_number, ncoord.f90:86-144 (complete work) */
+    /* get_partitioned_coordination_number, ncoord.f90:86-144; nparts = 1 is
+     * the complete work */
     double cutoff2 = cutoff * cutoff;
     for (int i = 0; i < nat; i++) cn[i] = 0.0;
 #pragma omp parallel
@@ -306,6 +307,7 @@ static void partitioned_cn(int nat, const double *xyz, const int *id, const doub
         for (int i = 0; i < nat; i++) {
             int izp = id[i];
             for (int j = 0; j <= i; j++) {
+                if (!owns_pair(part, nparts, i, j)) continue;
                 int jzp = id[j];
                 double rc = rcov[izp] + rcov[jzp];
                 for (int t = 0; t < ntr; t++) {
@@ -329,9 +331,10 @@ static void partitioned_cn(int nat, const double *xyz, const int *id, const doub
 
 static void add_cn_derivs(int nat, const double *xyz, const int *id, const double *rcov,
                           const double *trans, int ntr, double cutoff, const double *dEdcn,
-                          double *gradient, double *sigma)
+                          double *gradient, double *sigma, int part, int nparts)
 {
-    /* add_coordination_number_derivs, ncoord.f90:152-228 (complete work) */
+    /* add_coordination_number_derivs, ncoord.f90:152-228; nparts = 1 is the
+     * complete work */
     double cutoff2 = cutoff * cutoff;
 #pragma omp parallel
     {
@@ -341,6 +344,7 @@ static void add_cn_derivs(int nat, const double *xyz, const int *id, const doubl
         for (int i = 0; i < nat; i++) {
             int izp = id[i];
             for (int j = 0; j <= i; j++) {
+                if (!owns_pair(part, nparts, i, j)) continue;
                 int jzp = id[j];
                 double rc = rcov[izp] + rcov[jzp];
                 for (int t = 0; t < ntr; t++) {
@@ -383,7 +387,7 @@ int oracle_coordination_number(int nat, const int *numbers, const double *xyz,
     int ntr;
     double zero[9] = {0};
     double *trans = lattice_points(lattice ? lattice : zero, periodic, cutoff, &ntr);
-    partitioned_cn(nat, xyz, m.id, m.rcov, trans, ntr, cutoff, cn);
+    partitioned_cn(nat, xyz, m.id, m.rcov, trans, ntr, cutoff, cn, 0, 1);
     free(trans);
     model_free(&m);
     return 0;
@@ -733,13 +737,17 @@ static void dispersion3(const model_t *m, const oracle_param *p, int nat, const 
 
 /* ------------------------------------------------------------- pipeline -- */
 
-int oracle_get_dispersion(int nat, const int *numbers, const double *xyz,
-                          const double *lattice, const int *periodic, const int *ghost,
-                          const oracle_param *param, const oracle_cutoff *cutoff,
-                          int part, int nparts, double *energy, double *energies,
-                          double *gradient, double *sigma, double *cn_out, double *dEdcn_out)
+static int pipeline(int nat, const int *numbers, const double *xyz, const double *lattice,
+                    const int *periodic, const int *ghost, const oracle_param *param,
+                    const oracle_cutoff *cutoff, int part, int nparts, oracle_reducer reduce, void *user,
+                    double *energy, double *energies, double *gradient, double *sigma, double *cn_out,
+                    double *dEdcn_out)
 {
-    /* get_dispersion_atomic_v2, disp.f90:56-185, and the scalar sum at :397 */
+    /* get_dispersion_atomic_v2, disp.f90:56-185, and the scalar sum at :397.
+     * With a reducer, the CN loop is partitioned and the CN and dE/dCN are
+     * summed over the parts before use (disp.f90:120-126,166-171), and the
+     * atom-resolved energies, gradient and virial afterwards
+     * (get_dispersion_mpi_atomic, mpi.f90). */
     model_t m;
     if (model_new(&m, nat, numbers, ghost)) return 1;
     double zero[9] = {0};
@@ -750,11 +758,17 @@ int oracle_get_dispersion(int nat, const int *numbers, const double *xyz,
     int mref = m.mref;
     int threebody = fabs(param->s9) >= EPS;
     int ntr;
+    int cn_part = reduce ? part : 0, cn_nparts = reduce ? nparts : 1;
 
     double *cn = malloc(sizeof(double) * (nat > 0 ? nat : 1));
     double *trans = lattice_points(lat, per, cutoff->cn, &ntr);
-    partitioned_cn(nat, xyz, m.id, m.rcov, trans, ntr, cutoff->cn, cn);
+    partitioned_cn(nat, xyz, m.id, m.rcov, trans, ntr, cutoff->cn, cn, cn_part, cn_nparts);
     free(trans);
+    if (reduce && reduce(cn, nat, user)) {
+        free(cn);
+        model_free(&m);
+        return 2;
+    }
 
     double *gwvec = malloc(sizeof(double) * (size_t)(nat > 0 ? nat : 1) * mref);
     double *gwdcn = grad ? malloc(sizeof(double) * (size_t)(nat > 0 ? nat : 1) * mref) : NULL;
@@ -781,12 +795,33 @@ int oracle_get_dispersion(int nat, const int *numbers, const double *xyz,
     dispersion3(&m, param, nat, xyz, trans, ntr, cutoff->disp3, cutoff->width3, c6, dc6dcn,
                 en, dEdcn, gl, sl, part, nparts);
     free(trans);
-    if (dEdcn_out && grad)
-        for (int i = 0; i < nat; i++) dEdcn_out[i] = dEdcn[i];
+    int rc = 0;
     if (grad) {
+        if (reduce && reduce(dEdcn, nat, user)) rc = 2;
+        if (dEdcn_out)
+            for (int i = 0; i < nat; i++) dEdcn_out[i] = dEdcn[i];
         trans = lattice_points(lat, per, cutoff->cn, &ntr);
-        add_cn_derivs(nat, xyz, m.id, m.rcov, trans, ntr, cutoff->cn, dEdcn, gl, sl);
+        add_cn_derivs(nat, xyz, m.id, m.rcov, trans, ntr, cutoff->cn, dEdcn, gl, sl, cn_part, cn_nparts);
         free(trans);
+    }
+    if (reduce && rc == 0) {
+        /* one fused sum of [energies | gradient | virial] */
+        size_t len = (size_t)nat + (grad ? 3 * (size_t)nat + 9 : 0);
+        double *buf = malloc(sizeof(double) * (len > 0 ? len : 1));
+        memcpy(buf, en, sizeof(double) * nat);
+        if (grad) {
+            memcpy(buf + nat, gl, sizeof(double) * 3 * nat);
+            memcpy(buf + 4 * (size_t)nat, sl, sizeof(double) * 9);
+        }
+        if (reduce(buf, (int)len, user)) rc = 2;
+        memcpy(en, buf, sizeof(double) * nat);
+        if (grad) {
+            memcpy(gl, buf + nat, sizeof(double) * 3 * nat);
+            memcpy(sl, buf + 4 * (size_t)nat, sizeof(double) * 9);
+        }
+        free(buf);
+    }
+    if (grad) {
         if (gradient) memcpy(gradient, gl, sizeof(double) * 3 * nat);
         if (sigma) memcpy(sigma, sl, sizeof(double) * 9);
     }
@@ -799,5 +834,26 @@ int oracle_get_dispersion(int nat, const int *numbers, const double *xyz,
     free(cn); free(gwvec); free(gwdcn); free(c6); free(dc6dcn);
     free(en); free(dEdcn); free(gl);
     model_free(&m);
-    return 0;
+    return rc;
+}
+
+int oracle_get_dispersion(int nat, const int *numbers, const double *xyz,
+                          const double *lattice, const int *periodic, const int *ghost,
+                          const oracle_param *param, const oracle_cutoff *cutoff,
+                          int part, int nparts, double *energy, double *energies,
+                          double *gradient, double *sigma, double *cn_out, double *dEdcn_out)
+{
+    return pipeline(nat, numbers, xyz, lattice, periodic, ghost, param, cutoff, part, nparts, NULL, NULL,
+                    energy, energies, gradient, sigma, cn_out, dEdcn_out);
+}
+
+int oracle_get_dispersion_reduced(int nat, const int *numbers, const double *xyz,
+                                  const double *lattice, const int *periodic, const int *ghost,
+                                  const oracle_param *param, const oracle_cutoff *cutoff,
+                                  int part, int nparts, oracle_reducer reduce, void *user,
+                                  double *energy, double *energies, double *gradient, double *sigma)
+{
+    if (!reduce) return 3;
+    return pipeline(nat, numbers, xyz, lattice, periodic, ghost, param, cutoff, part, nparts, reduce, user,
+                    energy, energies, gradient, sigma, NULL, NULL);
 }

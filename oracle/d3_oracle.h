@@ -43,6 +43,21 @@ int oracle_get_dispersion(int nat, const int *numbers, const double *xyz,
                           double *energy, double *energies, double *gradient,
                           double *sigma, double *cn_out, double *dEdcn_out);
 
+/* In-place sum of count doubles over all parts; returns 0 on success. */
+typedef int (*oracle_reducer)(double *buffer, int count, void *user);
+
+/* The partitioned evaluation with a reducer (the reference's MPI path,
+ * disp.f90:120-171 with `reducer`, and get_dispersion_mpi_atomic, mpi.f90):
+ * part `part` of `nparts` evaluates its share of every pair and triple loop,
+ * the CN and dE/dCN are summed over the parts before they are used, and the
+ * atom energies, gradient and virial are summed at the end, so that every
+ * part returns the complete result.  Returns 2 if the reducer failed. */
+int oracle_get_dispersion_reduced(int nat, const int *numbers, const double *xyz,
+                                  const double *lattice, const int *periodic, const int *ghost,
+                                  const oracle_param *param, const oracle_cutoff *cutoff,
+                                  int part, int nparts, oracle_reducer reduce, void *user,
+                                  double *energy, double *energies, double *gradient, double *sigma);
+
 /* Coordination numbers alone (ncoord.f90:86-144). */
 int oracle_coordination_number(int nat, const int *numbers, const double *xyz,
                                const double *lattice, const int *periodic,

@@ -717,6 +717,17 @@ double dftd3_b200_autotune_batch(dftd3_error error, dftd3_b200_batch batch, dftd
     return ms;
 }
 
+void dftd3_b200_set_batch_reducer(dftd3_error error, dftd3_b200_batch batch, dftd3_b200_reducer reducer, void* user,
+                                  int part, int nparts)
+{
+    if (!error) return;
+    if (!batch) {
+        fail(error, "Batch is missing");
+        return;
+    }
+    guarded(error, [&] { batch->engine->set_reducer(reducer, user, part, nparts); });
+}
+
 void dftd3_b200_delete_batch(dftd3_b200_batch* batch)
 {
     if (batch && *batch) {

@@ -521,6 +521,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     launch_tile_bounds(b, d_tile_sys_, ntiles_, d_tiles_, stream);
     mark(1);
     launch_coordination_number(b, s, c, part_, w, stream);
+    if (reducer_) reduce(w.cn, natoms_, stream);
     mark(2);
     launch_weights(b, s, c, w, stream);
     mark(3);
@@ -553,9 +554,31 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
         w.pg_s9_scale = 1.0;
     }
     mark(5);
-    if (grad) launch_cn_chain_rule(b, s, c, part_, w, stream);
+    if (grad) {
+        if (reducer_) reduce(w.dEdcn, natoms_, stream);
+        launch_cn_chain_rule(b, s, c, part_, w, stream);
+    }
     mark(6);
-    launch_reduce_systems(b, c, w, d_energies, d_sigma9, d_param_grad, d_gradient, stream);
+    if (!reducer_) {
+        launch_reduce_systems(b, c, w, d_energies, d_sigma9, d_param_grad, d_gradient, stream);
+    } else {
+        // this part's results in one buffer, summed over the parts in one call
+        double* re = d_red_;
+        double* rp = re + nsys_;
+        double* rs = rp + (size_t)kParamGrad * nsys_;
+        double* rg = rs + 9 * (size_t)nsys_;
+        launch_reduce_systems(b, c, w, re, grad ? rs : nullptr, pg ? rp : nullptr, grad ? rg : nullptr, stream);
+        if (!pg) check(cudaMemsetAsync(rp, 0, sizeof(double) * kParamGrad * nsys_, stream), "memset");
+        const size_t len = (size_t)nsys_ * (1 + kParamGrad) + (grad ? 9 * (size_t)nsys_ + 3 * (size_t)natoms_ : 0);
+        reduce(d_red_, (int)len, stream);
+        auto out = [&](double* dst, const double* src, size_t n) {
+            if (dst) check(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream), "results");
+        };
+        out(d_energies, re, nsys_);
+        out(d_param_grad, rp, (size_t)kParamGrad * nsys_);
+        out(d_sigma9, rs, 9 * (size_t)nsys_);
+        out(d_gradient, rg, 3 * (size_t)natoms_);
+    }
     mark(7);
     if (!capturing_) ev_recorded_ = profiling_;
     check(cudaGetLastError(), "kernel launch");
@@ -683,9 +706,36 @@ void Engine::drop_graph()
     graph_valid_ = false;
 }
 
+void Engine::reduce(double* buffer, int count, cudaStream_t stream)
+{
+    check(cudaGetLastError(), "kernel launch");
+    if (reducer_(buffer, count, stream, reducer_user_) != 0) throw Error("The reducer reported an error");
+}
+
+void Engine::set_reducer(Reducer fn, void* user, int part, int nparts)
+{
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    if (fn && graph_on_) throw Error("A reducer cannot be combined with the captured launch sequence");
+    if (fn && (nparts < 1 || part < 0 || part >= nparts)) throw Error("Invalid dispersion work partition");
+    reducer_ = fn;
+    reducer_user_ = user;
+    if (fn) {
+        if (!d_red_) {
+            const size_t len = (size_t)nsys_ * (1 + kParamGrad + 9) + 3 * (size_t)natoms_;
+            d_red_ = dev_alloc<double>(len);
+            check(cudaMemsetAsync(d_red_, 0, sizeof(double) * len, stream_), "memset");
+            check(cudaStreamSynchronize(stream_), "memset");
+        }
+        set_partition(part, nparts, true);
+    } else {
+        set_partition(0, 1, false);
+    }
+}
+
 void Engine::set_graph(bool on)
 {
     check(cudaSetDevice(device_), "cudaSetDevice");
+    if (on && reducer_) throw Error("A reducer cannot be combined with the captured launch sequence");
     if (!on) drop_graph();
     graph_on_ = on;
 }

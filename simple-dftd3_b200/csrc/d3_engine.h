@@ -93,6 +93,20 @@ public:
     void set_graph(bool on);
     bool graph() const { return graph_on_; }
 
+    // Partitioned evaluation over several processes (the reference's MPI
+    // path, disp.f90:120-171 with a reducer, and mpi.f90): this engine
+    // evaluates part `part` of `nparts` of every pair and triple loop,
+    // including the CN and chain-rule loops, and calls `fn` to sum a device
+    // buffer over all parts in place: the CN, then dE/dCN, then the results
+    // [energies | parameter derivatives | virials | gradient] in one call.
+    // `fn` is called on the host between launches and must order its work on
+    // the given stream (a collective enqueued there, or a synchronisation
+    // before a host exchange); it returns 0 on success.  All parts must have
+    // the same systems, positions, parameters and launch shapes.  fn = null
+    // ends the partition.  Not combinable with the captured graph.
+    using Reducer = int (*)(double* buffer, int count, void* stream, void* user);
+    void set_reducer(Reducer fn, void* user, int part, int nparts);
+
     // Launch shapes (spatial sort cell, atoms per pair block, resident triple
     // blocks per SM).  autotune() times the candidates on the given device
     // positions and keeps the fastest; it returns that time in ms.
@@ -116,6 +130,11 @@ private:
     void run(const Damp& d, const double* d_positions, double* d_energies, double* d_gradient,
              double* d_sigma9, double* d_param_grad, bool grad, cudaStream_t stream);
     template <class T> T* dev_alloc(size_t n);
+
+    void reduce(double* buffer, int count, cudaStream_t stream);
+    Reducer reducer_ = nullptr;
+    void* reducer_user_ = nullptr;
+    double* d_red_ = nullptr;    // [nsys | 5 nsys | 9 nsys | 3 natoms] results of this part
 
     // graph state
     struct GraphKey {

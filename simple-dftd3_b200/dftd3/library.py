@@ -349,6 +349,12 @@ def autotune_batch(batch: BatchHandle, param: ParamHandle, positions: np.ndarray
         batch.handle, param.handle, _cast("double*", positions), 1 if grad else 0))
 
 
+def set_batch_reducer(batch: BatchHandle, reducer, part: int, nparts: int) -> None:
+    """reducer: a cffi callback of type dftd3_b200_reducer (keep it alive), or None."""
+    error_check(lib.dftd3_b200_set_batch_reducer)(batch.handle, reducer if reducer is not None else ffi.NULL,
+                                                  ffi.NULL, part, nparts)
+
+
 def fma_peak(precision: int) -> float:
     """Measured FMA throughput (TFLOP/s) of the FP64 or FP32 pipe."""
     return float(error_check(lib.dftd3_b200_fma_peak)(precision))

@@ -27,6 +27,8 @@ class OracleCutoff(C.Structure):
 
 
 _lib = None
+# in-place sum of count doubles over all parts; 0 on success
+REDUCER = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p)
 
 
 def lib():
@@ -43,6 +45,11 @@ def lib():
             C.c_int, ip, dp, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(OracleParam),
             C.POINTER(OracleCutoff), C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
             C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.oracle_get_dispersion_reduced.restype = C.c_int
+        _lib.oracle_get_dispersion_reduced.argtypes = [
+            C.c_int, ip, dp, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(OracleParam),
+            C.POINTER(OracleCutoff), C.c_int, C.c_int, REDUCER, C.c_void_p, C.c_void_p, C.c_void_p,
+            C.c_void_p, C.c_void_p]
         _lib.oracle_coordination_number.argtypes = [C.c_int, ip, dp, C.c_void_p, C.c_void_p,
                                                     C.c_double, dp]
         _lib.oracle_weight_references.argtypes = [C.c_int, ip, dp, C.POINTER(C.c_int),
@@ -137,3 +144,45 @@ def lattice_points(lattice, periodic, cutoff):
     t = np.zeros((n, 3))
     lib().oracle_lattice_points(lat, _ptr(per), cutoff, _ptr(t), n)
     return t
+
+
+def dispersion_reduced(numbers, positions, param, reduce, part, nparts, lattice=None, periodic=None, grad=True,
+                       cutoff=(60.0, 40.0, 40.0, 0.0, 0.0)):
+    """Partitioned oracle evaluation with a reducer (the reference's MPI path):
+    `reduce(address, count)` sums count doubles at address over all parts in
+    place.  Returns the complete energy, gradient and virial on every part."""
+    numbers = np.ascontiguousarray(numbers, dtype=np.int32)
+    xyz = np.array(positions, dtype=np.float64).reshape(-1, 3).copy()
+    nat = len(numbers)
+    lat = None if lattice is None else np.ascontiguousarray(lattice, dtype=np.float64).reshape(3, 3)
+    per = None
+    if periodic is not None:
+        per = np.ascontiguousarray([1 if p else 0 for p in np.ravel(periodic)], dtype=np.int32)
+    elif lat is not None:
+        per = np.ones(3, dtype=np.int32)
+    if per is not None and per.any():
+        lib().oracle_wrap_to_central_cell(nat, xyz, lat, _ptr(per))
+
+    def cb(address, count, user):
+        try:
+            reduce(address, count)
+        except Exception:
+            return 1
+        return 0
+
+    cfun = REDUCER(cb)
+    e = np.zeros(1)
+    energies = np.zeros(max(nat, 1))
+    g = np.zeros((max(nat, 1), 3)) if grad else None
+    s = np.zeros((3, 3)) if grad else None
+    prm = make_param(param)
+    cut = OracleCutoff(*cutoff)
+    rc = lib().oracle_get_dispersion_reduced(nat, numbers, xyz, _ptr(lat), _ptr(per), None, C.byref(prm),
+                                             C.byref(cut), part, nparts, cfun, None, _ptr(e), _ptr(energies),
+                                             _ptr(g), _ptr(s))
+    if rc != 0:
+        raise RuntimeError(f"oracle: reduced evaluation failed ({rc})")
+    out = {"energy": float(e[0]), "energies": energies[:nat]}
+    if grad:
+        out.update(gradient=g[:nat], virial=s)
+    return out
