@@ -58,6 +58,9 @@ def parse_args():
     ap.add_argument("--natoms", type=int, default=None, help="atoms per system (smaller cases for profiling)")
     ap.add_argument("--nsys", type=int, default=None, help="systems of the batched workloads")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
+    ap.add_argument("--shard", action="store_true",
+                    help="with N > 1: all ranks share one copy of the workload (partitioned loops, NCCL "
+                         "all-reduce of CN, dE/dCN and results; strong scaling) instead of one copy per rank")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true")
@@ -283,15 +286,26 @@ def run_ours(args, rank, world, dist):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-    systems, par = make_workload(args.workload, seed=rank, natoms=args.natoms, nsys=args.nsys)
+    shard = args.shard and world > 1
+    systems, par = make_workload(args.workload, seed=0 if shard else rank, natoms=args.natoms, nsys=args.nsys)
     run = Runner(systems, par)
+    if shard:
+        from dftd3 import parallel
+        lib.set_batch_tuning(run.batch, 3.0, 8, 0)
+        run.reducer = parallel.make_device_reducer()
+        lib.set_batch_reducer(run.batch, run.reducer, rank, world)
     counts = run.counts()
+    if shard:
+        # each rank counted its share of the loops
+        ct = torch.tensor([counts[k] for k in sorted(counts)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(ct)
+        counts = {k: int(v) for k, v in zip(sorted(counts), ct.tolist())}
     precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     sampler = ClockSampler(local)
     sampler.start()
     res = {p: run.time(p, args.steps, args.warmup, flush, dist) for p in precs}
     extra = {}
-    if not args.no_extra and args.workload == "cell2000":
+    if not args.no_extra and args.workload == "cell2000" and not shard:
         for name, steps in (("cluster5000", 3), ("batch4096", 3), ("frames256", 1)):
             nsys = 16 if name == "frames256" else None
             sy, pr = make_workload(name, seed=rank, nsys=nsys)
@@ -317,7 +331,7 @@ def run_ours(args, rank, world, dist):
     clocks = sampler.summary()
 
     e2e_ms = None
-    if not args.no_e2e and len(systems) == 1:
+    if not args.no_e2e and len(systems) == 1 and not shard:
         num, pos, lat, per = systems[0]
         mol = DispersionModel(np.asarray(num), np.asarray(pos, dtype=float), lat, per)
         mol.set_precision("mixed" if "mixed" in precs else "fp64")
@@ -357,22 +371,24 @@ def run_ours(args, rank, world, dist):
     kern = "k_triples" if atm else "k_two_body_tiled"
     line = {
         "metric": METRIC if args.workload == "cell2000" else f"{unit} ({args.workload})",
-        "value": world * units / (ms * 1e-3),
+        "value": (1 if shard else world) * units / (ms * 1e-3),
         "unit": unit,
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": ms,
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong" if shard else "weak",
         "vs_baseline": None,
         "dtype": "f32 pair/triple terms, f64 accumulation, weights and reductions" if head == "mixed" else "f64",
         "data": f"synthetic (seeded generator dftd3/synthetic.py, {args.workload})",
         "config": {"workload": {"cell2000": "cell2000: periodic triclinic 2000 atoms, D3(BJ) two-body + CN chain "
                                             "rule, E+grad+virial, disp2 60 / CN 40 Bohr"}.get(args.workload, args.workload),
                    "systems": len(systems), "atoms": int(run.natoms.sum()), **counts,
-                   "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}"},
-        "precision_results": {p: {"value": world * units / (res[p]["ms_per_step"] * 1e-3), **res[p]} for p in precs},
+                   "l2": "flushed between timed steps (256 MB write)",
+                   "parallelism": f"pair partition x{world} (NCCL)" if shard else f"replicas x{world}"},
+        "precision_results": {p: {"value": (1 if shard else world) * units / (res[p]["ms_per_step"] * 1e-3), **res[p]}
+                              for p in precs},
         "gpu_launches": None,
         "roofline": None,
         "clocks": clocks,
