@@ -213,6 +213,15 @@ dftd3_b200_get_dispersion_noalloc(dftd3_error /* error */,
                                   double* /* d_sigma [9] or NULL */,
                                   void* /* stream */);
 
+/* Values of a damping parameter handle: *kind 0 rational, 1 zero;
+ * values[8] = s6, s8, s9, a1, a2, rs6, rs8, alp.  For inspecting parameters
+ * loaded by method name (dftd3_load_*_damping). */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_get_param_values(dftd3_error /* error */,
+                            dftd3_param /* param */,
+                            int* /* kind */,
+                            double* /* values[8] */);
+
 /* Measured fused-multiply-add throughput of the current device in TFLOP/s
  * (precision DFTD3_B200_PRECISION_FP64: FP64 pipe, _MIXED: FP32 pipe); the
  * denominator of the roofline fraction the benchmark reports. */

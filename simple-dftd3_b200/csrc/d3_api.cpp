@@ -15,6 +15,7 @@
 
 #include "../../include/dftd3_b200.h"
 #include "d3_engine.h"
+#include "d3_params.h"
 #include "d3_tables.h"
 
 namespace d3 {
@@ -89,6 +90,57 @@ void guarded(dftd3_error err, F&& f)
     } catch (const std::exception& e) {
         fail(err, e.what());
     }
+}
+
+}  // namespace
+
+namespace {
+
+// Method id of a method name as get_method_id does it (param.f90:96-114):
+// '-' removed, letters outside quotes in lower case, trailing blanks ignored.
+int method_id(const char* method)
+{
+    std::string lc;
+    for (const char* c = method; *c; c++)
+        if (*c != '-') lc.push_back(*c);
+    bool quoted = false;
+    char quote = 0;
+    for (char& c : lc) {
+        if (!quoted && (c == '"' || c == '\'')) { quoted = true; quote = c; continue; }
+        if (quoted && c == quote) { quoted = false; continue; }
+        if (!quoted && c >= 'A' && c <= 'Z') c = char(c - 'A' + 'a');
+    }
+    while (!lc.empty() && lc.back() == ' ') lc.pop_back();
+    for (int k = 0; k < d3_n_method_aliases; k++)
+        if (lc == d3_method_aliases[k].name) return d3_method_aliases[k].id;
+    return 0;
+}
+
+// get_{rational,zero,mrational}_damping (param.f90:302-, 805-, 1091-) and the
+// load_*_damping entries (api.f90:588-625, 656-690, 710-745): the record of
+// the method, s9 = 1 when the three-body term is requested.
+dftd3_param load_param(dftd3_error error, const char* method, bool atm, const d3_param_record* table, int n,
+                       int kind)
+{
+    if (!error) return nullptr;
+    if (!method) {
+        fail(error, "Method name is missing");
+        return nullptr;
+    }
+    const int id = method_id(method);
+    const d3_param_record* rec = nullptr;
+    for (int k = 0; id && k < n && !rec; k++)
+        if (table[k].id == id) rec = &table[k];
+    if (!rec) {
+        fail(error, std::string("No entry for '") + method + "' present");
+        return nullptr;
+    }
+    auto* p = new _dftd3_param();
+    p->damp.kind = kind;
+    p->damp.s6 = rec->v[0]; p->damp.s8 = rec->v[1]; p->damp.s9 = atm ? 1.0 : rec->v[2];
+    p->damp.rs6 = rec->v[3]; p->damp.rs8 = rec->v[4];
+    p->damp.a1 = rec->v[5]; p->damp.a2 = rec->v[6]; p->damp.alp = rec->v[7];
+    return p;
 }
 
 }  // namespace
@@ -299,6 +351,23 @@ dftd3_param dftd3_new_rational_damping(dftd3_error error, double s6, double s8, 
     return p;
 }
 
+dftd3_param dftd3_load_zero_damping(dftd3_error error, char* method, bool atm)
+{
+    return load_param(error, method, atm, d3_zero_params, d3_n_zero_params, d3::kZero);
+}
+
+dftd3_param dftd3_load_rational_damping(dftd3_error error, char* method, bool atm)
+{
+    return load_param(error, method, atm, d3_rational_params, d3_n_rational_params, d3::kRational);
+}
+
+dftd3_param dftd3_load_mrational_damping(dftd3_error error, char* method, bool atm)
+{
+    // the modified rational records are evaluated with the rational damping
+    // function (api.f90:710-745 constructs a rational_damping_param)
+    return load_param(error, method, atm, d3_mrational_params, d3_n_mrational_params, d3::kRational);
+}
+
 #define D3_UNSUPPORTED_LOAD(name, what)                                   \
     dftd3_param name(dftd3_error error, char*, bool)                      \
     {                                                                     \
@@ -307,10 +376,7 @@ dftd3_param dftd3_new_rational_damping(dftd3_error error, double s6, double s8, 
         return nullptr;                                                   \
     }
 
-D3_UNSUPPORTED_LOAD(dftd3_load_zero_damping, "Loading parameters by method name")
-D3_UNSUPPORTED_LOAD(dftd3_load_rational_damping, "Loading parameters by method name")
 D3_UNSUPPORTED_LOAD(dftd3_load_mzero_damping, "Modified zero damping")
-D3_UNSUPPORTED_LOAD(dftd3_load_mrational_damping, "Modified rational damping")
 D3_UNSUPPORTED_LOAD(dftd3_load_optimizedpower_damping, "Optimized power damping")
 D3_UNSUPPORTED_LOAD(dftd3_load_cso_damping, "CSO damping")
 D3_UNSUPPORTED_LOAD(dftd3_load_z_damping, "Z damping")
@@ -630,6 +696,19 @@ void dftd3_b200_get_dispersion_noalloc(dftd3_error error, dftd3_param param, int
     if (!d3::noalloc_dispersion(param->damp, natoms, numbers, d_positions, lattice, periodic, cutoffs, precision,
                                 d_energy, d_gradient, d_sigma, static_cast<cudaStream_t>(stream), msg))
         fail(error, msg);
+}
+
+void dftd3_b200_get_param_values(dftd3_error error, dftd3_param param, int* kind, double* values)
+{
+    if (!error) return;
+    if (!param || !kind || !values) {
+        fail(error, "Damping parameters are missing");
+        return;
+    }
+    const d3::Damp& d = param->damp;
+    *kind = d.kind;
+    const double v[8] = {d.s6, d.s8, d.s9, d.a1, d.a2, d.rs6, d.rs8, d.alp};
+    for (int k = 0; k < 8; k++) values[k] = v[k];
 }
 
 double dftd3_b200_fma_peak(dftd3_error error, int precision)

@@ -355,6 +355,17 @@ def set_batch_reducer(batch: BatchHandle, reducer, part: int, nparts: int) -> No
                                                   ffi.NULL, part, nparts)
 
 
+PARAM_FIELDS = ("s6", "s8", "s9", "a1", "a2", "rs6", "rs8", "alp")
+
+
+def get_param_values(param: ParamHandle) -> dict:
+    """Damping kind and values of a parameter handle."""
+    kind = ffi.new("int*")
+    v = np.zeros(len(PARAM_FIELDS))
+    error_check(lib.dftd3_b200_get_param_values)(param.handle, kind, _cast("double*", v))
+    return dict(zip(PARAM_FIELDS, v.tolist()), damping="rational" if kind[0] == 0 else "zero")
+
+
 def fma_peak(precision: int) -> float:
     """Measured FMA throughput (TFLOP/s) of the FP64 or FP32 pipe."""
     return float(error_check(lib.dftd3_b200_fma_peak)(precision))
