@@ -110,3 +110,24 @@ def test_batched_atm_matches_single():
         ref = O.dispersion(d["numbers"][k], d["positions"][k], par)
         assert abs(res["energy"][k] - ref["energy"]) <= RTOL64 * abs(ref["energy"])
         assert np.abs(res["gradient"][k] - ref["gradient"]).max() <= GTOL64 * np.abs(ref["gradient"]).max()
+
+
+def test_named_methods_reproduce_fixtures():
+    """Parameters loaded by method name, as the reference's Python tests do
+    (RationalDampingParam(method="pbe0"), test_interface.py), give the
+    fixture energies at the fixtures' tolerance and exactly the energies of
+    the same parameters given explicitly."""
+    from dftd3.interface import DispersionModel, RationalDampingParam, ZeroDampingParam
+    entry = json.loads((GOLDEN / "python.json").read_text())[0]
+    model = DispersionModel(np.array(entry["numbers"]), np.array(entry["positions"]))
+    checked = 0
+    for case in entry["cases"]:
+        par = case["param"]
+        method = par["source"].split("(")[-1].rstrip(")")
+        cls = RationalDampingParam if par["damping"] == "rational" else ZeroDampingParam
+        by_name = model.get_dispersion(cls(method=method, atm=par["s9"] != 0.0), grad=False)["energy"]
+        explicit = gpu_dispersion(entry["numbers"], entry["positions"], par, grad=False)["energy"]
+        assert float(by_name) == float(explicit)
+        assert abs(float(by_name) - case["energy"]) <= entry.get("tol_rel", 1e-6) * abs(case["energy"])
+        checked += 1
+    assert checked >= 2
