@@ -28,6 +28,7 @@
 #include <cstdint>
 
 #include "d3_device.cuh"
+#include "d3_atm_common.cuh"
 
 namespace d3 {
 
@@ -39,9 +40,6 @@ constexpr int kThreadsAtm = 256; // 16 x 16
 constexpr int kAcc = 5;          // per-entry accumulators: S, Gx, Gy, Gz, dE/dCN of the partner
 
 // ------------------------------------------------------------ C6 matrix ----
-
-template <class R>
-struct C6Entry { R sc6, qrc, qcr; };
 
 // {sqrt(C6_rc), dC6_rc/dCN_r / C6_rc, dC6_rc/dCN_c / C6_rc} for every ordered
 // pair (r, c) of each system (get_atomic_c6, model.f90:432-461); ghosts give 0.
@@ -90,12 +88,16 @@ __global__ void k_c6_matrix(Batch b, Species s, Work w, const long long* mat_off
 __device__ __forceinline__ bool in_shell(double r2, double cut2) { return !(r2 > cut2 || r2 < DBL_EPSILON); }
 
 // Number of entries (j <= i, T) with eps <= |x_j + T - x_i|^2 <= cutoff^2.
-__global__ void k_nbr_count(Batch b, Config c, int* cnt, int* max_cnt)
+__global__ void k_nbr_count(Batch b, Config c, const uint8_t* sys_skip, int* cnt, int* max_cnt)
 {
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= b.natoms) return;
     const int sys = b.sys_of_atom[i];
+    if (sys_skip && sys_skip[sys]) {
+        if (lane == 0) cnt[i] = 0;
+        return;
+    }
     const int j0 = b.atom_off[sys];
     const int t0 = b.img_off[kImgDisp3 * (b.nsys + 1) + sys], t1 = b.img_off[kImgDisp3 * (b.nsys + 1) + sys + 1];
     const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
@@ -122,13 +124,14 @@ __global__ void k_atm_guard(const long long* total, const int* max_cnt, long lon
 }
 
 // Entries of root i in (j, T) order.  vec = (x_j + T) - x_i as in atm.f90:718.
-__global__ void k_nbr_fill(Batch b, Config c, const long long* off, int* nbr_j, int* nbr_gend,
-                           double4* nbr_v, const int* guard)
+__global__ void k_nbr_fill(Batch b, Config c, const uint8_t* sys_skip, const long long* off, int* nbr_j,
+                           int* nbr_gend, double4* nbr_v, const int* guard)
 {
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= b.natoms || *guard) return;
     const int sys = b.sys_of_atom[i];
+    if (sys_skip && sys_skip[sys]) return;   // no entries were counted for this root
     const int j0 = b.atom_off[sys];
     const int t0 = b.img_off[kImgDisp3 * (b.nsys + 1) + sys], t1 = b.img_off[kImgDisp3 * (b.nsys + 1) + sys + 1];
     const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
@@ -171,36 +174,6 @@ __global__ void k_nbr_fill(Batch b, Config c, const long long* off, int* nbr_j, 
 
 // ------------------------------------------------------------ triple sum ----
 
-template <class R>
-__device__ __forceinline__ R rsqrt_r(R x) { if constexpr (sizeof(R) == 8) return rsqrt(x); else return rsqrtf(x); }
-
-// Reciprocal of the triple arithmetic: IEEE in the FP64 form, the hardware
-// approximation (a few ulp) in the FP32 part of the mixed form.
-template <class R>
-__device__ __forceinline__ R rcp_r(R x) { if constexpr (sizeof(R) == 8) return R(1) / x; else return __fdividef(1.0f, x); }
-
-// log and exp in the precision of the form (natural base for FP64, base 2
-// with the hardware units for FP32; only their composition matters).
-template <class R>
-__device__ __forceinline__ R rlog(R x) { if constexpr (sizeof(R) == 8) return log(x); else return __log2f(x); }
-template <class R>
-__device__ __forceinline__ R rexp(R x) { if constexpr (sizeof(R) == 8) return exp(x); else return exp2f(x); }
-
-template <class R>
-__device__ __forceinline__ void smooth(R r, R cutoff, R width, R& sw, R& dsw)
-{
-    // cutoff.f90:73-99
-    if (width <= R(0) || width >= cutoff) { sw = R(1); dsw = R(0); return; }
-    const R inner = cutoff - width;
-    if (r <= inner) { sw = R(1); dsw = R(0); }
-    else if (r >= cutoff) { sw = R(0); dsw = R(0); }
-    else {
-        const R x = (cutoff - r) / width;
-        sw = x * x * x * (R(10) + x * (R(-15) + R(6) * x));
-        dsw = R(-30) * x * x * (R(1) - x) * (R(1) - x) / width;
-    }
-}
-
 template <class R> struct Vec4;
 template <> struct Vec4<double> { using type = double4; };
 template <> struct Vec4<float> { using type = float4; };
@@ -214,23 +187,6 @@ struct Slot {
     typename Vec4<R>::type s;   // 1/r, switch, dsw/dr / r, -
     int4 meta;                  // atom, group end, species, input index
 };
-
-__device__ __forceinline__ bool owns_pair_atm(const Partition& p, int i, int j)
-{
-    long long hi = i > j ? i : j, lo = i > j ? j : i;
-    return (hi * (hi + 1) / 2 + lo) % p.nparts == p.part;
-}
-
-// P(x; y, z) = x^3 + x^2 (y + z) + x (3 y^2 + 2 y z + 3 z^2) - 5 (y - z)^2 (y + z),
-// the numerator of the angular derivative along x (atm.f90:751-776), with
-// s1 = x + y + z.
-template <class R>
-__device__ __forceinline__ R ang_deriv(R x, R y, R z, R s1)
-{
-    const R u = y + z, d = y - z;
-    const R w = d * d;
-    return x * (x * s1 + w + R(2) * u * u) - R(5) * u * w;
-}
 
 template <class R, bool GRAD>
 __global__ void __launch_bounds__(kThreadsAtm, sizeof(R) == 4 ? 3 : 1) k_triples(Batch b, Species sp, Damp d, Config c, Partition part,
@@ -550,10 +506,11 @@ void launch_c6_matrix(const Batch& b, const Species& s, const Work& w, const lon
     else k_c6_matrix<double><<<(unsigned)blocks, threads, 0, stream>>>(b, s, w, d_mat_off, (C6Entry<double>*)mat, total);
 }
 
-void launch_nbr_count(const Batch& b, const Config& c, int* cnt, int* max_cnt, cudaStream_t stream)
+void launch_nbr_count(const Batch& b, const Config& c, const uint8_t* sys_skip, int* cnt, int* max_cnt,
+                      cudaStream_t stream)
 {
     if (b.natoms <= 0) return;
-    k_nbr_count<<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, c, cnt, max_cnt);
+    k_nbr_count<<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, c, sys_skip, cnt, max_cnt);
 }
 
 size_t scan_temp_bytes(int n)
@@ -575,11 +532,11 @@ void launch_atm_guard(const long long* total, const int* max_cnt, long long cap,
     k_atm_guard<<<1, 1, 0, stream>>>(total, max_cnt, cap, stride, guard);
 }
 
-void launch_nbr_fill(const Batch& b, const Config& c, const long long* off, int* nbr_j, int* nbr_gend,
-                     double4* nbr_v, const int* guard, cudaStream_t stream)
+void launch_nbr_fill(const Batch& b, const Config& c, const uint8_t* sys_skip, const long long* off, int* nbr_j,
+                     int* nbr_gend, double4* nbr_v, const int* guard, cudaStream_t stream)
 {
     if (b.natoms <= 0) return;
-    k_nbr_fill<<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, c, off, nbr_j, nbr_gend, nbr_v, guard);
+    k_nbr_fill<<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, c, sys_skip, off, nbr_j, nbr_gend, nbr_v, guard);
 }
 
 template <class R>

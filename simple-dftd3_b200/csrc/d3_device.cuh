@@ -142,7 +142,10 @@ void launch_cn_chain_rule_tiled(const Batch& b, const Species& s, const Config& 
 size_t atm_c6_entry_bytes(bool mixed);
 void launch_c6_matrix(const Batch& b, const Species& s, const Work& w, const long long* d_mat_off,
                       void* mat, long long total, bool mixed, cudaStream_t stream);
-void launch_nbr_count(const Batch& b, const Config& c, int* cnt, int* max_cnt, cudaStream_t stream);
+// sys_skip[nsys] (or null): systems whose roots get no entries (handled by
+// the molecule kernel)
+void launch_nbr_count(const Batch& b, const Config& c, const uint8_t* sys_skip, int* cnt, int* max_cnt,
+                      cudaStream_t stream);
 size_t scan_temp_bytes(int n);
 void launch_scan(void* temp, size_t temp_bytes, const int* cnt_ext, long long* off, int n,
                  cudaStream_t stream);
@@ -150,8 +153,8 @@ void launch_scan(void* temp, size_t temp_bytes, const int* cnt_ext, long long* o
 // list exceeds stride; the fill and triple kernels then return at once.
 void launch_atm_guard(const long long* total, const int* max_cnt, long long cap, int stride, int* guard,
                       cudaStream_t stream);
-void launch_nbr_fill(const Batch& b, const Config& c, const long long* off, int* nbr_j, int* nbr_gend,
-                     double4* nbr_v, const int* guard, cudaStream_t stream);
+void launch_nbr_fill(const Batch& b, const Config& c, const uint8_t* sys_skip, const long long* off, int* nbr_j,
+                     int* nbr_gend, double4* nbr_v, const int* guard, cudaStream_t stream);
 int atm_blocks_per_sm(bool mixed, bool grad);
 size_t atm_slot_bytes(bool mixed);
 void launch_triples(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
@@ -159,6 +162,14 @@ void launch_triples(const Batch& b, const Species& s, const Damp& d, const Confi
                     const int* cnt, const int* nbr_j, const int* nbr_gend, const double4* nbr_v,
                     unsigned int* queue, double* slot_acc, void* slot_scr, int slot_stride, int blocks,
                     double* e3, double* sig3, cudaStream_t stream);
+// Three-body term of whole molecules, one block per system (d3_atm_mol.cu):
+// the non-periodic systems of at most atm_mol_max_atoms() atoms listed in
+// mol_order (largest first).  Writes e3/sig3 for every atom of those systems.
+int atm_mol_max_atoms();
+int atm_mol_blocks_per_sm(bool mixed, bool grad);
+void launch_triples_mol(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
+                        const Work& w, const void* mat, const long long* mat_off, const int* mol_order, int nmol,
+                        unsigned int* queue, int blocks, double* e3, double* sig3, cudaStream_t stream);
 void launch_cn_chain_rule(const Batch& b, const Species& s, const Config& c, const Partition& p,
                           const Work& w, cudaStream_t stream);
 void launch_reduce_systems(const Batch& b, const Config& c, const Work& w, double* energies,

@@ -267,6 +267,25 @@ Engine::Engine(int nsys, const int* natoms, const int* numbers, const double* la
         off += (long long)natoms[s] * natoms[s];
     }
     c6mat_total_ = off;
+    // molecules for the block-per-system three-body kernel: no periodic
+    // direction and at most atm_mol_max_atoms() atoms; largest first
+    std::vector<uint8_t> is_mol(nsys, 0);
+    for (int s = 0; s < nsys; s++) {
+        const bool per_any = per_[3 * s] || per_[3 * s + 1] || per_[3 * s + 2];
+        if (!per_any && natoms[s] <= atm_mol_max_atoms()) {
+            is_mol[s] = 1;
+            mol_order_.push_back(s);
+        } else {
+            root_atoms_ += natoms[s];
+        }
+    }
+    std::stable_sort(mol_order_.begin(), mol_order_.end(), [&](int a, int b) { return natoms[a] > natoms[b]; });
+    if (!mol_order_.empty()) {
+        d_mol_order_ = dev_alloc<int>(mol_order_.size());
+        d_sys_mol_ = dev_alloc<uint8_t>(nsys);
+        up(d_mol_order_, mol_order_.data(), sizeof(int) * mol_order_.size());
+        up(d_sys_mol_, is_mol.data(), nsys);
+    }
     check(cudaStreamSynchronize(stream_), "upload sync");
 }
 
@@ -607,7 +626,7 @@ void Engine::run_three_body(const Batch& b, const Species& s, const Damp& d, con
         d_cnt_ = dev_alloc<int>(n + 1);
         d_off_ = dev_alloc<long long>(n + 1);
         d_maxcnt_ = dev_alloc<int>(1);
-        d_queue_ = dev_alloc<unsigned int>(1);
+        d_queue_ = dev_alloc<unsigned int>(2);   // root queue, molecule queue
         d_e3_ = dev_alloc<double>(n);
         d_sig3_ = dev_alloc<double>((size_t)kSigma * n);
         scan_bytes_ = scan_temp_bytes(n);
@@ -618,56 +637,66 @@ void Engine::run_three_body(const Batch& b, const Species& s, const Damp& d, con
         atm_ready_ = true;
     }
     launch_c6_matrix(b, s, w, d_c6mat_off_, d_c6mat_, c6mat_total_, c.mixed, stream);
-    check(cudaMemsetAsync(d_maxcnt_, 0, sizeof(int), stream), "memset");
-    check(cudaMemsetAsync(d_cnt_ + n, 0, sizeof(int), stream), "memset");
-    launch_nbr_count(b, c, d_cnt_, d_maxcnt_, stream);
-    launch_scan(d_scan_temp_, scan_bytes_, d_cnt_, d_off_, n, stream);
-    const int blocks = std::max(1, std::min(n, sms_ * atm_blocks(c.mixed, c.grad)));
-    int stride = atm_stride_;
-    if (!capturing_) {
-        check(cudaMemcpyAsync(h_atm_counts_, d_off_ + n, sizeof(long long), cudaMemcpyDeviceToHost, stream), "total");
-        check(cudaMemcpyAsync(h_atm_counts_ + 1, d_maxcnt_, sizeof(int), cudaMemcpyDeviceToHost, stream), "max");
-        check(cudaStreamSynchronize(stream), "neighbour count");
-        const long long total = h_atm_counts_[0];
-        const int maxcnt = (int)(reinterpret_cast<int*>(h_atm_counts_ + 1)[0]);
-        last_triples_entries_ = total;
-        if (total > nbr_cap_) {
-            void* pj = d_nbr_j_; void* pgd = d_nbr_gend_; void* pv = d_nbr_v_;
-            free_block(pj); free_block(pgd); free_block(pv);
-            nbr_cap_ = total + total / 4 + 1024;
-            d_nbr_j_ = dev_alloc<int>(nbr_cap_);
-            d_nbr_gend_ = dev_alloc<int>(nbr_cap_);
-            d_nbr_v_ = dev_alloc<double4>(nbr_cap_);
+    if (root_atoms_ > 0) {
+        check(cudaMemsetAsync(d_maxcnt_, 0, sizeof(int), stream), "memset");
+        check(cudaMemsetAsync(d_cnt_ + n, 0, sizeof(int), stream), "memset");
+        launch_nbr_count(b, c, d_sys_mol_, d_cnt_, d_maxcnt_, stream);
+        launch_scan(d_scan_temp_, scan_bytes_, d_cnt_, d_off_, n, stream);
+        const int blocks = std::max(1, std::min(n, sms_ * atm_blocks(c.mixed, c.grad)));
+        int stride = atm_stride_;
+        if (!capturing_) {
+            check(cudaMemcpyAsync(h_atm_counts_, d_off_ + n, sizeof(long long), cudaMemcpyDeviceToHost, stream), "total");
+            check(cudaMemcpyAsync(h_atm_counts_ + 1, d_maxcnt_, sizeof(int), cudaMemcpyDeviceToHost, stream), "max");
+            check(cudaStreamSynchronize(stream), "neighbour count");
+            const long long total = h_atm_counts_[0];
+            const int maxcnt = (int)(reinterpret_cast<int*>(h_atm_counts_ + 1)[0]);
+            last_triples_entries_ = total;
+            if (total > nbr_cap_) {
+                void* pj = d_nbr_j_; void* pgd = d_nbr_gend_; void* pv = d_nbr_v_;
+                free_block(pj); free_block(pgd); free_block(pv);
+                nbr_cap_ = total + total / 4 + 1024;
+                d_nbr_j_ = dev_alloc<int>(nbr_cap_);
+                d_nbr_gend_ = dev_alloc<int>(nbr_cap_);
+                d_nbr_v_ = dev_alloc<double4>(nbr_cap_);
+            }
+            // a captured sequence keeps the list length it was captured with: reserve headroom
+            stride = std::max(maxcnt, 1);
+            if (graph_on_) {
+                if (maxcnt > atm_stride_) atm_stride_ = maxcnt + maxcnt / 4 + 32;
+                stride = atm_stride_;
+            }
+            // the slot buffers are sized for the largest resident grid (one block per SM and unit of occupancy)
+            const long long grid = (long long)sms_ * std::max(atm_occupancy(c.mixed, true), atm_occupancy(c.mixed, false));
+            const long long need = grid * stride * 8;   // per-entry accumulators (up to 8 doubles)
+            if (need > slot_cap_) {
+                void* p = d_slot_acc_;
+                free_block(p);
+                slot_cap_ = need + need / 4;
+                d_slot_acc_ = dev_alloc<double>(slot_cap_);
+            }
+            const long long scr_need = grid * stride * (long long)atm_slot_bytes(false);
+            if (scr_need > slot_scr_cap_) {
+                void* p = d_slot_scr_;
+                free_block(p);
+                slot_scr_cap_ = scr_need + scr_need / 4;
+                d_slot_scr_ = dev_alloc<unsigned char>(slot_scr_cap_);
+            }
         }
-        // a captured sequence keeps the list length it was captured with: reserve headroom
-        stride = std::max(maxcnt, 1);
-        if (graph_on_) {
-            if (maxcnt > atm_stride_) atm_stride_ = maxcnt + maxcnt / 4 + 32;
-            stride = atm_stride_;
-        }
-        // the slot buffers are sized for the largest resident grid (one block per SM and unit of occupancy)
-        const long long grid = (long long)sms_ * std::max(atm_occupancy(c.mixed, true), atm_occupancy(c.mixed, false));
-        const long long need = grid * stride * 8;   // per-entry accumulators (up to 8 doubles)
-        if (need > slot_cap_) {
-            void* p = d_slot_acc_;
-            free_block(p);
-            slot_cap_ = need + need / 4;
-            d_slot_acc_ = dev_alloc<double>(slot_cap_);
-        }
-        const long long scr_need = grid * stride * (long long)atm_slot_bytes(false);
-        if (scr_need > slot_scr_cap_) {
-            void* p = d_slot_scr_;
-            free_block(p);
-            slot_scr_cap_ = scr_need + scr_need / 4;
-            d_slot_scr_ = dev_alloc<unsigned char>(slot_scr_cap_);
-        }
+        launch_atm_guard(d_off_ + n, d_maxcnt_, nbr_cap_, stride, d_guard_, stream);
+        launch_nbr_fill(b, c, d_sys_mol_, d_off_, d_nbr_j_, d_nbr_gend_, d_nbr_v_, d_guard_, stream);
+        check(cudaMemsetAsync(d_queue_, 0, sizeof(unsigned int), stream), "memset");
+        w.atm_guard = d_guard_;
+        launch_triples(b, s, d, c, part_, w, d_c6mat_, d_c6mat_off_, d_off_, d_cnt_, d_nbr_j_, d_nbr_gend_, d_nbr_v_,
+                       d_queue_, d_slot_acc_, d_slot_scr_, stride, blocks, d_e3_, d_sig3_, stream);
     }
-    launch_atm_guard(d_off_ + n, d_maxcnt_, nbr_cap_, stride, d_guard_, stream);
-    launch_nbr_fill(b, c, d_off_, d_nbr_j_, d_nbr_gend_, d_nbr_v_, d_guard_, stream);
-    check(cudaMemsetAsync(d_queue_, 0, sizeof(unsigned int), stream), "memset");
-    w.atm_guard = d_guard_;
-    launch_triples(b, s, d, c, part_, w, d_c6mat_, d_c6mat_off_, d_off_, d_cnt_, d_nbr_j_, d_nbr_gend_, d_nbr_v_,
-                   d_queue_, d_slot_acc_, d_slot_scr_, stride, blocks, d_e3_, d_sig3_, stream);
+    if (!mol_order_.empty()) {
+        // after the root kernel, which writes zeros for the molecules' atoms
+        const int nmol = (int)mol_order_.size();
+        const int mblocks = std::max(1, std::min(nmol, sms_ * atm_mol_occupancy(c.mixed, c.grad)));
+        check(cudaMemsetAsync(d_queue_ + 1, 0, sizeof(unsigned int), stream), "memset");
+        launch_triples_mol(b, s, d, c, part_, w, d_c6mat_, d_c6mat_off_, d_mol_order_, nmol, d_queue_ + 1, mblocks,
+                           d_e3_, d_sig3_, stream);
+    }
     w.e3_atom = d_e3_;
     w.sig3_atom = c.grad ? d_sig3_ : nullptr;
 }
@@ -688,6 +717,13 @@ int Engine::atm_occupancy(bool mixed, bool grad)
 {
     int& occ = atm_occ_[mixed ? 1 : 0][grad ? 1 : 0];
     if (occ == 0) occ = atm_blocks_per_sm(mixed, grad);
+    return occ;
+}
+
+int Engine::atm_mol_occupancy(bool mixed, bool grad)
+{
+    int& occ = atm_mol_occ_[mixed ? 1 : 0][grad ? 1 : 0];
+    if (occ == 0) occ = atm_mol_blocks_per_sm(mixed, grad);
     return occ;
 }
 

@@ -150,6 +150,12 @@ private:
     void drop_graph();
     int atm_blocks(bool mixed, bool grad);      // resident triple blocks per SM (tuned)
     int atm_occupancy(bool mixed, bool grad);   // occupancy limit
+    int atm_mol_occupancy(bool mixed, bool grad);
+    int atm_mol_occ_[2][2] = {{0, 0}, {0, 0}};
+    std::vector<int> mol_order_;         // systems of the molecule kernel, largest first
+    int* d_mol_order_ = nullptr;
+    uint8_t* d_sys_mol_ = nullptr;       // [nsys] 1 for those systems
+    long long root_atoms_ = 0;           // atoms of the other systems
     bool graph_on_ = false, capturing_ = false, graph_valid_ = false;
     cudaGraphExec_t graph_exec_ = nullptr;
     GraphKey graph_key_{};

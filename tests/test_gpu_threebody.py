@@ -131,3 +131,42 @@ def test_named_methods_reproduce_fixtures():
         assert abs(float(by_name) - case["energy"]) <= entry.get("tol_rel", 1e-6) * abs(case["energy"])
         checked += 1
     assert checked >= 2
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_mixed_batch_molecules_and_clusters(precision):
+    """One batch with molecules (block-per-molecule kernel) and systems above
+    its size or periodic (neighbour-list kernel), compared per system."""
+    from dftd3 import synthetic as S
+    from dftd3.interface import BatchedDispersion, RationalDampingParam
+    mols = S.batch4096(nmol=6, seed=21)
+    big = S.cluster5000(seed=22, natoms=280)
+    nums = list(mols["numbers"]) + [big["numbers"]]
+    pos = list(mols["positions"]) + [big["positions"]]
+    par = dict(S.PBE_BJ, damping="rational", s9=1.0)
+    bat = BatchedDispersion(nums, pos)
+    bat.set_precision(precision)
+    res = bat.get_dispersion(RationalDampingParam(**{k: par[k] for k in ("s6", "s8", "a1", "a2", "alp", "s9")}),
+                             grad=True)
+    etol, gtol = (RTOL64, GTOL64) if precision == "fp64" else (ETOL_MIXED, None)
+    for k in range(len(nums)):
+        ref = O.dispersion(nums[k], pos[k], par)
+        assert abs(res["energy"][k] - ref["energy"]) <= etol * abs(ref["energy"]), k
+        if gtol:
+            assert np.abs(res["gradient"][k] - ref["gradient"]).max() <= gtol * np.abs(ref["gradient"]).max(), k
+            assert np.abs(res["virial"][k] - ref["virial"]).max() <= gtol * np.abs(ref["virial"]).max(), k
+        else:
+            assert np.abs(res["gradient"][k] - ref["gradient"]).max() <= GTOL_MIXED, k
+
+
+def test_molecule_kernel_energy_only_and_mixed():
+    """Energy-only evaluation and the mixed form of the block-per-molecule kernel."""
+    from dftd3 import synthetic as S
+    d = S.molecule100(seed=8)
+    par = dict(S.PBE_BJ, damping="rational", s9=1.0)
+    ref = O.dispersion(d["numbers"], d["positions"], par)
+    e = gpu_dispersion(d["numbers"], d["positions"], par, grad=False)
+    assert abs(float(e["energy"]) - ref["energy"]) <= RTOL64 * abs(ref["energy"])
+    r = gpu_dispersion(d["numbers"], d["positions"], par, precision="mixed")
+    assert abs(float(r["energy"]) - ref["energy"]) <= ETOL_MIXED * abs(ref["energy"])
+    assert np.abs(r["gradient"] - ref["gradient"]).max() <= GTOL_MIXED
