@@ -39,6 +39,20 @@ struct Batch {
     const int* perm = nullptr;           // [natoms] or null (input order)
     const double4* tiles = nullptr;      // [ntiles] bounding sphere (centre, radius) of 32 slots, or null
     const int* tile_off = nullptr;       // [nsys + 1] first tile of each system
+    const int* tile_sys = nullptr;       // [ntiles] system of each tile
+};
+
+// Tile-pair work units of the two-body sum (d3_pair_tt.cu): for every
+// system, the pairs (it >= jt) of its tiles in the order it = 0.., jt = 0..it,
+// starting at unit_base[sys]; per-unit slots of kTile lanes.
+struct PairUnits {
+    const int2* units = nullptr;         // [nunits] global tile indices (it, jt)
+    int nunits = 0;
+    const int* unit_base = nullptr;      // [nsys]
+    void* U = nullptr;                   // [natoms][nid][kMaxRef] species vectors (R)
+    void* dU = nullptr;                  // same with dgw
+    double* unit_i = nullptr;            // [nunits][kTile][15]
+    double* unit_j = nullptr;            // [nunits][kTile][4]
 };
 
 constexpr int kTile = 32;               // atoms per tile (one warp)
@@ -137,6 +151,13 @@ void launch_two_body_tiled(const Batch& b, const Species& s, const Damp& d, cons
                            const Work& w, cudaStream_t stream);
 void launch_cn_chain_rule_tiled(const Batch& b, const Species& s, const Config& c, const Partition& p,
                                 const Work& w, cudaStream_t stream);
+
+// Two-body sum over tile-pair units, each atom pair once, with the per-atom
+// gather (d3_pair_tt.cu); writes e_atom, dEdcn, grad, sig_atom, pg_atom.
+size_t pair_unit_slot_doubles();   // per unit: i and j slots
+size_t pair_unit_i_doubles();      // per unit: i slots
+void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
+                           const Work& w, const PairUnits& pu, cudaStream_t stream);
 
 // Three-body term (d3_atm.cu): C6 table, neighbour lists, triple sum.
 size_t atm_c6_entry_bytes(bool mixed);

@@ -255,6 +255,26 @@ Engine::Engine(int nsys, const int* natoms, const int* numbers, const double* la
         for (int t = 0; t < nt; t++) tile_sys.push_back(sy);
     }
     ntiles_ = tile_off[nsys];
+    // two-body units: tile pairs (it >= jt) of each system
+    std::vector<int2> units;
+    std::vector<int> unit_base(nsys, 0);
+    for (int sy = 0; sy < nsys; sy++) {
+        unit_base[sy] = (int)units.size();
+        const int nt = tile_off[sy + 1] - tile_off[sy];
+        for (int it = 0; it < nt; it++)
+            for (int jt = 0; jt <= it; jt++) units.push_back(make_int2(tile_off[sy] + it, tile_off[sy] + jt));
+    }
+    pu_.nunits = (int)units.size();
+    d_units_ = dev_alloc<int2>(std::max<size_t>(units.size(), 1));
+    d_unit_base_ = dev_alloc<int>(nsys);
+    up(d_units_, units.data(), sizeof(int2) * units.size());
+    up(d_unit_base_, unit_base.data(), sizeof(int) * nsys);
+    pu_.units = d_units_;
+    pu_.unit_base = d_unit_base_;
+    pu_.U = dev_alloc<double>((size_t)natoms_ * nid * kMaxRef);
+    pu_.dU = dev_alloc<double>((size_t)natoms_ * nid * kMaxRef);
+    pu_.unit_i = dev_alloc<double>((size_t)std::max(pu_.nunits, 1) * pair_unit_slot_doubles());
+    pu_.unit_j = pu_.unit_i + (size_t)std::max(pu_.nunits, 1) * pair_unit_i_doubles();
     d_tile_off_ = dev_alloc<int>(nsys + 1);
     d_tile_sys_ = dev_alloc<int>(std::max(ntiles_, 1));
     up(d_tile_off_, tile_off.data(), sizeof(int) * (nsys + 1));
@@ -510,7 +530,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     b.sys_of_atom = d_sys_of_atom_; b.atom_off = d_atom_off_; b.local = d_local_sorted_; b.sp = d_sp_sorted_;
     b.ghost = d_ghost_sorted_; b.img_off = d_img_off_; b.img = d_img_;
     b.x = d_x_; b.y = d_y_; b.z = d_z_; b.xhi = d_xhi_; b.xlo = d_xlo_;
-    b.perm = d_perm_; b.tiles = d_tiles_; b.tile_off = d_tile_off_;
+    b.perm = d_perm_; b.tiles = d_tiles_; b.tile_off = d_tile_off_; b.tile_sys = d_tile_sys_;
     Species s;
     s.rcov = d_rcov_; s.nref = d_nref_; s.refcn = d_refcn_; s.c6ref = d_c6ref_;
     s.c6ref_f = d_c6ref_f_; s.pair = d_pair_; s.atm_r0 = d_atm_r0_;
@@ -545,7 +565,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     launch_weights(b, s, c, w, stream);
     mark(3);
     if (std::fabs(d.s6) >= DBL_EPSILON || std::fabs(d.s8) >= DBL_EPSILON || pg) {
-        launch_two_body(b, s, d, c, part_, w, stream);
+        launch_two_body_units(b, s, d, c, part_, w, pu_, stream);
     } else {
         check(cudaMemsetAsync(w.e_atom, 0, sizeof(double) * natoms_, stream), "memset");
         if (grad) {

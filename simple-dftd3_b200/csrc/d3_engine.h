@@ -152,6 +152,10 @@ private:
     int atm_occupancy(bool mixed, bool grad);   // occupancy limit
     int atm_mol_occupancy(bool mixed, bool grad);
     int atm_mol_occ_[2][2] = {{0, 0}, {0, 0}};
+    // two-body tile-pair units
+    PairUnits pu_;
+    int2* d_units_ = nullptr;
+    int* d_unit_base_ = nullptr;
     std::vector<int> mol_order_;         // systems of the molecule kernel, largest first
     int* d_mol_order_ = nullptr;
     uint8_t* d_sys_mol_ = nullptr;       // [nsys] 1 for those systems

@@ -110,6 +110,11 @@ __device__ __forceinline__ unsigned reach(const typename ShOf<R>::type* buf, int
     return __ballot_sync(0xffffffffu, ok);
 }
 
+// Reciprocal and reciprocal square root of the pair arithmetic: IEEE in the
+// FP64 form, the hardware approximations (a few ulp) in the FP32 part of the
+// mixed form.
+template <class R> __device__ __forceinline__ R r_rcp(R x) { if constexpr (sizeof(R) == 8) return R(1) / x; else return __fdividef(1.0f, x); }
+template <class R> __device__ __forceinline__ R r_rsqrt(R x) { if constexpr (sizeof(R) == 8) return R(1) / sqrt(x); else return rsqrtf(x); }
 template <class R> __device__ __forceinline__ R r_sqrt(R x) { if constexpr (sizeof(R) == 8) return sqrt(x); else return sqrtf(x); }
 template <class R> __device__ __forceinline__ R r_exp(R x) { if constexpr (sizeof(R) == 8) return exp(x); else return expf(x); }
 template <class R> __device__ __forceinline__ R r_pow(R x, R a) { if constexpr (sizeof(R) == 8) return pow(x, a); else return powf(x, a); }
@@ -126,6 +131,22 @@ __device__ __forceinline__ void smooth(R r, R cutoff, R width, R& sw, R& dswdr)
         const R x = (cutoff - r) / width;
         sw = x * x * x * (R(10) + x * (R(-15) + R(6) * x));
         dswdr = R(-30) * x * x * (R(1) - x) * (R(1) - x) / width;
+    }
+}
+
+// Counting function 1 / (1 + exp(-kcn (rc / r - 1))) (ncoord.f90:124-131);
+// optionally returns 1 / r.
+template <class R>
+__device__ __forceinline__ R r_cn_count(R rc, R r2, R* inv_r = nullptr)
+{
+    if constexpr (sizeof(R) == 8) {
+        const R r1 = sqrt(r2);
+        if (inv_r) *inv_r = R(1) / r1;
+        return R(1) / (R(1) + exp(-R(kKcn) * (rc / r1 - R(1))));
+    } else {
+        const R ir = rsqrtf(r2);
+        if (inv_r) *inv_r = ir;
+        return __fdividef(1.0f, 1.0f + expf(-R(kKcn) * (rc * ir - R(1))));
     }
 }
 
@@ -193,8 +214,7 @@ __global__ void __launch_bounds__(32 * W, 16 / W) k_cn_tiled(Batch b, Species s,
                     disp(sbuf[wib][k], xj, yj, zj, hj, lj, vx, vy, vz);
                     const R r2 = vx * vx + vy * vy + vz * vz;
                     if (!valid || r2 > cut2 || r2 < R(1.0e-12)) continue;
-                    const R r1 = r_sqrt<R>(r2);
-                    tacc += R(1) / (R(1) + r_exp<R>(-R(kKcn) * (rc / r1 - R(1))));
+                    tacc += r_cn_count<R>(rc, r2);
                     nterm += (jj <= i);
                 }
             }
@@ -324,7 +344,7 @@ __global__ void __launch_bounds__(32 * W, 16 / W) k_two_body_tiled(Batch b, Spec
                         // rational.f90:462-497: q1 = R0^6, q2 = R0^8, q3 = R0, q4 = sqrt(rrij)
                         const R r4 = r2 * r2;
                         const R a6 = r4 * r2 + q1, a8 = r4 * r4 + q2;
-                        const R inv = R(1) / (a6 * a8);
+                        const R inv = r_rcp<R>(a6 * a8);
                         const R t6 = a8 * inv;
                         const R t8 = a6 * inv;
                         const R d6 = R(-6) * r4 * t6 * t6;
@@ -473,11 +493,19 @@ __global__ void __launch_bounds__(32 * W, 16 / W) k_chain_tiled(Batch b, Species
                     disp(sbuf[wib][k], xj, yj, zj, hj, lj, vx, vy, vz);
                     const R r2 = vx * vx + vy * vy + vz * vz;
                     if (!valid || r2 > cut2 || r2 < R(1.0e-12)) continue;
-                    const R r1 = r_sqrt<R>(r2);
-                    const R expterm = r_exp<R>(-R(kKcn) * (rc / r1 - R(1)));
-                    const R cf = R(1) / (R(1) + expterm);
-                    const R dcf = -cf * (R(1) - cf) * R(kKcn) * rc / r2;
-                    const R f = dcf / r1 * dsum;
+                    R f;
+                    if constexpr (sizeof(R) == 8) {
+                        // ncoord.f90:198-206
+                        const R r1 = sqrt(r2);
+                        const R cf = R(1) / (R(1) + exp(-R(kKcn) * (rc / r1 - R(1))));
+                        const R dcf = -cf * (R(1) - cf) * R(kKcn) * rc / r2;
+                        f = dcf / r1 * dsum;
+                    } else {
+                        R irr;
+                        const R cf = r_cn_count<R>(rc, r2, &irr);
+                        // dcf / r = -cf (1 - cf) kcn rc / r^3
+                        f = -cf * (R(1) - cf) * R(kKcn) * rc * (irr * irr * irr) * dsum;
+                    }
                     const R cx = f * vx, cy = f * vy, cz = f * vz;
                     if (jj != i) { tgx += cx; tgy += cy; tgz += cz; }
                     txx += cx * vx; tyy += cy * vy; tzz += cz * vz;

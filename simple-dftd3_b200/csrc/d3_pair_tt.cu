@@ -1,0 +1,466 @@
+// Two-body dispersion over tile pairs, each unordered atom pair once.
+//
+// The sorted atoms of every system form tiles of 32 (d3_pair.cu).  A work
+// unit is a pair of tiles (it >= jt) of one system; one warp evaluates it with
+// one lane per atom i of tile it, while the partner atom j of tile jt and the
+// lattice translation T are the same for the whole warp at each step.  The
+// translations that can join the two tiles' bounding spheres within the
+// cutoff are compacted per chunk of 128 into shared memory.  Every pair
+// (i, j, T) of the reference's loop (rational.f90:438-514, zero.f90:455-553)
+// is evaluated once: i's energy, virial and parameter-derivative shares hold
+// both halves of the pair, i's gradient and dE/dCN stay in the lane, and j's
+// gradient and dE/dCN are summed over the warp once per (chunk, j).  C6 and
+// its CN derivatives come from per-atom species vectors
+// U_j[s][r] = sum_r' C6ref(r, r', s, s_j) gw_j[r'] (get_atomic_c6,
+// model.f90:432-461): seven multiply-adds per (i, j).  Each unit writes its
+// per-lane sums to its own slots; a gather kernel adds the slots of every
+// atom in a fixed order, so results are deterministic and no atomics are used.
+#include <cfloat>
+#include <cstdint>
+
+#include "d3_device.cuh"
+
+namespace d3 {
+
+namespace {
+
+constexpr int kTTWarps = 4;
+constexpr int kTTThreads = 32 * kTTWarps;
+constexpr int kTTChunk = 128;     // translations tested per pass
+constexpr int kUnitI = 15;        // per-lane i sums: E, dE/dCN, g(3), sigma(6), dE/dparam(4)
+constexpr int kUnitJ = 4;         // per-lane j sums: dE/dCN, g(3)
+constexpr int kSplitJ = 2;        // a unit is evaluated as kSplitJ x kSplitT items
+constexpr int kSplitT = 2;        // (halves of the j tile and of the translation list)
+constexpr int kSplit = kSplitJ * kSplitT;
+
+template <class R> struct T4;
+template <> struct T4<float> { using type = float4; };
+template <> struct T4<double> { using type = double4; };
+
+template <class R> __device__ __forceinline__ R tt_rcp(R x) { if constexpr (sizeof(R) == 8) return R(1) / x; else return __fdividef(1.0f, x); }
+template <class R> __device__ __forceinline__ R tt_sqrt(R x) { if constexpr (sizeof(R) == 8) return sqrt(x); else return sqrtf(x); }
+template <class R> __device__ __forceinline__ R tt_pow(R x, R a) { if constexpr (sizeof(R) == 8) return pow(x, a); else return powf(x, a); }
+
+template <class R>
+__device__ __forceinline__ void tt_smooth(R r, R cutoff, R width, R& sw, R& dswdr)
+{
+    // cutoff.f90:73-99
+    if (width <= R(0) || width >= cutoff) { sw = R(1); dswdr = R(0); return; }
+    const R inner = cutoff - width;
+    if (r <= inner) { sw = R(1); dswdr = R(0); }
+    else if (r >= cutoff) { sw = R(0); dswdr = R(0); }
+    else {
+        const R x = (cutoff - r) / width;
+        sw = x * x * x * (R(10) + x * (R(-15) + R(6) * x));
+        dswdr = R(-30) * x * x * (R(1) - x) * (R(1) - x) / width;
+    }
+}
+
+__device__ __forceinline__ bool tt_owns(const Partition& p, int i, int j)
+{
+    // partition.f90:127-147 on system-local input indices
+    if (p.nparts <= 1) return true;
+    long long hi = i > j ? i : j, lo = i > j ? j : i;
+    return (hi * (hi + 1) / 2 + lo) % p.nparts == p.part;
+}
+
+template <class R>
+__device__ __forceinline__ R wsum_tt(R v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Species vectors U[a][s][r] and dU[a][s][r] of every atom (sorted order).
+template <class R>
+__global__ void k_species_vectors(Batch b, Species s, Work w, R* U, R* dU)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long total = (long long)b.natoms * b.nid * kMaxRef;
+    if (t >= total) return;
+    const int a = (int)(t / (b.nid * kMaxRef));
+    const int rem = (int)(t % (b.nid * kMaxRef));
+    const int sx = rem / kMaxRef, r = rem % kMaxRef;
+    const int sa = b.sp[a];
+    double u = 0.0, du = 0.0;
+    if (!(b.ghost && b.ghost[a]) && r < s.nref[sx]) {
+        const double* ref = s.c6ref + ((size_t)(sx * b.nid + sa) * kMaxRef + r) * kMaxRef;
+        for (int q = 0; q < s.nref[sa]; q++) {
+            u += w.gw[a * kMaxRef + q] * __ldg(ref + q);
+            du += w.dgw[a * kMaxRef + q] * __ldg(ref + q);
+        }
+    }
+    U[t] = R(u);
+    dU[t] = R(du);
+}
+
+template <class R, int DAMP, bool GRAD, bool PG>
+__global__ void __launch_bounds__(kTTThreads)
+k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const int2* units, int nunits,
+              const R* U, const R* dU, double* unit_i, double* unit_j)
+{
+    using V = typename T4<R>::type;
+    __shared__ V sth[kTTWarps][kTTChunk];
+    __shared__ V stl[kTTWarps][kTTChunk];
+    __shared__ int sidx[kTTWarps][kTTChunk];     // image index of each compacted translation
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int item = blockIdx.x * kTTWarps + wid;
+    if (item >= nunits * kSplit) return;
+    const int u = item / kSplit, sub = item % kSplit;
+    const int jh = sub / kSplitT, th = sub % kSplitT;
+    const int it = units[u].x, jt = units[u].y;
+    const int sys = b.tile_sys[it];
+    const int t0 = b.tile_off[sys];
+    const int as = b.atom_off[sys], ae = b.atom_off[sys + 1];
+    const int ia0 = as + kTile * (it - t0), ja0 = as + kTile * (jt - t0);
+    const int ni = min(kTile, ae - ia0), nj = min(kTile, ae - ja0);
+    const bool diag = it == jt;
+    const int i = ia0 + lane;
+    const bool ivalid = lane < ni;
+    const int ic = ivalid ? i : ia0;
+    const int si = b.sp[ic], li = b.local[ic];
+    const bool gi = b.ghost && b.ghost[ic];
+    const double xi = b.x[ic], yi = b.y[ic], zi = b.z[ic];
+    R hix, hiy, hiz, lix = R(0), liy = R(0), liz = R(0);
+    if constexpr (sizeof(R) == 8) { hix = xi; hiy = yi; hiz = zi; }
+    else {
+        hix = __double2float_rn(xi); lix = __double2float_rn(xi - (double)hix);
+        hiy = __double2float_rn(yi); liy = __double2float_rn(yi - (double)hiy);
+        hiz = __double2float_rn(zi); liz = __double2float_rn(zi - (double)hiz);
+    }
+    R gwi[kMaxRef], dgwi[kMaxRef];
+#pragma unroll
+    for (int r = 0; r < kMaxRef; r++) {
+        if constexpr (sizeof(R) == 8) { gwi[r] = w.gw[ic * kMaxRef + r]; dgwi[r] = w.dgw[ic * kMaxRef + r]; }
+        else { gwi[r] = w.gwf[ic * kMaxRef + r]; dgwi[r] = w.dgwf[ic * kMaxRef + r]; }
+    }
+    const int tt0 = b.img_off[kImgDisp2 * (b.nsys + 1) + sys], tt1 = b.img_off[kImgDisp2 * (b.nsys + 1) + sys + 1];
+    const double4 ci = b.tiles[it], cj = b.tiles[jt];
+    const double lim = c.cut2 + ci.w + cj.w + 1.0e-6 * c.cut2 + 1.0e-6;
+    const double limj = c.cut2 + ci.w + 1.0e-6 * c.cut2 + 1.0e-6;   // one atom j against tile it
+    const double dcx = ci.x - cj.x, dcy = ci.y - cj.y, dcz = ci.z - cj.z;
+    const R cutoff = R(c.cut2), cut2 = R(c.cut2 * c.cut2), width = R(c.width2);
+    const bool smooth_on = c.width2 > 0.0 && c.width2 < c.cut2;
+    const R s6 = R(d.s6), s8 = R(d.s8);
+    const R alp6 = R(d.alp), alp8 = R(d.alp + 2.0);
+    const int nid = b.nid;
+    // i sums (FP64) and their FP32 partials
+    double a_e = 0, a_de = 0, a_gx = 0, a_gy = 0, a_gz = 0;
+    double a_xx = 0, a_yy = 0, a_zz = 0, a_xy = 0, a_xz = 0, a_yz = 0;
+    double a_p0 = 0, a_p1 = 0, a_p2 = 0, a_p3 = 0;
+    R te = R(0), tde = R(0), tgx = R(0), tgy = R(0), tgz = R(0);
+    R txx = R(0), tyy = R(0), tzz = R(0), txy = R(0), txz = R(0), tyz = R(0);
+    R tp0 = R(0), tp1 = R(0), tp2 = R(0), tp3 = R(0);
+    int pending = 0;          // terms in the FP32 partials (warp-uniform)
+    // j sums of atom ja0 + lane (FP64)
+    double b_de = 0, b_gx = 0, b_gy = 0, b_gz = 0;
+    unsigned long long nterm = 0;
+
+    auto flush = [&]() {
+        a_e += double(te); a_de += double(tde);
+        te = tde = R(0);
+        if (GRAD) {
+            a_gx += double(tgx); a_gy += double(tgy); a_gz += double(tgz);
+            a_xx += double(txx); a_yy += double(tyy); a_zz += double(tzz);
+            a_xy += double(txy); a_xz += double(txz); a_yz += double(tyz);
+            tgx = tgy = tgz = txx = tyy = tzz = txy = txz = tyz = R(0);
+        }
+        if (PG) {
+            a_p0 += double(tp0); a_p1 += double(tp1); a_p2 += double(tp2); a_p3 += double(tp3);
+            tp0 = tp1 = tp2 = tp3 = R(0);
+        }
+        pending = 0;
+    };
+
+    for (int tc = tt0; tc < tt1; tc += kTTChunk) {
+        const int nt = min(kTTChunk, tt1 - tc);
+        // translations that can join the two tiles
+        int nreach = 0;
+#pragma unroll
+        for (int q = 0; q < kTTChunk / 32; q++) {
+            const int k = 32 * q + lane;
+            bool ok = false;
+            double tx = 0, ty = 0, tz = 0;
+            if (k < nt) {
+                tx = __ldg(b.img + 3 * (tc + k)); ty = __ldg(b.img + 3 * (tc + k) + 1);
+                tz = __ldg(b.img + 3 * (tc + k) + 2);
+                const double ex = dcx - tx, ey = dcy - ty, ez = dcz - tz;
+                ok = ex * ex + ey * ey + ez * ez <= lim * lim;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (ok) {
+                const int pos = nreach + __popc(m & ((1u << lane) - 1u));
+                sidx[wid][pos] = tc + k;
+                if constexpr (sizeof(R) == 8) {
+                    sth[wid][pos] = make_double4(tx, ty, tz, 0.0);
+                } else {
+                    const float hx = __double2float_rn(tx), hy = __double2float_rn(ty), hz = __double2float_rn(tz);
+                    sth[wid][pos] = make_float4(hx, hy, hz, 0.f);
+                    stl[wid][pos] = make_float4(__double2float_rn(tx - (double)hx), __double2float_rn(ty - (double)hy),
+                                                __double2float_rn(tz - (double)hz), 0.f);
+                }
+            }
+            nreach += __popc(m);
+        }
+        __syncwarp();
+        if (nreach == 0) continue;
+        // this item's half of the reachable translations
+        const int qhalf = (nreach + kSplitT - 1) / kSplitT;
+        const int qbeg = th * qhalf, qend = min(nreach, qbeg + qhalf);
+        if (qbeg >= qend) continue;
+        const int jl0 = jh * (kTile / kSplitJ), jl1 = min(nj, jl0 + kTile / kSplitJ);
+        for (int jl = jl0; jl < jl1; jl++) {
+            const int j = ja0 + jl;
+            const bool self = diag && jl == lane;
+            bool valid = ivalid && (!diag || jl <= lane) && !gi;
+            const int lj = b.local[j];
+            if (valid && p.nparts > 1) valid = tt_owns(p, li, lj);
+            const int sj = b.sp[j];
+            // C6 and its CN derivatives from the species vectors of j
+            R c6 = R(0), dc6i = R(0), dc6j = R(0);
+            if (valid) {
+                const R* uj = U + ((size_t)j * nid + si) * kMaxRef;
+                const R* duj = dU + ((size_t)j * nid + si) * kMaxRef;
+#pragma unroll
+                for (int r = 0; r < kMaxRef; r++) {
+                    const R ur = __ldg(uj + r), dur = __ldg(duj + r);
+                    c6 += gwi[r] * ur;
+                    dc6i += dgwi[r] * ur;
+                    dc6j += gwi[r] * dur;
+                }
+                valid = c6 != R(0);
+            }
+            if (!__any_sync(0xffffffffu, valid)) continue;
+            const double xj = b.x[j], yj = b.y[j], zj = b.z[j];
+            R dhx, dhy, dhz, dlx = R(0), dly = R(0), dlz = R(0);
+            if constexpr (sizeof(R) == 8) { dhx = xi - xj; dhy = yi - yj; dhz = zi - zj; }
+            else {
+                const float4 hj = b.xhi[j], lj4 = b.xlo[j];
+                dhx = hix - hj.x; dhy = hiy - hj.y; dhz = hiz - hj.z;
+                dlx = lix - lj4.x; dly = liy - lj4.y; dlz = liz - lj4.z;
+            }
+            const double* pr = s.pair + kPairSlots * (si * nid + sj);
+            const R rrij = R(__ldg(pr + 0));
+            const R q1 = R(__ldg(pr + 1)), q2 = R(__ldg(pr + 2)), q3 = R(__ldg(pr + 3)), q4 = R(__ldg(pr + 4));
+            // both halves of a pair go to i; a self pair (j = i, T != 0) is one half
+            const R we = self ? R(0.5) : R(1);
+            R jde = R(0), jgx = R(0), jgy = R(0), jgz = R(0);
+            // translations of this half that can bring j within the cutoff of tile it
+            unsigned jm[(kTTChunk / kSplitT + 31) / 32];
+#pragma unroll
+            for (int h = 0; h < (kTTChunk / kSplitT + 31) / 32; h++) {
+                const int q = qbeg + 32 * h + lane;
+                bool ok = false;
+                if (q < qend) {
+                    const int tix = sidx[wid][q];   // absolute image index
+                    const double ex = ci.x - xj - __ldg(b.img + 3 * tix), ey = ci.y - yj - __ldg(b.img + 3 * tix + 1),
+                                 ez = ci.z - zj - __ldg(b.img + 3 * tix + 2);
+                    ok = ex * ex + ey * ey + ez * ez <= limj * limj;
+                }
+                jm[h] = __ballot_sync(0xffffffffu, ok);
+            }
+#pragma unroll
+            for (int h = 0; h < (kTTChunk / kSplitT + 31) / 32; h++)
+            for (unsigned mm = jm[h]; mm; mm &= mm - 1) {
+                const int q = qbeg + 32 * h + __ffs(mm) - 1;
+                const V th = sth[wid][q];
+                R vx, vy, vz;
+                if constexpr (sizeof(R) == 8) { vx = dhx - th.x; vy = dhy - th.y; vz = dhz - th.z; }
+                else {
+                    const V tl = stl[wid][q];
+                    vx = (dhx - th.x) + (dlx - tl.x);
+                    vy = (dhy - th.y) + (dly - tl.y);
+                    vz = (dhz - th.z) + (dlz - tl.z);
+                }
+                const R r2 = vx * vx + vy * vy + vz * vz;
+                if (!valid || r2 > cut2 || r2 < R(DBL_EPSILON)) continue;
+                nterm++;
+                R sw = R(1), dswdr = R(0), r1 = R(0);
+                if (smooth_on) { r1 = tt_sqrt<R>(r2); tt_smooth<R>(r1, cutoff, width, sw, dswdr); }
+                R edisp0, gdisp0, e6, e8, dpa = R(0), dpb = R(0);
+                if constexpr (DAMP == kRational) {
+                    // rational.f90:462-497: q1 = R0^6, q2 = R0^8, q3 = R0, q4 = sqrt(rrij)
+                    const R r4 = r2 * r2;
+                    const R a6 = r4 * r2 + q1, a8 = r4 * r4 + q2;
+                    const R inv = tt_rcp<R>(a6 * a8);
+                    const R t6 = a8 * inv;
+                    const R t8 = a6 * inv;
+                    const R d6 = R(-6) * r4 * t6 * t6;
+                    const R d8 = R(-8) * r4 * r2 * t8 * t8;
+                    e6 = t6; e8 = rrij * t8;
+                    edisp0 = s6 * t6 + s8 * rrij * t8;
+                    gdisp0 = s6 * d6 + s8 * rrij * d8;
+                    if (PG) {
+                        const R dedr0 = s6 * R(-6) * (q1 / q3) * t6 * t6 + s8 * rrij * R(-8) * (q2 / q3) * t8 * t8;
+                        dpa = dedr0 * q4;
+                        dpb = dedr0;
+                    }
+                } else {
+                    // zero.f90:490-536: q1 = rs6 R0, q2 = rs8 R0
+                    if (!smooth_on) r1 = tt_sqrt<R>(r2);
+                    const R r6 = r2 * r2 * r2;
+                    const R r8 = r6 * r2;
+                    const R t6 = tt_pow<R>(q1 / r1, alp6);
+                    const R t8 = tt_pow<R>(q2 / r1, alp8);
+                    const R f6 = R(1) / (R(1) + R(6) * t6);
+                    const R f8 = R(1) / (R(1) + R(6) * t8);
+                    const R d6 = R(-6) * f6 / r2 + R(6) * alp6 * t6 * (f6 * f6) / r2;
+                    const R d8 = R(-8) * f8 / r2 + R(6) * alp8 * t8 * (f8 * f8) / r2;
+                    e6 = f6 / r6; e8 = rrij * f8 / r8;
+                    edisp0 = s6 * f6 / r6 + s8 * rrij * f8 / r8;
+                    gdisp0 = s6 * d6 / r6 + s8 * rrij * d8 / r8;
+                    if (PG) {
+                        dpa = d.rs6 != 0.0 ? s6 / r6 * R(-6) * f6 * f6 * alp6 * t6 / R(d.rs6) : R(0);
+                        dpb = d.rs8 != 0.0 ? s8 * rrij / r8 * R(-6) * f8 * f8 * alp8 * t8 / R(d.rs8) : R(0);
+                    }
+                }
+                const R edisp = sw * edisp0;
+                te -= c6 * edisp * we;
+                tde -= dc6i * edisp;
+                if (!self) jde -= dc6j * edisp;
+                if (PG) {
+                    const R hc = -c6 * sw * we;
+                    tp0 += hc * e6; tp1 += hc * e8;
+                    tp2 += hc * dpa; tp3 += hc * dpb;
+                }
+                if (GRAD) {
+                    R gdisp = sw * gdisp0;
+                    if (smooth_on) gdisp += dswdr * edisp0 / r1;
+                    const R f = -c6 * gdisp;
+                    const R dgx = f * vx, dgy = f * vy, dgz = f * vz;
+                    if (!self) {
+                        tgx += dgx; tgy += dgy; tgz += dgz;
+                        jgx -= dgx; jgy -= dgy; jgz -= dgz;
+                    }
+                    const R fx = we * dgx, fy = we * dgy, fz = we * dgz;
+                    txx += fx * vx; tyy += fy * vy; tzz += fz * vz;
+                    txy += fx * vy; txz += fx * vz; tyz += fy * vz;
+                }
+            }
+            // j's share, summed over the warp's atoms i
+            jde = wsum_tt<R>(jde);
+            if (GRAD) { jgx = wsum_tt<R>(jgx); jgy = wsum_tt<R>(jgy); jgz = wsum_tt<R>(jgz); }
+            if (lane == jl) {
+                b_de += double(jde);
+                if (GRAD) { b_gx += double(jgx); b_gy += double(jgy); b_gz += double(jgz); }
+            }
+            if constexpr (sizeof(R) == 4) {
+                pending += qend - qbeg;
+                if (pending >= 128) flush();
+            }
+        }
+    }
+    flush();
+    double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
+    oi[0] = a_e; oi[1] = a_de;
+    oi[2] = a_gx; oi[3] = a_gy; oi[4] = a_gz;
+    oi[5] = a_xx; oi[6] = a_yy; oi[7] = a_zz; oi[8] = a_xy; oi[9] = a_xz; oi[10] = a_yz;
+    oi[11] = a_p0; oi[12] = a_p1; oi[13] = a_p2; oi[14] = a_p3;
+    double* oj = unit_j + ((size_t)item * kTile + lane) * kUnitJ;
+    oj[0] = b_de; oj[1] = b_gx; oj[2] = b_gy; oj[3] = b_gz;
+    if (w.counts) {
+        for (int off = 16; off > 0; off >>= 1) nterm += __shfl_xor_sync(0xffffffffu, nterm, off);
+        if (lane == 0) atomicAdd(w.counts + 0, nterm);
+    }
+}
+
+// Per-atom sums of the unit slots in a fixed order: one warp per atom, the
+// lanes take the atom's slots (its i slots of the units (t, jt <= t), then
+// its j slots of the units (it >= t, t)) round robin and a fixed shuffle tree
+// adds the lane sums.
+__global__ void k_unit_gather(Batch b, Config c, const int* unit_base, const double* unit_i, const double* unit_j,
+                              Work w)
+{
+    const int lane = threadIdx.x & 31;
+    const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (a >= b.natoms) return;
+    const int sys = b.sys_of_atom[a];
+    const int as = b.atom_off[sys];
+    const int t0 = b.tile_off[sys], t1 = b.tile_off[sys + 1];
+    const int tl = (a - as) / kTile;              // tile of a, local to the system
+    const int sl = (a - as) % kTile;              // slot lane
+    const int nt = t1 - t0;
+    const long long base = unit_base[sys];
+    double v[kUnitI];
+#pragma unroll
+    for (int k = 0; k < kUnitI; k++) v[k] = 0.0;
+    const int ni = (tl + 1) * kSplit, nj = (nt - tl) * kSplit;
+    for (int q = lane; q < ni; q += 32) {
+        const int jt = q / kSplit, sb = q % kSplit;
+        const long long item = (base + (long long)tl * (tl + 1) / 2 + jt) * kSplit + sb;
+        const double* o = unit_i + (item * kTile + sl) * kUnitI;
+#pragma unroll
+        for (int k = 0; k < kUnitI; k++) v[k] += o[k];
+    }
+    for (int q = lane; q < nj; q += 32) {
+        const int it = tl + q / kSplit, sb = q % kSplit;
+        const long long item = (base + (long long)it * (it + 1) / 2 + tl) * kSplit + sb;
+        const double* o = unit_j + (item * kTile + sl) * kUnitJ;
+        v[1] += o[0]; v[2] += o[1]; v[3] += o[2]; v[4] += o[3];
+    }
+#pragma unroll
+    for (int k = 0; k < kUnitI; k++) v[k] = wsum_tt<double>(v[k]);
+    if (lane != 0) return;
+    w.e_atom[a] = v[0];
+    if (w.dEdcn) w.dEdcn[a] = v[1];
+    if (c.grad) {
+        w.grad[3 * a + 0] = v[2]; w.grad[3 * a + 1] = v[3]; w.grad[3 * a + 2] = v[4];
+        double* sg = w.sig_atom + kSigma * a;
+        for (int k = 0; k < kSigma; k++) sg[k] = v[5 + k];
+    }
+    if (c.param_grad && w.pg_atom) {
+        double* pg = w.pg_atom + kParamGrad * a;
+        for (int k = 0; k < 4; k++) pg[k] = v[11 + k];
+    }
+}
+
+template <class R, int DAMP, bool GRAD, bool PG>
+void launch_tt(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p, const Work& w,
+               const PairUnits& pu, cudaStream_t stream)
+{
+    const int blocks = (pu.nunits * kSplit + kTTWarps - 1) / kTTWarps;
+    k_two_body_tt<R, DAMP, GRAD, PG><<<blocks, kTTThreads, 0, stream>>>(
+        b, s, d, c, p, w, pu.units, pu.nunits, (const R*)pu.U, (const R*)pu.dU, pu.unit_i, pu.unit_j);
+}
+
+template <class R, int DAMP>
+void launch_tt_flags(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
+                     const Work& w, const PairUnits& pu, cudaStream_t stream)
+{
+    if (c.grad) {
+        if (c.param_grad) launch_tt<R, DAMP, true, true>(b, s, d, c, p, w, pu, stream);
+        else launch_tt<R, DAMP, true, false>(b, s, d, c, p, w, pu, stream);
+    } else {
+        if (c.param_grad) launch_tt<R, DAMP, false, true>(b, s, d, c, p, w, pu, stream);
+        else launch_tt<R, DAMP, false, false>(b, s, d, c, p, w, pu, stream);
+    }
+}
+
+}  // namespace
+
+size_t pair_unit_slot_doubles() { return (size_t)kSplit * kTile * (kUnitI + kUnitJ); }
+size_t pair_unit_i_doubles() { return (size_t)kSplit * kTile * kUnitI; }
+
+void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
+                           const Work& w, const PairUnits& pu, cudaStream_t stream)
+{
+    if (b.natoms <= 0) return;
+    const long long nsv = (long long)b.natoms * b.nid * kMaxRef;
+    if (c.mixed)
+        k_species_vectors<float><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (float*)pu.U, (float*)pu.dU);
+    else
+        k_species_vectors<double><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (double*)pu.U, (double*)pu.dU);
+    if (pu.nunits > 0) {
+        if (d.kind == kRational) {
+            if (c.mixed) launch_tt_flags<float, kRational>(b, s, d, c, p, w, pu, stream);
+            else launch_tt_flags<double, kRational>(b, s, d, c, p, w, pu, stream);
+        } else {
+            if (c.mixed) launch_tt_flags<float, kZero>(b, s, d, c, p, w, pu, stream);
+            else launch_tt_flags<double, kZero>(b, s, d, c, p, w, pu, stream);
+        }
+    }
+    k_unit_gather<<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, c, pu.unit_base, pu.unit_i, pu.unit_j, w);
+}
+
+}  // namespace d3
