@@ -154,6 +154,10 @@ void launch_cn_chain_rule_tiled(const Batch& b, const Species& s, const Config& 
 
 // Two-body sum over tile-pair units, each atom pair once, with the per-atom
 // gather (d3_pair_tt.cu); writes e_atom, dEdcn, grad, sig_atom, pg_atom.
+// Coordination number (chain = false, writes cn) or its chain rule (chain =
+// true, adds to grad and sig_atom) over the same units (d3_pair_tt.cu).
+void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Partition& p, const Work& w,
+                     const PairUnits& pu, bool chain, cudaStream_t stream);
 size_t pair_unit_slot_doubles();   // per unit: i and j slots
 size_t pair_unit_i_doubles();      // per unit: i slots
 void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,

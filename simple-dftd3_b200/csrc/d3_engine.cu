@@ -559,7 +559,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
                          d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed_, stream);
     launch_tile_bounds(b, d_tile_sys_, ntiles_, d_tiles_, stream);
     mark(1);
-    launch_coordination_number(b, s, c, part_, w, stream);
+    launch_cn_units(b, s, c, part_, w, pu_, false, stream);
     if (reducer_) reduce(w.cn, natoms_, stream);
     mark(2);
     launch_weights(b, s, c, w, stream);
@@ -595,7 +595,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     mark(5);
     if (grad) {
         if (reducer_) reduce(w.dEdcn, natoms_, stream);
-        launch_cn_chain_rule(b, s, c, part_, w, stream);
+        launch_cn_units(b, s, c, part_, w, pu_, true, stream);
     }
     mark(6);
     if (!reducer_) {

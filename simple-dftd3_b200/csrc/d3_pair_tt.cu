@@ -72,6 +72,64 @@ __device__ __forceinline__ R wsum_tt(R v)
     return v;
 }
 
+// Compacts the translations tc .. tc+nt-1 that can join two tile spheres
+// (centre difference dc, reach lim) into the warp's lists; returns their count.
+template <class V>
+__device__ __forceinline__ int tt_reach(const double* img, int tc, int nt, double dcx, double dcy, double dcz,
+                                        double lim, int lane, V* sth, V* stl, int* sidx)
+{
+    int nreach = 0;
+#pragma unroll
+    for (int q = 0; q < kTTChunk / 32; q++) {
+        const int k = 32 * q + lane;
+        bool ok = false;
+        double tx = 0, ty = 0, tz = 0;
+        if (k < nt) {
+            tx = __ldg(img + 3 * (tc + k)); ty = __ldg(img + 3 * (tc + k) + 1); tz = __ldg(img + 3 * (tc + k) + 2);
+            const double ex = dcx - tx, ey = dcy - ty, ez = dcz - tz;
+            ok = ex * ex + ey * ey + ez * ez <= lim * lim;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+            const int pos = nreach + __popc(m & ((1u << lane) - 1u));
+            sidx[pos] = tc + k;
+            if constexpr (sizeof(V) == 32) {
+                sth[pos] = make_double4(tx, ty, tz, 0.0);
+            } else {
+                const float hx = __double2float_rn(tx), hy = __double2float_rn(ty), hz = __double2float_rn(tz);
+                sth[pos] = make_float4(hx, hy, hz, 0.f);
+                stl[pos] = make_float4(__double2float_rn(tx - (double)hx), __double2float_rn(ty - (double)hy),
+                                       __double2float_rn(tz - (double)hz), 0.f);
+            }
+        }
+        nreach += __popc(m);
+    }
+    __syncwarp();
+    return nreach;
+}
+
+constexpr int kJMaskWords = (kTTChunk / kSplitT + 31) / 32;   // translations of an item, in ballot words
+
+// Of the compacted translations [qbeg, qend), those that can bring atom j
+// (position xj) within reach limj of the tile centre c: one bit each.
+__device__ __forceinline__ void tt_jmask(const double* img, const int* sidx, int qbeg, int qend, double4 c,
+                                         double xj, double yj, double zj, double limj, int lane,
+                                         unsigned jm[kJMaskWords])
+{
+#pragma unroll
+    for (int h = 0; h < kJMaskWords; h++) {
+        const int q = qbeg + 32 * h + lane;
+        bool ok = false;
+        if (q < qend) {
+            const int tix = sidx[q];
+            const double ex = c.x - xj - __ldg(img + 3 * tix), ey = c.y - yj - __ldg(img + 3 * tix + 1),
+                         ez = c.z - zj - __ldg(img + 3 * tix + 2);
+            ok = ex * ex + ey * ey + ez * ez <= limj * limj;
+        }
+        jm[h] = __ballot_sync(0xffffffffu, ok);
+    }
+}
+
 // Species vectors U[a][s][r] and dU[a][s][r] of every atom (sorted order).
 template <class R>
 __global__ void k_species_vectors(Batch b, Species s, Work w, R* U, R* dU)
@@ -176,34 +234,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     for (int tc = tt0; tc < tt1; tc += kTTChunk) {
         const int nt = min(kTTChunk, tt1 - tc);
         // translations that can join the two tiles
-        int nreach = 0;
-#pragma unroll
-        for (int q = 0; q < kTTChunk / 32; q++) {
-            const int k = 32 * q + lane;
-            bool ok = false;
-            double tx = 0, ty = 0, tz = 0;
-            if (k < nt) {
-                tx = __ldg(b.img + 3 * (tc + k)); ty = __ldg(b.img + 3 * (tc + k) + 1);
-                tz = __ldg(b.img + 3 * (tc + k) + 2);
-                const double ex = dcx - tx, ey = dcy - ty, ez = dcz - tz;
-                ok = ex * ex + ey * ey + ez * ez <= lim * lim;
-            }
-            const unsigned m = __ballot_sync(0xffffffffu, ok);
-            if (ok) {
-                const int pos = nreach + __popc(m & ((1u << lane) - 1u));
-                sidx[wid][pos] = tc + k;
-                if constexpr (sizeof(R) == 8) {
-                    sth[wid][pos] = make_double4(tx, ty, tz, 0.0);
-                } else {
-                    const float hx = __double2float_rn(tx), hy = __double2float_rn(ty), hz = __double2float_rn(tz);
-                    sth[wid][pos] = make_float4(hx, hy, hz, 0.f);
-                    stl[wid][pos] = make_float4(__double2float_rn(tx - (double)hx), __double2float_rn(ty - (double)hy),
-                                                __double2float_rn(tz - (double)hz), 0.f);
-                }
-            }
-            nreach += __popc(m);
-        }
-        __syncwarp();
+        const int nreach = tt_reach<V>(b.img, tc, nt, dcx, dcy, dcz, lim, lane, sth[wid], stl[wid], sidx[wid]);
         if (nreach == 0) continue;
         // this item's half of the reachable translations
         const int qhalf = (nreach + kSplitT - 1) / kSplitT;
@@ -247,21 +278,10 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
             const R we = self ? R(0.5) : R(1);
             R jde = R(0), jgx = R(0), jgy = R(0), jgz = R(0);
             // translations of this half that can bring j within the cutoff of tile it
-            unsigned jm[(kTTChunk / kSplitT + 31) / 32];
+            unsigned jm[kJMaskWords];
+            tt_jmask(b.img, sidx[wid], qbeg, qend, ci, xj, yj, zj, limj, lane, jm);
 #pragma unroll
-            for (int h = 0; h < (kTTChunk / kSplitT + 31) / 32; h++) {
-                const int q = qbeg + 32 * h + lane;
-                bool ok = false;
-                if (q < qend) {
-                    const int tix = sidx[wid][q];   // absolute image index
-                    const double ex = ci.x - xj - __ldg(b.img + 3 * tix), ey = ci.y - yj - __ldg(b.img + 3 * tix + 1),
-                                 ez = ci.z - zj - __ldg(b.img + 3 * tix + 2);
-                    ok = ex * ex + ey * ey + ez * ez <= limj * limj;
-                }
-                jm[h] = __ballot_sync(0xffffffffu, ok);
-            }
-#pragma unroll
-            for (int h = 0; h < (kTTChunk / kSplitT + 31) / 32; h++)
+            for (int h = 0; h < kJMaskWords; h++)
             for (unsigned mm = jm[h]; mm; mm &= mm - 1) {
                 const int q = qbeg + 32 * h + __ffs(mm) - 1;
                 const V th = sth[wid][q];
@@ -415,6 +435,211 @@ __global__ void k_unit_gather(Batch b, Config c, const int* unit_base, const dou
     }
 }
 
+constexpr double kKcnTT = 16.0;   // ncoord.f90:31
+
+// Coordination number (CHAIN = false, ncoord.f90:86-144) or its chain rule
+// (CHAIN = true, ncoord.f90:152-228) over the tile-pair units with the CN
+// lattice points.  Slots: CN: i [cn], j [cn]; chain: i [g(3), sigma(6)],
+// j [g(3)].
+template <class R, bool CHAIN>
+__global__ void __launch_bounds__(kTTThreads)
+k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, int nunits, double* unit_i,
+        double* unit_j)
+{
+    using V = typename T4<R>::type;
+    __shared__ V sth[kTTWarps][kTTChunk];
+    __shared__ V stl[kTTWarps][kTTChunk];
+    __shared__ int sidx[kTTWarps][kTTChunk];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int item = blockIdx.x * kTTWarps + wid;
+    if (item >= nunits * kSplit) return;
+    const int u = item / kSplit, sub = item % kSplit;
+    const int jh = sub / kSplitT, th = sub % kSplitT;
+    const int it = units[u].x, jt = units[u].y;
+    const int sys = b.tile_sys[it];
+    const int t0 = b.tile_off[sys];
+    const int as = b.atom_off[sys], ae = b.atom_off[sys + 1];
+    const int ia0 = as + kTile * (it - t0), ja0 = as + kTile * (jt - t0);
+    const int ni = min(kTile, ae - ia0), nj = min(kTile, ae - ja0);
+    const bool diag = it == jt;
+    const bool ivalid = lane < ni;
+    const int ic = ivalid ? ia0 + lane : ia0;
+    const int li = b.local[ic];
+    const double rci = s.rcov[b.sp[ic]];
+    const double dei = CHAIN ? w.dEdcn[ic] : 0.0;
+    const double xi = b.x[ic], yi = b.y[ic], zi = b.z[ic];
+    R hix, hiy, hiz, lix = R(0), liy = R(0), liz = R(0);
+    if constexpr (sizeof(R) == 8) { hix = xi; hiy = yi; hiz = zi; }
+    else {
+        hix = __double2float_rn(xi); lix = __double2float_rn(xi - (double)hix);
+        hiy = __double2float_rn(yi); liy = __double2float_rn(yi - (double)hiy);
+        hiz = __double2float_rn(zi); liz = __double2float_rn(zi - (double)hiz);
+    }
+    const int tt0 = b.img_off[kImgCN * (b.nsys + 1) + sys], tt1 = b.img_off[kImgCN * (b.nsys + 1) + sys + 1];
+    const double4 ci = b.tiles[it], cj = b.tiles[jt];
+    const double lim = c.cut_cn + ci.w + cj.w + 1.0e-6 * c.cut_cn + 1.0e-6;
+    const double limj = c.cut_cn + ci.w + 1.0e-6 * c.cut_cn + 1.0e-6;
+    const double dcx = ci.x - cj.x, dcy = ci.y - cj.y, dcz = ci.z - cj.z;
+    const R cut2 = R(c.cut_cn * c.cut_cn);
+    // i sums: CN: a0 = cn; chain: a1..a3 gradient, a4..a8 virial xx yy zz xy xz, a0 virial yz
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0, a7 = 0, a8 = 0;
+    R t0_ = R(0), t1_ = R(0), t2_ = R(0), t3_ = R(0), t4_ = R(0), t5_ = R(0), t6_ = R(0), t7_ = R(0), t8_ = R(0);
+    double b0 = 0, b1 = 0, b2 = 0;                                                   // cn | g(3) of j
+    int pending = 0;
+    unsigned long long nterm = 0;
+    auto flush = [&]() {
+        a0 += double(t0_); t0_ = R(0);
+        if (CHAIN) {
+            a1 += double(t1_); a2 += double(t2_); a3 += double(t3_); a4 += double(t4_); a5 += double(t5_);
+            a6 += double(t6_); a7 += double(t7_); a8 += double(t8_);
+            t1_ = t2_ = t3_ = t4_ = t5_ = t6_ = t7_ = t8_ = R(0);
+        }
+        pending = 0;
+    };
+    for (int tc = tt0; tc < tt1; tc += kTTChunk) {
+        const int nt = min(kTTChunk, tt1 - tc);
+        const int nreach = tt_reach<V>(b.img, tc, nt, dcx, dcy, dcz, lim, lane, sth[wid], stl[wid], sidx[wid]);
+        if (nreach == 0) continue;
+        const int qhalf = (nreach + kSplitT - 1) / kSplitT;
+        const int qbeg = th * qhalf, qend = min(nreach, qbeg + qhalf);
+        if (qbeg >= qend) continue;
+        const int jl0 = jh * (kTile / kSplitJ), jl1 = min(nj, jl0 + kTile / kSplitJ);
+        for (int jl = jl0; jl < jl1; jl++) {
+            const int j = ja0 + jl;
+            const bool self = diag && jl == lane;
+            bool valid = ivalid && (!diag || jl <= lane);
+            if (valid && c.cn_partitioned && p.nparts > 1) valid = tt_owns(p, li, b.local[j]);
+            if (!__any_sync(0xffffffffu, valid)) continue;
+            const double xj = b.x[j], yj = b.y[j], zj = b.z[j];
+            R dhx, dhy, dhz, dlx = R(0), dly = R(0), dlz = R(0);
+            if constexpr (sizeof(R) == 8) { dhx = xi - xj; dhy = yi - yj; dhz = zi - zj; }
+            else {
+                const float4 hj = b.xhi[j], lj4 = b.xlo[j];
+                dhx = hix - hj.x; dhy = hiy - hj.y; dhz = hiz - hj.z;
+                dlx = lix - lj4.x; dly = liy - lj4.y; dlz = liz - lj4.z;
+            }
+            const R rc = R(rci + s.rcov[b.sp[j]]);
+            // chain rule weight of the pair: dE/dCN_i + dE/dCN_j, or dE/dCN_i for j = i (ncoord.f90:205-213)
+            const R dsum = CHAIN ? R(dei + w.dEdcn[j]) : R(0);
+            const R dsig = CHAIN ? (self ? R(dei) : dsum) : R(0);
+            R j0 = R(0), j1 = R(0), j2 = R(0);
+            unsigned jm[kJMaskWords];
+            tt_jmask(b.img, sidx[wid], qbeg, qend, ci, xj, yj, zj, limj, lane, jm);
+#pragma unroll
+            for (int h = 0; h < kJMaskWords; h++)
+            for (unsigned mm = jm[h]; mm; mm &= mm - 1) {
+                const int q = qbeg + 32 * h + __ffs(mm) - 1;
+                const V thv = sth[wid][q];
+                R vx, vy, vz;
+                if constexpr (sizeof(R) == 8) { vx = dhx - thv.x; vy = dhy - thv.y; vz = dhz - thv.z; }
+                else {
+                    const V tl = stl[wid][q];
+                    vx = (dhx - thv.x) + (dlx - tl.x);
+                    vy = (dhy - thv.y) + (dly - tl.y);
+                    vz = (dhz - thv.z) + (dlz - tl.z);
+                }
+                const R r2 = vx * vx + vy * vy + vz * vz;
+                if (!valid || r2 > cut2 || r2 < R(1.0e-12)) continue;
+                nterm++;
+                if (!CHAIN) {
+                    R cf;
+                    if constexpr (sizeof(R) == 8) cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / sqrt(r2) - R(1))));
+                    else cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * rsqrtf(r2) - R(1))));
+                    t0_ += cf;
+                    if (!self) j0 += cf;
+                } else {
+                    R f;
+                    if constexpr (sizeof(R) == 8) {
+                        // ncoord.f90:198-206
+                        const R r1 = sqrt(r2);
+                        const R cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / r1 - R(1))));
+                        const R dcf = -cf * (R(1) - cf) * R(kKcnTT) * rc / r2;
+                        f = dcf / r1;
+                    } else {
+                        const R ir = rsqrtf(r2);
+                        const R cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * ir - R(1))));
+                        f = -cf * (R(1) - cf) * R(kKcnTT) * rc * (ir * ir * ir);
+                    }
+                    const R cx = f * vx, cy = f * vy, cz = f * vz;   // countd
+                    if (!self) {
+                        t1_ += cx * dsum; t2_ += cy * dsum; t3_ += cz * dsum;
+                        j0 -= cx * dsum; j1 -= cy * dsum; j2 -= cz * dsum;
+                    }
+                    t4_ += cx * vx * dsig; t5_ += cy * vy * dsig; t6_ += cz * vz * dsig;
+                    t7_ += cx * vy * dsig; t8_ += cx * vz * dsig; t0_ += cy * vz * dsig;
+                }
+            }
+            j0 = wsum_tt<R>(j0);
+            if (CHAIN) { j1 = wsum_tt<R>(j1); j2 = wsum_tt<R>(j2); }
+            if (lane == jl) { b0 += double(j0); b1 += double(j1); b2 += double(j2); }
+            if constexpr (sizeof(R) == 4) {
+                pending += qend - qbeg;
+                if (pending >= 128) flush();
+            }
+        }
+    }
+    flush();
+    double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
+    double* oj = unit_j + ((size_t)item * kTile + lane) * kUnitJ;
+    if (!CHAIN) {
+        oi[0] = a0;
+        oj[0] = b0;
+    } else {
+        // g(3), sigma xx yy zz xy xz yz
+        oi[0] = a1; oi[1] = a2; oi[2] = a3;
+        oi[3] = a4; oi[4] = a5; oi[5] = a6; oi[6] = a7; oi[7] = a8; oi[8] = a0;
+        oj[0] = b0; oj[1] = b1; oj[2] = b2;
+    }
+    if (!CHAIN && w.counts) {
+        for (int off = 16; off > 0; off >>= 1) nterm += __shfl_xor_sync(0xffffffffu, nterm, off);
+        if (lane == 0) atomicAdd(w.counts + 2, nterm);
+    }
+}
+
+// Gather of the CN (assign) or chain-rule (add to gradient and virial) slots,
+// one warp per atom, in the fixed order of k_unit_gather.
+template <bool CHAIN>
+__global__ void k_cn_gather(Batch b, const int* unit_base, const double* unit_i, const double* unit_j, Work w)
+{
+    const int lane = threadIdx.x & 31;
+    const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (a >= b.natoms) return;
+    const int sys = b.sys_of_atom[a];
+    const int as = b.atom_off[sys];
+    const int t0 = b.tile_off[sys], t1 = b.tile_off[sys + 1];
+    const int tl = (a - as) / kTile, sl = (a - as) % kTile;
+    const int nt = t1 - t0;
+    const long long base = unit_base[sys];
+    constexpr int kI = CHAIN ? 9 : 1, kJ = CHAIN ? 3 : 1;
+    double v[kI];
+#pragma unroll
+    for (int k = 0; k < kI; k++) v[k] = 0.0;
+    const int ni = (tl + 1) * kSplit, nj = (nt - tl) * kSplit;
+    for (int q = lane; q < ni; q += 32) {
+        const long long item = (base + (long long)tl * (tl + 1) / 2 + q / kSplit) * kSplit + q % kSplit;
+        const double* o = unit_i + (item * kTile + sl) * kUnitI;
+#pragma unroll
+        for (int k = 0; k < kI; k++) v[k] += o[k];
+    }
+    for (int q = lane; q < nj; q += 32) {
+        const int itl = tl + q / kSplit;
+        const long long item = (base + (long long)itl * (itl + 1) / 2 + tl) * kSplit + q % kSplit;
+        const double* o = unit_j + (item * kTile + sl) * kUnitJ;
+#pragma unroll
+        for (int k = 0; k < kJ; k++) v[k] += o[k];
+    }
+#pragma unroll
+    for (int k = 0; k < kI; k++) v[k] = wsum_tt<double>(v[k]);
+    if (lane != 0) return;
+    if (!CHAIN) {
+        w.cn[a] = v[0];
+    } else {
+        w.grad[3 * a + 0] += v[0]; w.grad[3 * a + 1] += v[1]; w.grad[3 * a + 2] += v[2];
+        double* sg = w.sig_atom + kSigma * a;
+        for (int k = 0; k < kSigma; k++) sg[k] += v[3 + k];
+    }
+}
+
 template <class R, int DAMP, bool GRAD, bool PG>
 void launch_tt(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p, const Work& w,
                const PairUnits& pu, cudaStream_t stream)
@@ -438,6 +663,24 @@ void launch_tt_flags(const Batch& b, const Species& s, const Damp& d, const Conf
 }
 
 }  // namespace
+
+void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Partition& p, const Work& w,
+                     const PairUnits& pu, bool chain, cudaStream_t stream)
+{
+    if (b.natoms <= 0) return;
+    const int blocks = (pu.nunits * kSplit + kTTWarps - 1) / kTTWarps;
+    if (pu.nunits > 0) {
+        if (chain) {
+            if (c.mixed) k_cn_tt<float, true><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.unit_i, pu.unit_j);
+            else k_cn_tt<double, true><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.unit_i, pu.unit_j);
+        } else {
+            if (c.mixed) k_cn_tt<float, false><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.unit_i, pu.unit_j);
+            else k_cn_tt<double, false><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.unit_i, pu.unit_j);
+        }
+    }
+    if (chain) k_cn_gather<true><<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, pu.unit_base, pu.unit_i, pu.unit_j, w);
+    else k_cn_gather<false><<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, pu.unit_base, pu.unit_i, pu.unit_j, w);
+}
 
 size_t pair_unit_slot_doubles() { return (size_t)kSplit * kTile * (kUnitI + kUnitJ); }
 size_t pair_unit_i_doubles() { return (size_t)kSplit * kTile * kUnitI; }
