@@ -16,6 +16,13 @@
 
 typedef struct _dftd3_b200_batch* dftd3_b200_batch;
 
+/* Launch shapes of a model created by dftd3_new_d3_model (tuning[4] as for
+ * dftd3_b200_set_batch_tuning). */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_set_model_tuning(dftd3_error /* error */,
+                            dftd3_model /* model */,
+                            const double* /* tuning[4] */);
+
 /* Select the arithmetic of a model created by dftd3_new_d3_model. */
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_b200_set_model_precision(dftd3_error /* error */,
@@ -124,17 +131,20 @@ dftd3_b200_set_batch_graph(dftd3_error /* error */,
                            int /* enable */);
 
 /* Launch shapes of a batch: tuning[0] the cell of the spatial sort key
- * (Bohr, > 0), tuning[1] atoms per block of the pair sweeps (4 or 8),
- * tuning[2] resident three-body blocks per SM (0 = occupancy limit). */
+ * (Bohr, > 0), tuning[1] work items per tile pair of the pair sweeps (1, 2
+ * or 4), tuning[2] resident blocks per SM of the neighbour-list three-body
+ * kernel (0 = occupancy limit), tuning[3] the block-per-molecule three-body
+ * kernel for non-periodic systems of at most 256 atoms (0: when the batch has
+ * at least one such molecule per SM, 1: always, 2: never). */
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_b200_set_batch_tuning(dftd3_error /* error */,
                             dftd3_b200_batch /* batch */,
-                            const double* /* tuning[3] */);
+                            const double* /* tuning[4] */);
 
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_b200_get_batch_tuning(dftd3_error /* error */,
                             dftd3_b200_batch /* batch */,
-                            double* /* tuning[3] */);
+                            double* /* tuning[4] */);
 
 /* Autotuner: time the candidate launch shapes on these positions (host,
  * [sum natoms][3], wrapped like dftd3_b200_get_dispersion_batched) with the

@@ -44,6 +44,8 @@ struct _dftd3_model {
     std::vector<uint8_t> ghost;
     int part = 0, nparts = 1;
     int precision = DFTD3_B200_PRECISION_FP64;
+    bool has_tuning = false;
+    d3::Tuning tuning;
     std::unique_ptr<d3::Engine> engine;
 };
 
@@ -95,6 +97,19 @@ void guarded(dftd3_error err, F&& f)
 }  // namespace
 
 namespace {
+
+// Launch shapes from the C array of dftd3_b200_set_*_tuning.
+d3::Tuning tuning_from(const double* tuning)
+{
+    d3::Tuning t;
+    t.morton_cell = tuning[0];
+    t.pair_split = (int)tuning[1];
+    t.atm_blocks_per_sm = (int)tuning[2];
+    t.atm_mol = (int)tuning[3];
+    if ((double)t.pair_split != tuning[1] || (double)t.atm_blocks_per_sm != tuning[2] || (double)t.atm_mol != tuning[3])
+        throw d3::Error("Launch shape counts must be integers");
+    return t;
+}
 
 // Method id of a method name as get_method_id does it (param.f90:96-114):
 // '-' removed, letters outside quotes in lower case, trailing blanks ignored.
@@ -493,6 +508,7 @@ void dftd3_get_dispersion(dftd3_error error, dftd3_structure mol, dftd3_model di
             disp->engine->set_ghost(disp->ghost);
             disp->engine->set_partition(disp->part, disp->nparts, false);
             disp->engine->set_precision(disp->precision);
+            if (disp->has_tuning) disp->engine->set_tuning(disp->tuning);
         }
         disp->engine->set_lattices(mol->lattice);
         double e = 0.0;
@@ -524,6 +540,23 @@ void dftd3_get_counterpoise_hessian(dftd3_error error, dftd3_structure, dftd3_gc
 }
 
 // ------------------------------------------------------------- extensions --
+
+void dftd3_b200_set_model_tuning(dftd3_error error, dftd3_model model, const double* tuning)
+{
+    if (!error) return;
+    if (!model || !tuning) {
+        fail(error, "D3 dispersion model is missing");
+        return;
+    }
+    guarded(error, [&] {
+        const d3::Tuning t = tuning_from(tuning);
+        if (t.pair_split != 1 && t.pair_split != 2 && t.pair_split != 4)
+            throw d3::Error("Work items per tile pair must be 1, 2 or 4");
+        model->tuning = t;
+        model->has_tuning = true;
+        if (model->engine) model->engine->set_tuning(t);
+    });
+}
 
 void dftd3_b200_set_model_precision(dftd3_error error, dftd3_model model, int precision)
 {
@@ -737,13 +770,7 @@ void dftd3_b200_set_batch_tuning(dftd3_error error, dftd3_b200_batch batch, cons
         return;
     }
     guarded(error, [&] {
-        d3::Tuning t;
-        t.morton_cell = tuning[0];
-        t.pair_warps = (int)tuning[1];
-        t.atm_blocks_per_sm = (int)tuning[2];
-        if ((double)t.pair_warps != tuning[1] || (double)t.atm_blocks_per_sm != tuning[2])
-            throw d3::Error("Launch shape counts must be integers");
-        batch->engine->set_tuning(t);
+        batch->engine->set_tuning(tuning_from(tuning));
     });
 }
 
@@ -756,8 +783,9 @@ void dftd3_b200_get_batch_tuning(dftd3_error error, dftd3_b200_batch batch, doub
     }
     const d3::Tuning& t = batch->engine->tuning();
     tuning[0] = t.morton_cell;
-    tuning[1] = t.pair_warps;
+    tuning[1] = t.pair_split;
     tuning[2] = t.atm_blocks_per_sm;
+    tuning[3] = t.atm_mol;
 }
 
 double dftd3_b200_autotune_batch(dftd3_error error, dftd3_b200_batch batch, dftd3_param param,

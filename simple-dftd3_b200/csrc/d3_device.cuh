@@ -49,6 +49,7 @@ struct PairUnits {
     const int2* units = nullptr;         // [nunits] global tile indices (it, jt)
     int nunits = 0;
     const int* unit_base = nullptr;      // [nsys]
+    int split = 4;                       // items per unit: 1, 2 (translation halves), 4 (and j halves)
     void* U = nullptr;                   // [natoms][nid][kMaxRef] species vectors (R)
     void* dU = nullptr;                  // same with dgw
     double* unit_i = nullptr;            // [nunits][kTile][15]
@@ -117,8 +118,10 @@ struct Config {
 // Launch-shape choices of one batch, picked by the autotuner or set by hand.
 struct Tuning {
     double morton_cell = 3.0;      // Bohr; quantisation of the spatial sort key
-    int pair_warps = 8;            // atoms per block of the pair sweeps (4 or 8)
-    int atm_blocks_per_sm = 0;     // resident triple-sum blocks per SM; 0 = occupancy limit
+    int pair_split = 4;            // work items per tile pair of the pair sweeps: 1, 2 or 4
+    int atm_blocks_per_sm = 0;     // resident blocks per SM of the neighbour-list triple kernel; 0 = occupancy
+    int atm_mol = 0;               // molecule triple kernel: 0 for batches of at least one molecule per SM,
+                                   // 1 for every eligible system, 2 never
 };
 
 // FMA throughput of the FP64 (fp64=true) or FP32 pipe in TFLOP/s (blocking).

@@ -287,25 +287,10 @@ Engine::Engine(int nsys, const int* natoms, const int* numbers, const double* la
         off += (long long)natoms[s] * natoms[s];
     }
     c6mat_total_ = off;
-    // molecules for the block-per-system three-body kernel: no periodic
-    // direction and at most atm_mol_max_atoms() atoms; largest first
-    std::vector<uint8_t> is_mol(nsys, 0);
-    for (int s = 0; s < nsys; s++) {
-        const bool per_any = per_[3 * s] || per_[3 * s + 1] || per_[3 * s + 2];
-        if (!per_any && natoms[s] <= atm_mol_max_atoms()) {
-            is_mol[s] = 1;
-            mol_order_.push_back(s);
-        } else {
-            root_atoms_ += natoms[s];
-        }
-    }
-    std::stable_sort(mol_order_.begin(), mol_order_.end(), [&](int a, int b) { return natoms[a] > natoms[b]; });
-    if (!mol_order_.empty()) {
-        d_mol_order_ = dev_alloc<int>(mol_order_.size());
-        d_sys_mol_ = dev_alloc<uint8_t>(nsys);
-        up(d_mol_order_, mol_order_.data(), sizeof(int) * mol_order_.size());
-        up(d_sys_mol_, is_mol.data(), nsys);
-    }
+    sys_natoms_.assign(natoms, natoms + nsys);
+    d_mol_order_ = dev_alloc<int>(nsys);
+    d_sys_mol_ = dev_alloc<uint8_t>(nsys);
+    configure_molecules();
     check(cudaStreamSynchronize(stream_), "upload sync");
 }
 
@@ -321,6 +306,34 @@ Engine::~Engine()
     if (h_atm_counts_) cudaFreeHost(h_atm_counts_);
     if (h_guard_) cudaFreeHost(h_guard_);
     if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::configure_molecules()
+{
+    // molecules for the block-per-system three-body kernel: no periodic
+    // direction and at most atm_mol_max_atoms() atoms, largest first
+    std::vector<uint8_t> is_mol(nsys_, 0);
+    mol_order_.clear();
+    root_atoms_ = 0;
+    for (int s = 0; s < nsys_; s++) {
+        const bool per_any = per_[3 * s] || per_[3 * s + 1] || per_[3 * s + 2];
+        if (tune_.atm_mol != 2 && !per_any && sys_natoms_[s] <= atm_mol_max_atoms()) mol_order_.push_back(s);
+        else root_atoms_ += sys_natoms_[s];
+    }
+    // one block per molecule pays off for many molecules; a few are spread
+    // over all SMs by the neighbour-list kernel instead
+    if (tune_.atm_mol == 0 && (int)mol_order_.size() < sms_) {
+        for (int sy : mol_order_) root_atoms_ += sys_natoms_[sy];
+        mol_order_.clear();
+    }
+    std::stable_sort(mol_order_.begin(), mol_order_.end(),
+                     [&](int a, int b) { return sys_natoms_[a] > sys_natoms_[b]; });
+    for (int sy : mol_order_) is_mol[sy] = 1;
+    check(cudaStreamSynchronize(stream_), "molecules");
+    if (!mol_order_.empty())
+        check(cudaMemcpy(d_mol_order_, mol_order_.data(), sizeof(int) * mol_order_.size(), cudaMemcpyHostToDevice),
+              "molecule order");
+    check(cudaMemcpy(d_sys_mol_, is_mol.data(), nsys_, cudaMemcpyHostToDevice), "molecule flags");
 }
 
 void Engine::build_tables(const int* numbers)
@@ -538,7 +551,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     c.cut_cn = cut_.cn; c.cut2 = cut_.disp2; c.cut3 = cut_.disp3;
     c.width2 = cut_.width2; c.width3 = cut_.width3;
     c.grad = grad; c.mixed = mixed_; c.param_grad = pg; c.cn_partitioned = cn_partitioned_;
-    c.pair_warps = tune_.pair_warps;
+    pu_.split = tune_.pair_split;
     Work w = work_;
     w.counts = counting_ ? d_counts_ : nullptr;
     w.e3_atom = nullptr;
@@ -798,10 +811,15 @@ void Engine::set_graph(bool on)
 
 void Engine::set_tuning(const Tuning& t)
 {
-    if (t.pair_warps != 4 && t.pair_warps != 8) throw Error("Atoms per pair block must be 4 or 8");
+    if (t.pair_split != 1 && t.pair_split != 2 && t.pair_split != 4)
+        throw Error("Work items per tile pair must be 1, 2 or 4");
     if (!(t.morton_cell > 0.0) || !std::isfinite(t.morton_cell)) throw Error("Sort cell must be positive");
     if (t.atm_blocks_per_sm < 0) throw Error("Three-body blocks per SM must not be negative");
+    if (t.atm_mol < 0 || t.atm_mol > 2) throw Error("Molecule kernel mode must be 0, 1 or 2");
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    const bool remol = t.atm_mol != tune_.atm_mol;
     tune_ = t;
+    if (remol) configure_molecules();
     graph_valid_ = false;
 }
 
@@ -922,9 +940,26 @@ double Engine::autotune(const Damp& d, const double* d_positions, bool grad, cud
         };
         for (double cell : {2.0, 3.0, 4.5, 6.0})
             if (cell != best.morton_cell) { Tuning t = best; t.morton_cell = cell; consider(t); }
-        for (int pw : {4, 8})
-            if (pw != best.pair_warps) { Tuning t = best; t.pair_warps = pw; consider(t); }
+        for (int sp : {1, 2, 4})
+            if (sp != best.pair_split) { Tuning t = best; t.pair_split = sp; consider(t); }
         if (threebody) {
+            // molecules: one block each, or the neighbour-list kernel
+            bool any_mol = false;
+            for (int sy = 0; sy < nsys_; sy++)
+                any_mol = any_mol || (!(per_[3 * sy] || per_[3 * sy + 1] || per_[3 * sy + 2]) &&
+                                      sys_natoms_[sy] <= atm_mol_max_atoms());
+            if (any_mol)
+                for (int mode : {1, 2})
+                    if (mode != best.atm_mol) {
+                        Tuning t = best; t.atm_mol = mode;
+                        const bool remol = t.atm_mol != tune_.atm_mol;
+                        tune_ = t;
+                        if (remol) configure_molecules();
+                        const double ms = time_once();
+                        if (ms < best_ms) { best_ms = ms; best = t; }
+                        tune_ = best;
+                        configure_molecules();
+                    }
             const int occ = atm_occupancy(mixed_, grad);
             const int cur = best.atm_blocks_per_sm > 0 ? std::min(best.atm_blocks_per_sm, occ) : occ;
             for (int bps = 1; bps <= occ; bps++)
@@ -932,12 +967,14 @@ double Engine::autotune(const Damp& d, const double* d_positions, bool grad, cud
         }
     } catch (...) {
         tune_ = best;
+        configure_molecules();
         profiling_ = prof;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         throw;
     }
     tune_ = best;
+    configure_molecules();
     profiling_ = prof;
     graph_valid_ = false;
     cudaEventDestroy(e0);

@@ -158,6 +158,8 @@ private:
     int* d_unit_base_ = nullptr;
     std::vector<int> mol_order_;         // systems of the molecule kernel, largest first
     int* d_mol_order_ = nullptr;
+    std::vector<int> sys_natoms_;
+    void configure_molecules();          // mol_order_ and root_atoms_ from tune_.atm_mol
     uint8_t* d_sys_mol_ = nullptr;       // [nsys] 1 for those systems
     long long root_atoms_ = 0;           // atoms of the other systems
     bool graph_on_ = false, capturing_ = false, graph_valid_ = false;

@@ -29,9 +29,8 @@ constexpr int kTTThreads = 32 * kTTWarps;
 constexpr int kTTChunk = 128;     // translations tested per pass
 constexpr int kUnitI = 15;        // per-lane i sums: E, dE/dCN, g(3), sigma(6), dE/dparam(4)
 constexpr int kUnitJ = 4;         // per-lane j sums: dE/dCN, g(3)
-constexpr int kSplitJ = 2;        // a unit is evaluated as kSplitJ x kSplitT items
-constexpr int kSplitT = 2;        // (halves of the j tile and of the translation list)
-constexpr int kSplit = kSplitJ * kSplitT;
+constexpr int kSplitMax = 4;      // a unit is evaluated as 1, 2 (translation halves) or 4 items
+                                  // (and j-tile halves); slots are sized for the largest split
 
 template <class R> struct T4;
 template <> struct T4<float> { using type = float4; };
@@ -108,7 +107,7 @@ __device__ __forceinline__ int tt_reach(const double* img, int tc, int nt, doubl
     return nreach;
 }
 
-constexpr int kJMaskWords = (kTTChunk / kSplitT + 31) / 32;   // translations of an item, in ballot words
+constexpr int kJMaskWords = kTTChunk / 32;   // translations of an item, in ballot words
 
 // Of the compacted translations [qbeg, qend), those that can bring atom j
 // (position xj) within reach limj of the tile centre c: one bit each.
@@ -155,7 +154,7 @@ __global__ void k_species_vectors(Batch b, Species s, Work w, R* U, R* dU)
 
 template <class R, int DAMP, bool GRAD, bool PG>
 __global__ void __launch_bounds__(kTTThreads)
-k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const int2* units, int nunits,
+k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const int2* units, int nunits, int split,
               const R* U, const R* dU, double* unit_i, double* unit_j)
 {
     using V = typename T4<R>::type;
@@ -164,9 +163,10 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     __shared__ int sidx[kTTWarps][kTTChunk];     // image index of each compacted translation
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int item = blockIdx.x * kTTWarps + wid;
-    if (item >= nunits * kSplit) return;
-    const int u = item / kSplit, sub = item % kSplit;
-    const int jh = sub / kSplitT, th = sub % kSplitT;
+    if (item >= nunits * split) return;
+    const int u = item / split, sub = item % split;
+    const int splitT = split >= 2 ? 2 : 1, splitJ = split / splitT;
+    const int jh = sub / splitT, th = sub % splitT;
     const int it = units[u].x, jt = units[u].y;
     const int sys = b.tile_sys[it];
     const int t0 = b.tile_off[sys];
@@ -237,10 +237,10 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
         const int nreach = tt_reach<V>(b.img, tc, nt, dcx, dcy, dcz, lim, lane, sth[wid], stl[wid], sidx[wid]);
         if (nreach == 0) continue;
         // this item's half of the reachable translations
-        const int qhalf = (nreach + kSplitT - 1) / kSplitT;
+        const int qhalf = (nreach + splitT - 1) / splitT;
         const int qbeg = th * qhalf, qend = min(nreach, qbeg + qhalf);
         if (qbeg >= qend) continue;
-        const int jl0 = jh * (kTile / kSplitJ), jl1 = min(nj, jl0 + kTile / kSplitJ);
+        const int jl0 = jh * (kTile / splitJ), jl1 = min(nj, jl0 + kTile / splitJ);
         for (int jl = jl0; jl < jl1; jl++) {
             const int j = ja0 + jl;
             const bool self = diag && jl == lane;
@@ -389,8 +389,8 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
 // lanes take the atom's slots (its i slots of the units (t, jt <= t), then
 // its j slots of the units (it >= t, t)) round robin and a fixed shuffle tree
 // adds the lane sums.
-__global__ void k_unit_gather(Batch b, Config c, const int* unit_base, const double* unit_i, const double* unit_j,
-                              Work w)
+__global__ void k_unit_gather(Batch b, Config c, const int* unit_base, int split, const double* unit_i,
+                              const double* unit_j, Work w)
 {
     const int lane = threadIdx.x & 31;
     const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -405,17 +405,17 @@ __global__ void k_unit_gather(Batch b, Config c, const int* unit_base, const dou
     double v[kUnitI];
 #pragma unroll
     for (int k = 0; k < kUnitI; k++) v[k] = 0.0;
-    const int ni = (tl + 1) * kSplit, nj = (nt - tl) * kSplit;
+    const int ni = (tl + 1) * split, nj = (nt - tl) * split;
     for (int q = lane; q < ni; q += 32) {
-        const int jt = q / kSplit, sb = q % kSplit;
-        const long long item = (base + (long long)tl * (tl + 1) / 2 + jt) * kSplit + sb;
+        const int jt = q / split, sb = q % split;
+        const long long item = (base + (long long)tl * (tl + 1) / 2 + jt) * split + sb;
         const double* o = unit_i + (item * kTile + sl) * kUnitI;
 #pragma unroll
         for (int k = 0; k < kUnitI; k++) v[k] += o[k];
     }
     for (int q = lane; q < nj; q += 32) {
-        const int it = tl + q / kSplit, sb = q % kSplit;
-        const long long item = (base + (long long)it * (it + 1) / 2 + tl) * kSplit + sb;
+        const int it = tl + q / split, sb = q % split;
+        const long long item = (base + (long long)it * (it + 1) / 2 + tl) * split + sb;
         const double* o = unit_j + (item * kTile + sl) * kUnitJ;
         v[1] += o[0]; v[2] += o[1]; v[3] += o[2]; v[4] += o[3];
     }
@@ -443,7 +443,7 @@ constexpr double kKcnTT = 16.0;   // ncoord.f90:31
 // j [g(3)].
 template <class R, bool CHAIN>
 __global__ void __launch_bounds__(kTTThreads)
-k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, int nunits, double* unit_i,
+k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, int nunits, int split, double* unit_i,
         double* unit_j)
 {
     using V = typename T4<R>::type;
@@ -452,9 +452,10 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
     __shared__ int sidx[kTTWarps][kTTChunk];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int item = blockIdx.x * kTTWarps + wid;
-    if (item >= nunits * kSplit) return;
-    const int u = item / kSplit, sub = item % kSplit;
-    const int jh = sub / kSplitT, th = sub % kSplitT;
+    if (item >= nunits * split) return;
+    const int u = item / split, sub = item % split;
+    const int splitT = split >= 2 ? 2 : 1, splitJ = split / splitT;
+    const int jh = sub / splitT, th = sub % splitT;
     const int it = units[u].x, jt = units[u].y;
     const int sys = b.tile_sys[it];
     const int t0 = b.tile_off[sys];
@@ -500,10 +501,10 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
         const int nt = min(kTTChunk, tt1 - tc);
         const int nreach = tt_reach<V>(b.img, tc, nt, dcx, dcy, dcz, lim, lane, sth[wid], stl[wid], sidx[wid]);
         if (nreach == 0) continue;
-        const int qhalf = (nreach + kSplitT - 1) / kSplitT;
+        const int qhalf = (nreach + splitT - 1) / splitT;
         const int qbeg = th * qhalf, qend = min(nreach, qbeg + qhalf);
         if (qbeg >= qend) continue;
-        const int jl0 = jh * (kTile / kSplitJ), jl1 = min(nj, jl0 + kTile / kSplitJ);
+        const int jl0 = jh * (kTile / splitJ), jl1 = min(nj, jl0 + kTile / splitJ);
         for (int jl = jl0; jl < jl1; jl++) {
             const int j = ja0 + jl;
             const bool self = diag && jl == lane;
@@ -599,7 +600,8 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
 // Gather of the CN (assign) or chain-rule (add to gradient and virial) slots,
 // one warp per atom, in the fixed order of k_unit_gather.
 template <bool CHAIN>
-__global__ void k_cn_gather(Batch b, const int* unit_base, const double* unit_i, const double* unit_j, Work w)
+__global__ void k_cn_gather(Batch b, const int* unit_base, int split, const double* unit_i, const double* unit_j,
+                            Work w)
 {
     const int lane = threadIdx.x & 31;
     const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -614,16 +616,16 @@ __global__ void k_cn_gather(Batch b, const int* unit_base, const double* unit_i,
     double v[kI];
 #pragma unroll
     for (int k = 0; k < kI; k++) v[k] = 0.0;
-    const int ni = (tl + 1) * kSplit, nj = (nt - tl) * kSplit;
+    const int ni = (tl + 1) * split, nj = (nt - tl) * split;
     for (int q = lane; q < ni; q += 32) {
-        const long long item = (base + (long long)tl * (tl + 1) / 2 + q / kSplit) * kSplit + q % kSplit;
+        const long long item = (base + (long long)tl * (tl + 1) / 2 + q / split) * split + q % split;
         const double* o = unit_i + (item * kTile + sl) * kUnitI;
 #pragma unroll
         for (int k = 0; k < kI; k++) v[k] += o[k];
     }
     for (int q = lane; q < nj; q += 32) {
-        const int itl = tl + q / kSplit;
-        const long long item = (base + (long long)itl * (itl + 1) / 2 + tl) * kSplit + q % kSplit;
+        const int itl = tl + q / split;
+        const long long item = (base + (long long)itl * (itl + 1) / 2 + tl) * split + q % split;
         const double* o = unit_j + (item * kTile + sl) * kUnitJ;
 #pragma unroll
         for (int k = 0; k < kJ; k++) v[k] += o[k];
@@ -644,9 +646,9 @@ template <class R, int DAMP, bool GRAD, bool PG>
 void launch_tt(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p, const Work& w,
                const PairUnits& pu, cudaStream_t stream)
 {
-    const int blocks = (pu.nunits * kSplit + kTTWarps - 1) / kTTWarps;
+    const int blocks = (pu.nunits * pu.split + kTTWarps - 1) / kTTWarps;
     k_two_body_tt<R, DAMP, GRAD, PG><<<blocks, kTTThreads, 0, stream>>>(
-        b, s, d, c, p, w, pu.units, pu.nunits, (const R*)pu.U, (const R*)pu.dU, pu.unit_i, pu.unit_j);
+        b, s, d, c, p, w, pu.units, pu.nunits, pu.split, (const R*)pu.U, (const R*)pu.dU, pu.unit_i, pu.unit_j);
 }
 
 template <class R, int DAMP>
@@ -668,22 +670,22 @@ void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Pa
                      const PairUnits& pu, bool chain, cudaStream_t stream)
 {
     if (b.natoms <= 0) return;
-    const int blocks = (pu.nunits * kSplit + kTTWarps - 1) / kTTWarps;
+    const int blocks = (pu.nunits * pu.split + kTTWarps - 1) / kTTWarps;
     if (pu.nunits > 0) {
         if (chain) {
-            if (c.mixed) k_cn_tt<float, true><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.unit_i, pu.unit_j);
-            else k_cn_tt<double, true><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.unit_i, pu.unit_j);
+            if (c.mixed) k_cn_tt<float, true><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.split, pu.unit_i, pu.unit_j);
+            else k_cn_tt<double, true><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.split, pu.unit_i, pu.unit_j);
         } else {
-            if (c.mixed) k_cn_tt<float, false><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.unit_i, pu.unit_j);
-            else k_cn_tt<double, false><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.unit_i, pu.unit_j);
+            if (c.mixed) k_cn_tt<float, false><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.split, pu.unit_i, pu.unit_j);
+            else k_cn_tt<double, false><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.split, pu.unit_i, pu.unit_j);
         }
     }
-    if (chain) k_cn_gather<true><<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, pu.unit_base, pu.unit_i, pu.unit_j, w);
-    else k_cn_gather<false><<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, pu.unit_base, pu.unit_i, pu.unit_j, w);
+    if (chain) k_cn_gather<true><<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
+    else k_cn_gather<false><<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
 }
 
-size_t pair_unit_slot_doubles() { return (size_t)kSplit * kTile * (kUnitI + kUnitJ); }
-size_t pair_unit_i_doubles() { return (size_t)kSplit * kTile * kUnitI; }
+size_t pair_unit_slot_doubles() { return (size_t)kSplitMax * kTile * (kUnitI + kUnitJ); }
+size_t pair_unit_i_doubles() { return (size_t)kSplitMax * kTile * kUnitI; }
 
 void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
                            const Work& w, const PairUnits& pu, cudaStream_t stream)
@@ -703,7 +705,7 @@ void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, cons
             else launch_tt_flags<double, kZero>(b, s, d, c, p, w, pu, stream);
         }
     }
-    k_unit_gather<<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, c, pu.unit_base, pu.unit_i, pu.unit_j, w);
+    k_unit_gather<<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, c, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
 }
 
 }  // namespace d3

@@ -245,6 +245,10 @@ class DispersionModel(Structure):
         the parts sum to the complete result."""
         library.set_model_work_partition(self._disp, part, nparts)
 
+    def set_tuning(self, morton_cell: float, pair_split: int, atm_blocks_per_sm: int = 0, atm_mol: int = 0) -> None:
+        """Launch shapes (extension, see dftd3_b200_set_model_tuning)."""
+        library.set_model_tuning(self._disp, morton_cell, pair_split, atm_blocks_per_sm, atm_mol)
+
     def set_precision(self, precision: str) -> None:
         """'fp64' (default) or 'mixed' (FP32 pair arithmetic, FP64 accumulation)."""
         modes = {"fp64": library.PRECISION_FP64, "mixed": library.PRECISION_MIXED}
@@ -360,8 +364,8 @@ class BatchedDispersion:
         ms = library.autotune_batch(self._batch, param._param, self._positions, grad)
         return dict(library.get_batch_tuning(self._batch), ms=ms)
 
-    def set_tuning(self, morton_cell: float, atoms_per_block: int, atm_blocks_per_sm: int = 0) -> None:
-        library.set_batch_tuning(self._batch, morton_cell, atoms_per_block, atm_blocks_per_sm)
+    def set_tuning(self, morton_cell: float, pair_split: int, atm_blocks_per_sm: int = 0, atm_mol: int = 0) -> None:
+        library.set_batch_tuning(self._batch, morton_cell, pair_split, atm_blocks_per_sm, atm_mol)
 
     def update(self, positions, lattices: Optional[np.ndarray] = None) -> None:
         self._positions = self._flatten(positions)

@@ -329,18 +329,25 @@ def set_batch_graph(batch: BatchHandle, enable: bool) -> None:
     error_check(lib.dftd3_b200_set_batch_graph)(batch.handle, 1 if enable else 0)
 
 
-TUNING = ("morton_cell", "atoms_per_block", "atm_blocks_per_sm")
+TUNING = ("morton_cell", "pair_split", "atm_blocks_per_sm", "atm_mol")
 
 
-def set_batch_tuning(batch: BatchHandle, morton_cell: float, atoms_per_block: int, atm_blocks_per_sm: int) -> None:
-    t = np.array([morton_cell, atoms_per_block, atm_blocks_per_sm], dtype=float)
+def set_batch_tuning(batch: BatchHandle, morton_cell: float, pair_split: int, atm_blocks_per_sm: int,
+                     atm_mol: int = 0) -> None:
+    t = np.array([morton_cell, pair_split, atm_blocks_per_sm, atm_mol], dtype=float)
     error_check(lib.dftd3_b200_set_batch_tuning)(batch.handle, _cast("double*", t))
 
 
+def set_model_tuning(disp: ModelHandle, morton_cell: float, pair_split: int, atm_blocks_per_sm: int,
+                     atm_mol: int = 0) -> None:
+    t = np.array([morton_cell, pair_split, atm_blocks_per_sm, atm_mol], dtype=float)
+    error_check(lib.dftd3_b200_set_model_tuning)(disp.handle, _cast("double*", t))
+
+
 def get_batch_tuning(batch: BatchHandle) -> dict:
-    t = np.zeros(3)
+    t = np.zeros(4)
     error_check(lib.dftd3_b200_get_batch_tuning)(batch.handle, _cast("double*", t))
-    return {"morton_cell": float(t[0]), "atoms_per_block": int(t[1]), "atm_blocks_per_sm": int(t[2])}
+    return dict(zip(TUNING, (float(t[0]), int(t[1]), int(t[2]), int(t[3]))))
 
 
 def autotune_batch(batch: BatchHandle, param: ParamHandle, positions: np.ndarray, grad: bool) -> float:

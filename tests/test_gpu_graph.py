@@ -76,7 +76,7 @@ def test_graph_list_overflow_falls_back():
             assert np.abs(res["gradient"][k] - ref["gradient"]).max() <= GTOL64 * np.abs(ref["gradient"]).max()
 
 
-@pytest.mark.parametrize("shape", [(3.0, 4, 1), (2.0, 8, 2), (6.0, 4, 0)])
+@pytest.mark.parametrize("shape", [(3.0, 4, 1, 1), (2.0, 1, 2, 2), (6.0, 2, 0, 1), (4.5, 4, 0, 0)])
 def test_launch_shapes(shape):
     from dftd3.interface import BatchedDispersion
     d = _molecules(12, seed=13)
@@ -94,14 +94,17 @@ def test_autotune_keeps_results():
     bat = BatchedDispersion(d["numbers"], d["positions"])
     tuned = bat.autotune(param, grad=True)
     assert tuned["ms"] > 0
-    assert tuned["atoms_per_block"] in (4, 8)
+    assert tuned["pair_split"] in (1, 2, 4)
+    assert tuned["atm_mol"] in (0, 1, 2)
     assert tuned["morton_cell"] in (2.0, 3.0, 4.5, 6.0)
     bat.set_graph(True)
     for _ in range(2):
         res = bat.get_dispersion(param, grad=True)
     _check(res, d, par, range(0, 16, 4))
-    with pytest.raises(RuntimeError, match="4 or 8"):
+    with pytest.raises(RuntimeError, match="1, 2 or 4"):
         library.set_batch_tuning(bat._batch, 3.0, 6, 0)
+    with pytest.raises(RuntimeError, match="0, 1 or 2"):
+        library.set_batch_tuning(bat._batch, 3.0, 4, 0, 5)
 
 
 def test_device_api_graph_with_parameter_derivatives():

@@ -170,3 +170,54 @@ def test_molecule_kernel_energy_only_and_mixed():
     r = gpu_dispersion(d["numbers"], d["positions"], par, precision="mixed")
     assert abs(float(r["energy"]) - ref["energy"]) <= ETOL_MIXED * abs(ref["energy"])
     assert np.abs(r["gradient"] - ref["gradient"]).max() <= GTOL_MIXED
+
+
+MOL = (3.0, 4, 0, 1)     # launch shapes forcing the block-per-molecule triple kernel
+
+
+@pytest.mark.parametrize("case", THREE_BODY[:3], ids=[c[0] for c in THREE_BODY[:3]])
+def test_golden_atm_molecule_kernel(case):
+    name, numbers, pos, param = case
+    ref = O.dispersion(numbers, pos, param)
+    res = gpu_dispersion(numbers, pos, param, tuning=MOL)
+    assert_close(res, ref, RTOL64, GTOL64)
+
+
+def test_molecule_kernel_smooth_ghosts_partition():
+    from dftd3 import synthetic as S
+    d = S.molecule100(seed=5)
+    par = dict(S.PBE_BJ, damping="rational", s9=1.0)
+    cut = (30.0, 12.0, 25.0, 4.0, 3.0)
+    ghost = [1, 7, 33]
+    ref = O.dispersion(d["numbers"], d["positions"], par, cutoff=cut, ghost=ghost)
+    res = gpu_dispersion(d["numbers"], d["positions"], par, cutoff=cut, ghost=ghost, tuning=MOL)
+    assert_close(res, ref, RTOL64, GTOL64)
+    for part in range(3):
+        r = gpu_dispersion(d["numbers"], d["positions"], par, partition=(part, 3), tuning=MOL)
+        rp = O.dispersion(d["numbers"], d["positions"], par, part=part, nparts=3)
+        assert_close(r, rp, 1.0e-11, 1.0e-11)
+    e = gpu_dispersion(d["numbers"], d["positions"], par, grad=False, tuning=MOL)
+    ref0 = O.dispersion(d["numbers"], d["positions"], par)
+    assert abs(float(e["energy"]) - ref0["energy"]) <= RTOL64 * abs(ref0["energy"])
+    m = gpu_dispersion(d["numbers"], d["positions"], par, precision="mixed", tuning=MOL)
+    assert abs(float(m["energy"]) - ref0["energy"]) <= ETOL_MIXED * abs(ref0["energy"])
+    assert np.abs(m["gradient"] - ref0["gradient"]).max() <= GTOL_MIXED
+
+
+def test_molecule_kernel_by_count():
+    """At least one molecule per SM selects the block-per-molecule kernel by
+    itself; the batch agrees with the oracle either way."""
+    from dftd3 import synthetic as S
+    from dftd3.interface import BatchedDispersion, RationalDampingParam
+    d = S.batch4096(nmol=200, seed=23, nmax=40)
+    par = dict(S.PBE_BJ, damping="rational", s9=1.0)
+    bat = BatchedDispersion(d["numbers"], d["positions"])
+    p = RationalDampingParam(**{k: par[k] for k in ("s6", "s8", "a1", "a2", "alp", "s9")})
+    auto = bat.get_dispersion(p, grad=True)
+    bat.set_tuning(3.0, 4, 0, 2)
+    roots = bat.get_dispersion(p, grad=True)
+    assert np.allclose(auto["energy"], roots["energy"], rtol=1e-12, atol=0)
+    for k in (0, 77, 199):
+        ref = O.dispersion(d["numbers"][k], d["positions"][k], par)
+        assert abs(auto["energy"][k] - ref["energy"]) <= RTOL64 * abs(ref["energy"])
+        assert np.abs(auto["gradient"][k] - ref["gradient"]).max() <= GTOL64 * np.abs(ref["gradient"]).max()

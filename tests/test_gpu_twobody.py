@@ -34,7 +34,7 @@ def _param_obj(p):
 
 
 def gpu_dispersion(numbers, positions, param, lattice=None, periodic=None, grad=True, cutoff=None,
-                   precision="fp64", ghost=None, partition=None):
+                   precision="fp64", ghost=None, partition=None, tuning=None):
     from dftd3.interface import DispersionModel
     model = DispersionModel(np.asarray(numbers), np.asarray(positions, dtype=float),
                             None if lattice is None else np.asarray(lattice, dtype=float),
@@ -46,6 +46,8 @@ def gpu_dispersion(numbers, positions, param, lattice=None, periodic=None, grad=
     if partition is not None:
         model.set_work_partition(*partition)
     model.set_precision(precision)
+    if tuning is not None:
+        model.set_tuning(*tuning)
     return model.get_dispersion(_param_obj(param), grad=grad)
 
 
