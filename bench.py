@@ -42,9 +42,9 @@ L2_FLUSH_BYTES = 256 << 20     # larger than the 126 MB L2
 FLOPS_PER_PAIR = 65            # two-body BJ term with gradient, virial and dE/dCN
 FLOPS_PER_TRIPLE = 220         # ATM term with gradient, virial and dE/dCN
 METRIC = "pair-terms/s, D3(BJ) two-body E+grad+virial (mixed FP32/FP64, <=1e-7 rel. E error)"
-# DRAM bytes (read + write) of one k_two_body_tiled<float> launch on cell2000, from the
-# ncu capture summarised in profiles/k_two_body_tiled_cell2000_mixed.md
-TWO_BODY_TRAFFIC_BYTES = 325632
+# DRAM bytes (read + write) of one k_two_body_tt<float, rational> launch on cell2000, from
+# the ncu capture summarised in profiles/k_two_body_tt_cell2000_mixed.md
+TWO_BODY_TRAFFIC_BYTES = 1014784
 
 
 def parse_args():
@@ -291,7 +291,7 @@ def run_ours(args, rank, world, dist):
     run = Runner(systems, par)
     if shard:
         from dftd3 import parallel
-        lib.set_batch_tuning(run.batch, 3.0, 4, 0, 0)
+        lib.set_batch_tuning(run.batch, 3.0, 0, 0, 0)
         run.reducer = parallel.make_device_reducer()
         lib.set_batch_reducer(run.batch, run.reducer, rank, world)
     counts = run.counts()
@@ -366,9 +366,10 @@ def run_ours(args, rank, world, dist):
     units = counts[unit_key]
     peak64 = lib.fma_peak(lib.PRECISION_FP64)
     peak32 = lib.fma_peak(lib.PRECISION_MIXED)
-    stage = "three_body" if atm else "two_body"
+    # the dominant kernel alone, timed with CUDA events around its launch
+    stage = "three_body_kernel" if atm else "two_body_kernel"
     flops = FLOPS_PER_TRIPLE if atm else FLOPS_PER_PAIR
-    kern = "k_triples" if atm else "k_two_body_tiled"
+    kern = "k_triples" if atm else "k_two_body_tt"
     line = {
         "metric": METRIC if args.workload == "cell2000" else f"{unit} ({args.workload})",
         "value": (1 if shard else world) * units / (ms * 1e-3),
@@ -419,7 +420,8 @@ def run_ours(args, rank, world, dist):
         line["extra_workloads"] = extra
         for name, entry in extra.items():
             entry["roofline_mixed"] = roofline(entry["triple_terms"], FLOPS_PER_TRIPLE,
-                                               entry["mixed"]["stage_ms"]["three_body"], peak32, "k_triples<float>",
+                                               entry["mixed"]["stage_ms"]["three_body_kernel"], peak32,
+                                               "k_triples_mol<float>" if name == "batch4096" else "k_triples<float>",
                                                "fp32")
     if world == 1 and not args.no_cpu:
         sample = systems if len(systems) == 1 else systems[:64]

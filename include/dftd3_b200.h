@@ -107,7 +107,9 @@ dftd3_b200_get_batch_counts(dftd3_error /* error */,
 /* Device time of each pipeline stage of the last evaluation in ms, recorded
  * with CUDA events while profiling is enabled: [0] position split, [1]
  * coordination number, [2] reference weights, [3] two-body, [4] three-body,
- * [5] CN chain rule, [6] per-system reductions. */
+ * [5] CN chain rule, [6] per-system reductions; then [7] the two-body
+ * tile-pair kernel alone and [8] the three-body triple kernels alone (0 when
+ * not run). */
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_b200_set_batch_profiling(dftd3_error /* error */,
                                dftd3_b200_batch /* batch */,
@@ -116,7 +118,7 @@ dftd3_b200_set_batch_profiling(dftd3_error /* error */,
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_b200_get_batch_stage_times(dftd3_error /* error */,
                                  dftd3_b200_batch /* batch */,
-                                 double* /* ms[7] */);
+                                 double* /* ms[9] */);
 
 /* Replay the whole pipeline of an evaluation as one captured CUDA graph
  * (enable != 0).  The first evaluation for a parameter set, derivative set
@@ -132,7 +134,8 @@ dftd3_b200_set_batch_graph(dftd3_error /* error */,
 
 /* Launch shapes of a batch: tuning[0] the cell of the spatial sort key
  * (Bohr, > 0), tuning[1] work items per tile pair of the pair sweeps (1, 2
- * or 4), tuning[2] resident blocks per SM of the neighbour-list three-body
+ * or 4; 0 chooses 1 for batches of molecules, else 2 in the mixed and 4 in
+ * the FP64 form), tuning[2] resident blocks per SM of the neighbour-list three-body
  * kernel (0 = occupancy limit), tuning[3] the block-per-molecule three-body
  * kernel for non-periodic systems of at most 256 atoms (0: when the batch has
  * at least one such molecule per SM, 1: always, 2: never). */

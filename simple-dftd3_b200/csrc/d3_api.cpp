@@ -550,8 +550,8 @@ void dftd3_b200_set_model_tuning(dftd3_error error, dftd3_model model, const dou
     }
     guarded(error, [&] {
         const d3::Tuning t = tuning_from(tuning);
-        if (t.pair_split != 1 && t.pair_split != 2 && t.pair_split != 4)
-            throw d3::Error("Work items per tile pair must be 1, 2 or 4");
+        if (t.pair_split != 0 && t.pair_split != 1 && t.pair_split != 2 && t.pair_split != 4)
+            throw d3::Error("Work items per tile pair must be 1, 2 or 4 (0 chooses)");
         model->tuning = t;
         model->has_tuning = true;
         if (model->engine) model->engine->set_tuning(t);

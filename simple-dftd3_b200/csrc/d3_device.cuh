@@ -118,7 +118,8 @@ struct Config {
 // Launch-shape choices of one batch, picked by the autotuner or set by hand.
 struct Tuning {
     double morton_cell = 3.0;      // Bohr; quantisation of the spatial sort key
-    int pair_split = 4;            // work items per tile pair of the pair sweeps: 1, 2 or 4
+    int pair_split = 0;            // work items per tile pair of the pair sweeps: 1, 2 or 4; 0 = 1 for
+                                   // molecules, else 2 (mixed form) or 4 (FP64 form)
     int atm_blocks_per_sm = 0;     // resident blocks per SM of the neighbour-list triple kernel; 0 = occupancy
     int atm_mol = 0;               // molecule triple kernel: 0 for batches of at least one molecule per SM,
                                    // 1 for every eligible system, 2 never
@@ -163,8 +164,10 @@ void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Pa
                      const PairUnits& pu, bool chain, cudaStream_t stream);
 size_t pair_unit_slot_doubles();   // per unit: i and j slots
 size_t pair_unit_i_doubles();      // per unit: i slots
+// ev_begin/ev_end (or null) are recorded around the tile-pair kernel alone.
 void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
-                           const Work& w, const PairUnits& pu, cudaStream_t stream);
+                           const Work& w, const PairUnits& pu, cudaStream_t stream, cudaEvent_t ev_begin = nullptr,
+                           cudaEvent_t ev_end = nullptr);
 
 // Three-body term (d3_atm.cu): C6 table, neighbour lists, triple sum.
 size_t atm_c6_entry_bytes(bool mixed);

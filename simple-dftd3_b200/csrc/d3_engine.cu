@@ -288,6 +288,9 @@ Engine::Engine(int nsys, const int* natoms, const int* numbers, const double* la
     }
     c6mat_total_ = off;
     sys_natoms_.assign(natoms, natoms + nsys);
+    auto_split_ = 1;
+    for (int sy = 0; sy < nsys; sy++)
+        if (per_[3 * sy] || per_[3 * sy + 1] || per_[3 * sy + 2]) auto_split_ = 2;
     d_mol_order_ = dev_alloc<int>(nsys);
     d_sys_mol_ = dev_alloc<uint8_t>(nsys);
     configure_molecules();
@@ -299,6 +302,8 @@ Engine::~Engine()
     cudaSetDevice(device_);
     if (stream_) cudaStreamSynchronize(stream_);
     for (auto& e : ev_)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : kev_)
         if (e) cudaEventDestroy(e);
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     for (void* p : allocations_) cudaFree(p);
@@ -551,7 +556,9 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     c.cut_cn = cut_.cn; c.cut2 = cut_.disp2; c.cut3 = cut_.disp3;
     c.width2 = cut_.width2; c.width3 = cut_.width3;
     c.grad = grad; c.mixed = mixed_; c.param_grad = pg; c.cn_partitioned = cn_partitioned_;
-    pu_.split = tune_.pair_split;
+    // automatic split: one item per tile pair for molecules; for periodic
+    // systems two (mixed form) or four (FP64 form), measured on B200
+    pu_.split = tune_.pair_split ? tune_.pair_split : (auto_split_ == 1 ? 1 : (mixed_ ? 2 : 4));
     Work w = work_;
     w.counts = counting_ ? d_counts_ : nullptr;
     w.e3_atom = nullptr;
@@ -563,8 +570,11 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     auto mark = [&](int k) {
         if (timed) check(cudaEventRecord(ev_[k], stream), "cudaEventRecord");
     };
-    if (timed && !ev_[0])
+    if (timed && !ev_[0]) {
         for (auto& e : ev_) check(cudaEventCreate(&e), "cudaEventCreate");
+        for (auto& e : kev_) check(cudaEventCreate(&e), "cudaEventCreate");
+    }
+    kev3_recorded_ = false;
     mark(0);
     launch_spatial_sort(d_positions, natoms_, d_sys_of_atom_, tune_.morton_cell, d_keys_in_, d_keys_out_, d_idx_in_,
                         d_perm_, d_sort_temp_, sort_bytes_, stream);
@@ -578,7 +588,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     launch_weights(b, s, c, w, stream);
     mark(3);
     if (std::fabs(d.s6) >= DBL_EPSILON || std::fabs(d.s8) >= DBL_EPSILON || pg) {
-        launch_two_body_units(b, s, d, c, part_, w, pu_, stream);
+        launch_two_body_units(b, s, d, c, part_, w, pu_, stream, timed ? kev_[0] : nullptr, timed ? kev_[1] : nullptr);
     } else {
         check(cudaMemsetAsync(w.e_atom, 0, sizeof(double) * natoms_, stream), "memset");
         if (grad) {
@@ -719,24 +729,30 @@ void Engine::run_three_body(const Batch& b, const Species& s, const Damp& d, con
         launch_nbr_fill(b, c, d_sys_mol_, d_off_, d_nbr_j_, d_nbr_gend_, d_nbr_v_, d_guard_, stream);
         check(cudaMemsetAsync(d_queue_, 0, sizeof(unsigned int), stream), "memset");
         w.atm_guard = d_guard_;
+        if (profiling_ && !capturing_) check(cudaEventRecord(kev_[2], stream), "cudaEventRecord");
         launch_triples(b, s, d, c, part_, w, d_c6mat_, d_c6mat_off_, d_off_, d_cnt_, d_nbr_j_, d_nbr_gend_, d_nbr_v_,
                        d_queue_, d_slot_acc_, d_slot_scr_, stride, blocks, d_e3_, d_sig3_, stream);
     }
     if (!mol_order_.empty()) {
         // after the root kernel, which writes zeros for the molecules' atoms
+        if (profiling_ && !capturing_ && root_atoms_ == 0) check(cudaEventRecord(kev_[2], stream), "cudaEventRecord");
         const int nmol = (int)mol_order_.size();
         const int mblocks = std::max(1, std::min(nmol, sms_ * atm_mol_occupancy(c.mixed, c.grad)));
         check(cudaMemsetAsync(d_queue_ + 1, 0, sizeof(unsigned int), stream), "memset");
         launch_triples_mol(b, s, d, c, part_, w, d_c6mat_, d_c6mat_off_, d_mol_order_, nmol, d_queue_ + 1, mblocks,
                            d_e3_, d_sig3_, stream);
     }
+    if (profiling_ && !capturing_) {
+        check(cudaEventRecord(kev_[3], stream), "cudaEventRecord");
+        kev3_recorded_ = true;
+    }
     w.e3_atom = d_e3_;
     w.sig3_atom = c.grad ? d_sig3_ : nullptr;
 }
 
-void Engine::stage_times(double out[kStages])
+void Engine::stage_times(double out[kTimes])
 {
-    for (int k = 0; k < kStages; k++) out[k] = 0.0;
+    for (int k = 0; k < kTimes; k++) out[k] = 0.0;
     if (!ev_recorded_) return;
     check(cudaEventSynchronize(ev_[kStages]), "cudaEventSynchronize");
     for (int k = 0; k < kStages; k++) {
@@ -744,6 +760,11 @@ void Engine::stage_times(double out[kStages])
         check(cudaEventElapsedTime(&ms, ev_[k], ev_[k + 1]), "cudaEventElapsedTime");
         out[k] = ms;
     }
+    float ms = 0.f;
+    if (out[3] > 0.0 && cudaEventElapsedTime(&ms, kev_[0], kev_[1]) == cudaSuccess) out[kStages] = ms;
+    (void)cudaGetLastError();
+    if (kev3_recorded_ && cudaEventElapsedTime(&ms, kev_[2], kev_[3]) == cudaSuccess) out[kStages + 1] = ms;
+    (void)cudaGetLastError();
 }
 
 int Engine::atm_occupancy(bool mixed, bool grad)
@@ -811,8 +832,8 @@ void Engine::set_graph(bool on)
 
 void Engine::set_tuning(const Tuning& t)
 {
-    if (t.pair_split != 1 && t.pair_split != 2 && t.pair_split != 4)
-        throw Error("Work items per tile pair must be 1, 2 or 4");
+    if (t.pair_split != 0 && t.pair_split != 1 && t.pair_split != 2 && t.pair_split != 4)
+        throw Error("Work items per tile pair must be 1, 2 or 4 (0 chooses)");
     if (!(t.morton_cell > 0.0) || !std::isfinite(t.morton_cell)) throw Error("Sort cell must be positive");
     if (t.atm_blocks_per_sm < 0) throw Error("Three-body blocks per SM must not be negative");
     if (t.atm_mol < 0 || t.atm_mol > 2) throw Error("Molecule kernel mode must be 0, 1 or 2");
@@ -940,8 +961,9 @@ double Engine::autotune(const Damp& d, const double* d_positions, bool grad, cud
         };
         for (double cell : {2.0, 3.0, 4.5, 6.0})
             if (cell != best.morton_cell) { Tuning t = best; t.morton_cell = cell; consider(t); }
+        const int cur_split = best.pair_split ? best.pair_split : (auto_split_ == 1 ? 1 : (mixed_ ? 2 : 4));
         for (int sp : {1, 2, 4})
-            if (sp != best.pair_split) { Tuning t = best; t.pair_split = sp; consider(t); }
+            if (sp != cur_split) { Tuning t = best; t.pair_split = sp; consider(t); }
         if (threebody) {
             // molecules: one block each, or the neighbour-list kernel
             bool any_mol = false;

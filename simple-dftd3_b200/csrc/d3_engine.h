@@ -119,8 +119,11 @@ public:
     // Per-stage device times of the last evaluation (ms), recorded with CUDA
     // events when profiling is on.  Stages: see kStageNames.
     static constexpr int kStages = 7;
+    // stage_times() also returns, after the stages, the time of the two-body
+    // tile-pair kernel alone and of the three-body triple kernels alone
+    static constexpr int kTimes = kStages + 2;
     void set_profiling(bool on) { profiling_ = on; }
-    void stage_times(double out[kStages]);
+    void stage_times(double out[kTimes]);
 
 private:
     void build_tables(const int* numbers);
@@ -159,6 +162,7 @@ private:
     std::vector<int> mol_order_;         // systems of the molecule kernel, largest first
     int* d_mol_order_ = nullptr;
     std::vector<int> sys_natoms_;
+    int auto_split_ = 1;                 // pair split of tuning 0
     void configure_molecules();          // mol_order_ and root_atoms_ from tune_.atm_mol
     uint8_t* d_sys_mol_ = nullptr;       // [nsys] 1 for those systems
     long long root_atoms_ = 0;           // atoms of the other systems
@@ -189,6 +193,8 @@ private:
     bool counting_ = false;
     bool profiling_ = false;
     cudaEvent_t ev_[kStages + 1] = {};
+    cudaEvent_t kev_[4] = {};            // two-body kernel, triple kernels: begin, end
+    bool kev3_recorded_ = false;
     bool ev_recorded_ = false;
     bool images_valid_ = false;
     Damp last_damp_{};

@@ -153,7 +153,7 @@ __global__ void k_species_vectors(Batch b, Species s, Work w, R* U, R* dU)
 }
 
 template <class R, int DAMP, bool GRAD, bool PG>
-__global__ void __launch_bounds__(kTTThreads)
+__global__ void __launch_bounds__(kTTThreads, sizeof(R) == 4 ? 4 : 3)
 k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const int2* units, int nunits, int split,
               const R* U, const R* dU, double* unit_i, double* unit_j)
 {
@@ -161,6 +161,8 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     __shared__ V sth[kTTWarps][kTTChunk];
     __shared__ V stl[kTTWarps][kTTChunk];
     __shared__ int sidx[kTTWarps][kTTChunk];     // image index of each compacted translation
+    // FP64 sums of the lanes, [value][lane]: i sums and j sums
+    __shared__ double sacc[kTTWarps][kUnitI + kUnitJ][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int item = blockIdx.x * kTTWarps + wid;
     if (item >= nunits * split) return;
@@ -203,29 +205,30 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     const R s6 = R(d.s6), s8 = R(d.s8);
     const R alp6 = R(d.alp), alp8 = R(d.alp + 2.0);
     const int nid = b.nid;
-    // i sums (FP64) and their FP32 partials
-    double a_e = 0, a_de = 0, a_gx = 0, a_gy = 0, a_gz = 0;
-    double a_xx = 0, a_yy = 0, a_zz = 0, a_xy = 0, a_xz = 0, a_yz = 0;
-    double a_p0 = 0, a_p1 = 0, a_p2 = 0, a_p3 = 0;
+    // i sums: FP32 partials over at most 128 terms (mixed form) added to the
+    // FP64 sums in shared memory; the FP64 form adds every term to its
+    // register sums and stores them at the end
+    double (*acc)[32] = sacc[wid];
+    for (int v = 0; v < kUnitI + kUnitJ; v++) acc[v][lane] = 0.0;
     R te = R(0), tde = R(0), tgx = R(0), tgy = R(0), tgz = R(0);
     R txx = R(0), tyy = R(0), tzz = R(0), txy = R(0), txz = R(0), tyz = R(0);
     R tp0 = R(0), tp1 = R(0), tp2 = R(0), tp3 = R(0);
     int pending = 0;          // terms in the FP32 partials (warp-uniform)
-    // j sums of atom ja0 + lane (FP64)
-    double b_de = 0, b_gx = 0, b_gy = 0, b_gz = 0;
     unsigned long long nterm = 0;
+    double b_de = 0, b_gx = 0, b_gy = 0, b_gz = 0;   // j sums of the FP64 form (registers)
 
     auto flush = [&]() {
-        a_e += double(te); a_de += double(tde);
+        acc[0][lane] += double(te); acc[1][lane] += double(tde);
         te = tde = R(0);
         if (GRAD) {
-            a_gx += double(tgx); a_gy += double(tgy); a_gz += double(tgz);
-            a_xx += double(txx); a_yy += double(tyy); a_zz += double(tzz);
-            a_xy += double(txy); a_xz += double(txz); a_yz += double(tyz);
+            acc[2][lane] += double(tgx); acc[3][lane] += double(tgy); acc[4][lane] += double(tgz);
+            acc[5][lane] += double(txx); acc[6][lane] += double(tyy); acc[7][lane] += double(tzz);
+            acc[8][lane] += double(txy); acc[9][lane] += double(txz); acc[10][lane] += double(tyz);
             tgx = tgy = tgz = txx = tyy = tzz = txy = txz = tyz = R(0);
         }
         if (PG) {
-            a_p0 += double(tp0); a_p1 += double(tp1); a_p2 += double(tp2); a_p3 += double(tp3);
+            acc[11][lane] += double(tp0); acc[12][lane] += double(tp1);
+            acc[13][lane] += double(tp2); acc[14][lane] += double(tp3);
             tp0 = tp1 = tp2 = tp3 = R(0);
         }
         pending = 0;
@@ -362,8 +365,16 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
             jde = wsum_tt<R>(jde);
             if (GRAD) { jgx = wsum_tt<R>(jgx); jgy = wsum_tt<R>(jgy); jgz = wsum_tt<R>(jgz); }
             if (lane == jl) {
-                b_de += double(jde);
-                if (GRAD) { b_gx += double(jgx); b_gy += double(jgy); b_gz += double(jgz); }
+                if constexpr (sizeof(R) == 4) {
+                    acc[kUnitI + 0][lane] += double(jde);
+                    if (GRAD) {
+                        acc[kUnitI + 1][lane] += double(jgx); acc[kUnitI + 2][lane] += double(jgy);
+                        acc[kUnitI + 3][lane] += double(jgz);
+                    }
+                } else {
+                    b_de += jde;
+                    if (GRAD) { b_gx += jgx; b_gy += jgy; b_gz += jgz; }
+                }
             }
             if constexpr (sizeof(R) == 4) {
                 pending += qend - qbeg;
@@ -372,13 +383,14 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
         }
     }
     flush();
+    if constexpr (sizeof(R) == 8) {
+        acc[kUnitI + 0][lane] = b_de; acc[kUnitI + 1][lane] = b_gx;
+        acc[kUnitI + 2][lane] = b_gy; acc[kUnitI + 3][lane] = b_gz;
+    }
     double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
-    oi[0] = a_e; oi[1] = a_de;
-    oi[2] = a_gx; oi[3] = a_gy; oi[4] = a_gz;
-    oi[5] = a_xx; oi[6] = a_yy; oi[7] = a_zz; oi[8] = a_xy; oi[9] = a_xz; oi[10] = a_yz;
-    oi[11] = a_p0; oi[12] = a_p1; oi[13] = a_p2; oi[14] = a_p3;
+    for (int v = 0; v < kUnitI; v++) oi[v] = acc[v][lane];
     double* oj = unit_j + ((size_t)item * kTile + lane) * kUnitJ;
-    oj[0] = b_de; oj[1] = b_gx; oj[2] = b_gy; oj[3] = b_gz;
+    for (int v = 0; v < kUnitJ; v++) oj[v] = acc[kUnitI + v][lane];
     if (w.counts) {
         for (int off = 16; off > 0; off >>= 1) nterm += __shfl_xor_sync(0xffffffffu, nterm, off);
         if (lane == 0) atomicAdd(w.counts + 0, nterm);
@@ -688,7 +700,8 @@ size_t pair_unit_slot_doubles() { return (size_t)kSplitMax * kTile * (kUnitI + k
 size_t pair_unit_i_doubles() { return (size_t)kSplitMax * kTile * kUnitI; }
 
 void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
-                           const Work& w, const PairUnits& pu, cudaStream_t stream)
+                           const Work& w, const PairUnits& pu, cudaStream_t stream, cudaEvent_t ev_begin,
+                           cudaEvent_t ev_end)
 {
     if (b.natoms <= 0) return;
     const long long nsv = (long long)b.natoms * b.nid * kMaxRef;
@@ -696,6 +709,7 @@ void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, cons
         k_species_vectors<float><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (float*)pu.U, (float*)pu.dU);
     else
         k_species_vectors<double><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (double*)pu.U, (double*)pu.dU);
+    if (ev_begin) cudaEventRecord(ev_begin, stream);
     if (pu.nunits > 0) {
         if (d.kind == kRational) {
             if (c.mixed) launch_tt_flags<float, kRational>(b, s, d, c, p, w, pu, stream);
@@ -705,6 +719,7 @@ void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, cons
             else launch_tt_flags<double, kZero>(b, s, d, c, p, w, pu, stream);
         }
     }
+    if (ev_end) cudaEventRecord(ev_end, stream);
     k_unit_gather<<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, c, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
 }
 

@@ -316,7 +316,8 @@ def set_batch_profiling(batch: BatchHandle, enable: bool) -> None:
     error_check(lib.dftd3_b200_set_batch_profiling)(batch.handle, 1 if enable else 0)
 
 
-STAGES = ("split", "cn", "weights", "two_body", "three_body", "cn_chain", "reduce")
+STAGES = ("split", "cn", "weights", "two_body", "three_body", "cn_chain", "reduce", "two_body_kernel",
+          "three_body_kernel")
 
 
 def get_batch_stage_times(batch: BatchHandle) -> dict:

@@ -94,7 +94,7 @@ def test_autotune_keeps_results():
     bat = BatchedDispersion(d["numbers"], d["positions"])
     tuned = bat.autotune(param, grad=True)
     assert tuned["ms"] > 0
-    assert tuned["pair_split"] in (1, 2, 4)
+    assert tuned["pair_split"] in (0, 1, 2, 4)
     assert tuned["atm_mol"] in (0, 1, 2)
     assert tuned["morton_cell"] in (2.0, 3.0, 4.5, 6.0)
     bat.set_graph(True)
