@@ -43,7 +43,7 @@ FLOPS_PER_PAIR = 65            # two-body BJ term with gradient, virial and dE/d
 FLOPS_PER_TRIPLE = 220         # ATM term with gradient, virial and dE/dCN
 METRIC = "pair-terms/s, D3(BJ) two-body E+grad+virial (mixed FP32/FP64, <=1e-7 rel. E error)"
 # DRAM bytes (read + write) of one k_two_body_tt<float, rational> launch on cell2000, from
-# the ncu capture summarised in profiles/k_two_body_tt_cell2000_mixed.md
+# an ncu capture of that launch
 TWO_BODY_TRAFFIC_BYTES = 1014784
 
 
@@ -398,7 +398,7 @@ def run_ours(args, rank, world, dist):
         line["mixed_speedup_vs_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
         line["mixed_vs_fp64_rel_energy_error"] = abs(res["mixed"]["energy"] - res["fp64"]["energy"]) / abs(
             res["fp64"]["energy"])
-    # kernels launched per step (ncu launch list, profiles/launch_list_cell2000.md): Morton
+    # kernels launched per step (counted in the ncu launch list of the headline): Morton
     # keys, radix sort (one kernel up to a few thousand atoms; histogram, scan and one
     # pass per key byte above), gather, tile bounds, CN tile pairs + gather, weights,
     # species vectors, two-body tile pairs + gather, chain rule tile pairs + gather,
@@ -411,7 +411,7 @@ def run_ours(args, rank, world, dist):
                   kern + ("<float>" if head == "mixed" else "<double>"), "fp32" if head == "mixed" else "fp64")
     rl["traffic"] = TWO_BODY_TRAFFIC_BYTES if (args.workload == "cell2000" and head == "mixed") else None
     if rl["traffic"] is not None:
-        rl["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch (profiles/)"
+        rl["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch"
     rl["peak_source"] = "measured in-run FMA throughput (MEASURED_PEAKS.json has no FP32/FP64 pipe figure)"
     if "fp64" in res:
         rl["fp64"] = roofline(units, flops, res["fp64"]["stage_ms"][stage], peak64, kern + "<double>", "fp64")
