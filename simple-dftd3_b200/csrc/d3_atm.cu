@@ -24,6 +24,8 @@
 //                   partner atoms).
 #include <cub/cub.cuh>
 
+#include <algorithm>
+
 #include <cfloat>
 #include <cstdint>
 
@@ -44,7 +46,7 @@ constexpr int kAcc = 5;          // per-entry accumulators: S, Gx, Gy, Gz, dE/dC
 // {sqrt(C6_rc), dC6_rc/dCN_r / C6_rc, dC6_rc/dCN_c / C6_rc} for every ordered
 // pair (r, c) of each system (get_atomic_c6, model.f90:432-461); ghosts give 0.
 template <class R>
-__global__ void k_c6_matrix(Batch b, Species s, Work w, const long long* mat_off, C6Entry<R>* mat,
+__global__ void k_c6_matrix(Batch b, Species s, Work w, double alp3, const long long* mat_off, C6Entry<R>* mat,
                             long long total)
 {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -60,7 +62,9 @@ __global__ void k_c6_matrix(Batch b, Species s, Work w, const long long* mat_off
     const int n = b.atom_off[sys + 1] - a0;
     const long long e = t - mat_off[sys];
     const int r = a0 + (int)(e / n), c = a0 + (int)(e % n);
-    C6Entry<R> out{R(0), R(0), R(0)};
+    const double r0 = __ldg(s.atm_r0 + b.sp[r] * b.nid + b.sp[c]);
+    const R lr0 = R(alp3 * (sizeof(R) == 8 ? log(r0) : log2(r0)));
+    C6Entry<R> out{R(0), R(0), R(0), lr0};
     const bool ghost = b.ghost && (b.ghost[r] || b.ghost[c]);
     if (!ghost) {
         const int sr = b.sp[r], sc = b.sp[c];
@@ -78,7 +82,7 @@ __global__ void k_c6_matrix(Batch b, Species s, Work w, const long long* mat_off
             dr += w.dgw[r * kMaxRef + ir] * a;
             dc += w.gw[r * kMaxRef + ir] * bb;
         }
-        if (c6 != 0.0) out = C6Entry<R>{R(sqrt(c6)), R(dr / c6), R(dc / c6)};
+        if (c6 != 0.0) out = C6Entry<R>{R(sqrt(c6)), R(dr / c6), R(dc / c6), lr0};
     }
     mat[t] = out;
 }
@@ -188,7 +192,7 @@ struct Slot {
     int4 meta;                  // atom, group end, species, input index
 };
 
-template <class R, bool GRAD>
+template <class R, bool GRAD, bool PER>
 __global__ void __launch_bounds__(kThreadsAtm, sizeof(R) == 4 ? 3 : 1) k_triples(Batch b, Species sp, Damp d, Config c, Partition part,
                                                          Work w, const C6Entry<R>* mat, const long long* mat_off,
                                                          const long long* off, const int* cnt, const int* nbr_j,
@@ -203,7 +207,6 @@ __global__ void __launch_bounds__(kThreadsAtm, sizeof(R) == 4 ? 3 : 1) k_triples
     auto sjk = reinterpret_cast<C6Entry<R>(*)[kTB]>(sb + kTB);
     auto kred = reinterpret_cast<R(*)[kTB / 2][kAcc]>(sjk + kTA);
     __shared__ int s_root;
-    __shared__ R slr0[kMaxSpeciesFast * kMaxSpeciesFast];
     __shared__ double wsum[kThreadsAtm / 32][13];
     const int tid = threadIdx.x;
     const int tx = tid & 15, ty = tid >> 4;
@@ -217,9 +220,6 @@ __global__ void __launch_bounds__(kThreadsAtm, sizeof(R) == 4 ? 3 : 1) k_triples
     const bool smooth_on = c.width3 > 0.0 && c.width3 < c.cut3;
     const R cutoff = R(c.cut3), width = R(c.width3);
     if (w.atm_guard && *w.atm_guard) return;   // lists did not fit the reserved buffers
-    const bool table_r0 = b.nid <= kMaxSpeciesFast;
-    if (table_r0)
-        for (int k = tid; k < b.nid * b.nid; k += kThreadsAtm) slr0[k] = rlog<R>(R(__ldg(sp.atm_r0 + k)));
     __syncthreads();
 
     for (;;) {
@@ -333,8 +333,8 @@ __global__ void __launch_bounds__(kThreadsAtm, sizeof(R) == 4 ? 3 : 1) k_triples
                             }
                             const R rc = vx * vx + vy * vy + vz * vz;   // r_jk^2
                             if (rc > cut2 || rc < R(DBL_EPSILON)) continue;
+                            // a ghost gives C6 = 0 and with it zero contributions
                             const C6Entry<R> ejk = sjk[ia][ib];
-                            if (GRAD && (A.c.x == R(0) || Bs.c.x == R(0) || ejk.sc6 == R(0))) continue;
                             if (part.nparts > 1) {
                                 // owner of the triple: the pair of its two largest input indices
                                 int o1 = orig_i, o2 = A.meta.w, o3 = Bs.meta.w, t;
@@ -350,18 +350,20 @@ __global__ void __launch_bounds__(kThreadsAtm, sizeof(R) == 4 ? 3 : 1) k_triples
                             const R ir2 = ir1 * ir1;
                             const R ir3 = ir2 * ir1;
                             const R ir5 = ir3 * ir2;
-                            const R lr0jk = table_r0 ? slr0[A.meta.z * b.nid + Bs.meta.z]
-                                                     : rlog<R>(R(__ldg(sp.atm_r0 + A.meta.z * b.nid + Bs.meta.z)));
+
                             // (r0/r1)^alp3, r0 = r0ij r0ik r0jk, r1 = r_ij r_ik r_jk
-                            const R t = rexp<R>(A.c.w + Bs.c.w + alp3 * (lr0jk - R(0.5) * rlog<R>(rc)));
+                            const R t = rexp<R>(A.c.w + Bs.c.w + ejk.lr0 - R(0.5) * alp3 * rlog<R>(rc));
                             const R fdmp = rcp_r<R>(R(1) + R(6) * t);
                             const R s1 = ra + rb + rc;
                             const R ang = R(0.375) * (s1 - R(2) * rb) * (s1 - R(2) * rc) * (s1 - R(2) * ra) * ir5 + ir3;
                             const R c9 = -s9 * A.c.x * Bs.c.x * ejk.sc6;
                             const int jat = A.meta.x, kat = Bs.meta.x;
-                            R triple;
-                            if (i == jat) triple = (i == kat) ? R(1.0 / 6.0) : R(0.5);
-                            else triple = (i != kat && jat != kat) ? R(1) : R(0.5);
+                            // triple_scale (atm.f90:954-980): repeated atoms only under periodicity
+                            R triple = R(1);
+                            if (PER) {
+                                if (i == jat) triple = (i == kat) ? R(1.0 / 6.0) : R(0.5);
+                                else triple = (i != kat && jat != kat) ? R(1) : R(0.5);
+                            }
                             R sw = R(1), swjk = R(1), dswjkr = R(0);
                             if (smooth_on) {
                                 R dsw;
@@ -496,14 +498,14 @@ __global__ void __launch_bounds__(kThreadsAtm, sizeof(R) == 4 ? 3 : 1) k_triples
 
 size_t atm_c6_entry_bytes(bool mixed) { return mixed ? sizeof(C6Entry<float>) : sizeof(C6Entry<double>); }
 
-void launch_c6_matrix(const Batch& b, const Species& s, const Work& w, const long long* d_mat_off,
+void launch_c6_matrix(const Batch& b, const Species& s, const Work& w, double alp3, const long long* d_mat_off,
                       void* mat, long long total, bool mixed, cudaStream_t stream)
 {
     if (total <= 0) return;
     const int threads = 256;
     const long long blocks = (total + threads - 1) / threads;
-    if (mixed) k_c6_matrix<float><<<(unsigned)blocks, threads, 0, stream>>>(b, s, w, d_mat_off, (C6Entry<float>*)mat, total);
-    else k_c6_matrix<double><<<(unsigned)blocks, threads, 0, stream>>>(b, s, w, d_mat_off, (C6Entry<double>*)mat, total);
+    if (mixed) k_c6_matrix<float><<<(unsigned)blocks, threads, 0, stream>>>(b, s, w, alp3, d_mat_off, (C6Entry<float>*)mat, total);
+    else k_c6_matrix<double><<<(unsigned)blocks, threads, 0, stream>>>(b, s, w, alp3, d_mat_off, (C6Entry<double>*)mat, total);
 }
 
 void launch_nbr_count(const Batch& b, const Config& c, const uint8_t* sys_skip, int* cnt, int* max_cnt,
@@ -545,17 +547,25 @@ size_t triple_smem()
     return sizeof(Slot<R>) * (kTA + kTB) + sizeof(C6Entry<R>) * kTA * kTB + sizeof(R) * 16 * (kTB / 2) * kAcc;
 }
 
-template <class R, bool GRAD>
-int triple_occupancy()
+template <class R, bool GRAD, bool PER>
+int triple_occupancy_of()
 {
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(k_triples<R, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)triple_smem<R>());
+        cudaFuncSetAttribute(k_triples<R, GRAD, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)triple_smem<R>());
         configured = true;
     }
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_triples<R, GRAD>, kThreadsAtm, triple_smem<R>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_triples<R, GRAD, PER>, kThreadsAtm, triple_smem<R>());
     return n > 0 ? n : 1;
+}
+
+template <class R, bool GRAD>
+int triple_occupancy()
+{
+    // both variants are configured; the occupancy is the smaller of the two
+    return std::min(triple_occupancy_of<R, GRAD, false>(), triple_occupancy_of<R, GRAD, true>());
 }
 
 int atm_blocks_per_sm(bool mixed, bool grad)
@@ -566,32 +576,37 @@ int atm_blocks_per_sm(bool mixed, bool grad)
 
 size_t atm_slot_bytes(bool mixed) { return mixed ? sizeof(Slot<float>) : sizeof(Slot<double>); }
 
+template <class R, bool GRAD, bool PER>
+void launch_triples_t(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
+                      const Work& w, const void* mat, const long long* mat_off, const long long* off, const int* cnt,
+                      const int* nbr_j, const int* nbr_gend, const double4* nbr_v, unsigned int* queue,
+                      double* slot_acc, void* slot_scr, int slot_stride, int blocks, double* e3, double* sig3,
+                      cudaStream_t stream)
+{
+    triple_occupancy_of<R, GRAD, PER>();
+    k_triples<R, GRAD, PER><<<blocks, kThreadsAtm, triple_smem<R>(), stream>>>(
+        b, s, d, c, p, w, (const C6Entry<R>*)mat, mat_off, off, cnt, nbr_j, nbr_gend, nbr_v, queue, slot_acc,
+        (Slot<R>*)slot_scr, slot_stride, e3, sig3);
+}
+
 void launch_triples(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
                     const Work& w, const void* mat, const long long* mat_off, const long long* off, const int* cnt,
                     const int* nbr_j, const int* nbr_gend, const double4* nbr_v, unsigned int* queue,
-                    double* slot_acc, void* slot_scr, int slot_stride, int blocks, double* e3, double* sig3,
-                    cudaStream_t stream)
+                    double* slot_acc, void* slot_scr, int slot_stride, int blocks, bool periodic, double* e3,
+                    double* sig3, cudaStream_t stream)
 {
     if (b.natoms <= 0) return;
+#define D3_TRIPLES(R, G, P)                                                                                  \
+    launch_triples_t<R, G, P>(b, s, d, c, p, w, mat, mat_off, off, cnt, nbr_j, nbr_gend, nbr_v, queue, slot_acc, \
+                              slot_scr, slot_stride, blocks, e3, sig3, stream)
     if (c.mixed) {
-        auto* m = (const C6Entry<float>*)mat;
-        auto* sc = (Slot<float>*)slot_scr;
-        if (c.grad)
-            k_triples<float, true><<<blocks, kThreadsAtm, triple_smem<float>(), stream>>>(b, s, d, c, p, w, m, mat_off, off, cnt, nbr_j,
-                nbr_gend, nbr_v, queue, slot_acc, sc, slot_stride, e3, sig3);
-        else
-            k_triples<float, false><<<blocks, kThreadsAtm, triple_smem<float>(), stream>>>(b, s, d, c, p, w, m, mat_off, off, cnt, nbr_j,
-                nbr_gend, nbr_v, queue, slot_acc, sc, slot_stride, e3, sig3);
+        if (c.grad) { if (periodic) D3_TRIPLES(float, true, true); else D3_TRIPLES(float, true, false); }
+        else { if (periodic) D3_TRIPLES(float, false, true); else D3_TRIPLES(float, false, false); }
     } else {
-        auto* m = (const C6Entry<double>*)mat;
-        auto* sc = (Slot<double>*)slot_scr;
-        if (c.grad)
-            k_triples<double, true><<<blocks, kThreadsAtm, triple_smem<double>(), stream>>>(b, s, d, c, p, w, m, mat_off, off, cnt, nbr_j,
-                nbr_gend, nbr_v, queue, slot_acc, sc, slot_stride, e3, sig3);
-        else
-            k_triples<double, false><<<blocks, kThreadsAtm, triple_smem<double>(), stream>>>(b, s, d, c, p, w, m, mat_off, off, cnt,
-                nbr_j, nbr_gend, nbr_v, queue, slot_acc, sc, slot_stride, e3, sig3);
+        if (c.grad) { if (periodic) D3_TRIPLES(double, true, true); else D3_TRIPLES(double, true, false); }
+        else { if (periodic) D3_TRIPLES(double, false, true); else D3_TRIPLES(double, false, false); }
     }
+#undef D3_TRIPLES
 }
 
 }  // namespace d3

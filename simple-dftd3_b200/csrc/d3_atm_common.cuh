@@ -10,9 +10,11 @@ namespace d3 {
 namespace {
 
 // {sqrt(C6_rc), dC6_rc/dCN_r / C6_rc, dC6_rc/dCN_c / C6_rc} of an ordered atom
-// pair (r, c) of a system (get_atomic_c6, model.f90:432-461); ghosts give 0.
+// pair (r, c) of a system (get_atomic_c6, model.f90:432-461), ghosts giving 0,
+// and alp3 log(r0_rc) of the ATM damping radius (atm.f90:744-749; natural log
+// in the FP64 form, base 2 in the mixed form).  One aligned vector load.
 template <class R>
-struct C6Entry { R sc6, qrc, qcr; };
+struct __align__(4 * sizeof(R)) C6Entry { R sc6, qrc, qcr, lr0; };
 
 template <class R>
 __device__ __forceinline__ R rsqrt_r(R x) { if constexpr (sizeof(R) == 8) return rsqrt(x); else return rsqrtf(x); }

@@ -50,8 +50,7 @@ __device__ __forceinline__ void split_pos(double x, R& h, R& l)
 // Pair record of (i, p) from shared positions and the C6 row of i.
 template <class R>
 __device__ __forceinline__ PairRec<R> make_rec(const double* px, const double* py, const double* pz, int ii, int pp,
-                                               bool in, const C6Entry<R>* row_i, const R* slr0_row,
-                                               const Species& sp, int nid, int si, int spp, R alp3, double cut2,
+                                               bool in, const C6Entry<R>* row_i, R alp3, double cut2,
                                                bool smooth_on, R cutoff, R width)
 {
     PairRec<R> r;
@@ -64,14 +63,12 @@ __device__ __forceinline__ PairRec<R> make_rec(const double* px, const double* p
     split_pos<R>(y, hy, ly);
     split_pos<R>(z, hz, lz);
     const double r2s = ok ? r2 : 1.0;
-    const C6Entry<R> e = ok ? row_i[pp] : C6Entry<R>{R(0), R(0), R(0)};
-    double lr0;
-    if (slr0_row) lr0 = (double)slr0_row[spp];
-    else lr0 = (sizeof(R) == 8) ? log(__ldg(sp.atm_r0 + si * nid + spp)) : log2(__ldg(sp.atm_r0 + si * nid + spp));
-    const double lg = (sizeof(R) == 8) ? (double)alp3 * (lr0 - 0.5 * log(r2s)) : (double)alp3 * (lr0 - 0.5 * log2(r2s));
+    const C6Entry<R> e = row_i[pp];
+    // alp3 log(r0_ip / r_ip) with the damping radius term of the C6 entry
+    const double lg = (double)e.lr0 - 0.5 * (double)alp3 * ((sizeof(R) == 8) ? log(r2s) : log2(r2s));
     r.h.x = hx; r.h.y = hy; r.h.z = hz; r.h.w = R(r2s);
     r.l.x = lx; r.l.y = ly; r.l.z = lz; r.l.w = R(1.0 / r2s);
-    r.c.x = e.sc6; r.c.y = e.qrc; r.c.z = e.qcr; r.c.w = R(lg);
+    r.c.x = ok ? e.sc6 : R(0); r.c.y = ok ? e.qrc : R(0); r.c.z = ok ? e.qcr : R(0); r.c.w = R(lg);
     r.s.x = R(rsqrt(r2s)); r.s.y = R(1); r.s.z = R(0); r.s.w = ok ? R(1) : R(0);
     if (smooth_on && ok) {
         R sw, dsw;
@@ -121,7 +118,6 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
     PairRec<R>* recs = reinterpret_cast<PairRec<R>*>(acc + 4 * kMolMax);   // [warps][32]
     int* spc = reinterpret_cast<int*>(recs + kMolWarps * 32);     // [kMolMax] species
     int* loc = spc + kMolMax;                                     // [kMolMax] input index
-    __shared__ R slr0[kMaxSpeciesFast * kMaxSpeciesFast];
     __shared__ double wred[kMolWarps][8];
     __shared__ int s_mol, s_item;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -132,9 +128,6 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
     const R cut2 = R(cut2d);
     const bool smooth_on = c.width3 > 0.0 && c.width3 < c.cut3;
     const R cutoff = R(c.cut3), width = R(c.width3);
-    const bool table_r0 = b.nid <= kMaxSpeciesFast;
-    if (table_r0)
-        for (int k = tid; k < b.nid * b.nid; k += kMolThreads) slr0[k] = rlog<R>(R(__ldg(sp.atm_r0 + k)));
     PairRec<R>* wrec = recs + wid * 32;
 
     for (;;) {
@@ -176,8 +169,6 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
             const int i = lo;
             const int nch = (i + 31) >> 5;
             const int chunk = nch - 1 - (t - (nitems - items_upto(i)));
-            const int si = spc[i];
-            const R* slr0_row = table_r0 ? slr0 + si * b.nid : nullptr;
             const C6Entry<R>* row_i = m0 + (size_t)i * n;
             // root position split (head, tail)
             R rhx, rlx, rhy, rly, rhz, rlz;
@@ -188,12 +179,10 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
             const int j = 32 * chunk + lane;
             const bool jin = j < i;
             const int jj = jin ? j : 0;
-            const PairRec<R> A = make_rec<R>(px, py, pz, i, jj, jin, row_i, slr0_row, sp, b.nid, si, spc[jj],
-                                             alp3, cut2d, smooth_on, cutoff, width);
+            const PairRec<R> A = make_rec<R>(px, py, pz, i, jj, jin, row_i, alp3, cut2d, smooth_on, cutoff, width);
             const bool jvalid = A.s.w != R(0);
             if (!__any_sync(0xffffffffu, jvalid)) continue;
             const int kend = min(i, 32 * chunk + 32) - 1;   // partners k < j <= kend
-            const int sj = spc[jj];
             const int lj = loc[jj];
             const int li = loc[i];
             // j-role and root sums
@@ -204,8 +193,7 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
                 const bool kin = kk < kend;
                 const int kc = kin ? kk : 0;
                 {
-                    const PairRec<R> Bown = make_rec<R>(px, py, pz, i, kc, kin, row_i, slr0_row, sp, b.nid, si,
-                                                        spc[kc], alp3, cut2d, smooth_on, cutoff, width);
+                    const PairRec<R> Bown = make_rec<R>(px, py, pz, i, kc, kin, row_i, alp3, cut2d, smooth_on, cutoff, width);
                     __syncwarp();
                     wrec[lane] = Bown;
                 }
@@ -231,7 +219,7 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
                     if (!__any_sync(0xffffffffu, valid)) continue;
                     // C6 of (k, j): row k, column j (consecutive over the lanes)
                     const C6Entry<R> ekj = m0[(size_t)k * n + jj];
-                    if (GRAD && (A.c.x == R(0) || B.c.x == R(0) || ekj.sc6 == R(0))) valid = false;
+                    // a ghost gives C6 = 0 and with it zero contributions
                     if (valid && part.nparts > 1) {
                         // owner of the triple: the pair of its two largest input indices
                         int o1 = li, o2 = lj, o3 = loc[k], tmp;
@@ -249,11 +237,8 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
                         const R ir2 = ir1 * ir1;
                         const R ir3 = ir2 * ir1;
                         const R ir5 = ir3 * ir2;
-                        const int sk = spc[k];
-                        const R lr0jk = table_r0 ? slr0[sj * b.nid + sk]
-                                                 : rlog<R>(R(__ldg(sp.atm_r0 + sj * b.nid + sk)));
                         // (r0/r1)^alp3 with r0 = r0ij r0ik r0jk, r1 = r_ij r_ik r_jk (atm.f90:744-749)
-                        const R tq = rexp<R>(A.c.w + B.c.w + alp3 * (lr0jk - R(0.5) * rlog<R>(rc)));
+                        const R tq = rexp<R>(A.c.w + B.c.w + ekj.lr0 - R(0.5) * alp3 * rlog<R>(rc));
                         const R fdmp = rcp_r<R>(R(1) + R(6) * tq);
                         const R s1 = ra + rb + rc;
                         const R ang = R(0.375) * (s1 - R(2) * rb) * (s1 - R(2) * rc) * (s1 - R(2) * ra) * ir5 + ir3;

@@ -171,7 +171,7 @@ void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, cons
 
 // Three-body term (d3_atm.cu): C6 table, neighbour lists, triple sum.
 size_t atm_c6_entry_bytes(bool mixed);
-void launch_c6_matrix(const Batch& b, const Species& s, const Work& w, const long long* d_mat_off,
+void launch_c6_matrix(const Batch& b, const Species& s, const Work& w, double alp3, const long long* d_mat_off,
                       void* mat, long long total, bool mixed, cudaStream_t stream);
 // sys_skip[nsys] (or null): systems whose roots get no entries (handled by
 // the molecule kernel)
@@ -192,7 +192,7 @@ void launch_triples(const Batch& b, const Species& s, const Damp& d, const Confi
                     const Work& w, const void* mat, const long long* mat_off, const long long* off,
                     const int* cnt, const int* nbr_j, const int* nbr_gend, const double4* nbr_v,
                     unsigned int* queue, double* slot_acc, void* slot_scr, int slot_stride, int blocks,
-                    double* e3, double* sig3, cudaStream_t stream);
+                    bool periodic, double* e3, double* sig3, cudaStream_t stream);
 // Three-body term of whole molecules, one block per system (d3_atm_mol.cu):
 // the non-periodic systems of at most atm_mol_max_atoms() atoms listed in
 // mol_order (largest first).  Writes e3/sig3 for every atom of those systems.

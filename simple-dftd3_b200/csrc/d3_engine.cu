@@ -291,6 +291,7 @@ Engine::Engine(int nsys, const int* natoms, const int* numbers, const double* la
     auto_split_ = 1;
     for (int sy = 0; sy < nsys; sy++)
         if (per_[3 * sy] || per_[3 * sy + 1] || per_[3 * sy + 2]) auto_split_ = 2;
+    any_periodic_ = auto_split_ == 2;
     d_mol_order_ = dev_alloc<int>(nsys);
     d_sys_mol_ = dev_alloc<uint8_t>(nsys);
     configure_molecules();
@@ -679,7 +680,7 @@ void Engine::run_three_body(const Batch& b, const Species& s, const Damp& d, con
         check(cudaMemsetAsync(d_guard_, 0, sizeof(int), stream), "memset");
         atm_ready_ = true;
     }
-    launch_c6_matrix(b, s, w, d_c6mat_off_, d_c6mat_, c6mat_total_, c.mixed, stream);
+    launch_c6_matrix(b, s, w, (d.alp + 2.0) / 3.0, d_c6mat_off_, d_c6mat_, c6mat_total_, c.mixed, stream);
     if (root_atoms_ > 0) {
         check(cudaMemsetAsync(d_maxcnt_, 0, sizeof(int), stream), "memset");
         check(cudaMemsetAsync(d_cnt_ + n, 0, sizeof(int), stream), "memset");
@@ -731,7 +732,7 @@ void Engine::run_three_body(const Batch& b, const Species& s, const Damp& d, con
         w.atm_guard = d_guard_;
         if (profiling_ && !capturing_) check(cudaEventRecord(kev_[2], stream), "cudaEventRecord");
         launch_triples(b, s, d, c, part_, w, d_c6mat_, d_c6mat_off_, d_off_, d_cnt_, d_nbr_j_, d_nbr_gend_, d_nbr_v_,
-                       d_queue_, d_slot_acc_, d_slot_scr_, stride, blocks, d_e3_, d_sig3_, stream);
+                       d_queue_, d_slot_acc_, d_slot_scr_, stride, blocks, any_periodic_, d_e3_, d_sig3_, stream);
     }
     if (!mol_order_.empty()) {
         // after the root kernel, which writes zeros for the molecules' atoms

@@ -163,6 +163,7 @@ private:
     int* d_mol_order_ = nullptr;
     std::vector<int> sys_natoms_;
     int auto_split_ = 1;                 // pair split of tuning 0
+    bool any_periodic_ = false;          // a system has a periodic direction
     void configure_molecules();          // mol_order_ and root_atoms_ from tune_.atm_mol
     uint8_t* d_sys_mol_ = nullptr;       // [nsys] 1 for those systems
     long long root_atoms_ = 0;           // atoms of the other systems
