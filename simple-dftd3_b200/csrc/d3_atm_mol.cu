@@ -8,8 +8,8 @@
 // to its warps.  A warp's lanes own one row j each; the warp sweeps the
 // partners k < j in blocks of 32, whose (i, k) pair records the lanes build
 // and share through shared memory.  Per triple the row keeps its j-role sums
-// in registers, the k-role sums of the block's 32 partners are reduced over
-// the warp with shuffles, and the root's sums stay in registers.  Per-atom
+// in registers, the k-role sums of the partners are reduced over the warp in
+// groups of four with a reduce-scatter, and the root's sums stay in registers.  Per-atom
 // gradient and dE/dCN accumulate in shared memory (FP64) and are added to the
 // global arrays once per molecule; energy and virial are reduced per block
 // in a fixed order.  No block-wide barrier separates the work items.
@@ -80,21 +80,11 @@ __device__ __forceinline__ PairRec<R> make_rec(const double* px, const double* p
     return r;
 }
 
-__device__ __forceinline__ float wsum32(float v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 __device__ __forceinline__ double wsum64(double v)
 {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
-}
-template <class R> __device__ __forceinline__ R wsum(R v)
-{
-    if constexpr (sizeof(R) == 8) return wsum64(v); else return wsum32(v);
 }
 
 // S(x) = sum_{i=1..x} ceil(i / 32): work items of the roots 1..x.
@@ -201,7 +191,10 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
                 R kS = R(0), kGx = R(0), kGy = R(0), kGz = R(0), kD = R(0);
                 R te = R(0), txx = R(0), tyy = R(0), tzz = R(0), txy = R(0), txz = R(0), tyz = R(0);
                 const int tn = min(32, kend - K0);
-                for (int tt = 0; tt < tn; tt++) {
+                // one candidate (row j, partner K0 + tt): root, row and virial sums
+                // here, the partner's five sums returned in cv
+                auto candidate = [&](int tt, R* cv) {
+                    R& cS = cv[0]; R& cGx = cv[1]; R& cGy = cv[2]; R& cGz = cv[3]; R& cD = cv[4];
                     const int k = K0 + tt;
                     const PairRec<R>& B = wrec[tt];
                     bool valid = jvalid && k < j && B.s.w != R(0);
@@ -216,7 +209,7 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
                     }
                     const R rc = vx * vx + vy * vy + vz * vz;
                     valid = valid && !(rc > cut2 || rc < R(DBL_EPSILON));
-                    if (!__any_sync(0xffffffffu, valid)) continue;
+                    if (!__any_sync(0xffffffffu, valid)) return;
                     // C6 of (k, j): row k, column j (consecutive over the lanes)
                     const C6Entry<R> ekj = m0[(size_t)k * n + jj];
                     // a ghost gives C6 = 0 and with it zero contributions
@@ -228,7 +221,6 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
                         if (o2 > o1) { tmp = o1; o1 = o2; o2 = tmp; }
                         valid = owns_pair_atm(part, o1, o2);
                     }
-                    R cS = R(0), cGx = R(0), cGy = R(0), cGz = R(0), cD = R(0);
                     if (valid) {
                         const R ra = A.h.w, rb = B.h.w;           // r_ij^2, r_ik^2
                         const R rsc = rsqrt_r<R>(rc);
@@ -277,11 +269,48 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
                             txy += gx * vy; txz += gx * vz; tyz += gy * vz;
                         }
                     }
+                };
+                // partners in groups of four; their sums are reduced over the
+                // warp with a reduce-scatter (10 + 5 + 3 x 5 shuffles for the
+                // group) and handed to the partner's own lane
+                for (int tg = 0; tg < tn; tg += 4) {
+                    R kv[4][5];
+#pragma unroll
+                    for (int g = 0; g < 4; g++) {
+#pragma unroll
+                        for (int v = 0; v < 5; v++) kv[g][v] = R(0);
+                        if (tg + g < tn) candidate(tg + g, kv[g]);
+                    }
                     if (GRAD) {
-                        // partner k's share, summed over the warp's rows
-                        cS = wsum<R>(cS); cGx = wsum<R>(cGx); cGy = wsum<R>(cGy); cGz = wsum<R>(cGz);
-                        cD = wsum<R>(cD);
-                        if (lane == tt) { kS += cS; kGx += cGx; kGy += cGy; kGz += cGz; kD += cD; }
+                        const bool up16 = (lane & 16) != 0, up8 = (lane & 8) != 0;
+                        R r2[2][5];
+#pragma unroll
+                        for (int h = 0; h < 2; h++)
+#pragma unroll
+                            for (int v = 0; v < 5; v++) {
+                                const R send = up16 ? kv[h][v] : kv[2 + h][v];
+                                const R keep = up16 ? kv[2 + h][v] : kv[h][v];
+                                r2[h][v] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+                            }
+                        R r1[5];
+#pragma unroll
+                        for (int v = 0; v < 5; v++) {
+                            const R send = up8 ? r2[0][v] : r2[1][v];
+                            const R keep = up8 ? r2[1][v] : r2[0][v];
+                            r1[v] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+                        }
+#pragma unroll
+                        for (int v = 0; v < 5; v++)
+#pragma unroll
+                            for (int o = 4; o > 0; o >>= 1) r1[v] += __shfl_xor_sync(0xffffffffu, r1[v], o);
+                        // lanes 16 b4 + 8 b3 + x now hold partner tg + 2 b4 + b3
+                        const int gl = lane - tg;
+                        const bool mine = gl >= 0 && gl < 4 && lane < tn;
+                        const int src = mine ? 16 * (gl >> 1) + 8 * (gl & 1) : 0;
+                        R got[5];
+#pragma unroll
+                        for (int v = 0; v < 5; v++) got[v] = __shfl_sync(0xffffffffu, r1[v], src);
+                        if (mine) { kS += got[0]; kGx += got[1]; kGy += got[2]; kGz += got[3]; kD += got[4]; }
                     }
                 }
                 e_l += double(te);
