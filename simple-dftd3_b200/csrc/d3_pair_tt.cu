@@ -75,7 +75,7 @@ __device__ __forceinline__ R wsum_tt(R v)
 // (centre difference dc, reach lim) into the warp's lists; returns their count.
 template <class V>
 __device__ __forceinline__ int tt_reach(const double* img, int tc, int nt, double dcx, double dcy, double dcz,
-                                        double lim, int lane, V* sth, V* stl, int* sidx)
+                                        double lim, int lane, V* sth, V* stl)
 {
     int nreach = 0;
 #pragma unroll
@@ -91,7 +91,6 @@ __device__ __forceinline__ int tt_reach(const double* img, int tc, int nt, doubl
         const unsigned m = __ballot_sync(0xffffffffu, ok);
         if (ok) {
             const int pos = nreach + __popc(m & ((1u << lane) - 1u));
-            sidx[pos] = tc + k;
             if constexpr (sizeof(V) == 32) {
                 sth[pos] = make_double4(tx, ty, tz, 0.0);
             } else {
@@ -110,23 +109,35 @@ __device__ __forceinline__ int tt_reach(const double* img, int tc, int nt, doubl
 constexpr int kJMaskWords = kTTChunk / 32;   // translations of an item, in ballot words
 
 // Of the compacted translations [qbeg, qend), those that can bring atom j
-// (position xj) within reach limj of the tile centre c: one bit each.
-__device__ __forceinline__ void tt_jmask(const double* img, const int* sidx, int qbeg, int qend, double4 c,
-                                         double xj, double yj, double zj, double limj, int lane,
-                                         unsigned jm[kJMaskWords])
+// (position xj) within reach limj of the tile centre c: one bit each, in
+// nwords = ceil((qend - qbeg) / 32) ballot words.  The test runs on the
+// staged translations (head + tail, FP32 in the mixed form) with the reach
+// widened by 1e-4 relative, so that it can only keep too many.
+template <class V>
+__device__ __forceinline__ int tt_jmask(const V* sth, const V* stl, int qbeg, int qend, double4 c, double xj,
+                                        double yj, double zj, double limj, int lane, unsigned jm[kJMaskWords])
 {
+    const int nwords = (qend - qbeg + 31) / 32;
+    using T = decltype(sth[0].x);
+    const T ex0 = T(c.x - xj), ey0 = T(c.y - yj), ez0 = T(c.z - zj);
+    const T lim2 = T(limj * limj * (1.0 + 2.0e-4));
 #pragma unroll
     for (int h = 0; h < kJMaskWords; h++) {
+        if (h >= nwords) { jm[h] = 0u; continue; }
         const int q = qbeg + 32 * h + lane;
         bool ok = false;
         if (q < qend) {
-            const int tix = sidx[q];
-            const double ex = c.x - xj - __ldg(img + 3 * tix), ey = c.y - yj - __ldg(img + 3 * tix + 1),
-                         ez = c.z - zj - __ldg(img + 3 * tix + 2);
-            ok = ex * ex + ey * ey + ez * ez <= limj * limj;
+            const V th = sth[q];
+            T ex = ex0 - th.x, ey = ey0 - th.y, ez = ez0 - th.z;
+            if constexpr (sizeof(T) == 4) {
+                const V tl = stl[q];
+                ex -= tl.x; ey -= tl.y; ez -= tl.z;
+            }
+            ok = ex * ex + ey * ey + ez * ez <= lim2;
         }
         jm[h] = __ballot_sync(0xffffffffu, ok);
     }
+    return nwords;
 }
 
 // Species vectors U[a][s][r] and dU[a][s][r] of every atom (sorted order).
@@ -160,7 +171,6 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     using V = typename T4<R>::type;
     __shared__ V sth[kTTWarps][kTTChunk];
     __shared__ V stl[kTTWarps][kTTChunk];
-    __shared__ int sidx[kTTWarps][kTTChunk];     // image index of each compacted translation
     // FP64 sums of the lanes, [value][lane]: i sums and j sums
     __shared__ double sacc[kTTWarps][kUnitI + kUnitJ][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -237,7 +247,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     for (int tc = tt0; tc < tt1; tc += kTTChunk) {
         const int nt = min(kTTChunk, tt1 - tc);
         // translations that can join the two tiles
-        const int nreach = tt_reach<V>(b.img, tc, nt, dcx, dcy, dcz, lim, lane, sth[wid], stl[wid], sidx[wid]);
+        const int nreach = tt_reach<V>(b.img, tc, nt, dcx, dcy, dcz, lim, lane, sth[wid], stl[wid]);
         if (nreach == 0) continue;
         // this item's half of the reachable translations
         const int qhalf = (nreach + splitT - 1) / splitT;
@@ -282,7 +292,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
             R jde = R(0), jgx = R(0), jgy = R(0), jgz = R(0);
             // translations of this half that can bring j within the cutoff of tile it
             unsigned jm[kJMaskWords];
-            tt_jmask(b.img, sidx[wid], qbeg, qend, ci, xj, yj, zj, limj, lane, jm);
+            tt_jmask<V>(sth[wid], stl[wid], qbeg, qend, ci, xj, yj, zj, limj, lane, jm);
 #pragma unroll
             for (int h = 0; h < kJMaskWords; h++)
             for (unsigned mm = jm[h]; mm; mm &= mm - 1) {
@@ -461,7 +471,6 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
     using V = typename T4<R>::type;
     __shared__ V sth[kTTWarps][kTTChunk];
     __shared__ V stl[kTTWarps][kTTChunk];
-    __shared__ int sidx[kTTWarps][kTTChunk];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int item = blockIdx.x * kTTWarps + wid;
     if (item >= nunits * split) return;
@@ -511,7 +520,7 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
     };
     for (int tc = tt0; tc < tt1; tc += kTTChunk) {
         const int nt = min(kTTChunk, tt1 - tc);
-        const int nreach = tt_reach<V>(b.img, tc, nt, dcx, dcy, dcz, lim, lane, sth[wid], stl[wid], sidx[wid]);
+        const int nreach = tt_reach<V>(b.img, tc, nt, dcx, dcy, dcz, lim, lane, sth[wid], stl[wid]);
         if (nreach == 0) continue;
         const int qhalf = (nreach + splitT - 1) / splitT;
         const int qbeg = th * qhalf, qend = min(nreach, qbeg + qhalf);
@@ -537,7 +546,7 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
             const R dsig = CHAIN ? (self ? R(dei) : dsum) : R(0);
             R j0 = R(0), j1 = R(0), j2 = R(0);
             unsigned jm[kJMaskWords];
-            tt_jmask(b.img, sidx[wid], qbeg, qend, ci, xj, yj, zj, limj, lane, jm);
+            tt_jmask<V>(sth[wid], stl[wid], qbeg, qend, ci, xj, yj, zj, limj, lane, jm);
 #pragma unroll
             for (int h = 0; h < kJMaskWords; h++)
             for (unsigned mm = jm[h]; mm; mm &= mm - 1) {
