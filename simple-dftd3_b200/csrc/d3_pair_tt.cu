@@ -289,87 +289,96 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
             const R q1 = R(__ldg(pr + 1)), q2 = R(__ldg(pr + 2)), q3 = R(__ldg(pr + 3)), q4 = R(__ldg(pr + 4));
             // both halves of a pair go to i; a self pair (j = i, T != 0) is one half
             const R we = self ? R(0.5) : R(1);
-            R jde = R(0), jgx = R(0), jgy = R(0), jgz = R(0);
+            // sums over the translations of this (i, j); C6 and its derivatives,
+            // which do not depend on T, multiply them afterwards
+            R se = R(0), se6 = R(0), se8 = R(0), spa = R(0), spb = R(0);
+            R sgx = R(0), sgy = R(0), sgz = R(0);
+            R sxx = R(0), syy = R(0), szz = R(0), sxy = R(0), sxz = R(0), syz = R(0);
+            const R s8rr = s8 * rrij;
             // translations of this half that can bring j within the cutoff of tile it
             unsigned jm[kJMaskWords];
-            tt_jmask<V>(sth[wid], stl[wid], qbeg, qend, ci, xj, yj, zj, limj, lane, jm);
+            const int nw = tt_jmask<V>(sth[wid], stl[wid], qbeg, qend, ci, xj, yj, zj, limj, lane, jm);
 #pragma unroll
-            for (int h = 0; h < kJMaskWords; h++)
-            for (unsigned mm = jm[h]; mm; mm &= mm - 1) {
-                const int q = qbeg + 32 * h + __ffs(mm) - 1;
-                const V th = sth[wid][q];
-                R vx, vy, vz;
-                if constexpr (sizeof(R) == 8) { vx = dhx - th.x; vy = dhy - th.y; vz = dhz - th.z; }
-                else {
-                    const V tl = stl[wid][q];
-                    vx = (dhx - th.x) + (dlx - tl.x);
-                    vy = (dhy - th.y) + (dly - tl.y);
-                    vz = (dhz - th.z) + (dlz - tl.z);
-                }
-                const R r2 = vx * vx + vy * vy + vz * vz;
-                if (!valid || r2 > cut2 || r2 < R(DBL_EPSILON)) continue;
-                nterm++;
-                R sw = R(1), dswdr = R(0), r1 = R(0);
-                if (smooth_on) { r1 = tt_sqrt<R>(r2); tt_smooth<R>(r1, cutoff, width, sw, dswdr); }
-                R edisp0, gdisp0, e6, e8, dpa = R(0), dpb = R(0);
-                if constexpr (DAMP == kRational) {
-                    // rational.f90:462-497: q1 = R0^6, q2 = R0^8, q3 = R0, q4 = sqrt(rrij)
-                    const R r4 = r2 * r2;
-                    const R a6 = r4 * r2 + q1, a8 = r4 * r4 + q2;
-                    const R inv = tt_rcp<R>(a6 * a8);
-                    const R t6 = a8 * inv;
-                    const R t8 = a6 * inv;
-                    const R d6 = R(-6) * r4 * t6 * t6;
-                    const R d8 = R(-8) * r4 * r2 * t8 * t8;
-                    e6 = t6; e8 = rrij * t8;
-                    edisp0 = s6 * t6 + s8 * rrij * t8;
-                    gdisp0 = s6 * d6 + s8 * rrij * d8;
-                    if (PG) {
-                        const R dedr0 = s6 * R(-6) * (q1 / q3) * t6 * t6 + s8 * rrij * R(-8) * (q2 / q3) * t8 * t8;
-                        dpa = dedr0 * q4;
-                        dpb = dedr0;
+            for (int h = 0; h < kJMaskWords; h++) {
+                if (h >= nw) break;
+                for (unsigned mm = jm[h]; mm; mm &= mm - 1) {
+                    const int q = qbeg + 32 * h + __ffs(mm) - 1;
+                    const V th = sth[wid][q];
+                    R vx, vy, vz;
+                    if constexpr (sizeof(R) == 8) { vx = dhx - th.x; vy = dhy - th.y; vz = dhz - th.z; }
+                    else {
+                        const V tl = stl[wid][q];
+                        vx = (dhx - th.x) + (dlx - tl.x);
+                        vy = (dhy - th.y) + (dly - tl.y);
+                        vz = (dhz - th.z) + (dlz - tl.z);
                     }
-                } else {
-                    // zero.f90:490-536: q1 = rs6 R0, q2 = rs8 R0
-                    if (!smooth_on) r1 = tt_sqrt<R>(r2);
-                    const R r6 = r2 * r2 * r2;
-                    const R r8 = r6 * r2;
-                    const R t6 = tt_pow<R>(q1 / r1, alp6);
-                    const R t8 = tt_pow<R>(q2 / r1, alp8);
-                    const R f6 = R(1) / (R(1) + R(6) * t6);
-                    const R f8 = R(1) / (R(1) + R(6) * t8);
-                    const R d6 = R(-6) * f6 / r2 + R(6) * alp6 * t6 * (f6 * f6) / r2;
-                    const R d8 = R(-8) * f8 / r2 + R(6) * alp8 * t8 * (f8 * f8) / r2;
-                    e6 = f6 / r6; e8 = rrij * f8 / r8;
-                    edisp0 = s6 * f6 / r6 + s8 * rrij * f8 / r8;
-                    gdisp0 = s6 * d6 / r6 + s8 * rrij * d8 / r8;
-                    if (PG) {
-                        dpa = d.rs6 != 0.0 ? s6 / r6 * R(-6) * f6 * f6 * alp6 * t6 / R(d.rs6) : R(0);
-                        dpb = d.rs8 != 0.0 ? s8 * rrij / r8 * R(-6) * f8 * f8 * alp8 * t8 / R(d.rs8) : R(0);
+                    const R r2 = vx * vx + vy * vy + vz * vz;
+                    if (!valid || r2 > cut2 || r2 < R(DBL_EPSILON)) continue;
+                    nterm++;
+                    R sw = R(1), dswdr = R(0), r1 = R(0);
+                    if (smooth_on) { r1 = tt_sqrt<R>(r2); tt_smooth<R>(r1, cutoff, width, sw, dswdr); }
+                    R edisp0, gdisp0, e6, e8, dpa = R(0), dpb = R(0);
+                    if constexpr (DAMP == kRational) {
+                        // rational.f90:462-497: q1 = R0^6, q2 = R0^8, q3 = R0, q4 = sqrt(rrij)
+                        const R r4 = r2 * r2;
+                        const R a6 = r4 * r2 + q1, a8 = r4 * r4 + q2;
+                        const R inv = tt_rcp<R>(a6 * a8);
+                        const R t6 = a8 * inv;
+                        const R t8 = a6 * inv;
+                        e6 = t6; e8 = rrij * t8;
+                        edisp0 = s6 * t6 + s8rr * t8;
+                        // s6 d6 + s8 rrij d8 with d6 = -6 r^4 t6^2, d8 = -8 r^6 t8^2
+                        gdisp0 = r4 * (R(-6) * s6 * t6 * t6 + R(-8) * s8rr * r2 * t8 * t8);
+                        if (PG) {
+                            const R dedr0 = s6 * R(-6) * (q1 / q3) * t6 * t6 + s8rr * R(-8) * (q2 / q3) * t8 * t8;
+                            dpa = dedr0 * q4;
+                            dpb = dedr0;
+                        }
+                    } else {
+                        // zero.f90:490-536: q1 = rs6 R0, q2 = rs8 R0
+                        if (!smooth_on) r1 = tt_sqrt<R>(r2);
+                        const R r6 = r2 * r2 * r2;
+                        const R r8 = r6 * r2;
+                        const R t6 = tt_pow<R>(q1 / r1, alp6);
+                        const R t8 = tt_pow<R>(q2 / r1, alp8);
+                        const R f6 = R(1) / (R(1) + R(6) * t6);
+                        const R f8 = R(1) / (R(1) + R(6) * t8);
+                        const R d6 = R(-6) * f6 / r2 + R(6) * alp6 * t6 * (f6 * f6) / r2;
+                        const R d8 = R(-8) * f8 / r2 + R(6) * alp8 * t8 * (f8 * f8) / r2;
+                        e6 = f6 / r6; e8 = rrij * f8 / r8;
+                        edisp0 = s6 * f6 / r6 + s8 * rrij * f8 / r8;
+                        gdisp0 = s6 * d6 / r6 + s8 * rrij * d8 / r8;
+                        if (PG) {
+                            dpa = d.rs6 != 0.0 ? s6 / r6 * R(-6) * f6 * f6 * alp6 * t6 / R(d.rs6) : R(0);
+                            dpb = d.rs8 != 0.0 ? s8 * rrij / r8 * R(-6) * f8 * f8 * alp8 * t8 / R(d.rs8) : R(0);
+                        }
+                    }
+                    se += sw * edisp0;
+                    if (PG) { se6 += sw * e6; se8 += sw * e8; spa += sw * dpa; spb += sw * dpb; }
+                    if (GRAD) {
+                        R gdisp = sw * gdisp0;
+                        if (smooth_on) gdisp += dswdr * edisp0 / r1;
+                        const R gx = gdisp * vx, gy = gdisp * vy, gz = gdisp * vz;
+                        sgx += gx; sgy += gy; sgz += gz;
+                        sxx += gx * vx; syy += gy * vy; szz += gz * vz;
+                        sxy += gx * vy; sxz += gx * vz; syz += gy * vz;
                     }
                 }
-                const R edisp = sw * edisp0;
-                te -= c6 * edisp * we;
-                tde -= dc6i * edisp;
-                if (!self) jde -= dc6j * edisp;
-                if (PG) {
-                    const R hc = -c6 * sw * we;
-                    tp0 += hc * e6; tp1 += hc * e8;
-                    tp2 += hc * dpa; tp3 += hc * dpb;
+            }
+            // E_pair = -1/2 C6 edisp per half, dE/dCN = -dC6/dCN edisp, gradient -C6 gdisp v
+            // (rational.f90:488-497); i takes both halves of E, sigma and dE/dparam
+            const R c6w = c6 * we;
+            te -= c6w * se;
+            tde -= dc6i * se;
+            R jde = self ? R(0) : -dc6j * se, jgx = R(0), jgy = R(0), jgz = R(0);
+            if (PG) { tp0 -= c6w * se6; tp1 -= c6w * se8; tp2 -= c6w * spa; tp3 -= c6w * spb; }
+            if (GRAD) {
+                if (!self) {
+                    tgx -= c6 * sgx; tgy -= c6 * sgy; tgz -= c6 * sgz;
+                    jgx = c6 * sgx; jgy = c6 * sgy; jgz = c6 * sgz;
                 }
-                if (GRAD) {
-                    R gdisp = sw * gdisp0;
-                    if (smooth_on) gdisp += dswdr * edisp0 / r1;
-                    const R f = -c6 * gdisp;
-                    const R dgx = f * vx, dgy = f * vy, dgz = f * vz;
-                    if (!self) {
-                        tgx += dgx; tgy += dgy; tgz += dgz;
-                        jgx -= dgx; jgy -= dgy; jgz -= dgz;
-                    }
-                    const R fx = we * dgx, fy = we * dgy, fz = we * dgz;
-                    txx += fx * vx; tyy += fy * vy; tzz += fz * vz;
-                    txy += fx * vy; txz += fx * vz; tyz += fy * vz;
-                }
+                txx -= c6w * sxx; tyy -= c6w * syy; tzz -= c6w * szz;
+                txy -= c6w * sxy; txz -= c6w * sxz; tyz -= c6w * syz;
             }
             // j's share, summed over the warp's atoms i
             jde = wsum_tt<R>(jde);
@@ -545,51 +554,64 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
             const R dsum = CHAIN ? R(dei + w.dEdcn[j]) : R(0);
             const R dsig = CHAIN ? (self ? R(dei) : dsum) : R(0);
             R j0 = R(0), j1 = R(0), j2 = R(0);
+            // sums over the translations of this (i, j); the pair weights
+            // dE/dCN_i + dE/dCN_j do not depend on T and multiply them afterwards
+            R sc = R(0), scx = R(0), scy = R(0), scz = R(0);
+            R sxx = R(0), syy = R(0), szz = R(0), sxy = R(0), sxz = R(0), syz = R(0);
             unsigned jm[kJMaskWords];
-            tt_jmask<V>(sth[wid], stl[wid], qbeg, qend, ci, xj, yj, zj, limj, lane, jm);
+            const int nw = tt_jmask<V>(sth[wid], stl[wid], qbeg, qend, ci, xj, yj, zj, limj, lane, jm);
 #pragma unroll
-            for (int h = 0; h < kJMaskWords; h++)
-            for (unsigned mm = jm[h]; mm; mm &= mm - 1) {
-                const int q = qbeg + 32 * h + __ffs(mm) - 1;
-                const V thv = sth[wid][q];
-                R vx, vy, vz;
-                if constexpr (sizeof(R) == 8) { vx = dhx - thv.x; vy = dhy - thv.y; vz = dhz - thv.z; }
-                else {
-                    const V tl = stl[wid][q];
-                    vx = (dhx - thv.x) + (dlx - tl.x);
-                    vy = (dhy - thv.y) + (dly - tl.y);
-                    vz = (dhz - thv.z) + (dlz - tl.z);
-                }
-                const R r2 = vx * vx + vy * vy + vz * vz;
-                if (!valid || r2 > cut2 || r2 < R(1.0e-12)) continue;
-                nterm++;
-                if (!CHAIN) {
-                    R cf;
-                    if constexpr (sizeof(R) == 8) cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / sqrt(r2) - R(1))));
-                    else cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * rsqrtf(r2) - R(1))));
-                    t0_ += cf;
-                    if (!self) j0 += cf;
-                } else {
-                    R f;
-                    if constexpr (sizeof(R) == 8) {
-                        // ncoord.f90:198-206
-                        const R r1 = sqrt(r2);
-                        const R cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / r1 - R(1))));
-                        const R dcf = -cf * (R(1) - cf) * R(kKcnTT) * rc / r2;
-                        f = dcf / r1;
+            for (int h = 0; h < kJMaskWords; h++) {
+                if (h >= nw) break;
+                for (unsigned mm = jm[h]; mm; mm &= mm - 1) {
+                    const int q = qbeg + 32 * h + __ffs(mm) - 1;
+                    const V thv = sth[wid][q];
+                    R vx, vy, vz;
+                    if constexpr (sizeof(R) == 8) { vx = dhx - thv.x; vy = dhy - thv.y; vz = dhz - thv.z; }
+                    else {
+                        const V tl = stl[wid][q];
+                        vx = (dhx - thv.x) + (dlx - tl.x);
+                        vy = (dhy - thv.y) + (dly - tl.y);
+                        vz = (dhz - thv.z) + (dlz - tl.z);
+                    }
+                    const R r2 = vx * vx + vy * vy + vz * vz;
+                    if (!valid || r2 > cut2 || r2 < R(1.0e-12)) continue;
+                    nterm++;
+                    if (!CHAIN) {
+                        R cf;
+                        if constexpr (sizeof(R) == 8) cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / sqrt(r2) - R(1))));
+                        else cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * rsqrtf(r2) - R(1))));
+                        sc += cf;
                     } else {
-                        const R ir = rsqrtf(r2);
-                        const R cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * ir - R(1))));
-                        f = -cf * (R(1) - cf) * R(kKcnTT) * rc * (ir * ir * ir);
+                        R f;
+                        if constexpr (sizeof(R) == 8) {
+                            // ncoord.f90:198-206
+                            const R r1 = sqrt(r2);
+                            const R cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / r1 - R(1))));
+                            const R dcf = -cf * (R(1) - cf) * R(kKcnTT) * rc / r2;
+                            f = dcf / r1;
+                        } else {
+                            const R ir = rsqrtf(r2);
+                            const R cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * ir - R(1))));
+                            f = -cf * (R(1) - cf) * R(kKcnTT) * rc * (ir * ir * ir);
+                        }
+                        const R cx = f * vx, cy = f * vy, cz = f * vz;   // countd
+                        scx += cx; scy += cy; scz += cz;
+                        sxx += cx * vx; syy += cy * vy; szz += cz * vz;
+                        sxy += cx * vy; sxz += cx * vz; syz += cy * vz;
                     }
-                    const R cx = f * vx, cy = f * vy, cz = f * vz;   // countd
-                    if (!self) {
-                        t1_ += cx * dsum; t2_ += cy * dsum; t3_ += cz * dsum;
-                        j0 -= cx * dsum; j1 -= cy * dsum; j2 -= cz * dsum;
-                    }
-                    t4_ += cx * vx * dsig; t5_ += cy * vy * dsig; t6_ += cz * vz * dsig;
-                    t7_ += cx * vy * dsig; t8_ += cx * vz * dsig; t0_ += cy * vz * dsig;
                 }
+            }
+            if (!CHAIN) {
+                t0_ += sc;
+                if (!self) j0 = sc;
+            } else {
+                if (!self) {
+                    t1_ += scx * dsum; t2_ += scy * dsum; t3_ += scz * dsum;
+                    j0 = -scx * dsum; j1 = -scy * dsum; j2 = -scz * dsum;
+                }
+                t4_ += sxx * dsig; t5_ += syy * dsig; t6_ += szz * dsig;
+                t7_ += sxy * dsig; t8_ += sxz * dsig; t0_ += syz * dsig;
             }
             j0 = wsum_tt<R>(j0);
             if (CHAIN) { j1 = wsum_tt<R>(j1); j2 = wsum_tt<R>(j2); }
