@@ -343,7 +343,9 @@ def run_ours(args, rank, world, dist):
     sampler.start()
     res = {p: run.time(p, args.steps, args.warmup, flush, dist) for p in precs}
     extra = {}
-    if not args.no_extra and args.workload == "cell2000" and not shard:
+    # the three-body workloads are reported at N = 1 (with N > 1 every rank would
+    # repeat minutes of single-GPU work that the scaling run does not need)
+    if not args.no_extra and args.workload == "cell2000" and not shard and world == 1:
         for name, steps in (("cluster5000", 3), ("batch4096", 3), ("frames256", 1)):
             nsys = 16 if name == "frames256" else None
             sy, pr = make_workload(name, seed=rank, nsys=nsys)
