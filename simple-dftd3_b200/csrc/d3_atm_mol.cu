@@ -64,12 +64,22 @@ __device__ __forceinline__ PairRec<R> make_rec(const double* px, const double* p
     split_pos<R>(z, hz, lz);
     const double r2s = ok ? r2 : 1.0;
     const C6Entry<R> e = row_i[pp];
-    // alp3 log(r0_ip / r_ip) with the damping radius term of the C6 entry
-    const double lg = (double)e.lr0 - 0.5 * (double)alp3 * ((sizeof(R) == 8) ? log(r2s) : log2(r2s));
     r.h.x = hx; r.h.y = hy; r.h.z = hz; r.h.w = R(r2s);
-    r.l.x = lx; r.l.y = ly; r.l.z = lz; r.l.w = R(1.0 / r2s);
-    r.c.x = ok ? e.sc6 : R(0); r.c.y = ok ? e.qrc : R(0); r.c.z = ok ? e.qcr : R(0); r.c.w = R(lg);
-    r.s.x = R(rsqrt(r2s)); r.s.y = R(1); r.s.z = R(0); r.s.w = ok ? R(1) : R(0);
+    r.l.x = lx; r.l.y = ly; r.l.z = lz;
+    r.c.x = ok ? e.sc6 : R(0); r.c.y = ok ? e.qrc : R(0); r.c.z = ok ? e.qcr : R(0);
+    r.s.y = R(1); r.s.z = R(0); r.s.w = ok ? R(1) : R(0);
+    // alp3 log(r0_ip / r_ip) with the damping radius term of the C6 entry,
+    // 1 / r^2 and 1 / r: FP64, or FP32 from the FP64 distance in the mixed form
+    if constexpr (sizeof(R) == 8) {
+        r.c.w = e.lr0 - 0.5 * (double)alp3 * log(r2s);
+        r.l.w = 1.0 / r2s;
+        r.s.x = rsqrt(r2s);
+    } else {
+        const float r2f = (float)r2s;
+        r.c.w = e.lr0 - 0.5f * alp3 * __log2f(r2f);
+        r.l.w = 1.0f / r2f;
+        r.s.x = rsqrtf(r2f);
+    }
     if (smooth_on && ok) {
         R sw, dsw;
         const R rr = R(sqrt(r2s));
