@@ -495,8 +495,14 @@ static void dispersion2(const model_t *m, const oracle_param *p, int nat, const 
                         const double *c6, const double *dc6dcn, double *energy,
                         double *dEdcn, double *gradient, double *sigma, int part, int nparts)
 {
-    /* rational.f90:220-514 and zero.f90:306-553; derivatives when dEdcn != NULL */
-    if (fabs(p->s6) < EPS && fabs(p->s8) < EPS) return;
+    /* rational.f90:220-514, zero.f90:306-553, mzero.f90:196-553,
+     * optimizedpower.f90:179-483, cso.f90:177-476 and z.f90:176-466;
+     * derivatives when dEdcn != NULL */
+    if (p->damping == ORACLE_CSO) {
+        if (fabs(p->s6) < EPS && fabs(p->a1) < EPS) return;      /* cso.f90:223 */
+    } else if (fabs(p->s6) < EPS && fabs(p->s8) < EPS) {
+        return;
+    }
     double cutoff2 = cutoff * cutoff;
     int grad = dEdcn != NULL;
     double alp6 = p->alp, alp8 = p->alp + 2.0;
@@ -515,15 +521,48 @@ static void dispersion2(const model_t *m, const oracle_param *p, int nat, const 
                 double rrij = 3 * m->r4r2[izp] * m->r4r2[jzp];
                 double c6ij = c6[(size_t)j * nat + i];
                 double r0ij = 0, r0ij6 = 0, r0ij8 = 0, rs6r0 = 0, rs8r0 = 0;
-                if (p->damping == ORACLE_RATIONAL) {
+                double irs6r0 = 0, irs8r0 = 0, betr0 = 0, betr02rs6 = 0, betr02rs8 = 0;
+                double abr0ij6 = 0, abr0ij8 = 0, d6_6 = 0, a2r0ij = 0, zr0c6 = 0;
+                switch (p->damping) {
+                case ORACLE_RATIONAL: {
                     r0ij = p->a1 * sqrt(rrij) + p->a2;
                     double r0ij2 = r0ij * r0ij;
                     r0ij6 = r0ij2 * r0ij2 * r0ij2;
                     r0ij8 = r0ij6 * r0ij2;
-                } else {
+                    break;
+                }
+                case ORACLE_ZERO:
                     r0ij = m->rvdw[jzp * m->nid + izp];
                     rs6r0 = p->rs6 * r0ij;
                     rs8r0 = p->rs8 * r0ij;
+                    break;
+                case ORACLE_MZERO:            /* mzero.f90:441-447 */
+                    r0ij = m->rvdw[jzp * m->nid + izp];
+                    irs6r0 = 1.0 / (p->rs6 * r0ij);
+                    irs8r0 = 1.0 / (p->rs8 * r0ij);
+                    betr0 = p->bet * r0ij;
+                    betr02rs6 = p->rs6 * p->bet * r0ij * r0ij;
+                    betr02rs8 = p->rs8 * p->bet * r0ij * r0ij;
+                    break;
+                case ORACLE_OPTIMIZEDPOWER: { /* optimizedpower.f90:421-429 */
+                    r0ij = p->a1 * sqrt(rrij) + p->a2;
+                    double r0ij2 = r0ij * r0ij;
+                    r0ij6 = r0ij2 * r0ij2 * r0ij2;
+                    r0ij8 = r0ij6 * r0ij2;
+                    double ab = pow(r0ij, p->bet);
+                    abr0ij6 = ab * r0ij6;
+                    abr0ij8 = ab * r0ij8;
+                    break;
+                }
+                case ORACLE_CSO:              /* cso.f90:421-426, a3 = rs6, a4 = rs8 */
+                    r0ij = sqrt(rrij);
+                    d6_6 = pow(p->rs6 * r0ij + p->rs8, 6);
+                    a2r0ij = p->a2 * r0ij;
+                    break;
+                default:                      /* Z, z.f90:412-414: species indices from 1 */
+                    r0ij = p->a1 / (double)((izp + 1) + (jzp + 1));
+                    zr0c6 = r0ij * c6ij;
+                    break;
                 }
                 for (int t = 0; t < ntr; t++) {
                     double v[3];
@@ -535,7 +574,11 @@ static void dispersion2(const model_t *m, const oracle_param *p, int nat, const 
                     double sw, dswdr;
                     smooth_cutoff(r1, cutoff, width, &sw, &dswdr);
                     double edisp0, gdisp0;
-                    if (p->damping == ORACLE_RATIONAL) {
+                    /* dE/dC6 of the pair is -sw * cdisp0 for every family; only
+                     * Z damping has cdisp0 != edisp0 (z.f90:431) */
+                    double cdisp0 = 0.0;
+                    switch (p->damping) {
+                    case ORACLE_RATIONAL: {
                         double r4 = r2 * r2;
                         double t6 = 1.0 / (r4 * r2 + r0ij6);
                         double t8 = 1.0 / (r4 * r4 + r0ij8);
@@ -543,7 +586,9 @@ static void dispersion2(const model_t *m, const oracle_param *p, int nat, const 
                         double d8 = -8 * r4 * r2 * t8 * t8;
                         edisp0 = p->s6 * t6 + p->s8 * rrij * t8;
                         gdisp0 = p->s6 * d6 + p->s8 * rrij * d8;
-                    } else {
+                        break;
+                    }
+                    case ORACLE_ZERO: {
                         double r6 = r2 * r2 * r2;
                         double r8 = r6 * r2;
                         double t6 = pow(rs6r0 / r1, alp6);
@@ -554,7 +599,57 @@ static void dispersion2(const model_t *m, const oracle_param *p, int nat, const 
                         double d8 = -8.0 * f8 / r2 + 6.0 * alp8 * t8 * (f8 * f8) / r2;
                         edisp0 = p->s6 * f6 / r6 + p->s8 * rrij * f8 / r8;
                         gdisp0 = p->s6 * d6 / r6 + p->s8 * rrij * d8 / r8;
+                        break;
                     }
+                    case ORACLE_MZERO: {      /* mzero.f90:456-472 */
+                        double r6 = r2 * r2 * r2;
+                        double r8 = r6 * r2;
+                        double t6 = pow(r1 * irs6r0 + betr0, -alp6);
+                        double t8 = pow(r1 * irs8r0 + betr0, -alp8);
+                        double f6 = 1.0 / (1.0 + 6.0 * t6);
+                        double f8 = 1.0 / (1.0 + 6.0 * t8);
+                        double d6 = -6.0 * f6 / r2 + 6.0 * alp6 * t6 * (f6 * f6) / (r2 + betr02rs6 * r1);
+                        double d8 = -8.0 * f8 / r2 + 6.0 * alp8 * t8 * (f8 * f8) / (r2 + betr02rs8 * r1);
+                        edisp0 = p->s6 * f6 / r6 + p->s8 * rrij * f8 / r8;
+                        gdisp0 = p->s6 * d6 / r6 + p->s8 * rrij * d8 / r8;
+                        break;
+                    }
+                    case ORACLE_OPTIMIZEDPOWER: { /* optimizedpower.f90:438-448 */
+                        double rb = pow(r2, p->bet * 0.5);
+                        double r4 = r2 * r2;
+                        double t6 = rb / (rb * r4 * r2 + abr0ij6);
+                        double t8 = rb / (rb * r4 * r4 + abr0ij8);
+                        double d6 = -6 * r4 * t6 * t6 + p->bet * abr0ij6 * t6 * t6 / (rb * r2);
+                        double d8 = -8 * r4 * r2 * t8 * t8 + p->bet * abr0ij8 * t8 * t8 / (rb * r2);
+                        edisp0 = p->s6 * t6 + p->s8 * rrij * t8;
+                        gdisp0 = p->s6 * d6 + p->s8 * rrij * d8;
+                        break;
+                    }
+                    case ORACLE_CSO: {        /* cso.f90:434-446 */
+                        double ef = exp(r1 - a2r0ij);
+                        double sf = 1.0 / (1.0 + ef);
+                        double sig = p->s6 + p->a1 * sf;
+                        double r4 = r2 * r2;
+                        double t6 = 1.0 / (r4 * r2 + d6_6);
+                        double dsig = -p->a1 * sf * (1.0 - sf) / r1;
+                        double dt6 = -6 * r4 * t6 * t6;
+                        edisp0 = sig * t6;
+                        gdisp0 = dsig * t6 + sig * dt6;
+                        break;
+                    }
+                    default: {                /* Z, z.f90:421-431 */
+                        double r4 = r2 * r2;
+                        double t6 = 1.0 / (r4 * r2 + zr0c6);
+                        double t8 = 1.0 / (r4 * r4 + zr0c6 * rrij);
+                        double d6 = -6 * r4 * t6 * t6;
+                        double d8 = -8 * r4 * r2 * t8 * t8;
+                        edisp0 = p->s6 * t6 + p->s8 * rrij * t8;
+                        gdisp0 = p->s6 * d6 + p->s8 * rrij * d8;
+                        cdisp0 = p->s6 * r4 * r2 * t6 * t6 + p->s8 * rrij * r4 * r4 * t8 * t8;
+                        break;
+                    }
+                    }
+                    if (p->damping != ORACLE_Z) cdisp0 = edisp0;
                     double edisp = sw * edisp0;
                     double dE = -c6ij * edisp * 0.5;
                     el[i] += dE;
@@ -566,10 +661,11 @@ static void dispersion2(const model_t *m, const oracle_param *p, int nat, const 
                     double dS[9];
                     for (int a = 0; a < 3; a++)
                         for (int b = 0; b < 3; b++) dS[a + 3 * b] = dG[a] * v[b] * 0.5;
-                    dl[i] -= dc6dcn[(size_t)i * nat + j] * edisp;
+                    double cdisp = sw * cdisp0;
+                    dl[i] -= dc6dcn[(size_t)i * nat + j] * cdisp;
                     for (int k = 0; k < 9; k++) sl[k] += dS[k];
                     if (i != j) {
-                        dl[j] -= dc6dcn[(size_t)j * nat + i] * edisp;
+                        dl[j] -= dc6dcn[(size_t)j * nat + i] * cdisp;
                         for (int c = 0; c < 3; c++) {
                             gl[3 * i + c] += dG[c];
                             gl[3 * j + c] -= dG[c];
@@ -748,6 +844,7 @@ static int pipeline(int nat, const int *numbers, const double *xyz, const double
      * summed over the parts before use (disp.f90:120-126,166-171), and the
      * atom-resolved energies, gradient and virial afterwards
      * (get_dispersion_mpi_atomic, mpi.f90). */
+    if (param->damping < ORACLE_RATIONAL || param->damping > ORACLE_Z) return 4;
     model_t m;
     if (model_new(&m, nat, numbers, ghost)) return 1;
     double zero[9] = {0};

@@ -13,14 +13,19 @@
 extern "C" {
 #endif
 
-enum { ORACLE_RATIONAL = 0, ORACLE_ZERO = 1 };
+/* damping families: rational (also the modified rational records), zero,
+ * modified zero, optimized power, CSO and Z (src/dftd3/damping/) */
+enum { ORACLE_RATIONAL = 0, ORACLE_ZERO = 1, ORACLE_MZERO = 2, ORACLE_OPTIMIZEDPOWER = 3,
+       ORACLE_CSO = 4, ORACLE_Z = 5 };
 
 typedef struct {
-    int damping;      /* ORACLE_RATIONAL or ORACLE_ZERO */
+    int damping;      /* ORACLE_* */
     double s6, s8, s9;
-    double a1, a2;    /* rational */
-    double rs6, rs8;  /* zero */
+    double a1, a2;    /* rational, optimized power, CSO, Z (a1) */
+    double rs6, rs8;  /* zero, modified zero; CSO keeps a3 and a4 here as
+                         new_cso_damping does (cso.f90:74-90) */
     double alp;
+    double bet;       /* modified zero, optimized power */
 } oracle_param;
 
 typedef struct {
@@ -35,7 +40,7 @@ typedef struct {
  *   partitions the coordination number like the reducer branch would.
  *   gradient[nat][3], sigma[3][3], energies[nat], cn[nat], dEdcn[nat] may be
  *   NULL.  Derivatives are computed when gradient or sigma is non-NULL.
- * Returns 0 on success, nonzero for unsupported elements. */
+ * Returns 0 on success, nonzero for unsupported elements or damping kinds. */
 int oracle_get_dispersion(int nat, const int *numbers, const double *xyz,
                           const double *lattice, const int *periodic,
                           const int *ghost, const oracle_param *param,

@@ -24,6 +24,14 @@ extern const d3_param_record d3_zero_params[];
 extern const int d3_n_zero_params;
 extern const d3_param_record d3_mrational_params[];
 extern const int d3_n_mrational_params;
+extern const d3_param_record d3_mzero_params[];
+extern const int d3_n_mzero_params;
+extern const d3_param_record d3_optimizedpower_params[];
+extern const int d3_n_optimizedpower_params;
+extern const d3_param_record d3_cso_params[];   /* a3, a4 in the rs6, rs8 slots */
+extern const int d3_n_cso_params;
+extern const d3_param_record d3_z_params[];
+extern const int d3_n_z_params;
 
 #ifdef __cplusplus
 }

@@ -1,13 +1,14 @@
 #!/usr/bin/env python3
-"""Generate d3_params.c, the damping parameter database behind
-dftd3_load_rational_damping / dftd3_load_zero_damping /
-dftd3_load_mrational_damping, from the reference's Fortran source.
+"""Generate d3_params.c, the damping parameter database behind the
+dftd3_load_*_damping entries, from the reference's Fortran source.
 
 Mechanical transcription (nothing typed by hand) of src/dftd3/param.f90:
   * the method names and aliases of get_method_id (param.f90:96-299),
   * the d3_param defaults (param.f90:38-48),
   * the parameter records of get_rational_damping (param.f90:302-802),
-    get_zero_damping (:805-1088) and get_mrational_damping (:1091-).
+    get_zero_damping (:805-1088), get_mrational_damping (:1091-1136),
+    get_mzero_damping (:1139-1184), get_optimizedpower_damping (:1187-1244),
+    get_cso_damping (:1248-1293) and get_z_damping (:1297-1326, no records).
 Method names are looked up as get_method_id does: '-' removed, lower case.
 
 Usage: python gen_params.py <reference root> > d3_params.c
@@ -16,7 +17,7 @@ import re
 import sys
 from pathlib import Path
 
-FAMILIES = ("rational", "zero", "mrational")
+FAMILIES = ("rational", "zero", "mrational", "mzero", "optimizedpower", "cso", "z")
 FIELDS = ("s6", "s8", "s9", "rs6", "rs8", "a1", "a2", "alp", "bet")
 
 
@@ -78,6 +79,8 @@ def emit(aliases, records):
         out.append("const d3_param_record d3_%s_params[] = {" % fam)
         for ident, v in records[fam]:
             out.append("    {%d, {%s}}," % (ident, ", ".join(repr(v[k]) for k in FIELDS)))
+        if not records[fam]:
+            out.append("    {0, {0}},   /* no records; the count below is 0 */")
         out.append("};")
         out.append("const int d3_n_%s_params = %d;" % (fam, len(records[fam])))
         out.append("")

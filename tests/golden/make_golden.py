@@ -84,11 +84,73 @@ def read_molfile(path):
     return nums, xyz, "angstrom"
 
 
+def read_pdb(path):
+    """ATOM/HETATM records: coordinates in columns 31-54, element in 77-78."""
+    nums, xyz = [], []
+    for ln in path.read_text().splitlines():
+        if ln.startswith(("ATOM", "HETATM")):
+            xyz.append([float(ln[30:38]), float(ln[38:46]), float(ln[46:54])])
+            nums.append(znum(ln[76:78].strip() or ln[12:16].strip()))
+    return nums, xyz, "angstrom"
+
+
+# 10-gradient-d3-op reads its .log file with `--input xyz`
 READERS = {".xyz": read_xyz, ".gen": read_gen, ".tmol": read_tmol,
-           ".coord": read_tmol, ".sdf": read_molfile, ".mol": read_molfile}
+           ".coord": read_tmol, ".sdf": read_molfile, ".mol": read_molfile,
+           ".pdb": read_pdb, ".log": read_xyz}
 
 PARAM_DEFAULTS = {"rational": dict(s6=1.0, s8=1.0, s9=0.0, a1=0.4, a2=5.0, alp=14.0),
                   "zero": dict(s6=1.0, s8=1.0, s9=0.0, rs6=1.0, rs8=1.0, alp=14.0)}
+PARAM_DEFAULTS["mrational"] = PARAM_DEFAULTS["rational"]
+PARAM_DEFAULTS["mzero"] = dict(PARAM_DEFAULTS["zero"], bet=0.0)
+PARAM_DEFAULTS["optimizedpower"] = dict(PARAM_DEFAULTS["rational"], bet=0.0)
+PARAM_DEFAULTS["z"] = dict(s6=1.0, s8=1.0, s9=0.0, a1=0.4, alp=14.0)
+
+_PARAM_DB = None
+
+
+def param_db(root):
+    """The records of src/dftd3/param.f90 as parsed for the library's
+    parameter table (simple-dftd3_b200/csrc/gen_params.py)."""
+    global _PARAM_DB
+    if _PARAM_DB is None:
+        sys.path.insert(0, str(HERE.parents[1] / "simple-dftd3_b200" / "csrc"))
+        import gen_params
+        aliases, records = gen_params.parse(root)
+        _PARAM_DB = (dict(aliases), records, gen_params.FIELDS)
+    return _PARAM_DB
+
+
+def param_f90(root, family, method, atm, **extra):
+    """get_<family>_damping(method) with s9 = 1 when atm (param.f90)."""
+    names, records, fields = param_db(root)
+    ident = names[method.replace("-", "").lower()]
+    values = next(v for i, v in records[family] if i == ident)
+    p = {k: values[k] for k in fields}
+    if atm:
+        p["s9"] = 1.0
+    p.update(extra)
+    p["damping"] = family
+    p["source"] = f"param.f90 get_{family}_damping ({method}){' + atm' if atm else ''}"
+    return p
+
+
+def param_toml(root, method, key):
+    """A record of assets/parameters.toml over its [default.parameter]
+    record and the d3_param defaults, as app/toml.f90:138-240 merges them."""
+    import tomllib
+    db = tomllib.loads((root / "assets/parameters.toml").read_text())
+    _, _, fields = param_db(root)
+    p = dict(s6=1.0, s8=1.0, s9=0.0, rs6=1.0, rs8=1.0, a1=0.4, a2=5.0, alp=14.0, bet=0.0)
+    p.update(db["default"]["parameter"]["d3"][key])
+    p.update(db["parameter"][method]["d3"][key])
+    p.pop("doi", None)
+    family = {"rational": "rational", "zero": "zero", "mzero": "mzero",
+              "optimizedpower": "optimizedpower", "cso": "cso"}[p.pop("damping")]
+    p = {k: float(p[k]) for k in fields}
+    p["damping"] = family
+    p["source"] = f"assets/parameters.toml [parameter.{method}] d3.{key} over [default.parameter]"
+    return p
 
 
 def param(damping, source, **kw):
@@ -124,10 +186,26 @@ VALIDATION = [
 ]
 
 
+def validation_families(root):
+    """The fixtures of the modified rational, modified zero and optimized
+    power families; their parameters come from the reference's tables."""
+    return [
+        ("03-energy-d3-bjm", "03-met-xag.coord", param_f90(root, "mrational", "b97d", False)),
+        ("04-energy-d3-zerom", "04-val-xad.mol", param_f90(root, "mzero", "bp", False)),
+        ("05-energy-d3-op", "05-cys-xag.sdf", param_f90(root, "optimizedpower", "tpss", False)),
+        ("08-gradient-d3-bjm", "08-teh2-hbr.mol", param_f90(root, "mrational", "pbe0", False)),
+        ("09-gradient-d3-zerom", "09-0a.pdb", param_f90(root, "mzero", "lcwpbe", False)),
+        ("10-gradient-d3-op", "10-but14diol.log", param_f90(root, "optimizedpower", "revpbe0", False)),
+        ("18-db-d3-bjm", "18-c1.pdb", param_toml(root, "blyp", "bjm")),
+        ("19-db-d3-zerom", "19-g1.mol", param_toml(root, "b2plyp", "zerom")),
+        ("20-db-d3-op", "20-i21p.tmol", param_toml(root, "ms2", "op")),
+    ]
+
+
 def validation(root):
     out = []
     vdir = root / "test/validation"
-    for name, geo, par in VALIDATION:
+    for name, geo, par in VALIDATION + validation_families(root):
         path = vdir / geo
         nums, xyz, unit = READERS[path.suffix](path)
         ref = json.loads((vdir / f"{name}.json").read_text())
@@ -182,9 +260,19 @@ def python_tests(root):
     for atm, e in ((True, b3lyp[0]), (False, b3lyp[1])):
         cases.append({"param": param("zero", "param.f90 get_zero_damping (b3lyp)", rs6=1.261, s8=1.703,
                                      s9=1.0 if atm else 0.0), "energy": e})
+    for fname, family, method in (("test_pbe_d3_bjm", "mrational", "pbe"), ("test_bp_d3_zerom", "mzero", "bp"),
+                                  ("test_b97d_d3_op", "optimizedpower", "b97d")):
+        e_atm, e_two = refs(fname)
+        cases.append({"param": param_f90(root, family, method, True), "energy": e_atm})
+        cases.append({"param": param_f90(root, family, method, False), "energy": e_two})
+    # ZDampingParam(a1=200770.0, s9=...) with the constructor defaults s6 = s8 = 1, alp = 14
+    e_atm, e_two = refs("test_pbe_d3_z")
+    for atm, e in ((True, e_atm), (False, e_two)):
+        cases.append({"param": param("z", "test_interface.py test_pbe_d3_z (interface.py ZDampingParam)",
+                                     a1=200770.0, s9=1.0 if atm else 0.0), "energy": e})
     interface = {"name": "test_interface.model", "numbers": numbers, "positions": positions,
                  "unit": "bohr", "cases": cases, "tol_rel": 1.0e-6,
-                 "source": "python/dftd3/test_interface.py:77-100,231-235,322-326 (pytest.approx rel 1e-6)"}
+                 "source": "python/dftd3/test_interface.py:77-100,231-235,322-358 (pytest.approx rel 1e-6)"}
 
     src = (pydir / "test_qcschema.py").read_text()
     tree = ast.parse(src)

@@ -18,7 +18,7 @@ AATOAU = 1.0 / AUTOAA
 class OracleParam(C.Structure):
     _fields_ = [("damping", C.c_int), ("s6", C.c_double), ("s8", C.c_double), ("s9", C.c_double),
                 ("a1", C.c_double), ("a2", C.c_double), ("rs6", C.c_double), ("rs8", C.c_double),
-                ("alp", C.c_double)]
+                ("alp", C.c_double), ("bet", C.c_double)]
 
 
 class OracleCutoff(C.Structure):
@@ -68,12 +68,18 @@ def _ptr(a):
     return None if a is None else a.ctypes.data
 
 
+DAMPING = {"rational": 0, "mrational": 0, "zero": 1, "mzero": 2, "optimizedpower": 3, "cso": 4, "z": 5}
+
+
 def make_param(p):
-    """Oracle parameter record from a fixture/param dict."""
-    rat = p.get("damping", "rational") == "rational"
-    return OracleParam(0 if rat else 1, p.get("s6", 1.0), p.get("s8", 1.0), p.get("s9", 0.0),
-                       p.get("a1", 0.4), p.get("a2", 5.0), p.get("rs6", 1.0), p.get("rs8", 1.0),
-                       p.get("alp", 14.0))
+    """Oracle parameter record from a fixture/param dict.  CSO's a3 and a4
+    travel in rs6 and rs8, as new_cso_damping stores them (cso.f90:74-90)."""
+    kind = p.get("damping", "rational")
+    rs6, rs8 = p.get("rs6", 1.0), p.get("rs8", 1.0)
+    if kind == "cso":
+        rs6, rs8 = p.get("a3", 0.0), p.get("a4", 6.25)
+    return OracleParam(DAMPING[kind], p.get("s6", 1.0), p.get("s8", 1.0), p.get("s9", 0.0),
+                       p.get("a1", 0.4), p.get("a2", 5.0), rs6, rs8, p.get("alp", 14.0), p.get("bet", 0.0))
 
 
 def dispersion(numbers, positions, param, lattice=None, periodic=None, grad=True,
