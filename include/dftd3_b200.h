@@ -226,14 +226,24 @@ dftd3_b200_get_dispersion_noalloc(dftd3_error /* error */,
                                   double* /* d_sigma [9] or NULL */,
                                   void* /* stream */);
 
-/* Values of a damping parameter handle: *kind 0 rational, 1 zero;
- * values[8] = s6, s8, s9, a1, a2, rs6, rs8, alp.  For inspecting parameters
- * loaded by method name (dftd3_load_*_damping). */
+/* Damping families of a parameter handle (dftd3_b200_get_param_values);
+ * the modified rational records are evaluated with the rational form. */
+#define DFTD3_B200_DAMPING_RATIONAL 0
+#define DFTD3_B200_DAMPING_ZERO 1
+#define DFTD3_B200_DAMPING_MZERO 2
+#define DFTD3_B200_DAMPING_OPTIMIZEDPOWER 3
+#define DFTD3_B200_DAMPING_CSO 4
+#define DFTD3_B200_DAMPING_Z 5
+
+/* Values of a damping parameter handle: *kind one of DFTD3_B200_DAMPING_*;
+ * values[9] = s6, s8, s9, a1, a2, rs6, rs8, alp, bet (CSO: a3 and a4 in the
+ * rs6 and rs8 places, as the reference's d3_param record holds them).  For
+ * inspecting parameters loaded by method name (dftd3_load_*_damping). */
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_b200_get_param_values(dftd3_error /* error */,
                             dftd3_param /* param */,
                             int* /* kind */,
-                            double* /* values[8] */);
+                            double* /* values[9] */);
 
 /* Measured fused-multiply-add throughput of the current device in TFLOP/s
  * (precision DFTD3_B200_PRECISION_FP64: FP64 pipe, _MIXED: FP32 pipe); the

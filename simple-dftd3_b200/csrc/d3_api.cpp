@@ -131,9 +131,9 @@ int method_id(const char* method)
     return 0;
 }
 
-// get_{rational,zero,mrational}_damping (param.f90:302-, 805-, 1091-) and the
-// load_*_damping entries (api.f90:588-625, 656-690, 710-745): the record of
-// the method, s9 = 1 when the three-body term is requested.
+// get_<family>_damping (param.f90:302-1326) and the load_*_damping entries
+// (api.f90:588-1018): the record of the method, s9 = 1 when the three-body
+// term is requested.
 dftd3_param load_param(dftd3_error error, const char* method, bool atm, const d3_param_record* table, int n,
                        int kind)
 {
@@ -154,7 +154,7 @@ dftd3_param load_param(dftd3_error error, const char* method, bool atm, const d3
     p->damp.kind = kind;
     p->damp.s6 = rec->v[0]; p->damp.s8 = rec->v[1]; p->damp.s9 = atm ? 1.0 : rec->v[2];
     p->damp.rs6 = rec->v[3]; p->damp.rs8 = rec->v[4];
-    p->damp.a1 = rec->v[5]; p->damp.a2 = rec->v[6]; p->damp.alp = rec->v[7];
+    p->damp.a1 = rec->v[5]; p->damp.a2 = rec->v[6]; p->damp.alp = rec->v[7]; p->damp.bet = rec->v[8];
     return p;
 }
 
@@ -383,24 +383,38 @@ dftd3_param dftd3_load_mrational_damping(dftd3_error error, char* method, bool a
     return load_param(error, method, atm, d3_mrational_params, d3_n_mrational_params, d3::kRational);
 }
 
-#define D3_UNSUPPORTED_LOAD(name, what)                                   \
-    dftd3_param name(dftd3_error error, char*, bool)                      \
-    {                                                                     \
-        if (!error) return nullptr;                                       \
-        unsupported(error, what);                                         \
-        return nullptr;                                                   \
-    }
-
-D3_UNSUPPORTED_LOAD(dftd3_load_mzero_damping, "Modified zero damping")
-D3_UNSUPPORTED_LOAD(dftd3_load_optimizedpower_damping, "Optimized power damping")
-D3_UNSUPPORTED_LOAD(dftd3_load_cso_damping, "CSO damping")
-D3_UNSUPPORTED_LOAD(dftd3_load_z_damping, "Z damping")
-
-dftd3_param dftd3_new_mzero_damping(dftd3_error error, double, double, double, double, double, double, double)
+dftd3_param dftd3_load_mzero_damping(dftd3_error error, char* method, bool atm)
 {
+    return load_param(error, method, atm, d3_mzero_params, d3_n_mzero_params, d3::kMZero);
+}
+
+dftd3_param dftd3_load_optimizedpower_damping(dftd3_error error, char* method, bool atm)
+{
+    return load_param(error, method, atm, d3_optimizedpower_params, d3_n_optimizedpower_params,
+                      d3::kOptimizedPower);
+}
+
+dftd3_param dftd3_load_cso_damping(dftd3_error error, char* method, bool atm)
+{
+    return load_param(error, method, atm, d3_cso_params, d3_n_cso_params, d3::kCSO);
+}
+
+dftd3_param dftd3_load_z_damping(dftd3_error error, char* method, bool atm)
+{
+    // get_z_damping has no records (param.f90:1297-1326): every name fails
+    return load_param(error, method, atm, d3_z_params, d3_n_z_params, d3::kZDamping);
+}
+
+dftd3_param dftd3_new_mzero_damping(dftd3_error error, double s6, double s8, double s9, double rs6, double rs8,
+                                    double alp, double bet)
+{
+    // new_mzero_damping_api, api.f90:748-777
     if (!error) return nullptr;
-    unsupported(error, "Modified zero damping");
-    return nullptr;
+    auto* p = new _dftd3_param();
+    p->damp.kind = d3::kMZero;
+    p->damp.s6 = s6; p->damp.s8 = s8; p->damp.s9 = s9;
+    p->damp.rs6 = rs6; p->damp.rs8 = rs8; p->damp.alp = alp; p->damp.bet = bet;
+    return p;
 }
 
 dftd3_param dftd3_new_mrational_damping(dftd3_error error, double s6, double s8, double s9, double a1, double a2,
@@ -411,26 +425,39 @@ dftd3_param dftd3_new_mrational_damping(dftd3_error error, double s6, double s8,
     return dftd3_new_rational_damping(error, s6, s8, s9, a1, a2, alp);
 }
 
-dftd3_param dftd3_new_optimizedpower_damping(dftd3_error error, double, double, double, double, double, double,
-                                             double)
+dftd3_param dftd3_new_optimizedpower_damping(dftd3_error error, double s6, double s8, double s9, double a1,
+                                             double a2, double alp, double bet)
 {
+    // new_optimizedpower_damping_api, api.f90:817-846
     if (!error) return nullptr;
-    unsupported(error, "Optimized power damping");
-    return nullptr;
+    auto* p = new _dftd3_param();
+    p->damp.kind = d3::kOptimizedPower;
+    p->damp.s6 = s6; p->damp.s8 = s8; p->damp.s9 = s9;
+    p->damp.a1 = a1; p->damp.a2 = a2; p->damp.alp = alp; p->damp.bet = bet;
+    return p;
 }
 
-dftd3_param dftd3_new_cso_damping(dftd3_error error, double, double, double, double, double, double, double)
+dftd3_param dftd3_new_cso_damping(dftd3_error error, double s6, double s9, double a1, double a2, double a3,
+                                  double a4, double alp)
 {
+    // new_cso_damping_api, api.f90:886-915: a3 and a4 travel as rs6 and rs8
     if (!error) return nullptr;
-    unsupported(error, "CSO damping");
-    return nullptr;
+    auto* p = new _dftd3_param();
+    p->damp.kind = d3::kCSO;
+    p->damp.s6 = s6; p->damp.s9 = s9;
+    p->damp.a1 = a1; p->damp.a2 = a2; p->damp.rs6 = a3; p->damp.rs8 = a4; p->damp.alp = alp;
+    return p;
 }
 
-dftd3_param dftd3_new_z_damping(dftd3_error error, double, double, double, double, double)
+dftd3_param dftd3_new_z_damping(dftd3_error error, double s6, double s8, double s9, double a1, double alp)
 {
+    // new_z_damping_api, api.f90:955-982 (a2 = 0)
     if (!error) return nullptr;
-    unsupported(error, "Z damping");
-    return nullptr;
+    auto* p = new _dftd3_param();
+    p->damp.kind = d3::kZDamping;
+    p->damp.s6 = s6; p->damp.s8 = s8; p->damp.s9 = s9;
+    p->damp.a1 = a1; p->damp.a2 = 0.0; p->damp.alp = alp;
+    return p;
 }
 
 void dftd3_delete_param(dftd3_param* param)
@@ -740,8 +767,8 @@ void dftd3_b200_get_param_values(dftd3_error error, dftd3_param param, int* kind
     }
     const d3::Damp& d = param->damp;
     *kind = d.kind;
-    const double v[8] = {d.s6, d.s8, d.s9, d.a1, d.a2, d.rs6, d.rs8, d.alp};
-    for (int k = 0; k < 8; k++) values[k] = v[k];
+    const double v[9] = {d.s6, d.s8, d.s9, d.a1, d.a2, d.rs6, d.rs8, d.alp, d.bet};
+    for (int k = 0; k < 9; k++) values[k] = v[k];
 }
 
 double dftd3_b200_fma_peak(dftd3_error error, int precision)

@@ -6,6 +6,8 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <cfloat>
+#include <cmath>
 #include <cstdint>
 
 namespace d3 {
@@ -15,9 +17,14 @@ constexpr int kImageKinds = 3;      // lattice point sets: CN, two-body, three-b
 constexpr int kImgCN = 0, kImgDisp2 = 1, kImgDisp3 = 2;
 constexpr int kSigma = 6;           // packed symmetric virial: xx yy zz xy xz yz
 constexpr int kParamGrad = 5;       // dE/d(s6, s8, a1|rs6, a2|rs8, s9)
-constexpr int kPairSlots = 6;       // per species pair: rrij, q1..q4, pad
+constexpr int kPairSlots = 6;       // per species pair: rrij, q1..q5 (family constants)
 
-enum Damping : int { kRational = 0, kZero = 1 };
+// Damping families of the two-body sum (src/dftd3/damping/); the modified
+// rational records are evaluated with kRational.
+enum Damping : int { kRational = 0, kZero = 1, kMZero = 2, kOptimizedPower = 3, kCSO = 4, kZDamping = 5 };
+constexpr int kDampingKinds = 6;
+// families with dE/d(damping parameter) in the kernels
+inline bool damping_has_param_grad(int kind) { return kind == kRational || kind == kZero; }
 
 // Per-batch geometry and bookkeeping.
 struct Batch {
@@ -26,6 +33,8 @@ struct Batch {
     const int* atom_off = nullptr;       // [nsys + 1]
     const int* local = nullptr;          // [natoms] index inside its system
     const int* sp = nullptr;             // [natoms] batch species index
+    const int* zid = nullptr;            // [natoms] species index inside its own system, from 1
+                                         // (first occurrence; the Z damping's mol%id)
     const uint8_t* ghost = nullptr;      // [natoms] or null
     const int* img_off = nullptr;        // [kImageKinds][nsys + 1]
     const double* img = nullptr;         // [nimg][3]
@@ -71,10 +80,21 @@ struct Species {
     const double* atm_r0 = nullptr;      // [nid][nid] rs9 * rvdw
 };
 
+// Damping parameters (the reference's d3_param record, param.f90:38-48):
+// CSO keeps its a3 and a4 in rs6 and rs8 as new_cso_damping does
+// (cso.f90:74-90); bet belongs to the modified zero and optimized power forms.
 struct Damp {
     int kind = kRational;
-    double s6 = 1, s8 = 1, s9 = 0, a1 = 0.4, a2 = 5, rs6 = 1, rs8 = 1, alp = 14;
+    double s6 = 1, s8 = 1, s9 = 0, a1 = 0.4, a2 = 5, rs6 = 1, rs8 = 1, alp = 14, bet = 0;
 };
+
+// Whether the two-body sum contributes: the early return of each family's
+// get_dispersion2 (rational.f90:266, cso.f90:223 tests s6 and a1).
+inline bool two_body_active(const Damp& d)
+{
+    if (d.kind == kCSO) return std::fabs(d.s6) >= DBL_EPSILON || std::fabs(d.a1) >= DBL_EPSILON;
+    return std::fabs(d.s6) >= DBL_EPSILON || std::fabs(d.s8) >= DBL_EPSILON;
+}
 
 struct Partition {
     int part = 0, nparts = 1;
@@ -145,7 +165,7 @@ void launch_spatial_sort(const double* pos, int natoms, const int* sys_of_atom, 
 void launch_gather_sorted(const double* pos, const int* perm, const int* sp_in, const uint8_t* ghost_in,
                           const int* sys_of_atom, const int* atom_off, int natoms, double* x, double* y,
                           double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost, int* local, bool mixed,
-                          cudaStream_t stream);
+                          cudaStream_t stream, const int* zid_in = nullptr, int* zid = nullptr);
 void launch_tile_bounds(const Batch& b, const int* tile_sys, int ntiles, double4* tiles, cudaStream_t stream);
 // Culled pair sweeps over sorted atoms and tiles (d3_pair.cu); used by the
 // launchers below when b.tiles is set and nid <= kMaxSpeciesFast.

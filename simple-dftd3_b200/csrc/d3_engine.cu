@@ -220,6 +220,7 @@ Engine::Engine(int nsys, const int* natoms, const int* numbers, const double* la
     d_atom_off_ = dev_alloc<int>(nsys + 1);
     d_local_ = dev_alloc<int>(natoms_);
     d_sp_ = dev_alloc<int>(natoms_);
+    d_zid_ = dev_alloc<int>(natoms_);
     d_ghost_ = dev_alloc<uint8_t>(natoms_);
     d_img_off_ = dev_alloc<int>(kImageKinds * (nsys + 1));
     d_rcov_ = dev_alloc<double>(nid);
@@ -237,6 +238,7 @@ Engine::Engine(int nsys, const int* natoms, const int* numbers, const double* la
     up(d_atom_off_, atom_off_.data(), sizeof(int) * (nsys + 1));
     up(d_local_, local_.data(), sizeof(int) * natoms_);
     up(d_sp_, sp_.data(), sizeof(int) * natoms_);
+    up(d_zid_, zid_.data(), sizeof(int) * natoms_);
     up(d_ghost_, ghost_.data(), natoms_);
     up(d_rcov_, tab_.rcov.data(), sizeof(double) * nid);
     up(d_nref_, tab_.nref.data(), sizeof(int) * nid);
@@ -357,6 +359,21 @@ void Engine::build_tables(const int* numbers)
             sp_[a] = (int)(it - tab_.num.begin());
         }
     }
+    // species by first occurrence inside each system, from 1: the species
+    // index mol%id of a structure of its own (used by the Z damping)
+    zid_.resize(natoms_);
+    for (size_t sy = 0; sy + 1 < atom_off_.size(); sy++) {
+        std::vector<int> seen;
+        for (int a = atom_off_[sy]; a < atom_off_[sy + 1]; a++) {
+            auto it = std::find(seen.begin(), seen.end(), numbers[a]);
+            if (it == seen.end()) {
+                seen.push_back(numbers[a]);
+                zid_[a] = (int)seen.size();
+            } else {
+                zid_[a] = (int)(it - seen.begin()) + 1;
+            }
+        }
+    }
     const int nid = tab_.nid();
     tab_.rcov.resize(nid);
     tab_.r4r2.resize(nid);
@@ -470,6 +487,7 @@ void Engine::ensure_workspace(bool grad, bool param_grad, bool threebody)
         d_perm_ = dev_alloc<int>(n);
         d_sp_sorted_ = dev_alloc<int>(n);
         d_local_sorted_ = dev_alloc<int>(n);
+        d_zid_sorted_ = dev_alloc<int>(n);
         d_ghost_sorted_ = dev_alloc<uint8_t>(n);
         d_tiles_ = dev_alloc<double4>(std::max(ntiles_, 1));
         sort_bytes_ = sort_temp_bytes(natoms_);
@@ -514,7 +532,8 @@ void Engine::upload_pair_table(const Damp& d, cudaStream_t stream)
             // rrij = 3 r4r2_i r4r2_j (rational.f90:458, zero.f90:475)
             const double rrij = 3 * tab_.r4r2[a] * tab_.r4r2[b];
             p[0] = rrij;
-            if (d.kind == kRational) {
+            switch (d.kind) {
+            case kRational: {
                 const double r0 = d.a1 * std::sqrt(rrij) + d.a2;
                 const double r02 = r0 * r0;
                 const double r06 = r02 * r02 * r02;
@@ -522,11 +541,41 @@ void Engine::upload_pair_table(const Damp& d, cudaStream_t stream)
                 p[2] = r06 * r02;
                 p[3] = r0;
                 p[4] = std::sqrt(rrij);
-            } else {
+                break;
+            }
+            case kZero: {
                 const double r0 = tab_.rvdw[b * nid + a];
                 p[1] = d.rs6 * r0;
                 p[2] = d.rs8 * r0;
                 p[3] = r0;
+                break;
+            }
+            case kMZero: {   // mzero.f90:441-447
+                const double r0 = tab_.rvdw[b * nid + a];
+                p[1] = 1.0 / (d.rs6 * r0);
+                p[2] = 1.0 / (d.rs8 * r0);
+                p[3] = d.bet * r0;
+                p[4] = d.rs6 * d.bet * r0 * r0;
+                p[5] = d.rs8 * d.bet * r0 * r0;
+                break;
+            }
+            case kOptimizedPower: {   // optimizedpower.f90:421-429
+                const double r0 = d.a1 * std::sqrt(rrij) + d.a2;
+                const double r02 = r0 * r0;
+                const double r06 = r02 * r02 * r02;
+                const double ab = std::pow(r0, d.bet);
+                p[1] = ab * r06;
+                p[2] = ab * r06 * r02;
+                break;
+            }
+            case kCSO: {   // cso.f90:421-426 with a3 = rs6, a4 = rs8
+                const double r0 = std::sqrt(rrij);
+                p[1] = std::pow(d.rs6 * r0 + d.rs8, 6);
+                p[2] = d.a2 * r0;
+                break;
+            }
+            default:       // Z damping: the constant depends on the atoms' species indices
+                break;
             }
         }
     check(cudaMemcpyAsync(d_pair_, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice, stream), "pair table");
@@ -539,6 +588,8 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
                  double* d_sigma9, double* d_param_grad, bool grad, cudaStream_t stream)
 {
     const bool pg = d_param_grad != nullptr;
+    if (pg && !damping_has_param_grad(d.kind))
+        throw Error("Damping parameter derivatives are available for the rational and zero damping only");
     const bool threebody = std::fabs(d.s9) >= DBL_EPSILON;
     ensure_images(stream);
     ensure_workspace(grad, pg, threebody);
@@ -547,6 +598,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     Batch b;
     b.nsys = nsys_; b.natoms = natoms_; b.nid = tab_.nid();
     b.sys_of_atom = d_sys_of_atom_; b.atom_off = d_atom_off_; b.local = d_local_sorted_; b.sp = d_sp_sorted_;
+    b.zid = d_zid_sorted_;
     b.ghost = d_ghost_sorted_; b.img_off = d_img_off_; b.img = d_img_;
     b.x = d_x_; b.y = d_y_; b.z = d_z_; b.xhi = d_xhi_; b.xlo = d_xlo_;
     b.perm = d_perm_; b.tiles = d_tiles_; b.tile_off = d_tile_off_; b.tile_sys = d_tile_sys_;
@@ -580,7 +632,8 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     launch_spatial_sort(d_positions, natoms_, d_sys_of_atom_, tune_.morton_cell, d_keys_in_, d_keys_out_, d_idx_in_,
                         d_perm_, d_sort_temp_, sort_bytes_, stream);
     launch_gather_sorted(d_positions, d_perm_, d_sp_, d_ghost_, d_sys_of_atom_, d_atom_off_, natoms_, d_x_, d_y_,
-                         d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed_, stream);
+                         d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed_, stream,
+                         d.kind == kZDamping ? d_zid_ : nullptr, d_zid_sorted_);
     launch_tile_bounds(b, d_tile_sys_, ntiles_, d_tiles_, stream);
     mark(1);
     launch_cn_units(b, s, c, part_, w, pu_, false, stream);
@@ -588,7 +641,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     mark(2);
     launch_weights(b, s, c, w, stream);
     mark(3);
-    if (std::fabs(d.s6) >= DBL_EPSILON || std::fabs(d.s8) >= DBL_EPSILON || pg) {
+    if (two_body_active(d) || pg) {
         launch_two_body_units(b, s, d, c, part_, w, pu_, stream, timed ? kev_[0] : nullptr, timed ? kev_[1] : nullptr);
     } else {
         check(cudaMemsetAsync(w.e_atom, 0, sizeof(double) * natoms_, stream), "memset");
@@ -896,6 +949,8 @@ void Engine::capture(const Damp& d, const GraphKey& key, bool grad, bool pg)
 
 void Engine::run_graphed(const Damp& d, bool grad, bool pg, cudaStream_t stream)
 {
+    if (pg && !damping_has_param_grad(d.kind))
+        throw Error("Damping parameter derivatives are available for the rational and zero damping only");
     ensure_images(stream);
     ensure_workspace(grad, pg, false);
     upload_pair_table(d, stream);

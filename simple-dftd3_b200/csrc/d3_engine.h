@@ -182,6 +182,7 @@ private:
     int device_ = 0;
     int nsys_ = 0, natoms_ = 0, max_sys_atoms_ = 0;
     std::vector<int> atom_off_, sys_of_atom_, local_, sp_;
+    std::vector<int> zid_;               // species index inside the own system, from 1
     std::vector<double> lat_;
     std::vector<bool> per_storage_;
     std::unique_ptr<bool[]> per_;
@@ -219,7 +220,7 @@ private:
     int* d_tile_off_ = nullptr;
     unsigned long long *d_keys_in_ = nullptr, *d_keys_out_ = nullptr;
     int *d_idx_in_ = nullptr, *d_perm_ = nullptr;
-    int *d_sp_sorted_ = nullptr, *d_local_sorted_ = nullptr;
+    int *d_sp_sorted_ = nullptr, *d_local_sorted_ = nullptr, *d_zid_ = nullptr, *d_zid_sorted_ = nullptr;
     uint8_t* d_ghost_sorted_ = nullptr;
     double4* d_tiles_ = nullptr;
     void* d_sort_temp_ = nullptr;

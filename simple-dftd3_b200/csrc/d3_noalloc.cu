@@ -190,6 +190,8 @@ bool noalloc_dispersion(const Damp& damp, int natoms, const int* numbers, const 
     if (!numbers || !d_positions || !d_energy) return fail("Invalid buffers for the allocation-free evaluation");
     if (std::fabs(damp.s9) >= DBL_EPSILON)
         return fail("The allocation-free evaluation covers the two-body term only; set s9 = 0");
+    if (damp.kind != kRational && damp.kind != kZero)
+        return fail("The allocation-free evaluation supports the rational and zero damping");
     if (precision != DFTD3_B200_PRECISION_FP64 && precision != DFTD3_B200_PRECISION_MIXED)
         return fail("Invalid precision selector");
 

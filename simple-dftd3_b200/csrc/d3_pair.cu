@@ -568,7 +568,7 @@ __global__ void k_morton(const double* __restrict__ pos, int n, const int* sys_o
 __global__ void k_gather_sorted(const double* __restrict__ pos, const int* perm, const int* sp_in,
                                 const uint8_t* ghost_in, const int* sys_of_atom, const int* atom_off, int n,
                                 double* x, double* y, double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost,
-                                int* local, bool mixed)
+                                int* local, bool mixed, const int* zid_in, int* zid)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= n) return;
@@ -583,6 +583,7 @@ __global__ void k_gather_sorted(const double* __restrict__ pos, const int* perm,
     sp[a] = sp_in[o];
     ghost[a] = ghost_in ? ghost_in[o] : 0;
     local[a] = o - atom_off[sys_of_atom[o]];
+    if (zid_in) zid[a] = zid_in[o];
 }
 
 // Bounding sphere (centroid, largest distance) of each tile; one warp per tile.
@@ -628,11 +629,12 @@ void launch_spatial_sort(const double* pos, int natoms, const int* sys_of_atom, 
 void launch_gather_sorted(const double* pos, const int* perm, const int* sp_in, const uint8_t* ghost_in,
                           const int* sys_of_atom, const int* atom_off, int natoms, double* x, double* y, double* z,
                           float4* xhi, float4* xlo, int* sp, uint8_t* ghost, int* local, bool mixed,
-                          cudaStream_t stream)
+                          cudaStream_t stream, const int* zid_in, int* zid)
 {
     if (natoms <= 0) return;
     k_gather_sorted<<<(natoms + 255) / 256, 256, 0, stream>>>(pos, perm, sp_in, ghost_in, sys_of_atom, atom_off,
-                                                              natoms, x, y, z, xhi, xlo, sp, ghost, local, mixed);
+                                                              natoms, x, y, z, xhi, xlo, sp, ghost, local, mixed,
+                                                              zid_in, zid);
 }
 
 void launch_tile_bounds(const Batch& b, const int* tile_sys, int ntiles, double4* tiles, cudaStream_t stream)

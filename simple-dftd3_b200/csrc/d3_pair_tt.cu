@@ -6,8 +6,9 @@
 // lattice translation T are the same for the whole warp at each step.  The
 // translations that can join the two tiles' bounding spheres within the
 // cutoff are compacted per chunk of 128 into shared memory.  Every pair
-// (i, j, T) of the reference's loop (rational.f90:438-514, zero.f90:455-553)
-// is evaluated once: i's energy, virial and parameter-derivative shares hold
+// (i, j, T) of the reference's loop (rational.f90:438-514, zero.f90:455-553,
+// mzero.f90:434-492, optimizedpower.f90:414-468, cso.f90:414-463,
+// z.f90:405-450) is evaluated once: i's energy, virial and parameter-derivative shares hold
 // both halves of the pair, i's gradient and dE/dCN stay in the lane, and j's
 // gradient and dE/dCN are summed over the warp once per (chunk, j).  C6 and
 // its CN derivatives come from per-atom species vectors
@@ -163,6 +164,76 @@ __global__ void k_species_vectors(Batch b, Species s, Work w, R* U, R* dU)
     dU[t] = R(du);
 }
 
+// One (i, j, T) term of the modified zero, optimized power, CSO and Z forms:
+// edisp0 and gdisp0 as the reference names them (E = -C6 edisp0 / 2 per
+// half, gradient -C6 gdisp0 v) and, for Z damping, cdisp0 = d(C6 edisp0)/dC6.
+// r1 is the distance when the smooth cutoff computed it.  Pair constants:
+//   kMZero:          q1 = 1/(rs6 R0), q2 = 1/(rs8 R0), q3 = bet R0,
+//                    q4 = rs6 bet R0^2, q5 = rs8 bet R0^2       (mzero.f90:441-472)
+//   kOptimizedPower: q1 = R0^bet R0^6, q2 = R0^bet R0^8         (optimizedpower.f90:421-448)
+//   kCSO:            q1 = (a3 sqrt(rrij) + a4)^6, q2 = a2 sqrt(rrij) (cso.f90:421-446)
+//   kZDamping:       zc = a1 C6 / (species index sum)          (z.f90:412-431)
+// The optimized power terms use r^-bet in place of the reference's
+// r^bet / (r^bet r^6 + ...) and the CSO derivative 1 - sf = ef sf in the
+// FP32 form, so that no intermediate leaves the FP32 range.
+template <class R, int DAMP>
+__device__ __forceinline__ void tt_family(R r2, R r1, bool have_r1, R rrij, R q1, R q2, R q3, R q4, R q5, R zc,
+                                          R s6, R s8, R alp6, R alp8, R bet, R a1, R& edisp0, R& gdisp0,
+                                          R& cdisp0)
+{
+    if constexpr (DAMP == kMZero) {
+        if (!have_r1) r1 = tt_sqrt<R>(r2);
+        const R r6 = r2 * r2 * r2;
+        const R r8 = r6 * r2;
+        const R t6 = tt_pow<R>(r1 * q1 + q3, -alp6);
+        const R t8 = tt_pow<R>(r1 * q2 + q3, -alp8);
+        const R f6 = R(1) / (R(1) + R(6) * t6);
+        const R f8 = R(1) / (R(1) + R(6) * t8);
+        const R d6 = R(-6) * f6 / r2 + R(6) * alp6 * t6 * (f6 * f6) / (r2 + q4 * r1);
+        const R d8 = R(-8) * f8 / r2 + R(6) * alp8 * t8 * (f8 * f8) / (r2 + q5 * r1);
+        edisp0 = s6 * f6 / r6 + s8 * rrij * f8 / r8;
+        gdisp0 = s6 * d6 / r6 + s8 * rrij * d8 / r8;
+    } else if constexpr (DAMP == kOptimizedPower) {
+        // t6 = r^b / (r^b r^6 + q1) = 1 / (r^6 + q1 r^-b)
+        const R ib = tt_pow<R>(r2, R(-0.5) * bet);
+        const R r4 = r2 * r2;
+        const R t6 = R(1) / (r4 * r2 + q1 * ib);
+        const R t8 = R(1) / (r4 * r4 + q2 * ib);
+        const R d6 = R(-6) * r4 * t6 * t6 + bet * q1 * t6 * t6 * ib / r2;
+        const R d8 = R(-8) * r4 * r2 * t8 * t8 + bet * q2 * t8 * t8 * ib / r2;
+        edisp0 = s6 * t6 + s8 * rrij * t8;
+        gdisp0 = s6 * d6 + s8 * rrij * d8;
+    } else if constexpr (DAMP == kCSO) {
+        if (!have_r1) r1 = tt_sqrt<R>(r2);
+        R sf, om;
+        if constexpr (sizeof(R) == 8) {
+            const R ef = exp(r1 - q2);
+            sf = R(1) / (R(1) + ef);
+            om = R(1) - sf;
+        } else {
+            const R ef = expf(fminf(r1 - q2, 80.f));
+            sf = R(1) / (R(1) + ef);
+            om = ef * sf;
+        }
+        const R sig = s6 + a1 * sf;
+        const R r4 = r2 * r2;
+        const R t6 = R(1) / (r4 * r2 + q1);
+        const R dsig = -a1 * sf * om / r1;
+        const R dt6 = R(-6) * r4 * t6 * t6;
+        edisp0 = sig * t6;
+        gdisp0 = dsig * t6 + sig * dt6;
+    } else {
+        const R r4 = r2 * r2;
+        const R r6 = r4 * r2, r8 = r4 * r4;
+        const R t6 = R(1) / (r6 + zc);
+        const R t8 = R(1) / (r8 + zc * rrij);
+        const R s8rr = s8 * rrij;
+        edisp0 = s6 * t6 + s8rr * t8;
+        gdisp0 = R(-6) * s6 * (r4 * t6) * t6 + R(-8) * s8rr * (r4 * r2 * t8) * t8;
+        cdisp0 = s6 * (r6 * t6) * t6 + s8rr * (r8 * t8) * t8;
+    }
+}
+
 template <class R, int DAMP, bool GRAD, bool PG>
 __global__ void __launch_bounds__(kTTThreads, sizeof(R) == 4 ? 4 : 3)
 k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const int2* units, int nunits, int split,
@@ -214,6 +285,8 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     const bool smooth_on = c.width2 > 0.0 && c.width2 < c.cut2;
     const R s6 = R(d.s6), s8 = R(d.s8);
     const R alp6 = R(d.alp), alp8 = R(d.alp + 2.0);
+    const R bet = R(d.bet), a1 = R(d.a1);
+    const int zsi = DAMP == kZDamping ? b.zid[ic] : 0;
     const int nid = b.nid;
     // i sums: FP32 partials over at most 128 terms (mixed form) added to the
     // FP64 sums in shared memory; the FP64 form adds every term to its
@@ -287,11 +360,15 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
             const double* pr = s.pair + kPairSlots * (si * nid + sj);
             const R rrij = R(__ldg(pr + 0));
             const R q1 = R(__ldg(pr + 1)), q2 = R(__ldg(pr + 2)), q3 = R(__ldg(pr + 3)), q4 = R(__ldg(pr + 4));
+            const R q5 = DAMP == kMZero ? R(__ldg(pr + 5)) : R(0);
+            // Z damping: R0 C6 with R0 = a1 / (species index sum) (z.f90:413)
+            const R zc = DAMP == kZDamping ? a1 / R(zsi + b.zid[j]) * c6 : R(0);
             // both halves of a pair go to i; a self pair (j = i, T != 0) is one half
             const R we = self ? R(0.5) : R(1);
             // sums over the translations of this (i, j); C6 and its derivatives,
             // which do not depend on T, multiply them afterwards
             R se = R(0), se6 = R(0), se8 = R(0), spa = R(0), spb = R(0);
+            R sc = R(0);   // Z damping: sum of sw d(C6 edisp)/dC6, the factor of dC6/dCN
             R sgx = R(0), sgy = R(0), sgz = R(0);
             R sxx = R(0), syy = R(0), szz = R(0), sxy = R(0), sxz = R(0), syz = R(0);
             const R s8rr = s8 * rrij;
@@ -317,7 +394,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
                     nterm++;
                     R sw = R(1), dswdr = R(0), r1 = R(0);
                     if (smooth_on) { r1 = tt_sqrt<R>(r2); tt_smooth<R>(r1, cutoff, width, sw, dswdr); }
-                    R edisp0, gdisp0, e6, e8, dpa = R(0), dpb = R(0);
+                    R edisp0, gdisp0, e6, e8, dpa = R(0), dpb = R(0), cdisp0 = R(0);
                     if constexpr (DAMP == kRational) {
                         // rational.f90:462-497: q1 = R0^6, q2 = R0^8, q3 = R0, q4 = sqrt(rrij)
                         const R r4 = r2 * r2;
@@ -334,7 +411,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
                             dpa = dedr0 * q4;
                             dpb = dedr0;
                         }
-                    } else {
+                    } else if constexpr (DAMP == kZero) {
                         // zero.f90:490-536: q1 = rs6 R0, q2 = rs8 R0
                         if (!smooth_on) r1 = tt_sqrt<R>(r2);
                         const R r6 = r2 * r2 * r2;
@@ -352,8 +429,13 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
                             dpa = d.rs6 != 0.0 ? s6 / r6 * R(-6) * f6 * f6 * alp6 * t6 / R(d.rs6) : R(0);
                             dpb = d.rs8 != 0.0 ? s8 * rrij / r8 * R(-6) * f8 * f8 * alp8 * t8 / R(d.rs8) : R(0);
                         }
+                    } else {
+                        e6 = e8 = R(0);
+                        tt_family<R, DAMP>(r2, r1, smooth_on, rrij, q1, q2, q3, q4, q5, zc, s6, s8, alp6, alp8, bet, a1,
+                                           edisp0, gdisp0, cdisp0);
                     }
                     se += sw * edisp0;
+                    if (DAMP == kZDamping) sc += sw * cdisp0;
                     if (PG) { se6 += sw * e6; se8 += sw * e8; spa += sw * dpa; spb += sw * dpb; }
                     if (GRAD) {
                         R gdisp = sw * gdisp0;
@@ -369,8 +451,10 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
             // (rational.f90:488-497); i takes both halves of E, sigma and dE/dparam
             const R c6w = c6 * we;
             te -= c6w * se;
-            tde -= dc6i * se;
-            R jde = self ? R(0) : -dc6j * se, jgx = R(0), jgy = R(0), jgz = R(0);
+            // dE/dCN = -dC6/dCN sum sw edisp; Z damping: dC6/dCN dE/dC6 (z.f90:431-445)
+            const R sdc = DAMP == kZDamping ? sc : se;
+            tde -= dc6i * sdc;
+            R jde = self ? R(0) : -dc6j * sdc, jgx = R(0), jgy = R(0), jgz = R(0);
             if (PG) { tp0 -= c6w * se6; tp1 -= c6w * se8; tp2 -= c6w * spa; tp3 -= c6w * spb; }
             if (GRAD) {
                 if (!self) {
@@ -694,6 +778,16 @@ void launch_tt(const Batch& b, const Species& s, const Damp& d, const Config& c,
         b, s, d, c, p, w, pu.units, pu.nunits, pu.split, (const R*)pu.U, (const R*)pu.dU, pu.unit_i, pu.unit_j);
 }
 
+// the families without damping-parameter derivatives (the engine refuses
+// them for those)
+template <class R, int DAMP>
+void launch_tt_family(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
+                      const Work& w, const PairUnits& pu, cudaStream_t stream)
+{
+    if (c.grad) launch_tt<R, DAMP, true, false>(b, s, d, c, p, w, pu, stream);
+    else launch_tt<R, DAMP, false, false>(b, s, d, c, p, w, pu, stream);
+}
+
 template <class R, int DAMP>
 void launch_tt_flags(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
                      const Work& w, const PairUnits& pu, cudaStream_t stream)
@@ -742,12 +836,31 @@ void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, cons
         k_species_vectors<double><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (double*)pu.U, (double*)pu.dU);
     if (ev_begin) cudaEventRecord(ev_begin, stream);
     if (pu.nunits > 0) {
-        if (d.kind == kRational) {
+        switch (d.kind) {
+        case kRational:
             if (c.mixed) launch_tt_flags<float, kRational>(b, s, d, c, p, w, pu, stream);
             else launch_tt_flags<double, kRational>(b, s, d, c, p, w, pu, stream);
-        } else {
+            break;
+        case kZero:
             if (c.mixed) launch_tt_flags<float, kZero>(b, s, d, c, p, w, pu, stream);
             else launch_tt_flags<double, kZero>(b, s, d, c, p, w, pu, stream);
+            break;
+        case kMZero:
+            if (c.mixed) launch_tt_family<float, kMZero>(b, s, d, c, p, w, pu, stream);
+            else launch_tt_family<double, kMZero>(b, s, d, c, p, w, pu, stream);
+            break;
+        case kOptimizedPower:
+            if (c.mixed) launch_tt_family<float, kOptimizedPower>(b, s, d, c, p, w, pu, stream);
+            else launch_tt_family<double, kOptimizedPower>(b, s, d, c, p, w, pu, stream);
+            break;
+        case kCSO:
+            if (c.mixed) launch_tt_family<float, kCSO>(b, s, d, c, p, w, pu, stream);
+            else launch_tt_family<double, kCSO>(b, s, d, c, p, w, pu, stream);
+            break;
+        default:
+            if (c.mixed) launch_tt_family<float, kZDamping>(b, s, d, c, p, w, pu, stream);
+            else launch_tt_family<double, kZDamping>(b, s, d, c, p, w, pu, stream);
+            break;
         }
     }
     if (ev_end) cudaEventRecord(ev_end, stream);

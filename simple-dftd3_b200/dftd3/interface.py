@@ -144,7 +144,7 @@ class ModifiedRationalDampingParam(DampingParam):
 
 
 class ModifiedZeroDampingParam(DampingParam):
-    """Modified zero damping (not evaluated by this library)."""
+    """Modified zero damping (mzero.f90)."""
 
     def __init__(self, **kwargs):
         _rename_kwargs(kwargs, "sr6", "rs6")
@@ -164,7 +164,7 @@ class ModifiedZeroDampingParam(DampingParam):
 
 
 class OptimizedPowerDampingParam(DampingParam):
-    """Optimized power damping (not evaluated by this library)."""
+    """Optimized power damping (optimizedpower.f90)."""
 
     def __init__(self, **kwargs):
         _rename_kwargs(kwargs, "alpha6", "alp")
@@ -182,7 +182,7 @@ class OptimizedPowerDampingParam(DampingParam):
 
 
 class CSODampingParam(DampingParam):
-    """C6-scaled-only damping (not evaluated by this library)."""
+    """C6-scaled-only damping (cso.f90)."""
 
     def __init__(self, **kwargs):
         _rename_kwargs(kwargs, "alpha6", "alp")
@@ -199,7 +199,7 @@ class CSODampingParam(DampingParam):
 
 
 class ZDampingParam(DampingParam):
-    """Z damping (not evaluated by this library)."""
+    """Z damping (z.f90): R0 = a1 / (sum of the species indices of the pair)."""
 
     def __init__(self, **kwargs):
         _rename_kwargs(kwargs, "alpha6", "alp")

@@ -363,15 +363,18 @@ def set_batch_reducer(batch: BatchHandle, reducer, part: int, nparts: int) -> No
                                                   ffi.NULL, part, nparts)
 
 
-PARAM_FIELDS = ("s6", "s8", "s9", "a1", "a2", "rs6", "rs8", "alp")
+PARAM_FIELDS = ("s6", "s8", "s9", "a1", "a2", "rs6", "rs8", "alp", "bet")
+# DFTD3_B200_DAMPING_* in kind order; the modified rational form is "rational"
+DAMPING_KINDS = ("rational", "zero", "mzero", "optimizedpower", "cso", "z")
 
 
 def get_param_values(param: ParamHandle) -> dict:
-    """Damping kind and values of a parameter handle."""
+    """Damping kind and values of a parameter handle (CSO: a3 and a4 in the
+    rs6 and rs8 places)."""
     kind = ffi.new("int*")
     v = np.zeros(len(PARAM_FIELDS))
     error_check(lib.dftd3_b200_get_param_values)(param.handle, kind, _cast("double*", v))
-    return dict(zip(PARAM_FIELDS, v.tolist()), damping="rational" if kind[0] == 0 else "zero")
+    return dict(zip(PARAM_FIELDS, v.tolist()), damping=DAMPING_KINDS[kind[0]])
 
 
 def fma_peak(precision: int) -> float:

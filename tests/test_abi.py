@@ -84,8 +84,7 @@ def test_model_setup_errors():
         model.set_work_partition(3, 3)
     with pytest.raises(RuntimeError, match="Index out of bounds"):
         model.set_ghost_atoms([5])
-    with pytest.raises(RuntimeError, match="not supported"):
-        ModifiedZeroDampingParam(s8=1.0, rs6=1.2, bet=1.0)
+    ModifiedZeroDampingParam(s8=1.0, rs6=1.2, bet=1.0)
     with pytest.raises(TypeError, match="s8"):
         RationalDampingParam(a1=0.4, a2=5.0)
     with pytest.raises(TypeError, match="a1"):
@@ -118,3 +117,37 @@ def test_error_buffer_truncation():
     size = L.ffi.new("int*", 8)
     L.lib.dftd3_get_error(err, buf, size)
     assert L.ffi.string(buf).decode() == "D3 disp"
+
+
+def test_family_constructor_arguments():
+    """Insufficient arguments of the other families' constructors raise
+    TypeError naming the missing parameter (test_interface.py:147-200)."""
+    from dftd3.interface import ModifiedZeroDampingParam, OptimizedPowerDampingParam, ZDampingParam
+    with pytest.raises(TypeError):
+        ModifiedZeroDampingParam()
+    with pytest.raises(TypeError, match="s8"):
+        ModifiedZeroDampingParam(rs6=1.2, bet=1.0)
+    with pytest.raises(TypeError, match="rs6"):
+        ModifiedZeroDampingParam(s8=1.0, bet=1.0)
+    with pytest.raises(TypeError, match="bet"):
+        ModifiedZeroDampingParam(s8=1.0, rs6=1.2)
+    with pytest.raises(TypeError):
+        ModifiedZeroDampingParam(s8=1.0, rs6=1.2, bet=1.0, method="abc")
+    with pytest.raises(TypeError):
+        OptimizedPowerDampingParam()
+    with pytest.raises(TypeError, match="s8"):
+        OptimizedPowerDampingParam(a1=0.3, a2=4.2, bet=1.0)
+    with pytest.raises(TypeError, match="a1"):
+        OptimizedPowerDampingParam(s8=1.0, a2=4.2, bet=1.0)
+    with pytest.raises(TypeError, match="a2"):
+        OptimizedPowerDampingParam(s8=1.0, a1=0.3, bet=1.0)
+    with pytest.raises(TypeError, match="bet"):
+        OptimizedPowerDampingParam(s8=1.0, a1=0.3, a2=4.2)
+    with pytest.raises(TypeError):
+        OptimizedPowerDampingParam(s8=1.0, a1=0.3, a2=4.2, bet=1.0, method="abc")
+    with pytest.raises(TypeError):
+        ZDampingParam()
+    with pytest.raises(TypeError, match="a1"):
+        ZDampingParam(s8=1.0)
+    with pytest.raises(TypeError):
+        ZDampingParam(a1=200770.0, method="abc")

@@ -27,10 +27,24 @@ def _positions(case):
 
 
 def _param_obj(p):
-    from dftd3.interface import RationalDampingParam, ZeroDampingParam
-    if p["damping"] == "rational":
-        return RationalDampingParam(s6=p["s6"], s8=p["s8"], s9=p["s9"], a1=p["a1"], a2=p["a2"], alp=p["alp"])
-    return ZeroDampingParam(s6=p["s6"], s8=p["s8"], s9=p["s9"], rs6=p["rs6"], rs8=p["rs8"], alp=p["alp"])
+    """The interface's parameter object of a fixture parameter dict."""
+    from dftd3 import interface as I
+    kind = p["damping"]
+    if kind in ("rational", "mrational"):
+        cls = I.RationalDampingParam if kind == "rational" else I.ModifiedRationalDampingParam
+        return cls(s6=p["s6"], s8=p["s8"], s9=p["s9"], a1=p["a1"], a2=p["a2"], alp=p["alp"])
+    if kind == "zero":
+        return I.ZeroDampingParam(s6=p["s6"], s8=p["s8"], s9=p["s9"], rs6=p["rs6"], rs8=p["rs8"], alp=p["alp"])
+    if kind == "mzero":
+        return I.ModifiedZeroDampingParam(s6=p["s6"], s8=p["s8"], s9=p["s9"], rs6=p["rs6"], rs8=p["rs8"],
+                                          alp=p["alp"], bet=p["bet"])
+    if kind == "optimizedpower":
+        return I.OptimizedPowerDampingParam(s6=p["s6"], s8=p["s8"], s9=p["s9"], a1=p["a1"], a2=p["a2"],
+                                            alp=p["alp"], bet=p["bet"])
+    if kind == "cso":
+        return I.CSODampingParam(s6=p["s6"], s9=p["s9"], a1=p["a1"], a2=p["a2"], a3=p["a3"], a4=p["a4"],
+                                 alp=p["alp"])
+    return I.ZDampingParam(s6=p["s6"], s8=p["s8"], s9=p["s9"], a1=p["a1"], alp=p["alp"])
 
 
 def gpu_dispersion(numbers, positions, param, lattice=None, periodic=None, grad=True, cutoff=None,
