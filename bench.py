@@ -329,7 +329,7 @@ def run_ours(args, rank, world, dist):
     run = Runner(systems, par)
     if shard:
         from dftd3 import parallel
-        lib.set_batch_tuning(run.batch, 3.0, 0, 0, 0)
+        lib.set_batch_tuning(run.batch, 0.0, 0, 0, 0)
         run.reducer = parallel.make_device_reducer()
         lib.set_batch_reducer(run.batch, run.reducer, rank, world)
     counts = run.counts()

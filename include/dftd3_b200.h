@@ -132,8 +132,11 @@ dftd3_b200_set_batch_graph(dftd3_error /* error */,
                            dftd3_b200_batch /* batch */,
                            int /* enable */);
 
-/* Launch shapes of a batch: tuning[0] the cell of the spatial sort key
- * (Bohr, > 0), tuning[1] work items per tile pair of the pair sweeps (1, 2
+/* Launch shapes of a batch: tuning[0] the spatial order of the atoms (0:
+ * column order, tiles of 32 atoms cut from slabs and columns of each system,
+ * the default, Morton order with 3 Bohr cells for systems above 16384 atoms;
+ * > 0: Morton order with keys quantised to cells of that many Bohr),
+ * tuning[1] work items per tile pair of the pair sweeps (1, 2
  * or 4; 0 chooses 1 for batches of molecules, else 2 in the mixed and 4 in
  * the FP64 form), tuning[2] resident blocks per SM of the neighbour-list three-body
  * kernel (0 = occupancy limit), tuning[3] the block-per-molecule three-body

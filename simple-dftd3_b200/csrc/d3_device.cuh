@@ -137,7 +137,9 @@ struct Config {
 
 // Launch-shape choices of one batch, picked by the autotuner or set by hand.
 struct Tuning {
-    double morton_cell = 3.0;      // Bohr; quantisation of the spatial sort key
+    double morton_cell = 0.0;      // spatial order: 0 = column order (compact tiles; Morton with 3 Bohr
+                                   // cells for systems above kRankOrderMax atoms), > 0 = Morton order
+                                   // with keys quantised to cells of this many Bohr
     int pair_split = 0;            // work items per tile pair of the pair sweeps: 1, 2 or 4; 0 = 1 for
                                    // molecules, else 2 (mixed form) or 4 (FP64 form)
     int atm_blocks_per_sm = 0;     // resident blocks per SM of the neighbour-list triple kernel; 0 = occupancy
@@ -162,6 +164,18 @@ size_t sort_temp_bytes(int natoms);
 void launch_spatial_sort(const double* pos, int natoms, const int* sys_of_atom, double cell,
                          unsigned long long* keys_in, unsigned long long* keys_out, int* idx_in, int* perm,
                          void* temp, size_t temp_bytes, cudaStream_t stream);
+// Column order (the default; d3_pair.cu) of batches whose systems have at
+// most kRankOrderMax atoms: per system nx slabs x ny columns of whole tiles,
+// z inside a column, by ranks; writes perm and the sorted atom arrays (the
+// tile bounds follow with launch_tile_bounds).  shape: [nsys], word_a and
+// word_b: [natoms] scratch.
+constexpr int kRankOrderMax = 16384;
+void launch_rank_order(const double* pos, int natoms, int nsys, int max_atoms, const int* sys_of_atom,
+                       const int* atom_off, const int* tile_off, int2* shape, unsigned long long* word_a,
+                       unsigned long long* word_b,
+                       const int* sp_in, const uint8_t* ghost_in, const int* zid_in, bool mixed, int* perm,
+                       double* x, double* y, double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost,
+                       int* local, int* zid, cudaStream_t stream);
 void launch_gather_sorted(const double* pos, const int* perm, const int* sp_in, const uint8_t* ghost_in,
                           const int* sys_of_atom, const int* atom_off, int natoms, double* x, double* y,
                           double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost, int* local, bool mixed,

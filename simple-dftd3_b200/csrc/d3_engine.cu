@@ -490,6 +490,7 @@ void Engine::ensure_workspace(bool grad, bool param_grad, bool threebody)
         d_zid_sorted_ = dev_alloc<int>(n);
         d_ghost_sorted_ = dev_alloc<uint8_t>(n);
         d_tiles_ = dev_alloc<double4>(std::max(ntiles_, 1));
+        d_shape_ = dev_alloc<int2>(std::max(nsys_, 1));
         sort_bytes_ = sort_temp_bytes(natoms_);
         d_sort_temp_ = dev_alloc<unsigned char>(sort_bytes_);
         d_xhi_ = dev_alloc<float4>(n); d_xlo_ = dev_alloc<float4>(n);
@@ -629,11 +630,20 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     }
     kev3_recorded_ = false;
     mark(0);
-    launch_spatial_sort(d_positions, natoms_, d_sys_of_atom_, tune_.morton_cell, d_keys_in_, d_keys_out_, d_idx_in_,
-                        d_perm_, d_sort_temp_, sort_bytes_, stream);
-    launch_gather_sorted(d_positions, d_perm_, d_sp_, d_ghost_, d_sys_of_atom_, d_atom_off_, natoms_, d_x_, d_y_,
-                         d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed_, stream,
-                         d.kind == kZDamping ? d_zid_ : nullptr, d_zid_sorted_);
+    // spatial order of the atoms and the sorted atom arrays
+    const int* zid_in = d.kind == kZDamping ? d_zid_ : nullptr;
+    if (!(tune_.morton_cell > 0.0) && max_sys_atoms_ <= kRankOrderMax) {
+        launch_rank_order(d_positions, natoms_, nsys_, max_sys_atoms_, d_sys_of_atom_, d_atom_off_, d_tile_off_,
+                          d_shape_, d_keys_in_, d_keys_out_, d_sp_, d_ghost_, zid_in, mixed_, d_perm_, d_x_, d_y_,
+                          d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, d_zid_sorted_,
+                          stream);
+    } else {
+        launch_spatial_sort(d_positions, natoms_, d_sys_of_atom_, tune_.morton_cell > 0.0 ? tune_.morton_cell : 3.0,
+                            d_keys_in_, d_keys_out_, d_idx_in_, d_perm_, d_sort_temp_, sort_bytes_, stream);
+        launch_gather_sorted(d_positions, d_perm_, d_sp_, d_ghost_, d_sys_of_atom_, d_atom_off_, natoms_, d_x_, d_y_,
+                             d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed_, stream,
+                             zid_in, d_zid_sorted_);
+    }
     launch_tile_bounds(b, d_tile_sys_, ntiles_, d_tiles_, stream);
     mark(1);
     launch_cn_units(b, s, c, part_, w, pu_, false, stream);
@@ -888,7 +898,8 @@ void Engine::set_tuning(const Tuning& t)
 {
     if (t.pair_split != 0 && t.pair_split != 1 && t.pair_split != 2 && t.pair_split != 4)
         throw Error("Work items per tile pair must be 1, 2 or 4 (0 chooses)");
-    if (!(t.morton_cell > 0.0) || !std::isfinite(t.morton_cell)) throw Error("Sort cell must be positive");
+    if (!(t.morton_cell >= 0.0) || !std::isfinite(t.morton_cell))
+        throw Error("Sort cell must be positive (Morton order) or 0 (column order)");
     if (t.atm_blocks_per_sm < 0) throw Error("Three-body blocks per SM must not be negative");
     if (t.atm_mol < 0 || t.atm_mol > 2) throw Error("Molecule kernel mode must be 0, 1 or 2");
     check(cudaSetDevice(device_), "cudaSetDevice");
@@ -1015,7 +1026,7 @@ double Engine::autotune(const Damp& d, const double* d_positions, bool grad, cud
             if (ms < best_ms) { best_ms = ms; best = t; }
             tune_ = best;
         };
-        for (double cell : {2.0, 3.0, 4.5, 6.0})
+        for (double cell : {0.0, 2.0, 3.0, 4.5, 6.0})
             if (cell != best.morton_cell) { Tuning t = best; t.morton_cell = cell; consider(t); }
         const int cur_split = best.pair_split ? best.pair_split : (auto_split_ == 1 ? 1 : (mixed_ ? 2 : 4));
         for (int sp : {1, 2, 4})

@@ -223,6 +223,7 @@ private:
     int *d_sp_sorted_ = nullptr, *d_local_sorted_ = nullptr, *d_zid_ = nullptr, *d_zid_sorted_ = nullptr;
     uint8_t* d_ghost_sorted_ = nullptr;
     double4* d_tiles_ = nullptr;
+    int2* d_shape_ = nullptr;            // column order: slabs and columns per system
     void* d_sort_temp_ = nullptr;
     size_t sort_bytes_ = 0;
     // workspace

@@ -27,6 +27,8 @@ namespace d3 {
 namespace {
 
 constexpr int kChunk = 128;            // translations staged per pass (4 ballot words)
+constexpr int kOrderThreads = 128;      // threads of the per-system shape blocks
+constexpr int kMaxColumns = 64;         // slabs per system and columns per slab at most (12-bit groups)
 constexpr double kKcn = 16.0;          // ncoord.f90:31
 
 __device__ __forceinline__ double warp_sum(double v)
@@ -565,6 +567,140 @@ __global__ void k_morton(const double* __restrict__ pos, int n, const int* sys_o
     idx[a] = a;
 }
 
+// Column order.  Every system is cut into nx slabs along x, each slab into
+// ny columns along y, and each column is ordered along z; slab and column
+// boundaries fall on multiples of kTile atoms, so every tile of 32
+// consecutive atoms is a compact box inside one column (a Morton curve puts
+// atoms from distant cells into one tile wherever the curve jumps).
+//
+// Each of three passes gives every atom its position inside its system in
+// the order of a 64-bit word (group, coordinate key, local index): pass 0
+// orders by x, pass 1 by (slab, y), pass 2 by (slab * ny + column, z), where
+// slab and column follow from the previous pass's position.  The position is
+// a count over the atoms of the system by a group of lanes (O(n^2) per
+// system, no sort and no barrier), the order of three stable sorts.  The shape kernel writes the
+// pass-0 words, each pass the words of the next, the last pass the sorted
+// atom arrays.
+
+// Order-preserving 32-bit key of a coordinate.
+__device__ __forceinline__ unsigned coord_key(double v)
+{
+    const unsigned u = __float_as_uint(__double2float_rn(v));
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// Largest s with floor(s n / k) <= t: the part (of k parts of n tiles) that
+// holds tile t.
+__device__ __forceinline__ int part_of(int t, int n, int k)
+{
+    return (int)(((long long)(t + 1) * k - 1) / n);
+}
+
+__device__ __forceinline__ unsigned long long order_word(unsigned long long group, double coord, int li)
+{
+    return (group << 52) | ((unsigned long long)coord_key(coord) << 20) | (unsigned long long)li;
+}
+
+// Slabs and columns of every system from its bounding box, boxes of about
+// equal edge holding one tile each; one block per system, which also writes
+// the pass-0 words of its atoms.
+__global__ void k_rank_shape(const double* __restrict__ pos, const int* atom_off, const int* tile_off, int2* shape,
+                             unsigned long long* word)
+{
+    __shared__ double red[6][kOrderThreads / 32];
+    const int sys = blockIdx.x;
+    const int a0 = atom_off[sys], a1 = atom_off[sys + 1];
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+        for (int c = 0; c < 3; c++) {
+            const double v = pos[3 * a + c];
+            lo[c] = fmin(lo[c], v);
+            hi[c] = fmax(hi[c], v);
+        }
+        word[a] = order_word(0, pos[3 * a], a - a0);
+    }
+    for (int c = 0; c < 3; c++)
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[c] = fmin(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+            hi[c] = fmax(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+        }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int c = 0; c < 3; c++) { red[c][wid] = lo[c]; red[3 + c][wid] = hi[c]; }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int w = 1; w < kOrderThreads / 32; w++)
+        for (int c = 0; c < 3; c++) {
+            lo[c] = fmin(lo[c], red[c][w]);
+            hi[c] = fmax(hi[c], red[3 + c][w]);
+        }
+    const int nt = tile_off[sys + 1] - tile_off[sys];
+    int nx = 1, ny = 1;
+    if (nt > 1) {
+        const double lx = fmax(hi[0] - lo[0], 1.0), ly = fmax(hi[1] - lo[1], 1.0), lz = fmax(hi[2] - lo[2], 1.0);
+        const double edge = cbrt(lx * ly * lz / nt);
+        nx = (int)fmin(fmax(rint(lx / edge), 1.0), (double)kMaxColumns);
+        nx = min(nx, nt);
+        ny = (int)fmin(fmax(rint(ly / edge), 1.0), (double)kMaxColumns);
+        ny = max(1, min(ny, nt / nx));
+    }
+    shape[sys] = make_int2(nx, ny);
+}
+
+template <int PASS, int G>
+__global__ void k_rank_pass(const double* __restrict__ pos, int n, const int* sys_of_atom, const int* atom_off,
+                            const int* tile_off, const int2* shape, const unsigned long long* __restrict__ word,
+                            unsigned long long* next, const int* sp_in, const uint8_t* ghost_in, const int* zid_in,
+                            bool mixed, int* perm, double* x, double* y, double* z, float4* xhi, float4* xlo,
+                            int* sp, uint8_t* ghost, int* local, int* zid)
+{
+    // G lanes per atom a (G = 4, 8 or 32 by the largest system)
+    const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int a = (int)(gt / G), lane = (int)(gt % G);
+    const bool valid = a < n;
+    int sys = 0, a0 = 0, a1 = 0;
+    unsigned long long wa = 0;
+    if (valid) {
+        sys = sys_of_atom[a];
+        a0 = atom_off[sys];
+        a1 = atom_off[sys + 1];
+        wa = word[a];
+    }
+    // position of a inside its system: the words below its own
+    int r = 0;
+    for (int j = a0 + lane; j < a1; j += G) r += (int)(word[j] < wa);
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    if (!valid || lane != 0) return;
+    const int li = a - a0;
+    if constexpr (PASS < 2) {
+        const int nt = tile_off[sys + 1] - tile_off[sys];
+        const int2 sh = shape[sys];
+        const int t = r / kTile;
+        const int slab = part_of(t, nt, sh.x);
+        unsigned long long group = (unsigned long long)slab;
+        if (PASS == 1) {
+            const int s0 = (int)((long long)slab * nt / sh.x), s1 = (int)((long long)(slab + 1) * nt / sh.x);
+            group = (unsigned long long)(slab * sh.y + part_of(t - s0, s1 - s0, sh.y));
+        }
+        next[a] = order_word(group, pos[3 * a + PASS + 1], li);
+    } else {
+        const int d = a0 + r;
+        const double px = pos[3 * a], py = pos[3 * a + 1], pz = pos[3 * a + 2];
+        perm[d] = a;
+        x[d] = px; y[d] = py; z[d] = pz;
+        if (mixed) {
+            const Sh32 s = split3(px, py, pz);
+            xhi[d] = s.hi;
+            xlo[d] = s.lo;
+        }
+        sp[d] = sp_in[a];
+        ghost[d] = ghost_in ? ghost_in[a] : 0;
+        local[d] = li;
+        if (zid_in) zid[d] = zid_in[a];
+    }
+}
+
 __global__ void k_gather_sorted(const double* __restrict__ pos, const int* perm, const int* sp_in,
                                 const uint8_t* ghost_in, const int* sys_of_atom, const int* atom_off, int n,
                                 double* x, double* y, double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost,
@@ -624,6 +760,33 @@ void launch_spatial_sort(const double* pos, int natoms, const int* sys_of_atom, 
     if (natoms <= 0) return;
     k_morton<<<(natoms + 255) / 256, 256, 0, stream>>>(pos, natoms, sys_of_atom, 1.0 / cell, keys_in, idx_in);
     cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, idx_in, perm, natoms, 0, 64, stream);
+}
+
+void launch_rank_order(const double* pos, int natoms, int nsys, int max_atoms, const int* sys_of_atom,
+                       const int* atom_off, const int* tile_off, int2* shape, unsigned long long* word_a,
+                       unsigned long long* word_b, const int* sp_in, const uint8_t* ghost_in, const int* zid_in, bool mixed, int* perm,
+                       double* x, double* y, double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost,
+                       int* local, int* zid, cudaStream_t stream)
+{
+    if (natoms <= 0 || nsys <= 0) return;
+    k_rank_shape<<<nsys, kOrderThreads, 0, stream>>>(pos, atom_off, tile_off, shape, word_a);
+    // lanes per atom: a whole warp for large systems, groups of 8 or 4 lanes
+    // for batches of molecules (a warp would idle on a few dozen words)
+    const int g = max_atoms > 512 ? 32 : (max_atoms > 64 ? 8 : 4);
+    const unsigned blocks = (unsigned)(((long long)natoms * g + 255) / 256);
+#define D3_RANK_PASS(P, W_IN, W_OUT)                                                                          \
+    do {                                                                                                     \
+        if (g == 32) k_rank_pass<P, 32><<<blocks, 256, 0, stream>>>RANK_ARGS(W_IN, W_OUT);                  \
+        else if (g == 8) k_rank_pass<P, 8><<<blocks, 256, 0, stream>>>RANK_ARGS(W_IN, W_OUT);               \
+        else k_rank_pass<P, 4><<<blocks, 256, 0, stream>>>RANK_ARGS(W_IN, W_OUT);                           \
+    } while (0)
+#define RANK_ARGS(W_IN, W_OUT) (pos, natoms, sys_of_atom, atom_off, tile_off, shape, W_IN, W_OUT, sp_in, ghost_in, \
+                                zid_in, mixed, perm, x, y, z, xhi, xlo, sp, ghost, local, zid)
+    D3_RANK_PASS(0, word_a, word_b);
+    D3_RANK_PASS(1, word_b, word_a);
+    D3_RANK_PASS(2, word_a, word_b);
+#undef RANK_ARGS
+#undef D3_RANK_PASS
 }
 
 void launch_gather_sorted(const double* pos, const int* perm, const int* sp_in, const uint8_t* ghost_in,

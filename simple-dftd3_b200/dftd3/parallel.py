@@ -85,7 +85,7 @@ class ShardedDispersion:
         library.set_batch_precision(self.batch, library.PRECISION_MIXED if precision == "mixed"
                                     else library.PRECISION_FP64)
         # the parts must order the atoms alike: fixed launch shapes on every process
-        library.set_batch_tuning(self.batch, *(tuning or (3.0, 0, 0, 0)))
+        library.set_batch_tuning(self.batch, *(tuning or (0.0, 0, 0, 0)))
         self._reducer = make_device_reducer(group)
         library.set_batch_reducer(self.batch, self._reducer, self.rank, self.world)
 

@@ -225,3 +225,59 @@ def test_batched_matches_single():
         ref = O.dispersion(d["numbers"][k], d["positions"][k], par)
         assert abs(res["energy"][k] - ref["energy"]) <= RTOL64 * abs(ref["energy"])
         assert np.abs(res["gradient"][k] - ref["gradient"]).max() <= GTOL64 * np.abs(ref["gradient"]).max()
+
+
+@pytest.fixture(scope="module")
+def large_batch():
+    """Six molecules and a 4500-atom cluster in one batch."""
+    from dftd3 import synthetic as S
+    mols = S.batch4096(nmol=6, seed=31, nmin=20, nmax=120)
+    big = S.cluster5000(seed=32, natoms=4500)
+    nums = list(mols["numbers"]) + [big["numbers"]]
+    pos = list(mols["positions"]) + [big["positions"]]
+    par = dict(S.PBE_BJ, damping="rational", s9=0.0)
+    refs = [O.dispersion(n, p, par, cutoff=(40.0, 40.0, 25.0, 0.0, 0.0)) for n, p in zip(nums, pos)]
+    return nums, pos, par, refs
+
+
+@pytest.mark.parametrize("order", [0.0, 3.0])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_spatial_orders_large_batch(large_batch, order, precision):
+    """Column order (0) and Morton order (3 Bohr cells) give the oracle's results."""
+    from dftd3.interface import BatchedDispersion, RationalDampingParam
+    nums, pos, par, refs = large_batch
+    bat = BatchedDispersion(nums, pos)
+    bat.set_realspace_cutoff(40.0, 40.0, 25.0)
+    bat.set_precision(precision)
+    bat.set_tuning(order, 0)
+    res = bat.get_dispersion(RationalDampingParam(**{k: par[k] for k in ("s6", "s8", "a1", "a2", "alp")}, s9=0.0),
+                             grad=True)
+    for k, ref in enumerate(refs):
+        if precision == "fp64":
+            assert abs(res["energy"][k] - ref["energy"]) <= RTOL64 * abs(ref["energy"])
+            assert np.abs(res["gradient"][k] - ref["gradient"]).max() <= GTOL64 * np.abs(ref["gradient"]).max()
+        else:
+            assert abs(res["energy"][k] - ref["energy"]) <= ETOL_MIXED * abs(ref["energy"])
+            assert np.abs(res["gradient"][k] - ref["gradient"]).max() <= GTOL_MIXED
+
+
+def test_spatial_orders_agree():
+    """Column order and Morton orders reproduce each other on a molecule
+    batch and on the periodic 2000-atom cell (FP64)."""
+    from dftd3 import synthetic as S
+    from dftd3.interface import BatchedDispersion, RationalDampingParam
+    param = RationalDampingParam(**S.PBE_BJ, s9=0.0)
+    d = S.batch4096(nmol=40, seed=33)
+    c = S.cell2000(natoms=600)
+    for nums, pos, lat, per in ((d["numbers"], d["positions"], None, None),
+                                ([c["numbers"]], [c["positions"]], np.asarray(c["lattice"])[None],
+                                 np.asarray(c["periodic"])[None])):
+        out = []
+        for order in (0.0, 2.0, 4.5):
+            bat = BatchedDispersion(nums, pos, lat, per)
+            bat.set_tuning(order, 0)
+            out.append(bat.get_dispersion(param, grad=True))
+        for r in out[1:]:
+            np.testing.assert_allclose(r["energy"], out[0]["energy"], rtol=1e-13, atol=0)
+            for g, g0 in zip(r["gradient"], out[0]["gradient"]):
+                assert np.abs(g - g0).max() <= 1e-12 * np.abs(g0).max()
