@@ -833,6 +833,170 @@ static void dispersion3(const model_t *m, const oracle_param *p, int nat, const 
 
 /* ------------------------------------------------------------- pipeline -- */
 
+/* ------------------------------------------------------------- pairwise -- */
+
+static void pairwise2(const model_t *m, const oracle_param *p, int nat, const double *xyz,
+                      const double *trans, int ntr, double cutoff, double width, const double *c6,
+                      double *energy)
+{
+    /* get_pairwise_dispersion2 of each family: rational.f90:623-705,
+     * zero.f90:662-755, mzero.f90, optimizedpower.f90, cso.f90, z.f90 (the
+     * energy expressions of the dispersion loops, without derivatives);
+     * energy[i][j] gets half of every (i, j, T) pair energy, energy[j][i] the
+     * other half, a self pair (j = i, T != 0) its half once */
+    double cutoff2 = cutoff * cutoff;
+    double alp6 = p->alp, alp8 = p->alp + 2.0;
+    for (int i = 0; i < nat; i++) {
+        int izp = m->id[i];
+        for (int j = 0; j <= i; j++) {
+            int jzp = m->id[j];
+            double rrij = 3 * m->r4r2[izp] * m->r4r2[jzp];
+            double c6ij = c6[(size_t)j * nat + i];
+            double rvdw = m->rvdw[jzp * m->nid + izp];
+            for (int t = 0; t < ntr; t++) {
+                double v[3];
+                for (int c = 0; c < 3; c++) v[c] = xyz[3 * i + c] - (xyz[3 * j + c] + trans[3 * t + c]);
+                double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+                if (r2 > cutoff2 || r2 < EPS) continue;
+                double r1 = sqrt(r2);
+                double sw, dswdr;
+                smooth_cutoff(r1, cutoff, width, &sw, &dswdr);
+                double r4 = r2 * r2, r6 = r4 * r2, r8 = r6 * r2, e0;
+                switch (p->damping) {
+                case ORACLE_RATIONAL: {
+                    double r0 = p->a1 * sqrt(rrij) + p->a2;
+                    double t6 = 1.0 / (r6 + pow(r0, 6)), t8 = 1.0 / (r8 + pow(r0, 8));
+                    e0 = p->s6 * t6 + p->s8 * rrij * t8;
+                    break;
+                }
+                case ORACLE_ZERO: {
+                    double t6 = pow(p->rs6 * rvdw / r1, alp6), t8 = pow(p->rs8 * rvdw / r1, alp8);
+                    e0 = p->s6 / (1.0 + 6.0 * t6) / r6 + p->s8 * rrij / (1.0 + 6.0 * t8) / r8;
+                    break;
+                }
+                case ORACLE_MZERO: {
+                    double t6 = pow(r1 / (p->rs6 * rvdw) + p->bet * rvdw, -alp6);
+                    double t8 = pow(r1 / (p->rs8 * rvdw) + p->bet * rvdw, -alp8);
+                    e0 = p->s6 / (1.0 + 6.0 * t6) / r6 + p->s8 * rrij / (1.0 + 6.0 * t8) / r8;
+                    break;
+                }
+                case ORACLE_OPTIMIZEDPOWER: {
+                    double r0 = p->a1 * sqrt(rrij) + p->a2, ab = pow(r0, p->bet), rb = pow(r2, p->bet * 0.5);
+                    double t6 = rb / (rb * r6 + ab * pow(r0, 6)), t8 = rb / (rb * r8 + ab * pow(r0, 8));
+                    e0 = p->s6 * t6 + p->s8 * rrij * t8;
+                    break;
+                }
+                case ORACLE_CSO: {
+                    double r0 = sqrt(rrij);
+                    double sf = 1.0 / (1.0 + exp(r1 - p->a2 * r0));
+                    e0 = (p->s6 + p->a1 * sf) / (r6 + pow(p->rs6 * r0 + p->rs8, 6));
+                    break;
+                }
+                default: {
+                    double zc = p->a1 / (double)((izp + 1) + (jzp + 1)) * c6ij;
+                    e0 = p->s6 / (r6 + zc) + p->s8 * rrij / (r8 + zc * rrij);
+                    break;
+                }
+                }
+                double dE = -c6ij * sw * e0 * 0.5;
+                energy[(size_t)i * nat + j] += dE;
+                if (i != j) energy[(size_t)j * nat + i] += dE;
+            }
+        }
+    }
+}
+
+static void pairwise3(const model_t *m, const oracle_param *p, int nat, const double *xyz,
+                      const double *trans, int ntr, double cutoff, double width, const double *c6,
+                      double *energy)
+{
+    /* get_atm_pairwise_dispersion, atm.f90:829-950 with rs9 = 4/3 and alp + 2:
+     * a sixth of every triple energy to each ordered pair of the triple */
+    if (fabs(p->s9) < EPS) return;
+    double cutoff2 = cutoff * cutoff;
+    double alp3 = (p->alp + 2.0) / 3.0;
+    for (int i = 0; i < nat; i++) {
+        int izp = m->id[i];
+        for (int j = 0; j <= i; j++) {
+            int jzp = m->id[j];
+            double c6ij = c6[(size_t)j * nat + i];
+            double r0ij = RS9 * m->rvdw[jzp * m->nid + izp];
+            for (int jt = 0; jt < ntr; jt++) {
+                double vij[3];
+                for (int c = 0; c < 3; c++) vij[c] = xyz[3 * j + c] + trans[3 * jt + c] - xyz[3 * i + c];
+                double r2ij = vij[0] * vij[0] + vij[1] * vij[1] + vij[2] * vij[2];
+                if (r2ij > cutoff2 || r2ij < EPS) continue;
+                double rij = sqrt(r2ij), swij, dsw;
+                smooth_cutoff(rij, cutoff, width, &swij, &dsw);
+                for (int k = 0; k <= j; k++) {
+                    int kzp = m->id[k];
+                    double c6ik = c6[(size_t)k * nat + i], c6jk = c6[(size_t)k * nat + j];
+                    double c9 = -p->s9 * sqrt(fabs(c6ij * c6ik * c6jk));
+                    double r0 = r0ij * RS9 * m->rvdw[kzp * m->nid + izp] * RS9 * m->rvdw[kzp * m->nid + jzp];
+                    double triple = triple_scale(i, j, k);
+                    for (int kt = 0; kt < ntr; kt++) {
+                        double vik[3], vjk[3];
+                        for (int c = 0; c < 3; c++) vik[c] = xyz[3 * k + c] + trans[3 * kt + c] - xyz[3 * i + c];
+                        double r2ik = vik[0] * vik[0] + vik[1] * vik[1] + vik[2] * vik[2];
+                        if (r2ik > cutoff2 || r2ik < EPS) continue;
+                        double rik = sqrt(r2ik), swik;
+                        smooth_cutoff(rik, cutoff, width, &swik, &dsw);
+                        for (int c = 0; c < 3; c++) vjk[c] = vik[c] - vij[c];
+                        double r2jk = vjk[0] * vjk[0] + vjk[1] * vjk[1] + vjk[2] * vjk[2];
+                        if (r2jk > cutoff2 || r2jk < EPS) continue;
+                        double rjk = sqrt(r2jk), swjk;
+                        smooth_cutoff(rjk, cutoff, width, &swjk, &dsw);
+                        double sw = swij * swik * swjk;
+                        double r2 = r2ij * r2ik * r2jk, r1 = sqrt(r2), r3 = r2 * r1, r5 = r3 * r2;
+                        double fdmp = 1.0 / (1.0 + 6.0 * pow(r0 / r1, alp3));
+                        double ang = 0.375 * (r2ij + r2jk - r2ik) * (r2ij - r2jk + r2ik) * (-r2ij + r2jk + r2ik) / r5
+                                   + 1.0 / r3;
+                        double dE = ang * fdmp * c9 * triple * sw / 6.0;
+                        energy[(size_t)i * nat + j] -= dE; energy[(size_t)i * nat + k] -= dE;
+                        energy[(size_t)j * nat + i] -= dE; energy[(size_t)j * nat + k] -= dE;
+                        energy[(size_t)k * nat + i] -= dE; energy[(size_t)k * nat + j] -= dE;
+                    }
+                }
+            }
+        }
+    }
+}
+
+int oracle_get_pairwise_dispersion(int nat, const int *numbers, const double *xyz, const double *lattice,
+                                   const int *periodic, const int *ghost, const oracle_param *param,
+                                   const oracle_cutoff *cutoff, double *pair2, double *pair3)
+{
+    /* get_pairwise_dispersion_v2, disp.f90:403-457 */
+    if (param->damping < ORACLE_RATIONAL || param->damping > ORACLE_Z) return 4;
+    model_t m;
+    if (model_new(&m, nat, numbers, ghost)) return 1;
+    double zero[9] = {0};
+    int per0[3] = {0, 0, 0};
+    const double *lat = lattice ? lattice : zero;
+    const int *per = periodic ? periodic : per0;
+    int ntr;
+    double *cn = malloc(sizeof(double) * (nat > 0 ? nat : 1));
+    double *trans = lattice_points(lat, per, cutoff->cn, &ntr);
+    partitioned_cn(nat, xyz, m.id, m.rcov, trans, ntr, cutoff->cn, cn, 0, 1);
+    free(trans);
+    double *gwvec = malloc(sizeof(double) * (size_t)(nat > 0 ? nat : 1) * m.mref);
+    weight_references(&m, nat, cn, gwvec, NULL);
+    size_t nn = (size_t)nat * nat;
+    double *c6 = malloc(sizeof(double) * (nn > 0 ? nn : 1));
+    get_atomic_c6(&m, nat, gwvec, NULL, c6, NULL, 0, 1);
+    memset(pair2, 0, sizeof(double) * nn);
+    memset(pair3, 0, sizeof(double) * nn);
+    trans = lattice_points(lat, per, cutoff->disp2, &ntr);
+    pairwise2(&m, param, nat, xyz, trans, ntr, cutoff->disp2, cutoff->width2, c6, pair2);
+    free(trans);
+    trans = lattice_points(lat, per, cutoff->disp3, &ntr);
+    pairwise3(&m, param, nat, xyz, trans, ntr, cutoff->disp3, cutoff->width3, c6, pair3);
+    free(trans);
+    free(cn); free(gwvec); free(c6);
+    model_free(&m);
+    return 0;
+}
+
 static int pipeline(int nat, const int *numbers, const double *xyz, const double *lattice,
                     const int *periodic, const int *ghost, const oracle_param *param,
                     const oracle_cutoff *cutoff, int part, int nparts, oracle_reducer reduce, void *user,

@@ -48,6 +48,15 @@ int oracle_get_dispersion(int nat, const int *numbers, const double *xyz,
                           double *energy, double *energies, double *gradient,
                           double *sigma, double *cn_out, double *dEdcn_out);
 
+/* Pairwise decomposition, mirrors get_pairwise_dispersion_v2 (disp.f90:403-457):
+ * pair2[nat][nat] the additive (two-body) and pair3[nat][nat] the
+ * non-additive (three-body) energy of every atom pair; both sum to the
+ * respective energy.  Returns 0 on success. */
+int oracle_get_pairwise_dispersion(int nat, const int *numbers, const double *xyz,
+                                   const double *lattice, const int *periodic, const int *ghost,
+                                   const oracle_param *param, const oracle_cutoff *cutoff,
+                                   double *pair2, double *pair3);
+
 /* In-place sum of count doubles over all parts; returns 0 on success. */
 typedef int (*oracle_reducer)(double *buffer, int count, void *user);
 

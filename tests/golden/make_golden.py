@@ -183,6 +183,18 @@ VALIDATION = [
     ("17-db-d3-zero", "17-li2-ch4.sdf",
      param("zero", "assets/parameters.toml:5-6,418-419 (pkzb, table default s9=1)",
            rs6=0.6327, s8=0.0, s9=1.0, rs8=1.0)),
+    # the pairwise sets 13-15 give their parameters on the command line
+    # (app/cli.f90: --bjm-param s6 s8 a1 a2, --zerom-param s6 s8 rs6 bet,
+    # --op-param s6 s8 a1 a2 bet, --atm-scale s9)
+    ("13-pairwise-d3-bjm", "13-c60.coord",
+     param("mrational", "--bjm-param 1.0 1.206988 0.240184 3.864426 --atm-scale 2.0",
+           s6=1.0, s8=1.206988, a1=0.240184, a2=3.864426, s9=2.0)),
+    ("14-pairwise-d3-zerom", "14-anthracene2.xyz",
+     param("mzero", "--zerom-param 1.0 1.841686 1.279637 0.014370 --atm-scale 0.5",
+           s6=1.0, s8=1.841686, rs6=1.279637, bet=0.014370, s9=0.5)),
+    ("15-pairwise-d3-op", "15-pxylene.mol",
+     param("optimizedpower", "--op-param 1.0 0.27632 0.700 2.500 8.0",
+           s6=1.0, s8=0.27632, a1=0.700, a2=2.500, bet=8.0)),
 ]
 
 
@@ -215,6 +227,9 @@ def validation(root):
         if "gradient" in ref:
             case["gradient"] = ref["gradient"]
             case["virial"] = ref["virial"]
+        if "additive pairwise energy" in ref:
+            case["pairwise2"] = ref["additive pairwise energy"]
+            case["pairwise3"] = ref["non-additive pairwise energy"]
         out.append(case)
     return out
 

@@ -34,6 +34,24 @@ def test_validation_fixture(case):
         np.testing.assert_allclose(res["virial"].ravel(), case["virial"], rtol=0, atol=case["tol_abs"])
 
 
+PAIRWISE = [c for c in _load("validation.json") if "pairwise2" in c]
+
+
+@pytest.mark.parametrize("case", PAIRWISE, ids=lambda c: c["name"])
+def test_pairwise_fixture(case):
+    """test/validation/1[1-5]-pairwise-*.json: the additive and non-additive
+    pair energy matrices (abs 1e-6, tester.py:61); they sum to the energy."""
+    res = O.pairwise_dispersion(case["numbers"], _positions(case), case["param"])
+    n = len(case["numbers"])
+    np.testing.assert_allclose(res["additive pairwise energy"], np.reshape(case["pairwise2"], (n, n)),
+                               rtol=0, atol=case["tol_abs"])
+    np.testing.assert_allclose(res["non-additive pairwise energy"], np.reshape(case["pairwise3"], (n, n)),
+                               rtol=0, atol=case["tol_abs"])
+    total = O.dispersion(case["numbers"], _positions(case), case["param"], grad=False)["energy"]
+    pair_sum = res["additive pairwise energy"].sum() + res["non-additive pairwise energy"].sum()
+    assert abs(pair_sum - total) <= 1e-12 * abs(total)
+
+
 @pytest.mark.parametrize("case", _load("python.json"), ids=lambda c: c["name"])
 def test_python_api_fixture(case):
     for sub in case["cases"]:
