@@ -498,6 +498,21 @@ void dftd3_delete_gcp(dftd3_gcp* gcp)
     }
 }
 
+// The model's engine, created on first use for the structure the model was
+// built for, with the model's settings; the lattice follows the structure.
+static void model_engine(dftd3_model disp, dftd3_structure mol)
+{
+    if (!disp->engine) {
+        disp->engine = std::make_unique<d3::Engine>(1, &mol->nat, mol->numbers.data(), mol->lattice, mol->periodic);
+        if (disp->has_cutoff) disp->engine->set_cutoffs(disp->cutoff);
+        disp->engine->set_ghost(disp->ghost);
+        disp->engine->set_partition(disp->part, disp->nparts, false);
+        disp->engine->set_precision(disp->precision);
+        if (disp->has_tuning) disp->engine->set_tuning(disp->tuning);
+    }
+    disp->engine->set_lattices(mol->lattice);
+}
+
 void dftd3_get_dispersion(dftd3_error error, dftd3_structure mol, dftd3_model disp, dftd3_param param,
                           double* energy, double* gradient, double* sigma)
 {
@@ -528,16 +543,7 @@ void dftd3_get_dispersion(dftd3_error error, dftd3_structure mol, dftd3_model di
         return;
     }
     guarded(error, [&] {
-        if (!disp->engine) {
-            disp->engine = std::make_unique<d3::Engine>(1, &mol->nat, mol->numbers.data(), mol->lattice,
-                                                        mol->periodic);
-            if (disp->has_cutoff) disp->engine->set_cutoffs(disp->cutoff);
-            disp->engine->set_ghost(disp->ghost);
-            disp->engine->set_partition(disp->part, disp->nparts, false);
-            disp->engine->set_precision(disp->precision);
-            if (disp->has_tuning) disp->engine->set_tuning(disp->tuning);
-        }
-        disp->engine->set_lattices(mol->lattice);
+        model_engine(disp, mol);
         double e = 0.0;
         double s9[9];
         disp->engine->evaluate_host(param->damp, mol->xyz.data(), &e, gradient, sigma ? s9 : nullptr);
@@ -546,9 +552,44 @@ void dftd3_get_dispersion(dftd3_error error, dftd3_structure mol, dftd3_model di
     });
 }
 
-void dftd3_get_pairwise_dispersion(dftd3_error error, dftd3_structure, dftd3_model, dftd3_param, double*, double*)
+void dftd3_get_pairwise_dispersion(dftd3_error error, dftd3_structure mol, dftd3_model disp, dftd3_param param,
+                                   double* pair_energy2, double* pair_energy3)
 {
-    if (error) unsupported(error, "The pairwise energy decomposition");
+    // get_pairwise_dispersion_api, api.f90:1180-1236: both [nat][nat]
+    // matrices are overwritten (symmetric, so either storage order reads them)
+    if (!error) return;
+    if (!mol) {
+        fail(error, "Molecular structure data is missing");
+        return;
+    }
+    if (!disp) {
+        fail(error, "Dispersion model is missing");
+        return;
+    }
+    if (!param) {
+        fail(error, "Damping parameters are missing");
+        return;
+    }
+    if (!param->supported) {
+        fail(error, "Damping parameters are not initialized");
+        return;
+    }
+    if (!pair_energy2 || !pair_energy3) {
+        fail(error, "Pairwise energy arrays are missing");
+        return;
+    }
+    if (disp->numbers != mol->numbers) {
+        fail(error, "Dispersion model does not match the molecular structure");
+        return;
+    }
+    if (!finite_all(mol->xyz.data(), mol->xyz.size())) {
+        fail(error, "Non-finite atomic positions");
+        return;
+    }
+    guarded(error, [&] {
+        model_engine(disp, mol);
+        disp->engine->pairwise_host(param->damp, mol->xyz.data(), pair_energy2, pair_energy3);
+    });
 }
 
 void dftd3_get_dispersion_hessian(dftd3_error error, dftd3_structure, dftd3_model, dftd3_param, double*, double*)

@@ -147,6 +147,13 @@ struct Tuning {
                                    // 1 for every eligible system, 2 never
 };
 
+// Pairwise decomposition (d3_pairwise.cu), FP64: energy2 and energy3 of every
+// system as [n_s][n_s] blocks at off[sys] (input atom order); c6 is scratch of
+// the same size.  Needs the sorted atoms and the reference weights.
+void launch_pairwise(const Batch& b, const Species& s, const Damp& d, const Config& c, const Work& w,
+                     const long long* off, long long total, double* c6, double* e2, double* e3,
+                     cudaStream_t stream);
+
 // FMA throughput of the FP64 (fp64=true) or FP32 pipe in TFLOP/s (blocking).
 double measure_fma_peak(bool fp64);
 

@@ -585,6 +585,75 @@ void Engine::upload_pair_table(const Damp& d, cudaStream_t stream)
     pair_valid_ = true;
 }
 
+void Engine::make_views(Batch& b, Species& s) const
+{
+    b.nsys = nsys_; b.natoms = natoms_; b.nid = tab_.nid();
+    b.sys_of_atom = d_sys_of_atom_; b.atom_off = d_atom_off_; b.local = d_local_sorted_; b.sp = d_sp_sorted_;
+    b.zid = d_zid_sorted_;
+    b.ghost = d_ghost_sorted_; b.img_off = d_img_off_; b.img = d_img_;
+    b.x = d_x_; b.y = d_y_; b.z = d_z_; b.xhi = d_xhi_; b.xlo = d_xlo_;
+    b.perm = d_perm_; b.tiles = d_tiles_; b.tile_off = d_tile_off_; b.tile_sys = d_tile_sys_;
+    s.rcov = d_rcov_; s.nref = d_nref_; s.refcn = d_refcn_; s.c6ref = d_c6ref_;
+    s.c6ref_f = d_c6ref_f_; s.pair = d_pair_; s.atm_r0 = d_atm_r0_;
+}
+
+// Spatial order of the atoms, the sorted atom arrays and the tile bounds.
+void Engine::order_atoms(const Damp& d, const double* d_positions, const Batch& b, bool mixed, cudaStream_t stream)
+{
+    const int* zid_in = d.kind == kZDamping ? d_zid_ : nullptr;
+    if (!(tune_.morton_cell > 0.0) && max_sys_atoms_ <= kRankOrderMax) {
+        launch_rank_order(d_positions, natoms_, nsys_, max_sys_atoms_, d_sys_of_atom_, d_atom_off_, d_tile_off_,
+                          d_shape_, d_keys_in_, d_keys_out_, d_sp_, d_ghost_, zid_in, mixed, d_perm_, d_x_, d_y_,
+                          d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, d_zid_sorted_,
+                          stream);
+    } else {
+        launch_spatial_sort(d_positions, natoms_, d_sys_of_atom_, tune_.morton_cell > 0.0 ? tune_.morton_cell : 3.0,
+                            d_keys_in_, d_keys_out_, d_idx_in_, d_perm_, d_sort_temp_, sort_bytes_, stream);
+        launch_gather_sorted(d_positions, d_perm_, d_sp_, d_ghost_, d_sys_of_atom_, d_atom_off_, natoms_, d_x_, d_y_,
+                             d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed, stream,
+                             zid_in, d_zid_sorted_);
+    }
+    launch_tile_bounds(b, d_tile_sys_, ntiles_, d_tiles_, stream);
+}
+
+void Engine::pairwise_host(const Damp& d, const double* positions, double* energy2, double* energy3)
+{
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    cudaStream_t stream = stream_;
+    ensure_images(stream);
+    ensure_workspace(false, false, false);
+    upload_pair_table(d, stream);
+    const long long total = std::max<long long>(c6mat_total_, 1);
+    if (!d_pw_) {
+        d_pw_ = dev_alloc<double>(3 * (size_t)total);
+        d_pw_off_ = dev_alloc<long long>(nsys_);
+        check(cudaMemcpy(d_pw_off_, c6mat_off_.data(), sizeof(long long) * nsys_, cudaMemcpyHostToDevice),
+              "pairwise offsets");
+    }
+    check(cudaMemcpyAsync(d_pos_in_, positions, sizeof(double) * 3 * natoms_, cudaMemcpyHostToDevice, stream),
+          "positions");
+    Batch b;
+    Species s;
+    make_views(b, s);
+    Config c;
+    c.cut_cn = cut_.cn; c.cut2 = cut_.disp2; c.cut3 = cut_.disp3;
+    c.width2 = cut_.width2; c.width3 = cut_.width3;
+    c.grad = false; c.mixed = false; c.param_grad = false; c.cn_partitioned = false;
+    Work w = work_;
+    w.counts = nullptr; w.e3_atom = nullptr; w.sig3_atom = nullptr; w.pg_atom = nullptr;
+    pu_.split = tune_.pair_split ? tune_.pair_split : (auto_split_ == 1 ? 1 : 4);
+    order_atoms(d, d_pos_in_, b, false, stream);
+    launch_cn_units(b, s, c, Partition{}, w, pu_, false, stream);
+    launch_weights(b, s, c, w, stream);
+    launch_pairwise(b, s, d, c, w, d_pw_off_, c6mat_total_, d_pw_, d_pw_ + total, d_pw_ + 2 * total, stream);
+    check(cudaGetLastError(), "pairwise kernels");
+    check(cudaMemcpyAsync(energy2, d_pw_ + total, sizeof(double) * c6mat_total_, cudaMemcpyDeviceToHost, stream),
+          "pairwise energy2");
+    check(cudaMemcpyAsync(energy3, d_pw_ + 2 * total, sizeof(double) * c6mat_total_, cudaMemcpyDeviceToHost, stream),
+          "pairwise energy3");
+    check(cudaStreamSynchronize(stream), "pairwise");
+}
+
 void Engine::run(const Damp& d, const double* d_positions, double* d_energies, double* d_gradient,
                  double* d_sigma9, double* d_param_grad, bool grad, cudaStream_t stream)
 {
@@ -597,15 +666,8 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     upload_pair_table(d, stream);
 
     Batch b;
-    b.nsys = nsys_; b.natoms = natoms_; b.nid = tab_.nid();
-    b.sys_of_atom = d_sys_of_atom_; b.atom_off = d_atom_off_; b.local = d_local_sorted_; b.sp = d_sp_sorted_;
-    b.zid = d_zid_sorted_;
-    b.ghost = d_ghost_sorted_; b.img_off = d_img_off_; b.img = d_img_;
-    b.x = d_x_; b.y = d_y_; b.z = d_z_; b.xhi = d_xhi_; b.xlo = d_xlo_;
-    b.perm = d_perm_; b.tiles = d_tiles_; b.tile_off = d_tile_off_; b.tile_sys = d_tile_sys_;
     Species s;
-    s.rcov = d_rcov_; s.nref = d_nref_; s.refcn = d_refcn_; s.c6ref = d_c6ref_;
-    s.c6ref_f = d_c6ref_f_; s.pair = d_pair_; s.atm_r0 = d_atm_r0_;
+    make_views(b, s);
     Config c;
     c.cut_cn = cut_.cn; c.cut2 = cut_.disp2; c.cut3 = cut_.disp3;
     c.width2 = cut_.width2; c.width3 = cut_.width3;
@@ -630,21 +692,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     }
     kev3_recorded_ = false;
     mark(0);
-    // spatial order of the atoms and the sorted atom arrays
-    const int* zid_in = d.kind == kZDamping ? d_zid_ : nullptr;
-    if (!(tune_.morton_cell > 0.0) && max_sys_atoms_ <= kRankOrderMax) {
-        launch_rank_order(d_positions, natoms_, nsys_, max_sys_atoms_, d_sys_of_atom_, d_atom_off_, d_tile_off_,
-                          d_shape_, d_keys_in_, d_keys_out_, d_sp_, d_ghost_, zid_in, mixed_, d_perm_, d_x_, d_y_,
-                          d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, d_zid_sorted_,
-                          stream);
-    } else {
-        launch_spatial_sort(d_positions, natoms_, d_sys_of_atom_, tune_.morton_cell > 0.0 ? tune_.morton_cell : 3.0,
-                            d_keys_in_, d_keys_out_, d_idx_in_, d_perm_, d_sort_temp_, sort_bytes_, stream);
-        launch_gather_sorted(d_positions, d_perm_, d_sp_, d_ghost_, d_sys_of_atom_, d_atom_off_, natoms_, d_x_, d_y_,
-                             d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed_, stream,
-                             zid_in, d_zid_sorted_);
-    }
-    launch_tile_bounds(b, d_tile_sys_, ntiles_, d_tiles_, stream);
+    order_atoms(d, d_positions, b, mixed_, stream);
     mark(1);
     launch_cn_units(b, s, c, part_, w, pu_, false, stream);
     if (reducer_) reduce(w.cn, natoms_, stream);

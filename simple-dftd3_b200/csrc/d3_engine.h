@@ -79,6 +79,11 @@ public:
     void evaluate_device(const Damp& d, const double* d_positions, double* d_energies,
                          double* d_gradient, double* d_sigma9, double* d_param_grad,
                          cudaStream_t stream);
+    // Pairwise decomposition from host buffers (positions already wrapped),
+    // FP64 and without the work partition (get_pairwise_dispersion_v2):
+    // energy2 and energy3 receive [n_s][n_s] per system, one system after the
+    // other.  Blocking.
+    void pairwise_host(const Damp& d, const double* positions, double* energy2, double* energy3);
 
     cudaStream_t stream() const { return stream_; }
 
@@ -130,6 +135,10 @@ private:
     void ensure_images(cudaStream_t stream);
     void ensure_workspace(bool grad, bool param_grad, bool threebody);
     void upload_pair_table(const Damp& d, cudaStream_t stream);
+    void make_views(Batch& b, Species& s) const;
+    void order_atoms(const Damp& d, const double* d_positions, const Batch& b, bool mixed, cudaStream_t stream);
+    double* d_pw_ = nullptr;             // pairwise decomposition: C6, energy2, energy3 (3 x sum n_s^2)
+    long long* d_pw_off_ = nullptr;
     void run(const Damp& d, const double* d_positions, double* d_energies, double* d_gradient,
              double* d_sigma9, double* d_param_grad, bool grad, cudaStream_t stream);
     template <class T> T* dev_alloc(size_t n);

@@ -270,7 +270,8 @@ class DispersionModel(Structure):
         return results
 
     def get_pairwise_dispersion(self, param: DampingParam) -> dict:
-        """Pairwise energy decomposition (reported as not supported)."""
+        """Pairwise representation of the dispersion energy: the additive (two-body)
+        and non-additive (three-body) energy of every atom pair, FP64."""
         _pair_disp2 = np.zeros((len(self), len(self)))
         _pair_disp3 = np.zeros((len(self), len(self)))
         library.get_pairwise_dispersion(self._mol, self._disp, param._param, _pair_disp2, _pair_disp3)
