@@ -997,6 +997,626 @@ int oracle_get_pairwise_dispersion(int nat, const int *numbers, const double *xy
     return 0;
 }
 
+/* -------------------------------------------------------------- hessian -- */
+
+static void weight_references2(const model_t *m, int nat, const double *cn, double *gwvec,
+                               double *gwdcn, double *gwd2cn)
+{
+    /* model.f90:201-273, the branch with second derivatives */
+    int mref = m->mref;
+    double wf2 = 2 * WF;
+    for (int k = 0; k < nat * mref; k++) gwvec[k] = gwdcn[k] = gwd2cn[k] = 0.0;
+    for (int i = 0; i < nat; i++) {
+        int izp = m->id[i];
+        int nref = m->ref[izp];
+        const double *cnref = m->cn + izp * mref;
+        double gwt[D3_MAX_REF];
+        double norm = 0.0, dnorm = 0.0, d2norm = 0.0;
+        for (int r = 0; r < nref; r++) {
+            double gw = exp(-WF * (cn[i] - cnref[r]) * (cn[i] - cnref[r]));
+            gwt[r] = gw;
+            double dcn = cnref[r] - cn[i];
+            norm += gw;
+            dnorm += wf2 * dcn * gw;
+            d2norm += (wf2 * wf2 * dcn * dcn - wf2) * gw;
+        }
+        norm = 1.0 / norm;
+        double maxcn = cnref[0];
+        for (int r = 1; r < nref; r++) if (cnref[r] > maxcn) maxcn = cnref[r];
+        for (int r = 0; r < nref; r++) {
+            double expw = gwt[r];
+            double dcn = cnref[r] - cn[i];
+            double expd = wf2 * dcn * expw;
+            double expdd = (wf2 * wf2 * dcn * dcn - wf2) * expw;
+            double gwk = expw * norm;
+            if (is_exceptional(gwk)) gwk = (maxcn == cnref[r]) ? 1.0 : 0.0;
+            gwvec[i * mref + r] = gwk;
+            double dgwk = expd * norm - expw * dnorm * (norm * norm);
+            if (is_exceptional(dgwk)) dgwk = 0.0;
+            gwdcn[i * mref + r] = dgwk;
+            double d2gwk = expdd * norm - 2.0 * expd * dnorm * (norm * norm) - expw * d2norm * (norm * norm)
+                         + 2.0 * expw * dnorm * dnorm * (norm * norm * norm);
+            if (is_exceptional(d2gwk)) d2gwk = 0.0;
+            gwd2cn[i * mref + r] = d2gwk;
+        }
+    }
+}
+
+static void get_atomic_c6_2(const model_t *m, int nat, const double *gw, const double *dgw, const double *d2gw,
+                            double *c6, double *dc6dcn, double *d2c6dcn2, double *d2c6dcnij)
+{
+    /* model.f90:363-401: C6, dC6/dCN and the second derivatives; element
+     * (iat, jat) of each matrix at [iat*nat + jat] */
+    int mref = m->mref, nid = m->nid;
+    size_t nn = (size_t)nat * nat;
+    memset(c6, 0, sizeof(double) * nn);
+    memset(dc6dcn, 0, sizeof(double) * nn);
+    memset(d2c6dcn2, 0, sizeof(double) * nn);
+    memset(d2c6dcnij, 0, sizeof(double) * nn);
+    for (int i = 0; i < nat; i++) {
+        if (m->ghost[i]) continue;
+        int izp = m->id[i];
+        for (int j = 0; j <= i; j++) {
+            if (m->ghost[j]) continue;
+            int jzp = m->id[j];
+            double v = 0, di = 0, dj = 0, d2i = 0, d2j = 0, dmix = 0;
+            for (int ir = 0; ir < m->ref[izp]; ir++)
+                for (int jr = 0; jr < m->ref[jzp]; jr++) {
+                    double refc6 = m->c6[(((size_t)izp * nid + jzp) * mref + ir) * mref + jr];
+                    v += gw[i * mref + ir] * gw[j * mref + jr] * refc6;
+                    di += dgw[i * mref + ir] * gw[j * mref + jr] * refc6;
+                    dj += gw[i * mref + ir] * dgw[j * mref + jr] * refc6;
+                    d2i += d2gw[i * mref + ir] * gw[j * mref + jr] * refc6;
+                    d2j += gw[i * mref + ir] * d2gw[j * mref + jr] * refc6;
+                    dmix += dgw[i * mref + ir] * dgw[j * mref + jr] * refc6;
+                }
+            c6[(size_t)i * nat + j] = c6[(size_t)j * nat + i] = v;
+            dc6dcn[(size_t)i * nat + j] = di;
+            dc6dcn[(size_t)j * nat + i] = dj;
+            d2c6dcn2[(size_t)i * nat + j] = d2i;
+            d2c6dcn2[(size_t)j * nat + i] = d2j;
+            d2c6dcnij[(size_t)i * nat + j] = d2c6dcnij[(size_t)j * nat + i] = dmix;
+        }
+    }
+}
+
+static void cn_with_derivs(int nat, const double *xyz, const int *id, const double *rcov, const double *trans,
+                           int ntr, double cutoff, double *cn, double *dr)
+{
+    /* the coordination number (ncoord.f90:86-144) and dr[(3a+c)*nat + k] =
+     * dCN_k/dR_a,c, the derivative the reference takes from mctc-lib's
+     * counting-function CN (ncoord.f90:30-58) */
+    double cutoff2 = cutoff * cutoff;
+    memset(cn, 0, sizeof(double) * nat);
+    memset(dr, 0, sizeof(double) * 3 * (size_t)nat * nat);
+    for (int i = 0; i < nat; i++) {
+        int izp = id[i];
+        for (int j = 0; j <= i; j++) {
+            int jzp = id[j];
+            double rc = rcov[izp] + rcov[jzp];
+            for (int t = 0; t < ntr; t++) {
+                double v[3];
+                for (int c = 0; c < 3; c++) v[c] = xyz[3 * i + c] - (xyz[3 * j + c] + trans[3 * t + c]);
+                double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+                if (r2 > cutoff2 || r2 < 1.0e-12) continue;
+                double r1 = sqrt(r2);
+                double cf = 1.0 / (1.0 + exp(-KCN * (rc / r1 - 1.0)));
+                cn[i] += cf;
+                if (i == j) continue;
+                cn[j] += cf;
+                double dcf = -cf * (1.0 - cf) * KCN * rc / r2;
+                for (int c = 0; c < 3; c++) {
+                    double dg = dcf * v[c] / r1;
+                    dr[(size_t)(3 * i + c) * nat + i] += dg;
+                    dr[(size_t)(3 * i + c) * nat + j] += dg;
+                    dr[(size_t)(3 * j + c) * nat + i] -= dg;
+                    dr[(size_t)(3 * j + c) * nat + j] -= dg;
+                }
+            }
+        }
+    }
+}
+
+static void smooth_cutoff_r2(double r2, double cutoff, double width, double *sw, double *dsw, double *d2sw)
+{
+    /* cutoff.f90:104-134: the switch and its first two derivatives with
+     * respect to the squared distance */
+    double r1 = sqrt(r2), dswdr = 0.0, d2swdr2 = 0.0;
+    if (width <= 0.0 || width >= cutoff) {
+        *sw = 1.0;
+    } else {
+        double inner = cutoff - width;
+        if (r1 <= inner) {
+            *sw = 1.0;
+        } else if (r1 >= cutoff) {
+            *sw = 0.0;
+        } else {
+            double x = (cutoff - r1) / width;
+            *sw = x * x * x * (10.0 + x * (-15.0 + 6.0 * x));
+            dswdr = -30.0 * x * x * (1.0 - x) * (1.0 - x) / width;
+            d2swdr2 = 60.0 * x * (1.0 - x) * (1.0 - 2.0 * x) / (width * width);
+        }
+    }
+    *dsw = 0.5 * dswdr / r1;
+    *d2sw = 0.25 * (d2swdr2 - dswdr / r1) / r2;
+}
+
+static void damping_kernel(const model_t *m, const oracle_param *p, int izp, int jzp, double r2, double c6,
+                           double k[6])
+{
+    /* get_damping_kernel of each family (rational.f90, zero.f90, mzero.f90,
+     * optimizedpower.f90, cso.f90, z.f90): the pair energy e = -C6 p(u) with
+     * u = r^2 and its derivatives e_u, e_c, e_uu, e_uc, e_cc */
+    for (int q = 0; q < 6; q++) k[q] = 0.0;
+    if (p->damping != ORACLE_CSO && fabs(p->s6) < EPS && fabs(p->s8) < EPS) return;
+    double u = r2;
+    double rrij = 3 * m->r4r2[izp] * m->r4r2[jzp];
+    double rvdw = m->rvdw[jzp * m->nid + izp];
+    double pv, pd, pdd, pc = 0.0, puc = 0.0, pcc = 0.0;
+    switch (p->damping) {
+    case ORACLE_RATIONAL: {
+        double r0 = p->a1 * sqrt(rrij) + p->a2, r02 = r0 * r0, r06 = r02 * r02 * r02, r08 = r06 * r02;
+        double t6 = 1.0 / (u * u * u + r06), t8 = 1.0 / (u * u * u * u + r08);
+        double t6d = -3.0 * u * u * t6 * t6, t8d = -4.0 * u * u * u * t8 * t8;
+        double t6dd = -6.0 * u * t6 * t6 + 18.0 * pow(u, 4) * pow(t6, 3);
+        double t8dd = -12.0 * u * u * t8 * t8 + 32.0 * pow(u, 6) * pow(t8, 3);
+        pv = p->s6 * t6 + p->s8 * rrij * t8;
+        pd = p->s6 * t6d + p->s8 * rrij * t8d;
+        pdd = p->s6 * t6dd + p->s8 * rrij * t8dd;
+        break;
+    }
+    case ORACLE_ZERO:
+    case ORACLE_MZERO: {
+        double alp6 = p->alp, alp8 = p->alp + 2.0;
+        double t6, t8, t6d, t8d, t6dd, t8dd;
+        if (p->damping == ORACLE_ZERO) {
+            double a6 = 0.5 * alp6, a8 = 0.5 * alp8;
+            t6 = pow(p->rs6 * rvdw / sqrt(u), alp6);
+            t8 = pow(p->rs8 * rvdw / sqrt(u), alp8);
+            t6d = -a6 * t6 / u;
+            t8d = -a8 * t8 / u;
+            t6dd = a6 * (a6 + 1.0) * t6 / (u * u);
+            t8dd = a8 * (a8 + 1.0) * t8 / (u * u);
+        } else {
+            double r1 = sqrt(u), betr0 = p->bet * rvdw;
+            double w6 = r1 / (p->rs6 * rvdw) + betr0, w8 = r1 / (p->rs8 * rvdw) + betr0;
+            double w6d = 1.0 / (p->rs6 * rvdw * 2.0 * r1), w8d = 1.0 / (p->rs8 * rvdw * 2.0 * r1);
+            double w6dd = -1.0 / (p->rs6 * rvdw * 4.0 * u * r1), w8dd = -1.0 / (p->rs8 * rvdw * 4.0 * u * r1);
+            t6 = pow(w6, -alp6);
+            t8 = pow(w8, -alp8);
+            t6d = -alp6 * pow(w6, -alp6 - 1.0) * w6d;
+            t8d = -alp8 * pow(w8, -alp8 - 1.0) * w8d;
+            t6dd = alp6 * (alp6 + 1.0) * pow(w6, -alp6 - 2.0) * w6d * w6d - alp6 * pow(w6, -alp6 - 1.0) * w6dd;
+            t8dd = alp8 * (alp8 + 1.0) * pow(w8, -alp8 - 2.0) * w8d * w8d - alp8 * pow(w8, -alp8 - 1.0) * w8dd;
+        }
+        double f6 = 1.0 / (1.0 + 6.0 * t6), f8 = 1.0 / (1.0 + 6.0 * t8);
+        double f6d = -6.0 * t6d * f6 * f6, f8d = -6.0 * t8d * f8 * f8;
+        double f6dd = -6.0 * t6dd * f6 * f6 + 72.0 * t6d * t6d * pow(f6, 3);
+        double f8dd = -6.0 * t8dd * f8 * f8 + 72.0 * t8d * t8d * pow(f8, 3);
+        double c6t = f6 / pow(u, 3), c6td = f6d / pow(u, 3) - 3.0 * f6 / pow(u, 4);
+        double c6tdd = f6dd / pow(u, 3) - 6.0 * f6d / pow(u, 4) + 12.0 * f6 / pow(u, 5);
+        double c8t = f8 / pow(u, 4), c8td = f8d / pow(u, 4) - 4.0 * f8 / pow(u, 5);
+        double c8tdd = f8dd / pow(u, 4) - 8.0 * f8d / pow(u, 5) + 20.0 * f8 / pow(u, 6);
+        pv = p->s6 * c6t + p->s8 * rrij * c8t;
+        pd = p->s6 * c6td + p->s8 * rrij * c8td;
+        pdd = p->s6 * c6tdd + p->s8 * rrij * c8tdd;
+        break;
+    }
+    case ORACLE_OPTIMIZEDPOWER: {
+        double r0 = p->a1 * sqrt(rrij) + p->a2, r02 = r0 * r0, r06 = r02 * r02 * r02, r08 = r06 * r02;
+        double ab = pow(r0, p->bet), a6 = ab * r06, a8 = ab * r08, q = 0.5 * p->bet;
+        double d6 = pow(u, 3) + a6 * pow(u, -q), d8 = pow(u, 4) + a8 * pow(u, -q);
+        double d6d = 3.0 * u * u - q * a6 * pow(u, -q - 1.0), d8d = 4.0 * pow(u, 3) - q * a8 * pow(u, -q - 1.0);
+        double d6dd = 6.0 * u + q * (q + 1.0) * a6 * pow(u, -q - 2.0);
+        double d8dd = 12.0 * u * u + q * (q + 1.0) * a8 * pow(u, -q - 2.0);
+        double t6 = 1.0 / d6, t8 = 1.0 / d8;
+        double t6d = -d6d * t6 * t6, t8d = -d8d * t8 * t8;
+        double t6dd = -d6dd * t6 * t6 + 2.0 * d6d * d6d * pow(t6, 3);
+        double t8dd = -d8dd * t8 * t8 + 2.0 * d8d * d8d * pow(t8, 3);
+        pv = p->s6 * t6 + p->s8 * rrij * t8;
+        pd = p->s6 * t6d + p->s8 * rrij * t8d;
+        pdd = p->s6 * t6dd + p->s8 * rrij * t8dd;
+        break;
+    }
+    case ORACLE_CSO: {
+        double r1 = sqrt(u), r0 = sqrt(rrij);
+        double dd6_6 = pow(p->rs6 * r0 + p->rs8, 6);
+        double ef = exp(r1 - p->a2 * r0), sf = 1.0 / (1.0 + ef);
+        double sfd = -sf * (1.0 - sf), sfdd = sf * (1.0 - sf) * (1.0 - 2.0 * sf);
+        double sig = p->s6 + p->a1 * sf, sigd = p->a1 * sfd, sigdd = p->a1 * sfdd;
+        double sigu = 0.5 * sigd / r1, siguu = 0.25 * sigdd / u - 0.25 * sigd / (u * r1);
+        double t6 = 1.0 / (u * u * u + dd6_6);
+        double t6d = -3.0 * u * u * t6 * t6, t6dd = -6.0 * u * t6 * t6 + 18.0 * pow(u, 4) * pow(t6, 3);
+        pv = sig * t6;
+        pd = sigu * t6 + sig * t6d;
+        pdd = siguu * t6 + 2.0 * sigu * t6d + sig * t6dd;
+        break;
+    }
+    default: {
+        double r0 = p->a1 / (double)((izp + 1) + (jzp + 1)), b8 = r0 * rrij;
+        double t6 = 1.0 / (u * u * u + r0 * c6), t8 = 1.0 / (u * u * u * u + b8 * c6);
+        double t6u = -3.0 * u * u * t6 * t6, t8u = -4.0 * pow(u, 3) * t8 * t8;
+        double t6uu = -6.0 * u * t6 * t6 + 18.0 * pow(u, 4) * pow(t6, 3);
+        double t8uu = -12.0 * u * u * t8 * t8 + 32.0 * pow(u, 6) * pow(t8, 3);
+        double t6c = -r0 * t6 * t6, t8c = -b8 * t8 * t8;
+        double t6uc = 6.0 * u * u * r0 * pow(t6, 3), t8uc = 8.0 * pow(u, 3) * b8 * pow(t8, 3);
+        double t6cc = 2.0 * r0 * r0 * pow(t6, 3), t8cc = 2.0 * b8 * b8 * pow(t8, 3);
+        pv = p->s6 * t6 + p->s8 * rrij * t8;
+        pd = p->s6 * t6u + p->s8 * rrij * t8u;
+        pdd = p->s6 * t6uu + p->s8 * rrij * t8uu;
+        pc = p->s6 * t6c + p->s8 * rrij * t8c;
+        puc = p->s6 * t6uc + p->s8 * rrij * t8uc;
+        pcc = p->s6 * t6cc + p->s8 * rrij * t8cc;
+        break;
+    }
+    }
+    k[0] = -c6 * pv;
+    k[1] = -c6 * pd;
+    k[2] = -pv - c6 * pc;
+    k[3] = -c6 * pdd;
+    k[4] = -pd - c6 * puc;
+    k[5] = -2.0 * pc - c6 * pcc;
+}
+
+static void hessian2(const model_t *m, const oracle_param *p, int nat, const double *xyz, const double *trans,
+                     int ntr, double cutoff, double width, const double *c6, const double *dc6dcn,
+                     const double *d2c6dcn2, const double *d2c6dcnij, double *H, double *dEdcn, double *A,
+                     double *D, int part, int nparts)
+{
+    /* get_dispersion2_hessian, damping.f90:393-539: the geometric blocks
+     * into H [3N][3N], dE/dCN, d2E/dR dCN into A [3N][N] and d2E/dCN2 into
+     * D [N][N] */
+    size_t n3 = 3 * (size_t)nat;
+    double cutoff2 = cutoff * cutoff;
+    for (int i = 0; i < nat; i++) {
+        int izp = m->id[i];
+        for (int j = 0; j <= i; j++) {
+            if (!owns_pair(part, nparts, i, j)) continue;
+            int jzp = m->id[j];
+            double c6ij = c6[(size_t)j * nat + i];
+            double fac;
+            int nc, cnat[2];
+            double cnd[2], cnd2[2][2];
+            if (i != j) {
+                fac = 1.0; nc = 2; cnat[0] = i; cnat[1] = j;
+                cnd[0] = dc6dcn[(size_t)i * nat + j];
+                cnd[1] = dc6dcn[(size_t)j * nat + i];
+                cnd2[0][0] = d2c6dcn2[(size_t)i * nat + j];
+                cnd2[1][1] = d2c6dcn2[(size_t)j * nat + i];
+                cnd2[0][1] = cnd2[1][0] = d2c6dcnij[(size_t)i * nat + j];
+            } else {
+                fac = 0.5; nc = 1; cnat[0] = i;
+                cnd[0] = 2.0 * dc6dcn[(size_t)i * nat + i];
+                cnd2[0][0] = 2.0 * d2c6dcn2[(size_t)i * nat + i] + 2.0 * d2c6dcnij[(size_t)i * nat + i];
+            }
+            for (int t = 0; t < ntr; t++) {
+                double v[3];
+                for (int c = 0; c < 3; c++) v[c] = xyz[3 * i + c] - (xyz[3 * j + c] + trans[3 * t + c]);
+                double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+                if (r2 > cutoff2 || r2 < EPS) continue;
+                double k[6], sw, swr, swrr;
+                damping_kernel(m, p, izp, jzp, r2, c6ij, k);
+                smooth_cutoff_r2(r2, cutoff, width, &sw, &swr, &swrr);
+                double fr = fac * (swr * k[0] + sw * k[1]);
+                double frr = fac * (swrr * k[0] + 2.0 * swr * k[1] + sw * k[3]);
+                double fc = fac * sw * k[2];
+                double frc = fac * (swr * k[2] + sw * k[4]);
+                double fcc = fac * sw * k[5];
+                if (i != j) {
+                    for (int a = 0; a < 3; a++)
+                        for (int b = 0; b < 3; b++) {
+                            double blk = 4.0 * frr * v[a] * v[b] + (a == b ? 2.0 * fr : 0.0);
+                            H[(3 * i + a) * n3 + 3 * i + b] += blk;
+                            H[(3 * j + a) * n3 + 3 * j + b] += blk;
+                            H[(3 * i + a) * n3 + 3 * j + b] -= blk;
+                            H[(3 * j + a) * n3 + 3 * i + b] -= blk;
+                        }
+                }
+                for (int ia = 0; ia < nc; ia++) {
+                    dEdcn[cnat[ia]] += fc * cnd[ia];
+                    for (int ib = 0; ib < nc; ib++)
+                        D[(size_t)cnat[ia] * nat + cnat[ib]] += fcc * cnd[ia] * cnd[ib] + fc * cnd2[ia][ib];
+                }
+                if (i != j) {
+                    for (int ia = 0; ia < nc; ia++)
+                        for (int c = 0; c < 3; c++) {
+                            A[(size_t)(3 * i + c) * nat + cnat[ia]] += frc * 2.0 * v[c] * cnd[ia];
+                            A[(size_t)(3 * j + c) * nat + cnat[ia]] -= frc * 2.0 * v[c] * cnd[ia];
+                        }
+                }
+            }
+        }
+    }
+}
+
+static void hessian3(const model_t *m, const oracle_param *p, int nat, const double *xyz, const double *trans,
+                     int ntr, double cutoff, double width, const double *c6, const double *dc6dcn,
+                     const double *d2c6dcn2, const double *d2c6dcnij, double *H, double *dEdcn, double *A,
+                     double *D, int part, int nparts)
+{
+    /* get_atm_dispersion_hessian, atm.f90:38-429, with rs9 = 4/3 and alp + 2 */
+    if (fabs(p->s9) < EPS) return;
+    static const int sigp[3][3] = {{-1, -1, 0}, {1, 0, -1}, {0, 1, 1}};      /* [atom][pair] */
+    static const double cl[3][3] = {{1, -1, 1}, {1, 1, -1}, {-1, 1, 1}};    /* [l][pair] */
+    size_t n3 = 3 * (size_t)nat;
+    double cutoff2 = cutoff * cutoff;
+    double alp3 = (p->alp + 2.0) / 3.0, aexp = 0.5 * alp3;
+    for (int i = 0; i < nat; i++) {
+        int izp = m->id[i];
+        for (int j = 0; j <= i; j++) {
+            if (!owns_pair(part, nparts, i, j)) continue;
+            int jzp = m->id[j];
+            for (int jt = 0; jt < ntr; jt++) {
+                double vec[3][3], u[3];
+                for (int c = 0; c < 3; c++) vec[0][c] = xyz[3 * j + c] + trans[3 * jt + c] - xyz[3 * i + c];
+                u[0] = vec[0][0] * vec[0][0] + vec[0][1] * vec[0][1] + vec[0][2] * vec[0][2];
+                if (u[0] > cutoff2 || u[0] < EPS) continue;
+                for (int kk = 0; kk <= j; kk++) {
+                    int kzp = m->id[kk];
+                    double triple = triple_scale(i, j, kk);
+                    double r0 = RS9 * m->rvdw[jzp * m->nid + izp] * RS9 * m->rvdw[kzp * m->nid + izp]
+                              * RS9 * m->rvdw[kzp * m->nid + jzp];
+                    for (int kt = 0; kt < ntr; kt++) {
+                        for (int c = 0; c < 3; c++) vec[1][c] = xyz[3 * kk + c] + trans[3 * kt + c] - xyz[3 * i + c];
+                        u[1] = vec[1][0] * vec[1][0] + vec[1][1] * vec[1][1] + vec[1][2] * vec[1][2];
+                        if (u[1] > cutoff2 || u[1] < EPS) continue;
+                        for (int c = 0; c < 3; c++) vec[2][c] = vec[1][c] - vec[0][c];
+                        u[2] = vec[2][0] * vec[2][0] + vec[2][1] * vec[2][1] + vec[2][2] * vec[2][2];
+                        if (u[2] > cutoff2 || u[2] < EPS) continue;
+                        double c6t[3] = {c6[(size_t)j * nat + i], c6[(size_t)kk * nat + i], c6[(size_t)kk * nat + j]};
+                        if (fabs(c6t[0]) < EPS || fabs(c6t[1]) < EPS || fabs(c6t[2]) < EPS) continue;
+                        double swp[3], dswp[3], d2swp[3];
+                        for (int q = 0; q < 3; q++) smooth_cutoff_r2(u[q], cutoff, width, &swp[q], &dswp[q], &d2swp[q]);
+                        double sval = swp[0] * swp[1] * swp[2];
+                        double sp[3] = {dswp[0] * swp[1] * swp[2], swp[0] * dswp[1] * swp[2], swp[0] * swp[1] * dswp[2]};
+                        double spq[3][3];
+                        spq[0][0] = d2swp[0] * swp[1] * swp[2];
+                        spq[1][1] = swp[0] * d2swp[1] * swp[2];
+                        spq[2][2] = swp[0] * swp[1] * d2swp[2];
+                        spq[0][1] = spq[1][0] = dswp[0] * dswp[1] * swp[2];
+                        spq[0][2] = spq[2][0] = dswp[0] * swp[1] * dswp[2];
+                        spq[1][2] = spq[2][1] = swp[0] * dswp[1] * dswp[2];
+                        double ww = u[0] * u[1] * u[2];
+                        double wp[3] = {u[1] * u[2], u[0] * u[2], u[0] * u[1]};
+                        double wpq[3][3] = {{0, u[2], u[1]}, {u[2], 0, u[0]}, {u[1], u[0], 0}};
+                        double lval[3] = {u[0] + u[2] - u[1], u[0] - u[2] + u[1], -u[0] + u[2] + u[1]};
+                        double nval = lval[0] * lval[1] * lval[2];
+                        double np[3], npq[3][3];
+                        for (int a = 0; a < 3; a++)
+                            np[a] = cl[0][a] * lval[1] * lval[2] + cl[1][a] * lval[0] * lval[2]
+                                  + cl[2][a] * lval[0] * lval[1];
+                        for (int a = 0; a < 3; a++)
+                            for (int b = 0; b < 3; b++) {
+                                double tmp = 0.0;
+                                for (int il = 0; il < 3; il++)
+                                    for (int im = 0; im < 3; im++) {
+                                        if (il == im) continue;
+                                        tmp += cl[il][a] * cl[im][b] * lval[3 - il - im];
+                                    }
+                                npq[a][b] = tmp;
+                            }
+                        double gv = pow(ww, -2.5), gd = -2.5 * pow(ww, -3.5), gdd = 8.75 * pow(ww, -4.5);
+                        double hv = pow(ww, -1.5), hd = -1.5 * pow(ww, -2.5), hdd = 3.75 * pow(ww, -3.5);
+                        double ang = 0.375 * nval * gv + hv, angp[3], angpq[3][3];
+                        for (int a = 0; a < 3; a++) angp[a] = 0.375 * (np[a] * gv + nval * gd * wp[a]) + hd * wp[a];
+                        for (int a = 0; a < 3; a++)
+                            for (int b = 0; b < 3; b++)
+                                angpq[a][b] = 0.375 * (npq[a][b] * gv + np[a] * gd * wp[b] + np[b] * gd * wp[a]
+                                                       + nval * (gdd * wp[a] * wp[b] + gd * wpq[a][b]))
+                                            + hdd * wp[a] * wp[b] + hd * wpq[a][b];
+                        double cval = 6.0 * pow(r0, alp3);
+                        double tval = cval * pow(ww, -aexp), tp[3], tpq[3][3];
+                        for (int a = 0; a < 3; a++) tp[a] = -aexp * tval * wp[a] / ww;
+                        for (int a = 0; a < 3; a++)
+                            for (int b = 0; b < 3; b++)
+                                tpq[a][b] = aexp * (aexp + 1.0) * tval * wp[a] * wp[b] / (ww * ww)
+                                          - aexp * tval * wpq[a][b] / ww;
+                        double fd = 1.0 / (1.0 + tval), fdp[3], fdpq[3][3];
+                        for (int a = 0; a < 3; a++) fdp[a] = -tp[a] * fd * fd;
+                        for (int a = 0; a < 3; a++)
+                            for (int b = 0; b < 3; b++)
+                                fdpq[a][b] = -tpq[a][b] * fd * fd + 2.0 * tp[a] * tp[b] * fd * fd * fd;
+                        double av = ang * fd, ap[3], apq[3][3];
+                        for (int a = 0; a < 3; a++) ap[a] = angp[a] * fd + ang * fdp[a];
+                        for (int a = 0; a < 3; a++)
+                            for (int b = 0; b < 3; b++)
+                                apq[a][b] = angpq[a][b] * fd + angp[a] * fdp[b] + angp[b] * fdp[a] + ang * fdpq[a][b];
+                        double kv = sval * av, kp[3], kpq[3][3];
+                        for (int a = 0; a < 3; a++) kp[a] = sp[a] * av + sval * ap[a];
+                        for (int a = 0; a < 3; a++)
+                            for (int b = 0; b < 3; b++)
+                                kpq[a][b] = spq[a][b] * av + sp[a] * ap[b] + sp[b] * ap[a] + sval * apq[a][b];
+                        double qv = sqrt(fabs(c6t[0] * c6t[1] * c6t[2])), qm[3], qmn[3][3];
+                        for (int a = 0; a < 3; a++) qm[a] = 0.5 * qv / c6t[a];
+                        for (int a = 0; a < 3; a++)
+                            for (int b = 0; b < 3; b++)
+                                qmn[a][b] = (a == b) ? -0.25 * qv / (c6t[a] * c6t[a]) : 0.25 * qv / (c6t[a] * c6t[b]);
+                        double pref = p->s9 * triple;
+                        int at[3] = {i, j, kk};
+                        double grad[3][3][3];   /* [c][atom][pair] */
+                        for (int a = 0; a < 3; a++)
+                            for (int q = 0; q < 3; q++)
+                                for (int c = 0; c < 3; c++) grad[c][a][q] = 2.0 * sigp[a][q] * vec[q][c];
+                        double pq = pref * qv, gk[3][3][3], dg[3][3];
+                        for (int a = 0; a < 3; a++)
+                            for (int c = 0; c < 3; c++)
+                                for (int q = 0; q < 3; q++) {
+                                    double tmp = 0.0;
+                                    for (int s = 0; s < 3; s++) tmp += kpq[s][q] * grad[c][a][s];
+                                    gk[c][a][q] = pq * tmp;
+                                }
+                        for (int a = 0; a < 3; a++)
+                            for (int b = 0; b < 3; b++) {
+                                double tmp = 0.0;
+                                for (int s = 0; s < 3; s++) tmp += kp[s] * sigp[a][s] * sigp[b][s];
+                                dg[a][b] = 2.0 * pq * tmp;
+                            }
+                        for (int a = 0; a < 3; a++)
+                            for (int b = 0; b < 3; b++)
+                                for (int c = 0; c < 3; c++)
+                                    for (int d = 0; d < 3; d++) {
+                                        double tmp = 0.0;
+                                        for (int q = 0; q < 3; q++) tmp += gk[c][a][q] * grad[d][b][q];
+                                        if (c == d) tmp += dg[a][b];
+                                        H[(size_t)(3 * at[a] + c) * n3 + 3 * at[b] + d] += tmp;
+                                    }
+                        double ec[3], ecc[3][3], euc[3][3], egr[3][3][3];
+                        for (int a = 0; a < 3; a++) {
+                            ec[a] = pref * qm[a] * kv;
+                            for (int b = 0; b < 3; b++) {
+                                ecc[a][b] = pref * qmn[a][b] * kv;
+                                euc[b][a] = pref * qm[a] * kp[b];
+                            }
+                        }
+                        for (int a = 0; a < 3; a++)
+                            for (int c = 0; c < 3; c++)
+                                for (int mm = 0; mm < 3; mm++) {
+                                    double tmp = 0.0;
+                                    for (int s = 0; s < 3; s++) tmp += euc[s][mm] * grad[c][a][s];
+                                    egr[c][a][mm] = tmp;
+                                }
+                        int pat[3][2] = {{i, j}, {i, kk}, {j, kk}};
+                        int nent = 0, ent_atom[6], ent_pair[6];
+                        double ent_coef[6];
+                        for (int q = 0; q < 3; q++) {
+                            int a1 = pat[q][0], a2 = pat[q][1];
+                            if (a1 != a2) {
+                                ent_atom[nent] = a1; ent_pair[nent] = q;
+                                ent_coef[nent++] = dc6dcn[(size_t)a1 * nat + a2];
+                                ent_atom[nent] = a2; ent_pair[nent] = q;
+                                ent_coef[nent++] = dc6dcn[(size_t)a2 * nat + a1];
+                            } else {
+                                ent_atom[nent] = a1; ent_pair[nent] = q;
+                                ent_coef[nent++] = 2.0 * dc6dcn[(size_t)a1 * nat + a1];
+                            }
+                        }
+                        for (int e = 0; e < nent; e++) {
+                            dEdcn[ent_atom[e]] += ec[ent_pair[e]] * ent_coef[e];
+                            for (int f = 0; f < nent; f++)
+                                D[(size_t)ent_atom[e] * nat + ent_atom[f]] +=
+                                    ecc[ent_pair[e]][ent_pair[f]] * ent_coef[e] * ent_coef[f];
+                            for (int a = 0; a < 3; a++)
+                                for (int c = 0; c < 3; c++)
+                                    A[(size_t)(3 * at[a] + c) * nat + ent_atom[e]] += egr[c][a][ent_pair[e]] * ent_coef[e];
+                        }
+                        for (int q = 0; q < 3; q++) {
+                            int a1 = pat[q][0], a2 = pat[q][1];
+                            if (a1 != a2) {
+                                D[(size_t)a1 * nat + a1] += ec[q] * d2c6dcn2[(size_t)a1 * nat + a2];
+                                D[(size_t)a2 * nat + a2] += ec[q] * d2c6dcn2[(size_t)a2 * nat + a1];
+                                D[(size_t)a1 * nat + a2] += ec[q] * d2c6dcnij[(size_t)a1 * nat + a2];
+                                D[(size_t)a2 * nat + a1] += ec[q] * d2c6dcnij[(size_t)a1 * nat + a2];
+                            } else {
+                                D[(size_t)a1 * nat + a1] += ec[q] * (2.0 * d2c6dcn2[(size_t)a1 * nat + a1]
+                                                                    + 2.0 * d2c6dcnij[(size_t)a1 * nat + a1]);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+static void cn_hessian(int nat, const double *xyz, const int *id, const double *rcov, const double *trans,
+                       int ntr, double cutoff, const double *dEdcn, double *H)
+{
+    /* add_coordination_number_hessian, ncoord.f90:230-306 */
+    size_t n3 = 3 * (size_t)nat;
+    double cutoff2 = cutoff * cutoff;
+    for (int i = 0; i < nat; i++) {
+        int izp = id[i];
+        for (int j = 0; j < i; j++) {
+            int jzp = id[j];
+            double rc = rcov[izp] + rcov[jzp];
+            double dEdcnij = dEdcn[i] + dEdcn[j];
+            for (int t = 0; t < ntr; t++) {
+                double v[3];
+                for (int c = 0; c < 3; c++) v[c] = xyz[3 * i + c] - (xyz[3 * j + c] + trans[3 * t + c]);
+                double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+                if (r2 > cutoff2 || r2 < 1.0e-12) continue;
+                double r1 = sqrt(r2);
+                double cf = 1.0 / (1.0 + exp(-KCN * (rc / r1 - 1.0)));
+                double tmp = cf * (1.0 - cf);
+                double dcf = -tmp * KCN * rc / r2;
+                double d2cf = tmp * (1.0 - 2.0 * cf) * (KCN * rc) * (KCN * rc) / (r2 * r2)
+                            + 2.0 * tmp * KCN * rc / (r2 * r1);
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) {
+                        double blk = dEdcnij * (d2cf * v[a] * v[b] / r2 - dcf * v[a] * v[b] / (r2 * r1));
+                        if (a == b) blk += dEdcnij * dcf / r1;
+                        H[(3 * i + a) * n3 + 3 * i + b] += blk;
+                        H[(3 * j + a) * n3 + 3 * j + b] += blk;
+                        H[(3 * i + a) * n3 + 3 * j + b] -= blk;
+                        H[(3 * j + a) * n3 + 3 * i + b] -= blk;
+                    }
+            }
+        }
+    }
+}
+
+int oracle_get_dispersion_hessian(int nat, const int *numbers, const double *xyz, const double *lattice,
+                                  const int *periodic, const int *ghost, const oracle_param *param,
+                                  const oracle_cutoff *cutoff, int part, int nparts, double *hessian)
+{
+    /* get_dispersion_hessian, disp.f90:236-308 */
+    if (param->damping < ORACLE_RATIONAL || param->damping > ORACLE_Z) return 4;
+    model_t m;
+    if (model_new(&m, nat, numbers, ghost)) return 1;
+    double zero[9] = {0};
+    int per0[3] = {0, 0, 0};
+    const double *lat = lattice ? lattice : zero;
+    const int *per = periodic ? periodic : per0;
+    int mref = m.mref, ntr;
+    size_t n = (size_t)(nat > 0 ? nat : 1), n3 = 3 * n, nn = n * n;
+    double *cn = malloc(sizeof(double) * n);
+    double *B = malloc(sizeof(double) * n3 * n);
+    double *trans = lattice_points(lat, per, cutoff->cn, &ntr);
+    cn_with_derivs(nat, xyz, m.id, m.rcov, trans, ntr, cutoff->cn, cn, B);
+    free(trans);
+    double *gw = malloc(sizeof(double) * n * mref), *dgw = malloc(sizeof(double) * n * mref);
+    double *d2gw = malloc(sizeof(double) * n * mref);
+    weight_references2(&m, nat, cn, gw, dgw, d2gw);
+    double *c6 = malloc(sizeof(double) * nn), *dc6 = malloc(sizeof(double) * nn);
+    double *d2c6 = malloc(sizeof(double) * nn), *d2c6ij = malloc(sizeof(double) * nn);
+    get_atomic_c6_2(&m, nat, gw, dgw, d2gw, c6, dc6, d2c6, d2c6ij);
+    double *dEdcn = calloc(n, sizeof(double));
+    double *A = calloc(n3 * n, sizeof(double));
+    double *D = calloc(nn, sizeof(double));
+    memset(hessian, 0, sizeof(double) * 9 * (size_t)nat * nat);
+    trans = lattice_points(lat, per, cutoff->disp2, &ntr);
+    hessian2(&m, param, nat, xyz, trans, ntr, cutoff->disp2, cutoff->width2, c6, dc6, d2c6, d2c6ij, hessian, dEdcn,
+             A, D, part, nparts);
+    free(trans);
+    trans = lattice_points(lat, per, cutoff->disp3, &ntr);
+    hessian3(&m, param, nat, xyz, trans, ntr, cutoff->disp3, cutoff->width3, c6, dc6, d2c6, d2c6ij, hessian, dEdcn,
+             A, D, part, nparts);
+    free(trans);
+    trans = lattice_points(lat, per, cutoff->cn, &ntr);
+    cn_hessian(nat, xyz, m.id, m.rcov, trans, ntr, cutoff->cn, dEdcn, hessian);
+    free(trans);
+    /* H += A B^T + B A^T + B D B^T (disp.f90:299-301) */
+    size_t N3 = 3 * (size_t)nat;
+    double *DB = malloc(sizeof(double) * n * n3);   /* D B^T: [N][3N] */
+    for (int k = 0; k < nat; k++)
+        for (size_t b = 0; b < N3; b++) {
+            double s = 0.0;
+            for (int l = 0; l < nat; l++) s += D[(size_t)k * nat + l] * B[b * nat + l];
+            DB[(size_t)k * N3 + b] = s;
+        }
+    for (size_t a = 0; a < N3; a++)
+        for (size_t b = 0; b < N3; b++) {
+            double s = 0.0;
+            for (int k = 0; k < nat; k++)
+                s += A[a * nat + k] * B[b * nat + k] + B[a * nat + k] * A[b * nat + k] + B[a * nat + k] * DB[(size_t)k * N3 + b];
+            hessian[a * N3 + b] += s;
+        }
+    free(DB); free(cn); free(B); free(gw); free(dgw); free(d2gw); free(c6); free(dc6); free(d2c6); free(d2c6ij);
+    free(dEdcn); free(A); free(D);
+    model_free(&m);
+    return 0;
+}
+
 static int pipeline(int nat, const int *numbers, const double *xyz, const double *lattice,
                     const int *periodic, const int *ghost, const oracle_param *param,
                     const oracle_cutoff *cutoff, int part, int nparts, oracle_reducer reduce, void *user,

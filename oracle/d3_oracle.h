@@ -57,6 +57,14 @@ int oracle_get_pairwise_dispersion(int nat, const int *numbers, const double *xy
                                    const oracle_param *param, const oracle_cutoff *cutoff,
                                    double *pair2, double *pair3);
 
+/* Analytic Hessian, mirrors get_dispersion_hessian (disp.f90:236-308):
+ * hessian[3*nat][3*nat] (symmetric); part/nparts partition the pair and triple
+ * loops as the reference does.  Returns 0 on success. */
+int oracle_get_dispersion_hessian(int nat, const int *numbers, const double *xyz,
+                                  const double *lattice, const int *periodic, const int *ghost,
+                                  const oracle_param *param, const oracle_cutoff *cutoff,
+                                  int part, int nparts, double *hessian);
+
 /* In-place sum of count doubles over all parts; returns 0 on success. */
 typedef int (*oracle_reducer)(double *buffer, int count, void *user);
 

@@ -285,6 +285,15 @@ def python_tests(root):
     for atm, e in ((True, e_atm), (False, e_two)):
         cases.append({"param": param("z", "test_interface.py test_pbe_d3_z (interface.py ZDampingParam)",
                                      a1=200770.0, s9=1.0 if atm else 0.0), "energy": e})
+    # the water dimer of test_hessian / test_hessian_ghost_atoms (analytic
+    # Hessian against central differences of the gradient, step 1e-6, abs 1e-7)
+    hnum, hpos = _np_arrays(funcs["test_hessian"])
+    hseg = ast.get_source_segment(src, funcs["test_hessian_ghost_atoms"])
+    hghost = ast.literal_eval(re.search(r"set_ghost_atoms\((\[[^\]]*\])\)", hseg).group(1))
+    hessian_case = {"name": "test_interface.hessian", "numbers": hnum, "positions": hpos, "unit": "bohr",
+                    "param": param_f90(root, "rational", "pbe0", True), "ghost": hghost, "step": 1.0e-6,
+                    "tol_abs": 1.0e-7, "tol_sym": 1.0e-12,
+                    "source": "python/dftd3/test_interface.py test_hessian, test_hessian_ghost_atoms"}
     interface = {"name": "test_interface.model", "numbers": numbers, "positions": positions,
                  "unit": "bohr", "cases": cases, "tol_rel": 1.0e-6,
                  "source": "python/dftd3/test_interface.py:77-100,231-235,322-358 (pytest.approx rel 1e-6)"}
@@ -327,7 +336,7 @@ def python_tests(root):
                                                       rs6=1.166, s8=1.105, alp=14.0, s9=1.0),
                                        "gradient": tgrad}],
             "tol_abs": 1.0e-9, "source": "python/dftd3/test_qcschema.py:500-547 (abs 1e-9)"}
-    return [interface, molecule1, tpss]
+    return [interface, molecule1, tpss, hessian_case]
 
 
 def fortran_array(body):

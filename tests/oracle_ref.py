@@ -54,6 +54,10 @@ def lib():
         _lib.oracle_get_pairwise_dispersion.argtypes = [
             C.c_int, ip, dp, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(OracleParam),
             C.POINTER(OracleCutoff), dp, dp]
+        _lib.oracle_get_dispersion_hessian.restype = C.c_int
+        _lib.oracle_get_dispersion_hessian.argtypes = [
+            C.c_int, ip, dp, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(OracleParam),
+            C.POINTER(OracleCutoff), C.c_int, C.c_int, dp]
         _lib.oracle_coordination_number.argtypes = [C.c_int, ip, dp, C.c_void_p, C.c_void_p,
                                                     C.c_double, dp]
         _lib.oracle_weight_references.argtypes = [C.c_int, ip, dp, C.POINTER(C.c_int),
@@ -153,6 +157,34 @@ def pairwise_dispersion(numbers, positions, param, lattice=None, periodic=None,
     if rc != 0:
         raise ValueError("oracle: unsupported element or damping")
     return {"additive pairwise energy": e2[:nat, :nat], "non-additive pairwise energy": e3[:nat, :nat]}
+
+
+def hessian(numbers, positions, param, lattice=None, periodic=None, cutoff=(60.0, 40.0, 40.0, 0.0, 0.0),
+            ghost=None, part=0, nparts=1, wrap=True):
+    """Analytic Hessian of the oracle, (3 nat, 3 nat) in Hartree/Bohr^2."""
+    numbers = np.ascontiguousarray(numbers, dtype=np.int32)
+    xyz = np.array(positions, dtype=np.float64).reshape(-1, 3).copy()
+    nat = len(numbers)
+    lat = None if lattice is None else np.ascontiguousarray(lattice, dtype=np.float64).reshape(3, 3)
+    per = None
+    if periodic is not None:
+        per = np.ascontiguousarray([1 if p else 0 for p in np.ravel(periodic)], dtype=np.int32)
+    elif lat is not None:
+        per = np.ones(3, dtype=np.int32)
+    if wrap and per is not None and per.any():
+        lib().oracle_wrap_to_central_cell(nat, xyz, lat, _ptr(per))
+    ghost_arr = None
+    if ghost is not None:
+        ghost_arr = np.zeros(nat, dtype=np.int32)
+        ghost_arr[np.asarray(ghost, dtype=int)] = 1
+    h = np.zeros((3 * max(nat, 1), 3 * max(nat, 1)))
+    prm = make_param(param)
+    cut = OracleCutoff(*cutoff)
+    rc = lib().oracle_get_dispersion_hessian(nat, numbers, xyz, _ptr(lat), _ptr(per), _ptr(ghost_arr),
+                                             C.byref(prm), C.byref(cut), part, nparts, h)
+    if rc != 0:
+        raise ValueError("oracle: unsupported element or damping")
+    return h[:3 * nat, :3 * nat]
 
 
 def coordination_number(numbers, positions, cutoff, lattice=None, periodic=None):

@@ -52,7 +52,7 @@ def test_pairwise_fixture(case):
     assert abs(pair_sum - total) <= 1e-12 * abs(total)
 
 
-@pytest.mark.parametrize("case", _load("python.json"), ids=lambda c: c["name"])
+@pytest.mark.parametrize("case", [e for e in _load("python.json") if "cases" in e], ids=lambda c: c["name"])
 def test_python_api_fixture(case):
     for sub in case["cases"]:
         res = O.dispersion(case["numbers"], _positions(case), sub["param"], grad="gradient" in sub)
@@ -146,3 +146,67 @@ def test_oracle_numerical_sigma(damping):
             num[a, b] = 0.5 * (er - el) / step
     # the returned array is the Fortran sigma(3,3) in column-major order
     np.testing.assert_allclose(res["virial"].T, num, atol=1.0e-7, rtol=0)
+
+
+HESSIAN = next(e for e in _load("python.json") if e["name"] == "test_interface.hessian")
+
+
+def _numerical_hessian(nums, pos, par, step, ghost=None, **kw):
+    nh = np.zeros((3 * len(nums), 3 * len(nums)))
+    for i in range(len(nums)):
+        for c in range(3):
+            p = pos.copy(); p[i, c] += step
+            gr = O.dispersion(nums, p, par, ghost=ghost, **kw)["gradient"]
+            p[i, c] -= 2 * step
+            gl = O.dispersion(nums, p, par, ghost=ghost, **kw)["gradient"]
+            nh[3 * i + c] = 0.5 * (gr - gl).ravel() / step
+    return nh
+
+
+@pytest.mark.parametrize("ghost", [None, "fixture"])
+def test_oracle_hessian_fixture(ghost):
+    """test_interface.py test_hessian / test_hessian_ghost_atoms: the analytic
+    Hessian is symmetric (abs 1e-12) and matches central differences of the
+    gradient (step 1e-6, abs 1e-7)."""
+    case = HESSIAN
+    nums, pos = case["numbers"], _positions(case)
+    gh = case["ghost"] if ghost else None
+    h = O.hessian(nums, pos, case["param"], ghost=gh)
+    assert not np.isnan(h).any()
+    assert np.abs(h - h.T).max() <= case["tol_sym"]
+    nh = _numerical_hessian(nums, pos, case["param"], case["step"], ghost=gh)
+    assert np.abs(h - nh).max() <= case["tol_abs"]
+
+
+def _dense_cluster(n=16, seed=7):
+    from dftd3 import synthetic as S
+    rng = np.random.default_rng(seed)
+    nums = rng.choice([1, 6, 7, 8], size=n).astype(np.int32)
+    return nums, S.pack_box(rng, n, 0.0, 7.0, 2.0)
+
+
+@pytest.mark.parametrize("damping", sorted(FAMILIES))
+def test_oracle_hessian_families(damping):
+    """Every damping family on a dense cluster (three-body term included
+    where s9 != 0): the analytic Hessian against central differences of the
+    gradient, to 1e-6 of its largest element."""
+    nums, pos = _dense_cluster()
+    par = FAMILIES[damping]
+    h = O.hessian(nums, pos, par)
+    assert np.abs(h - h.T).max() <= 1e-12 * np.abs(h).max()
+    nh = _numerical_hessian(nums, pos, par, 1.0e-5)
+    assert np.abs(h - nh).max() <= 1e-6 * np.abs(h).max()
+
+
+def test_oracle_hessian_periodic_smooth_partition():
+    """A periodic cell with smooth cutoffs, and parts of the work partition
+    that sum to the complete Hessian."""
+    nums, pos, lat = _small_periodic()
+    par = FAMILIES["zero"]
+    cut = (20.0, 12.0, 15.0, 3.0, 2.0)
+    h = O.hessian(nums, pos, par, lattice=lat, cutoff=cut, wrap=False)
+    assert np.abs(h - h.T).max() <= 1e-12
+    nh = _numerical_hessian(nums, pos, par, 1.0e-5, lattice=lat, cutoff=cut, wrap=False)
+    assert np.abs(h - nh).max() <= 1e-7
+    parts = sum(O.hessian(nums, pos, par, lattice=lat, cutoff=cut, wrap=False, part=k, nparts=3) for k in range(3))
+    assert np.abs(parts - h).max() <= 1e-12 * np.abs(h).max()
