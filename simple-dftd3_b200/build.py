@@ -17,7 +17,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "lib" / "libsdftd3_b200.so"
 INCLUDE = PKG.parent / "include"
 
-SOURCES = ["d3_kernels.cu", "d3_pair.cu", "d3_pair_tt.cu", "d3_atm.cu", "d3_atm_mol.cu", "d3_pairwise.cu", "d3_engine.cu", "d3_noalloc.cu", "d3_api.cpp", "d3_tables.c", "d3_params.c"]
+SOURCES = ["d3_kernels.cu", "d3_pair.cu", "d3_pair_tt.cu", "d3_atm.cu", "d3_atm_mol.cu", "d3_pairwise.cu", "d3_hessian.cu", "d3_engine.cu", "d3_noalloc.cu", "d3_api.cpp", "d3_tables.c", "d3_params.c"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -592,9 +592,47 @@ void dftd3_get_pairwise_dispersion(dftd3_error error, dftd3_structure mol, dftd3
     });
 }
 
-void dftd3_get_dispersion_hessian(dftd3_error error, dftd3_structure, dftd3_model, dftd3_param, double*, double*)
+void dftd3_get_dispersion_hessian(dftd3_error error, dftd3_structure mol, dftd3_model disp, dftd3_param param,
+                                  double* energy, double* hessian)
 {
-    if (error) unsupported(error, "The analytical Hessian");
+    // get_dispersion_hessian_api, api.f90:1115-1176: the energy and the
+    // [3n][3n] Hessian (symmetric, so either storage order reads it)
+    if (!error) return;
+    if (!mol) {
+        fail(error, "Molecular structure data is missing");
+        return;
+    }
+    if (!disp) {
+        fail(error, "Dispersion model is missing");
+        return;
+    }
+    if (!param) {
+        fail(error, "Damping parameters are missing");
+        return;
+    }
+    if (!param->supported) {
+        fail(error, "Damping parameters are not initialized");
+        return;
+    }
+    if (!hessian) {
+        fail(error, "Hessian array is missing");
+        return;
+    }
+    if (disp->numbers != mol->numbers) {
+        fail(error, "Dispersion model does not match the molecular structure");
+        return;
+    }
+    if (!finite_all(mol->xyz.data(), mol->xyz.size())) {
+        fail(error, "Non-finite atomic positions");
+        return;
+    }
+    guarded(error, [&] {
+        model_engine(disp, mol);
+        double e = 0.0;
+        disp->engine->evaluate_host(param->damp, mol->xyz.data(), &e, nullptr, nullptr);
+        if (energy) *energy = e;
+        disp->engine->hessian_host(param->damp, mol->xyz.data(), hessian);
+    });
 }
 
 void dftd3_get_counterpoise(dftd3_error error, dftd3_structure, dftd3_gcp, double*, double*, double*)

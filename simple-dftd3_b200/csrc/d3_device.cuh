@@ -154,6 +154,15 @@ void launch_pairwise(const Batch& b, const Species& s, const Damp& d, const Conf
                      const long long* off, long long total, double* c6, double* e2, double* e3,
                      cudaStream_t stream);
 
+// Analytic Hessian of one structure (d3_hessian.cu), FP64, input atom order:
+// pos [n][3], sp, zid, ghost per atom; img_range = the [first, last) image
+// indices of the CN, two-body and three-body lattice points; rvdw [nid][nid];
+// scratch of hessian_scratch_doubles(n); H [3n][3n].
+size_t hessian_scratch_doubles(int n);
+void launch_hessian(const Species& s, const Damp& d, const Config& c, const Partition& p, int n, int nid,
+                    const double* pos, const int* sp, const int* zid, const uint8_t* ghost, const double* img,
+                    const int img_range[6], const double* rvdw, double* scratch, double* H, cudaStream_t stream);
+
 // FMA throughput of the FP64 (fp64=true) or FP32 pipe in TFLOP/s (blocking).
 double measure_fma_peak(bool fp64);
 

@@ -471,6 +471,7 @@ void Engine::ensure_images(cudaStream_t stream)
     }
     check(cudaMemcpyAsync(d_img_, all.data(), sizeof(double) * all.size(), cudaMemcpyHostToDevice, stream), "images");
     check(cudaMemcpyAsync(d_img_off_, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, stream), "img_off");
+    img_off_host_ = off;
     // the host vectors go out of scope: make the copies complete first
     check(cudaStreamSynchronize(stream), "images sync");
     images_valid_ = true;
@@ -652,6 +653,41 @@ void Engine::pairwise_host(const Damp& d, const double* positions, double* energ
     check(cudaMemcpyAsync(energy3, d_pw_ + 2 * total, sizeof(double) * c6mat_total_, cudaMemcpyDeviceToHost, stream),
           "pairwise energy3");
     check(cudaStreamSynchronize(stream), "pairwise");
+}
+
+void Engine::hessian_host(const Damp& d, const double* positions, double* hessian)
+{
+    if (nsys_ != 1) throw Error("The Hessian is evaluated for one structure at a time");
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    cudaStream_t stream = stream_;
+    ensure_images(stream);
+    ensure_workspace(false, false, false);
+    upload_pair_table(d, stream);
+    const int n = natoms_;
+    const size_t nh = 9 * (size_t)n * n;
+    if (!d_hs_) {
+        d_hs_ = dev_alloc<double>(hessian_scratch_doubles(n) + nh);
+        const int nid = tab_.nid();
+        d_rvdw_ = dev_alloc<double>((size_t)nid * nid);
+        check(cudaMemcpy(d_rvdw_, tab_.rvdw.data(), sizeof(double) * nid * nid, cudaMemcpyHostToDevice), "rvdw");
+    }
+    check(cudaMemcpyAsync(d_pos_in_, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, stream), "positions");
+    Batch b;
+    Species s;
+    make_views(b, s);
+    Config c;
+    c.cut_cn = cut_.cn; c.cut2 = cut_.disp2; c.cut3 = cut_.disp3;
+    c.width2 = cut_.width2; c.width3 = cut_.width3;
+    c.grad = true; c.mixed = false;
+    const int range[6] = {img_off_host_[kImgCN * 2], img_off_host_[kImgCN * 2 + 1], img_off_host_[kImgDisp2 * 2],
+                          img_off_host_[kImgDisp2 * 2 + 1], img_off_host_[kImgDisp3 * 2],
+                          img_off_host_[kImgDisp3 * 2 + 1]};
+    double* H = d_hs_ + hessian_scratch_doubles(n);
+    launch_hessian(s, d, c, part_, n, tab_.nid(), d_pos_in_, d_sp_, d_zid_, d_ghost_, d_img_, range, d_rvdw_, d_hs_,
+                   H, stream);
+    check(cudaGetLastError(), "hessian kernels");
+    check(cudaMemcpyAsync(hessian, H, sizeof(double) * nh, cudaMemcpyDeviceToHost, stream), "hessian");
+    check(cudaStreamSynchronize(stream), "hessian");
 }
 
 void Engine::run(const Damp& d, const double* d_positions, double* d_energies, double* d_gradient,

@@ -84,6 +84,10 @@ public:
     // energy2 and energy3 receive [n_s][n_s] per system, one system after the
     // other.  Blocking.
     void pairwise_host(const Damp& d, const double* positions, double* energy2, double* energy3);
+    // Analytic Hessian [3n][3n] of a batch of one structure from host
+    // positions (already wrapped), FP64 (get_dispersion_hessian); the work
+    // partition splits the pair and triple loops.  Blocking.
+    void hessian_host(const Damp& d, const double* positions, double* hessian);
 
     cudaStream_t stream() const { return stream_; }
 
@@ -137,6 +141,9 @@ private:
     void upload_pair_table(const Damp& d, cudaStream_t stream);
     void make_views(Batch& b, Species& s) const;
     void order_atoms(const Damp& d, const double* d_positions, const Batch& b, bool mixed, cudaStream_t stream);
+    double* d_hs_ = nullptr;             // Hessian scratch and result
+    double* d_rvdw_ = nullptr;           // [nid][nid] van der Waals radii (Hessian damping kernels)
+    std::vector<int> img_off_host_;      // host copy of the image offsets
     double* d_pw_ = nullptr;             // pairwise decomposition: C6, energy2, energy3 (3 x sum n_s^2)
     long long* d_pw_off_ = nullptr;
     void run(const Damp& d, const double* d_positions, double* d_energies, double* d_gradient,

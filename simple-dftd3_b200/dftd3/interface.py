@@ -278,7 +278,8 @@ class DispersionModel(Structure):
         return {"additive pairwise energy": _pair_disp2, "non-additive pairwise energy": _pair_disp3}
 
     def get_hessian(self, param: DampingParam) -> dict:
-        """Analytical Hessian (reported as not supported)."""
+        """Analytic Hessian of the dispersion energy, (3n, 3n) in Hartree/Bohr^2 (FP64),
+        and the energy."""
         _energy = np.array(0.0)
         _hessian = np.zeros((3 * len(self), 3 * len(self)))
         library.get_dispersion_hessian(self._mol, self._disp, param._param, _energy, _hessian)
