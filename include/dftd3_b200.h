@@ -29,6 +29,15 @@ dftd3_b200_set_model_precision(dftd3_error /* error */,
                                dftd3_model /* model */,
                                int /* precision */);
 
+/* Replay the evaluation of a model created by dftd3_new_d3_model as one
+ * captured CUDA graph (enable != 0), as dftd3_b200_set_batch_graph does for a
+ * batch: the first dftd3_get_dispersion after enabling captures, later calls
+ * with new positions replay it. */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_set_model_graph(dftd3_error /* error */,
+                           dftd3_model /* model */,
+                           int /* enable */);
+
 /* Create a batch of nsys independent systems.  Atoms are concatenated:
  * natoms[nsys], numbers[sum natoms].  lattices[nsys][3][3] and
  * periodic[nsys][3] may be NULL for molecules.  The batch keeps device

@@ -46,6 +46,7 @@ struct _dftd3_model {
     int precision = DFTD3_B200_PRECISION_FP64;
     bool has_tuning = false;
     d3::Tuning tuning;
+    bool graph = false;
     std::unique_ptr<d3::Engine> engine;
 };
 
@@ -509,6 +510,7 @@ static void model_engine(dftd3_model disp, dftd3_structure mol)
         disp->engine->set_partition(disp->part, disp->nparts, false);
         disp->engine->set_precision(disp->precision);
         if (disp->has_tuning) disp->engine->set_tuning(disp->tuning);
+        if (disp->graph) disp->engine->set_graph(true);
     }
     disp->engine->set_lattices(mol->lattice);
 }
@@ -677,6 +679,17 @@ void dftd3_b200_set_model_precision(dftd3_error error, dftd3_model model, int pr
     }
     model->precision = precision;
     if (model->engine) model->engine->set_precision(precision);
+}
+
+void dftd3_b200_set_model_graph(dftd3_error error, dftd3_model model, int enable)
+{
+    if (!error) return;
+    if (!model) {
+        fail(error, "D3 dispersion model is missing");
+        return;
+    }
+    model->graph = enable != 0;
+    if (model->engine) guarded(error, [&] { model->engine->set_graph(model->graph); });
 }
 
 dftd3_b200_batch dftd3_b200_new_batch(dftd3_error error, int nsys, const int* natoms, const int* numbers,

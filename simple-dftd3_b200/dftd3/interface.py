@@ -249,6 +249,12 @@ class DispersionModel(Structure):
         """Launch shapes (extension, see dftd3_b200_set_model_tuning)."""
         library.set_model_tuning(self._disp, morton_cell, pair_split, atm_blocks_per_sm, atm_mol)
 
+    def set_graph(self, enable: bool = True) -> None:
+        """Replay the evaluation as one captured CUDA graph (extension, see
+        dftd3_b200_set_model_graph): worth it for many evaluations of one
+        structure with new positions."""
+        library.set_model_graph(self._disp, enable)
+
     def set_precision(self, precision: str) -> None:
         """'fp64' (default) or 'mixed' (FP32 pair arithmetic, FP64 accumulation)."""
         modes = {"fp64": library.PRECISION_FP64, "mixed": library.PRECISION_MIXED}

@@ -183,6 +183,10 @@ def set_model_precision(disp: ModelHandle, precision: int) -> None:
     error_check(lib.dftd3_b200_set_model_precision)(disp.handle, precision)
 
 
+def set_model_graph(disp: ModelHandle, enable: bool) -> None:
+    error_check(lib.dftd3_b200_set_model_graph)(disp.handle, 1 if enable else 0)
+
+
 def new_zero_damping(s6: float, s8: float, s9: float, rs6: float, rs8: float, alp: float) -> ParamHandle:
     return ParamHandle.with_gc(error_check(lib.dftd3_new_zero_damping)(s6, s8, s9, rs6, rs8, alp))
 

@@ -131,3 +131,38 @@ def test_device_api_graph_with_parameter_derivatives():
         out[graph] = [t.cpu().numpy() for t in (e, g, sg, pg)]
     for a, b in zip(out[False], out[True]):
         assert np.abs(a - b).max() <= 1e-12 * max(np.abs(a).max(), 1e-30)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_model_graph_replay(precision):
+    """dftd3_get_dispersion of a model with dftd3_b200_set_model_graph: the
+    first call captures, later calls with new positions and a new lattice
+    replay, each matching the oracle."""
+    from dftd3 import synthetic as S
+    from dftd3.interface import DispersionModel, RationalDampingParam
+    import oracle_ref as O
+    rng = np.random.default_rng(41)
+    lat = S.triclinic(14.0, 14.5, 15.0, 89.0, 91.0, 92.0)
+    num = rng.choice([1, 6, 8], size=48).astype(np.int32)
+    pos = S.pack_cell(rng, 48, lat, 2.0)
+    par = dict(S.PBE_BJ, damping="rational", s9=1.0)
+    # cutoffs away from the cell edges: a self-image exactly on a cutoff
+    # sphere is in or out by the last bit of r^2
+    cut = (31.1, 16.3, 21.7, 0.0, 0.0)
+    model = DispersionModel(num, pos, lat, np.array([True] * 3))
+    model.set_realspace_cutoff(*cut)
+    model.set_precision(precision)
+    model.set_graph(True)
+    param = RationalDampingParam(**{k: par[k] for k in ("s6", "s8", "a1", "a2", "alp", "s9")})
+    for step in range(4):
+        p = pos + rng.normal(scale=0.05, size=pos.shape)
+        la = lat * (1.0 + 0.01 * step)
+        model.update(p @ np.linalg.inv(lat) @ la, la)
+        res = model.get_dispersion(param, grad=True)
+        ref = O.dispersion(num, p @ np.linalg.inv(lat) @ la, par, lattice=la, periodic=[True] * 3, cutoff=cut)
+        if precision == "fp64":
+            assert abs(float(res["energy"]) - ref["energy"]) <= RTOL64 * abs(ref["energy"])
+            assert np.abs(res["gradient"] - ref["gradient"]).max() <= GTOL64 * np.abs(ref["gradient"]).max()
+        else:
+            assert abs(float(res["energy"]) - ref["energy"]) <= 1e-7 * abs(ref["energy"])
+            assert np.abs(res["gradient"] - ref["gradient"]).max() <= 1e-7
