@@ -151,3 +151,36 @@ def test_family_constructor_arguments():
         ZDampingParam(s8=1.0)
     with pytest.raises(TypeError):
         ZDampingParam(a1=200770.0, method="abc")
+
+
+def test_pairwise_and_hessian_argument_errors():
+    """dftd3_get_pairwise_dispersion and dftd3_get_dispersion_hessian check
+    their handles before any device work (api.f90:1115-1236)."""
+    from dftd3 import library as L
+    from dftd3.interface import RationalDampingParam
+
+    def message(call, *args):
+        err = L.new_error()
+        call(err, *args)
+        assert L.lib.dftd3_check_error(err) == 1
+        buf = L.ffi.new("char[]", 512)
+        L.lib.dftd3_get_error(err, buf, L.ffi.NULL)
+        return L.ffi.string(buf).decode()
+
+    n = L.ffi.NULL
+    e = np.zeros(4)
+    p = L.ffi.cast("double*", e.ctypes.data)
+    assert message(L.lib.dftd3_get_pairwise_dispersion, n, n, n, p, p) == "Molecular structure data is missing"
+    assert message(L.lib.dftd3_get_dispersion_hessian, n, n, n, p, p) == "Molecular structure data is missing"
+    numbers = np.array([8, 1, 1], dtype=np.int32)
+    xyz = np.array([[0.0, 0.0, 0.0], [1.8, 0.0, 0.0], [-0.5, 1.7, 0.0]])
+    mol = L.new_structure(3, numbers, xyz, None, None)
+    disp = L.new_d3_model(mol)
+    assert message(L.lib.dftd3_get_pairwise_dispersion, mol.handle, disp.handle, n, p, p) == \
+        "Damping parameters are missing"
+    param = RationalDampingParam(method="pbe0")._param
+    assert message(L.lib.dftd3_get_pairwise_dispersion, mol.handle, disp.handle, param.handle, p, n) == \
+        "Pairwise energy arrays are missing"
+    assert message(L.lib.dftd3_get_dispersion_hessian, mol.handle, disp.handle, param.handle, p, n) == \
+        "Hessian array is missing"
+    assert message(L.lib.dftd3_b200_set_model_graph, n, 1) == "D3 dispersion model is missing"
