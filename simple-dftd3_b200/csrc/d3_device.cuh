@@ -63,6 +63,11 @@ struct PairUnits {
     void* dU = nullptr;                  // same with dgw
     double* unit_i = nullptr;            // [nunits][kTile][15]
     double* unit_j = nullptr;            // [nunits][kTile][4]
+    // chain-rule sums of the CN pass per (item, j, lane), or null: the CN
+    // pass stores them and the chain rule reads them instead of evaluating
+    // the terms again (systems of one translation chunk, cn_store_bytes)
+    void* cn_store = nullptr;            // [items][kTile][9][kTile] (R)
+    unsigned char* cn_store_ok = nullptr;   // [items]: the item stored its sums
 };
 
 constexpr int kTile = 32;               // atoms per tile (one warp)
@@ -210,6 +215,8 @@ void launch_cn_chain_rule_tiled(const Batch& b, const Species& s, const Config& 
 // gather (d3_pair_tt.cu); writes e_atom, dEdcn, grad, sig_atom, pg_atom.
 // Coordination number (chain = false, writes cn) or its chain rule (chain =
 // true, adds to grad and sig_atom) over the same units (d3_pair_tt.cu).
+size_t cn_store_bytes(const PairUnits& pu, bool mixed);   // d3_pair_tt.cu
+constexpr int kCnStoreChunk = 128; // translations of a system the stored chain rule covers
 void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Partition& p, const Work& w,
                      const PairUnits& pu, bool chain, cudaStream_t stream);
 size_t pair_unit_slot_doubles();   // per unit: i and j slots

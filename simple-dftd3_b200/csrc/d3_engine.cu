@@ -586,6 +586,17 @@ void Engine::upload_pair_table(const Damp& d, cudaStream_t stream)
     pair_valid_ = true;
 }
 
+bool Engine::cn_single_chunk() const
+{
+    // every system's CN lattice points within one chunk of the tile sweep
+    if (img_off_host_.empty()) return false;
+    for (int sy = 0; sy < nsys_; sy++) {
+        const int k0 = img_off_host_[kImgCN * (nsys_ + 1) + sy], k1 = img_off_host_[kImgCN * (nsys_ + 1) + sy + 1];
+        if (k1 - k0 > kCnStoreChunk) return false;
+    }
+    return true;
+}
+
 void Engine::make_views(Batch& b, Species& s) const
 {
     b.nsys = nsys_; b.natoms = natoms_; b.nid = tab_.nid();
@@ -643,6 +654,8 @@ void Engine::pairwise_host(const Damp& d, const double* positions, double* energ
     Work w = work_;
     w.counts = nullptr; w.e3_atom = nullptr; w.sig3_atom = nullptr; w.pg_atom = nullptr;
     pu_.split = tune_.pair_split ? tune_.pair_split : (auto_split_ == 1 ? 1 : 4);
+    pu_.cn_store = nullptr;
+    pu_.cn_store_ok = nullptr;
     order_atoms(d, d_pos_in_, b, false, stream);
     launch_cn_units(b, s, c, Partition{}, w, pu_, false, stream);
     launch_weights(b, s, c, w, stream);
@@ -711,6 +724,25 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     // automatic split: one item per tile pair for molecules; for periodic
     // systems two (mixed form) or four (FP64 form), measured on B200
     pu_.split = tune_.pair_split ? tune_.pair_split : (auto_split_ == 1 ? 1 : (mixed_ ? 2 : 4));
+    // the CN pass keeps the chain rule's per-pair sums when every system's CN
+    // translations fit one chunk and the buffer stays below kCnStoreCap
+    pu_.cn_store = nullptr;
+    pu_.cn_store_ok = nullptr;
+    if (grad && cn_single_chunk()) {
+        const size_t bytes = cn_store_bytes(pu_, mixed_);
+        if (bytes <= kCnStoreCap && (bytes <= cn_store_cap_ || !capturing_)) {
+            if (bytes > cn_store_cap_) {
+                free_block(d_cn_store_);
+                void* ok = d_cn_store_ok_;
+                free_block(ok);
+                d_cn_store_ = dev_alloc<unsigned char>(bytes);
+                d_cn_store_ok_ = dev_alloc<unsigned char>((size_t)pu_.nunits * 4);
+                cn_store_cap_ = bytes;
+            }
+            pu_.cn_store = d_cn_store_;
+            pu_.cn_store_ok = d_cn_store_ok_;
+        }
+    }
     Work w = work_;
     w.counts = counting_ ? d_counts_ : nullptr;
     w.e3_atom = nullptr;

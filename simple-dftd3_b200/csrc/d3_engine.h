@@ -140,6 +140,11 @@ private:
     void ensure_workspace(bool grad, bool param_grad, bool threebody);
     void upload_pair_table(const Damp& d, cudaStream_t stream);
     void make_views(Batch& b, Species& s) const;
+    bool cn_single_chunk() const;
+    static constexpr size_t kCnStoreCap = size_t(768) << 20;   // bytes of stored chain-rule sums at most
+    void* d_cn_store_ = nullptr;
+    unsigned char* d_cn_store_ok_ = nullptr;
+    size_t cn_store_cap_ = 0;
     void order_atoms(const Damp& d, const double* d_positions, const Batch& b, bool mixed, cudaStream_t stream);
     double* d_hs_ = nullptr;             // Hessian scratch and result
     double* d_rvdw_ = nullptr;           // [nid][nid] van der Waals radii (Hessian damping kernels)

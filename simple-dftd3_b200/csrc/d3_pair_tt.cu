@@ -30,6 +30,7 @@ constexpr int kTTThreads = 32 * kTTWarps;
 constexpr int kTTChunk = 128;     // translations tested per pass
 constexpr int kUnitI = 15;        // per-lane i sums: E, dE/dCN, g(3), sigma(6), dE/dparam(4)
 constexpr int kUnitJ = 4;         // per-lane j sums: dE/dCN, g(3)
+constexpr int kCnStore = 9;       // stored chain-rule sums per (i, j): countd (3), countd v^T (6)
 constexpr int kSplitMax = 4;      // a unit is evaluated as 1, 2 (translation halves) or 4 items
                                   // (and j-tile halves); slots are sized for the largest split
 
@@ -556,11 +557,16 @@ constexpr double kKcnTT = 16.0;   // ncoord.f90:31
 // (CHAIN = true, ncoord.f90:152-228) over the tile-pair units with the CN
 // lattice points.  Slots: CN: i [cn], j [cn]; chain: i [g(3), sigma(6)],
 // j [g(3)].
-template <class R, bool CHAIN>
+// MODE 0: coordination numbers; 1: CN chain rule; 2: coordination numbers
+// and, per (i, j) of the item, the translation sums of the chain rule's
+// countd = dcf v / r and countd v^T (ncoord.f90:198-206) into `store`, for
+// k_cn_chain_stored (systems of one translation chunk only).
+template <class R, int MODE>
 __global__ void __launch_bounds__(kTTThreads)
 k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, int nunits, int split, double* unit_i,
-        double* unit_j)
+        double* unit_j, R* store, unsigned char* store_ok)
 {
+    constexpr bool CHAIN = MODE == 1, STORE = MODE == 2;
     using V = typename T4<R>::type;
     __shared__ V sth[kTTWarps][kTTChunk];
     __shared__ V stl[kTTWarps][kTTChunk];
@@ -602,6 +608,7 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
     double b0 = 0, b1 = 0, b2 = 0;                                                   // cn | g(3) of j
     int pending = 0;
     unsigned long long nterm = 0;
+    bool ran = false;          // STORE: this item evaluated its (single) chunk
     auto flush = [&]() {
         a0 += double(t0_); t0_ = R(0);
         if (CHAIN) {
@@ -619,6 +626,7 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
         const int qbeg = th * qhalf, qend = min(nreach, qbeg + qhalf);
         if (qbeg >= qend) continue;
         const int jl0 = jh * (kTile / splitJ), jl1 = min(nj, jl0 + kTile / splitJ);
+        ran = true;
         for (int jl = jl0; jl < jl1; jl++) {
             const int j = ja0 + jl;
             const bool self = diag && jl == lane;
@@ -661,7 +669,24 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
                     const R r2 = vx * vx + vy * vy + vz * vz;
                     if (!valid || r2 > cut2 || r2 < R(1.0e-12)) continue;
                     nterm++;
-                    if (!CHAIN) {
+                    if (STORE) {
+                        // the count and the chain rule's countd of the same term
+                        R cf, f;
+                        if constexpr (sizeof(R) == 8) {
+                            const R r1 = sqrt(r2);
+                            cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / r1 - R(1))));
+                            f = -cf * (R(1) - cf) * R(kKcnTT) * rc / r2 / r1;
+                        } else {
+                            const R ir = rsqrtf(r2);
+                            cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * ir - R(1))));
+                            f = -cf * (R(1) - cf) * R(kKcnTT) * rc * (ir * ir * ir);
+                        }
+                        sc += cf;
+                        const R cx = f * vx, cy = f * vy, cz = f * vz;
+                        scx += cx; scy += cy; scz += cz;
+                        sxx += cx * vx; syy += cy * vy; szz += cz * vz;
+                        sxy += cx * vy; sxz += cx * vz; syz += cy * vz;
+                    } else if (!CHAIN) {
                         R cf;
                         if constexpr (sizeof(R) == 8) cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / sqrt(r2) - R(1))));
                         else cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * rsqrtf(r2) - R(1))));
@@ -685,6 +710,12 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
                         sxy += cx * vy; sxz += cx * vz; syz += cy * vz;
                     }
                 }
+            }
+            if (STORE) {
+                R* out = store + ((size_t)item * kTile + (jl - jl0)) * kCnStore * kTile + lane;
+                const R vals[kCnStore] = {scx, scy, scz, sxx, syy, szz, sxy, sxz, syz};
+#pragma unroll
+                for (int v = 0; v < kCnStore; v++) out[v * kTile] = vals[v];
             }
             if (!CHAIN) {
                 t0_ += sc;
@@ -718,10 +749,68 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
         oi[3] = a4; oi[4] = a5; oi[5] = a6; oi[6] = a7; oi[7] = a8; oi[8] = a0;
         oj[0] = b0; oj[1] = b1; oj[2] = b2;
     }
+    if (STORE && lane == 0) store_ok[item] = ran ? 1 : 0;
     if (!CHAIN && w.counts) {
         for (int off = 16; off > 0; off >>= 1) nterm += __shfl_xor_sync(0xffffffffu, nterm, off);
         if (lane == 0) atomicAdd(w.counts + 2, nterm);
     }
+}
+
+// CN chain rule from the sums k_cn_tt<R, 2> stored: per (i, j) of the item
+// the weight dE/dCN_i + dE/dCN_j (dE/dCN_i for j = i) times the stored
+// countd sums (ncoord.f90:205-213), into the same slots as k_cn_tt<R, 1>.
+template <class R>
+__global__ void __launch_bounds__(kTTThreads)
+k_cn_chain_stored(Batch b, Config c, Partition p, Work w, const int2* units, int nunits, int split, const R* store,
+                  const unsigned char* store_ok, double* unit_i, double* unit_j)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int item = blockIdx.x * kTTWarps + wid;
+    if (item >= nunits * split) return;
+    const int u = item / split, sub = item % split;
+    const int splitT = split >= 2 ? 2 : 1, splitJ = split / splitT;
+    const int jh = sub / splitT;
+    const int it = units[u].x, jt = units[u].y;
+    const int sys = b.tile_sys[it];
+    const int t0 = b.tile_off[sys];
+    const int as = b.atom_off[sys], ae = b.atom_off[sys + 1];
+    const int ia0 = as + kTile * (it - t0), ja0 = as + kTile * (jt - t0);
+    const int ni = min(kTile, ae - ia0), nj = min(kTile, ae - ja0);
+    const bool diag = it == jt;
+    const bool ivalid = lane < ni;
+    const int ic = ivalid ? ia0 + lane : ia0;
+    const int li = b.local[ic];
+    const double dei = w.dEdcn[ic];
+    double g[3] = {0, 0, 0}, sg[6] = {0, 0, 0, 0, 0, 0}, bj[3] = {0, 0, 0};
+    if (store_ok[item]) {
+        const int jl0 = jh * (kTile / splitJ), jl1 = min(nj, jl0 + kTile / splitJ);
+        for (int jl = jl0; jl < jl1; jl++) {
+            const int j = ja0 + jl;
+            const bool self = diag && jl == lane;
+            bool valid = ivalid && (!diag || jl <= lane);
+            if (valid && c.cn_partitioned && p.nparts > 1) valid = tt_owns(p, li, b.local[j]);
+            if (!__any_sync(0xffffffffu, valid)) continue;
+            const R* in = store + ((size_t)item * kTile + (jl - jl0)) * kCnStore * kTile + lane;
+            const double dsum = dei + w.dEdcn[j];
+            const double dsig = self ? dei : dsum;
+            double j0 = 0.0, j1 = 0.0, j2 = 0.0;
+            if (!self) {
+                const double sx = double(in[0]), sy = double(in[kTile]), sz = double(in[2 * kTile]);
+                g[0] += sx * dsum; g[1] += sy * dsum; g[2] += sz * dsum;
+                j0 = -sx * dsum; j1 = -sy * dsum; j2 = -sz * dsum;
+            }
+#pragma unroll
+            for (int v = 0; v < 6; v++) sg[v] += double(in[(3 + v) * kTile]) * dsig;
+            j0 = wsum_tt<double>(j0); j1 = wsum_tt<double>(j1); j2 = wsum_tt<double>(j2);
+            if (lane == jl) { bj[0] += j0; bj[1] += j1; bj[2] += j2; }
+        }
+    }
+    double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
+    double* oj = unit_j + ((size_t)item * kTile + lane) * kUnitJ;
+    // g(3), sigma xx yy zz xy xz yz (the layout of k_cn_tt<R, 1>)
+    oi[0] = g[0]; oi[1] = g[1]; oi[2] = g[2];
+    oi[3] = sg[0]; oi[4] = sg[1]; oi[5] = sg[2]; oi[6] = sg[3]; oi[7] = sg[4]; oi[8] = sg[5];
+    oj[0] = bj[0]; oj[1] = bj[1]; oj[2] = bj[2];
 }
 
 // Gather of the CN (assign) or chain-rule (add to gradient and virial) slots,
@@ -808,17 +897,39 @@ void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Pa
 {
     if (b.natoms <= 0) return;
     const int blocks = (pu.nunits * pu.split + kTTWarps - 1) / kTTWarps;
+    const bool stored = pu.cn_store != nullptr;
+#define D3_CN(R, MODE)                                                                                     \
+    k_cn_tt<R, MODE><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.split,     \
+                                                        pu.unit_i, pu.unit_j, (R*)pu.cn_store, pu.cn_store_ok)
     if (pu.nunits > 0) {
-        if (chain) {
-            if (c.mixed) k_cn_tt<float, true><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.split, pu.unit_i, pu.unit_j);
-            else k_cn_tt<double, true><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.split, pu.unit_i, pu.unit_j);
+        if (chain && stored) {
+            if (c.mixed)
+                k_cn_chain_stored<float><<<blocks, kTTThreads, 0, stream>>>(
+                    b, c, p, w, pu.units, pu.nunits, pu.split, (const float*)pu.cn_store, pu.cn_store_ok, pu.unit_i,
+                    pu.unit_j);
+            else
+                k_cn_chain_stored<double><<<blocks, kTTThreads, 0, stream>>>(
+                    b, c, p, w, pu.units, pu.nunits, pu.split, (const double*)pu.cn_store, pu.cn_store_ok, pu.unit_i,
+                    pu.unit_j);
+        } else if (chain) {
+            if (c.mixed) D3_CN(float, 1);
+            else D3_CN(double, 1);
+        } else if (stored) {
+            if (c.mixed) D3_CN(float, 2);
+            else D3_CN(double, 2);
         } else {
-            if (c.mixed) k_cn_tt<float, false><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.split, pu.unit_i, pu.unit_j);
-            else k_cn_tt<double, false><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.split, pu.unit_i, pu.unit_j);
+            if (c.mixed) D3_CN(float, 0);
+            else D3_CN(double, 0);
         }
     }
+#undef D3_CN
     if (chain) k_cn_gather<true><<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
     else k_cn_gather<false><<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
+}
+
+size_t cn_store_bytes(const PairUnits& pu, bool mixed)
+{
+    return (size_t)pu.nunits * pu.split * kTile * kCnStore * kTile * (mixed ? sizeof(float) : sizeof(double));
 }
 
 size_t pair_unit_slot_doubles() { return (size_t)kSplitMax * kTile * (kUnitI + kUnitJ); }
