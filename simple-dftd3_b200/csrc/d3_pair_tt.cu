@@ -784,25 +784,40 @@ k_cn_chain_stored(Batch b, Config c, Partition p, Work w, const int2* units, int
     double g[3] = {0, 0, 0}, sg[6] = {0, 0, 0, 0, 0, 0}, bj[3] = {0, 0, 0};
     if (store_ok[item]) {
         const int jl0 = jh * (kTile / splitJ), jl1 = min(nj, jl0 + kTile / splitJ);
-        for (int jl = jl0; jl < jl1; jl++) {
-            const int j = ja0 + jl;
-            const bool self = diag && jl == lane;
-            bool valid = ivalid && (!diag || jl <= lane);
-            if (valid && c.cn_partitioned && p.nparts > 1) valid = tt_owns(p, li, b.local[j]);
-            if (!__any_sync(0xffffffffu, valid)) continue;
-            const R* in = store + ((size_t)item * kTile + (jl - jl0)) * kCnStore * kTile + lane;
-            const double dsum = dei + w.dEdcn[j];
-            const double dsig = self ? dei : dsum;
-            double j0 = 0.0, j1 = 0.0, j2 = 0.0;
-            if (!self) {
-                const double sx = double(in[0]), sy = double(in[kTile]), sz = double(in[2 * kTile]);
-                g[0] += sx * dsum; g[1] += sy * dsum; g[2] += sz * dsum;
-                j0 = -sx * dsum; j1 = -sy * dsum; j2 = -sz * dsum;
+        // the sums of NQ partners are loaded together (memory-level parallelism);
+        // sums of a partner that no lane of the item took were not stored and
+        // are loaded but not used
+        constexpr int NQ = sizeof(R) == 4 ? 4 : 2;
+        for (int jg = jl0; jg < jl1; jg += NQ) {
+            R sv[NQ][kCnStore];
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                const R* in = store + ((size_t)item * kTile + min(jg + q, jl1 - 1) - jl0) * kCnStore * kTile + lane;
+#pragma unroll
+                for (int v = 0; v < kCnStore; v++) sv[q][v] = in[v * kTile];
             }
 #pragma unroll
-            for (int v = 0; v < 6; v++) sg[v] += double(in[(3 + v) * kTile]) * dsig;
-            j0 = wsum_tt<double>(j0); j1 = wsum_tt<double>(j1); j2 = wsum_tt<double>(j2);
-            if (lane == jl) { bj[0] += j0; bj[1] += j1; bj[2] += j2; }
+            for (int q = 0; q < NQ; q++) {
+                const int jl = jg + q;
+                if (jl >= jl1) break;
+                const int j = ja0 + jl;
+                const bool self = diag && jl == lane;
+                bool valid = ivalid && (!diag || jl <= lane);
+                if (valid && c.cn_partitioned && p.nparts > 1) valid = tt_owns(p, li, b.local[j]);
+                if (!__any_sync(0xffffffffu, valid)) continue;
+                const double dsum = dei + w.dEdcn[j];
+                const double dsig = self ? dei : dsum;
+                double j0 = 0.0, j1 = 0.0, j2 = 0.0;
+                if (!self) {
+                    const double sx = double(sv[q][0]), sy = double(sv[q][1]), sz = double(sv[q][2]);
+                    g[0] += sx * dsum; g[1] += sy * dsum; g[2] += sz * dsum;
+                    j0 = -sx * dsum; j1 = -sy * dsum; j2 = -sz * dsum;
+                }
+#pragma unroll
+                for (int v = 0; v < 6; v++) sg[v] += double(sv[q][3 + v]) * dsig;
+                j0 = wsum_tt<double>(j0); j1 = wsum_tt<double>(j1); j2 = wsum_tt<double>(j2);
+                if (lane == jl) { bj[0] += j0; bj[1] += j1; bj[2] += j2; }
+            }
         }
     }
     double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
