@@ -1,14 +1,20 @@
-"""Distribution of one evaluation over the processes of a torch.distributed
-group: the counterpart of the reference's MPI path (dftd3_set_model_mpi_comm,
-api.f90:483-506; get_dispersion_mpi_atomic, mpi.f90), with NCCL (GPU
-buffers) or gloo (host buffers) in place of MPI.
+"""Distribution of dispersion work over the processes of a torch.distributed
+group (one GPU per process), with NCCL (GPU buffers) or gloo (host buffers).
 
-Every process evaluates its share of the pair and triple loops (pair
-ownership of partition.f90:127-147); the coordination numbers and dE/dCN are
-summed over the group before they are used (disp.f90:120-126,166-171) and the
-results once at the end, so every process receives the complete energies,
-gradient and virial.  The library calls the reducer defined here between its
-kernel launches (``dftd3_b200_set_batch_reducer``).
+* One large system (ShardedDispersion): the counterpart of the reference's
+  MPI path (dftd3_set_model_mpi_comm, api.f90:483-506;
+  get_dispersion_mpi_atomic, mpi.f90).  Every process evaluates its share of
+  the pair and triple loops (pair ownership of partition.f90:127-147); the
+  coordination numbers and dE/dCN are summed over the group before they are
+  used (disp.f90:120-126,166-171) and the results once at the end, so every
+  process receives the complete energies, gradient and virial.  The library
+  calls the reducer defined here between its kernel launches
+  (``dftd3_b200_set_batch_reducer``).
+* Many independent systems (shard_systems, gather_results): whole systems
+  are dealt to the processes in bins of about equal cost, each process
+  evaluates its bin as one batch with no exchange during the evaluation, and
+  the per-system results are gathered once at the end if every process needs
+  them.
 """
 from typing import Optional, Sequence
 
@@ -96,3 +102,57 @@ class ShardedDispersion:
         """Device-pointer evaluation (see library.get_dispersion_device)."""
         library.get_dispersion_device(self.batch, param, d_positions, None, d_energies, d_gradient, d_sigma, 0,
                                       stream)
+
+
+def system_cost(natoms: int, periodic: bool = False) -> float:
+    """Relative cost of one system: its pair work plus its triple work (the
+    triple loop dominates from a few dozen atoms on).  Periodic systems
+    count their lattice images through a larger effective atom count."""
+    n = float(natoms) * (8.0 if periodic else 1.0)
+    return n * n + n * n * n / 64.0
+
+
+def shard_systems(costs: Sequence[float], nparts: int) -> list:
+    """Deal systems to nparts bins of about equal total cost: the largest
+    system first, each to the bin with the smallest total so far (ties to
+    the lowest bin).  Returns one ascending list of system indices per bin;
+    every process computing it from the same costs gets the same bins."""
+    if nparts < 1:
+        raise ValueError("nparts must be positive")
+    order = sorted(range(len(costs)), key=lambda k: (-float(costs[k]), k))
+    load = [0.0] * nparts
+    bins = [[] for _ in range(nparts)]
+    for k in order:
+        b = min(range(nparts), key=lambda q: (load[q], q))
+        bins[b].append(k)
+        load[b] += float(costs[k])
+    return [sorted(b) for b in bins]
+
+
+def gather_results(local: dict, indices: Sequence[int], nsys: int, group=None) -> dict:
+    """Per-system results of every process's bin, in system order, on every
+    process: ``local`` holds this process's "energy" (len(indices)) and
+    optionally "gradient" (a list of (n_k, 3) arrays) and "virial"
+    ((len(indices), 3, 3)); ``indices`` are its systems.  One all-gather of
+    host objects (works with the gloo and the NCCL backend)."""
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    parts = [None] * world
+    payload = {"indices": list(indices), "energy": np.asarray(local["energy"], dtype=float).tolist()}
+    if "gradient" in local:
+        payload["gradient"] = [np.asarray(g, dtype=float).tolist() for g in local["gradient"]]
+        payload["virial"] = np.asarray(local["virial"], dtype=float).tolist()
+    dist.all_gather_object(parts, payload, group=group)
+    energy = np.zeros(nsys)
+    gradient = [None] * nsys if "gradient" in local else None
+    virial = np.zeros((nsys, 3, 3)) if "gradient" in local else None
+    for part in parts:
+        for pos, k in enumerate(part["indices"]):
+            energy[k] = part["energy"][pos]
+            if gradient is not None:
+                gradient[k] = np.asarray(part["gradient"][pos])
+                virial[k] = np.asarray(part["virial"][pos])
+    out = {"energy": energy}
+    if gradient is not None:
+        out.update(gradient=gradient, virial=virial)
+    return out

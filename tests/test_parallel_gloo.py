@@ -127,3 +127,70 @@ def test_partition_parts_differ_from_serial():
              for p in range(2)]
     assert all(abs(p["energy"] - ref["energy"]) > 1e-6 * abs(ref["energy"]) for p in parts)
     assert abs(sum(p["energy"] for p in parts) - ref["energy"]) <= 1e-12 * abs(ref["energy"])
+
+
+def test_shard_systems_balance():
+    """Longest-first binning: every system in exactly one bin, bins
+    deterministic and within the largest system's cost of each other."""
+    from dftd3 import parallel
+    rng = np.random.default_rng(3)
+    sizes = np.exp(rng.uniform(np.log(8), np.log(257), size=500)).astype(int)
+    costs = [parallel.system_cost(n) for n in sizes]
+    for nparts in (1, 2, 3, 8):
+        bins = parallel.shard_systems(costs, nparts)
+        assert sorted(k for b in bins for k in b) == list(range(len(sizes)))
+        assert bins == parallel.shard_systems(costs, nparts)
+        loads = [sum(costs[k] for k in b) for b in bins]
+        assert max(loads) - min(loads) <= max(costs)
+    assert parallel.system_cost(64, periodic=True) > parallel.system_cost(64)
+
+
+def _gloo_batch_rank(rank, world, port, queue):
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    sys.path[:0] = [str(root / "tests"), str(root / "simple-dftd3_b200")]
+    import datetime
+    import torch.distributed as dist
+    import oracle_ref
+    from dftd3 import parallel, synthetic as S
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        d = S.batch4096(nmol=9, seed=17, nmin=6, nmax=20)
+        par = dict(S.PBE_BJ, damping="rational", s9=1.0)
+        bins = parallel.shard_systems([parallel.system_cost(len(n)) for n in d["numbers"]], world)
+        mine = bins[rank]
+        # this process's bin (the oracle stands in for the GPU batch here)
+        res = [oracle_ref.dispersion(d["numbers"][k], d["positions"][k], par) for k in mine]
+        local = {"energy": [r["energy"] for r in res], "gradient": [r["gradient"] for r in res],
+                 "virial": [r["virial"] for r in res]}
+        out = parallel.gather_results(local, mine, len(d["numbers"]))
+        queue.put((rank, out["energy"].tolist(), [g.tolist() for g in out["gradient"]]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_two_ranks_batch_shards():
+    """Two processes evaluate disjoint bins of a batch and both end with
+    every system's result, equal to evaluating the whole batch in one."""
+    import torch.multiprocessing as mp
+    from dftd3 import synthetic as S
+    ctx = mp.get_context("spawn")
+    queue = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gloo_batch_rank, args=(r, 2, port, queue)) for r in range(2)]
+    for p in procs:
+        p.start()
+    results = [queue.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    d = S.batch4096(nmol=9, seed=17, nmin=6, nmax=20)
+    par = dict(S.PBE_BJ, damping="rational", s9=1.0)
+    for _, energies, grads in results:
+        for k in range(9):
+            ref = O.dispersion(d["numbers"][k], d["positions"][k], par)
+            # the oracle's threaded sums are not bit-reproducible between runs
+            assert abs(energies[k] - ref["energy"]) <= 1e-12 * abs(ref["energy"])
+            assert np.abs(np.asarray(grads[k]) - ref["gradient"]).max() <= 1e-12 * np.abs(ref["gradient"]).max()
