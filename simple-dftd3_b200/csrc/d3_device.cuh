@@ -58,15 +58,14 @@ struct PairUnits {
     const int2* units = nullptr;         // [nunits] global tile indices (it, jt)
     int nunits = 0;
     const int* unit_base = nullptr;      // [nsys]
-    int split = 4;                       // items per unit: 1, 2 (translation halves), 4 (and j halves)
-    void* U = nullptr;                   // [natoms][nid][kMaxRef] species vectors (R)
-    void* dU = nullptr;                  // same with dgw
+    int split = 4;                       // items per unit: 1, 2 (j-tile halves), 4 (and translation halves)
+    void* U = nullptr;                   // [natoms][nid][16] species vectors U (7 + pad) and dU (7 + pad) (R)
     double* unit_i = nullptr;            // [nunits][kTile][15]
     double* unit_j = nullptr;            // [nunits][kTile][4]
     // chain-rule sums of the CN pass per (item, j, lane), or null: the CN
     // pass stores them and the chain rule reads them instead of evaluating
     // the terms again (systems of one translation chunk, cn_store_bytes)
-    void* cn_store = nullptr;            // [items][kTile][9][kTile] (R)
+    void* cn_store = nullptr;            // [items][kTile / splitJ][9][kTile] (R)
     unsigned char* cn_store_ok = nullptr;   // [items]: the item stored its sums
 };
 
@@ -221,6 +220,7 @@ void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Pa
                      const PairUnits& pu, bool chain, cudaStream_t stream);
 size_t pair_unit_slot_doubles();   // per unit: i and j slots
 size_t pair_unit_i_doubles();      // per unit: i slots
+size_t species_vector_doubles(int natoms, int nid);   // PairUnits::U (FP64 size)
 // ev_begin/ev_end (or null) are recorded around the tile-pair kernel alone.
 void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
                            const Work& w, const PairUnits& pu, cudaStream_t stream, cudaEvent_t ev_begin = nullptr,

@@ -273,8 +273,7 @@ Engine::Engine(int nsys, const int* natoms, const int* numbers, const double* la
     up(d_unit_base_, unit_base.data(), sizeof(int) * nsys);
     pu_.units = d_units_;
     pu_.unit_base = d_unit_base_;
-    pu_.U = dev_alloc<double>((size_t)natoms_ * nid * kMaxRef);
-    pu_.dU = dev_alloc<double>((size_t)natoms_ * nid * kMaxRef);
+    pu_.U = dev_alloc<double>(species_vector_doubles(natoms_, nid));
     pu_.unit_i = dev_alloc<double>((size_t)std::max(pu_.nunits, 1) * pair_unit_slot_doubles());
     pu_.unit_j = pu_.unit_i + (size_t)std::max(pu_.nunits, 1) * pair_unit_i_doubles();
     d_tile_off_ = dev_alloc<int>(nsys + 1);

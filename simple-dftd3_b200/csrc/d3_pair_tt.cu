@@ -31,8 +31,9 @@ constexpr int kTTChunk = 128;     // translations tested per pass
 constexpr int kUnitI = 15;        // per-lane i sums: E, dE/dCN, g(3), sigma(6), dE/dparam(4)
 constexpr int kUnitJ = 4;         // per-lane j sums: dE/dCN, g(3)
 constexpr int kCnStore = 9;       // stored chain-rule sums per (i, j): countd (3), countd v^T (6)
-constexpr int kSplitMax = 4;      // a unit is evaluated as 1, 2 (translation halves) or 4 items
-                                  // (and j-tile halves); slots are sized for the largest split
+constexpr int kSplitMax = 4;      // a unit is evaluated as 1, 2 (j-tile halves) or 4 items
+                                  // (and translation halves); slots are sized for the largest split
+constexpr int kRefPad = 8;        // species-vector stride: U[0..6], pad, dU[0..6], pad
 
 template <class R> struct T4;
 template <> struct T4<float> { using type = float4; };
@@ -71,6 +72,86 @@ __device__ __forceinline__ R wsum_tt(R v)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
+}
+
+// Warp sums of four values by a transposing butterfly (6 shuffles in place
+// of 20): lane l returns the sum of value l >> 3 (a, b, c, d) over the warp.
+template <class R>
+__device__ __forceinline__ R wsum4_tt(R a, R b, R c, R d, int lane)
+{
+    const bool hi16 = lane & 16, hi8 = lane & 8;
+    R x0 = hi16 ? c : a, x1 = hi16 ? d : b;
+    const R y0 = hi16 ? a : c, y1 = hi16 ? b : d;
+    x0 += __shfl_xor_sync(0xffffffffu, y0, 16);
+    x1 += __shfl_xor_sync(0xffffffffu, y1, 16);
+    R z = hi8 ? x1 : x0;
+    const R y = hi8 ? x0 : x1;
+    z += __shfl_xor_sync(0xffffffffu, y, 8);
+    z += __shfl_xor_sync(0xffffffffu, z, 4);
+    z += __shfl_xor_sync(0xffffffffu, z, 2);
+    z += __shfl_xor_sync(0xffffffffu, z, 1);
+    return z;
+}
+
+// The FP32 sweeps take two translations per step (the second masked off
+// when a mask word has an odd count), branch-free, for instruction-level
+// parallelism.  The FP64 sweeps, at the register limit, take one, and only
+// the lanes whose term is taken run the FP64 math (its library sqrt, exp and
+// divisions cost more issue slots than the divergence; measured on B200).
+template <class R> constexpr bool kPairStep = sizeof(R) == 4;
+
+// Distance vector v = x_i - x_j - T of a staged translation q (head and
+// tail in the mixed form) and whether its term is taken: r^2 in [eps, cut2v]
+// and `on`.  A term not taken gets r^2 = 1, so that the branch-free term
+// math stays finite, and weight 0.
+template <class R>
+struct TTGeo {
+    R vx, vy, vz, r2;
+    bool ok;
+};
+
+template <class R, class V>
+__device__ __forceinline__ TTGeo<R> tt_geo(const V* sth, const V* stl, int q, R dhx, R dhy, R dhz, R dlx, R dly,
+                                           R dlz, R cut2v, R eps, bool on)
+{
+    TTGeo<R> g;
+    const V th = sth[q];
+    if constexpr (sizeof(R) == 8) { g.vx = dhx - th.x; g.vy = dhy - th.y; g.vz = dhz - th.z; }
+    else {
+        const V tl = stl[q];
+        g.vx = (dhx - th.x) + (dlx - tl.x);
+        g.vy = (dhy - th.y) + (dly - tl.y);
+        g.vz = (dhz - th.z) + (dlz - tl.z);
+    }
+    const R r2 = g.vx * g.vx + g.vy * g.vy + g.vz * g.vz;
+    g.ok = on && r2 <= cut2v && r2 >= eps;
+    g.r2 = g.ok ? r2 : R(1);
+    return g;
+}
+
+// Items of a unit: split 2 halves the j tile, split 4 also halves the
+// translations; item sub of a unit takes j half sub % splitJ and
+// translation half sub / splitJ.
+__host__ __device__ __forceinline__ int tt_split_j(int split) { return split >= 2 ? 2 : 1; }
+
+// Species vectors U and dU of one (atom, species) entry, padded to 8.
+template <class R>
+__device__ __forceinline__ void tt_load_uv(const R* p, R u[kRefPad], R du[kRefPad])
+{
+    if constexpr (sizeof(R) == 4) {
+        const float4* q = reinterpret_cast<const float4*>(p);
+        const float4 a0 = __ldg(q), a1 = __ldg(q + 1), b0 = __ldg(q + 2), b1 = __ldg(q + 3);
+        u[0] = a0.x; u[1] = a0.y; u[2] = a0.z; u[3] = a0.w; u[4] = a1.x; u[5] = a1.y; u[6] = a1.z; u[7] = a1.w;
+        du[0] = b0.x; du[1] = b0.y; du[2] = b0.z; du[3] = b0.w; du[4] = b1.x; du[5] = b1.y; du[6] = b1.z; du[7] = b1.w;
+    } else {
+        const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+        for (int k = 0; k < kRefPad / 2; k++) {
+            const double2 a = __ldg(q + k), b = __ldg(q + kRefPad / 2 + k);
+            u[2 * k] = a.x; u[2 * k + 1] = a.y;
+            du[2 * k] = b.x; du[2 * k + 1] = b.y;
+        }
+    }
 }
 
 // Compacts the translations tc .. tc+nt-1 that can join two tile spheres
@@ -142,16 +223,17 @@ __device__ __forceinline__ int tt_jmask(const V* sth, const V* stl, int qbeg, in
     return nwords;
 }
 
-// Species vectors U[a][s][r] and dU[a][s][r] of every atom (sorted order).
+// Species vectors of every atom (sorted order): UV[a][s] = U[a][s][0..6], 0,
+// dU[a][s][0..6], 0 (kRefPad stride, for vector loads).
 template <class R>
-__global__ void k_species_vectors(Batch b, Species s, Work w, R* U, R* dU)
+__global__ void k_species_vectors(Batch b, Species s, Work w, R* UV)
 {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const long long total = (long long)b.natoms * b.nid * kMaxRef;
+    const long long total = (long long)b.natoms * b.nid * kRefPad;
     if (t >= total) return;
-    const int a = (int)(t / (b.nid * kMaxRef));
-    const int rem = (int)(t % (b.nid * kMaxRef));
-    const int sx = rem / kMaxRef, r = rem % kMaxRef;
+    const int a = (int)(t / (b.nid * kRefPad));
+    const int rem = (int)(t % (b.nid * kRefPad));
+    const int sx = rem / kRefPad, r = rem % kRefPad;
     const int sa = b.sp[a];
     double u = 0.0, du = 0.0;
     if (!(b.ghost && b.ghost[a]) && r < s.nref[sx]) {
@@ -161,8 +243,9 @@ __global__ void k_species_vectors(Batch b, Species s, Work w, R* U, R* dU)
             du += w.dgw[a * kMaxRef + q] * __ldg(ref + q);
         }
     }
-    U[t] = R(u);
-    dU[t] = R(du);
+    R* o = UV + ((size_t)a * b.nid + sx) * (2 * kRefPad);
+    o[r] = R(u);
+    o[kRefPad + r] = R(du);
 }
 
 // One (i, j, T) term of the modified zero, optimized power, CSO and Z forms:
@@ -238,19 +321,19 @@ __device__ __forceinline__ void tt_family(R r2, R r1, bool have_r1, R rrij, R q1
 template <class R, int DAMP, bool GRAD, bool PG>
 __global__ void __launch_bounds__(kTTThreads, sizeof(R) == 4 ? 4 : 3)
 k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const int2* units, int nunits, int split,
-              const R* U, const R* dU, double* unit_i, double* unit_j)
+              const R* UV, double* unit_i, double* unit_j)
 {
     using V = typename T4<R>::type;
     __shared__ V sth[kTTWarps][kTTChunk];
     __shared__ V stl[kTTWarps][kTTChunk];
-    // FP64 sums of the lanes, [value][lane]: i sums and j sums
+    // FP64 sums, [value][lane]: i sums of the lane's atom, j sums of partner lane
     __shared__ double sacc[kTTWarps][kUnitI + kUnitJ][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int item = blockIdx.x * kTTWarps + wid;
     if (item >= nunits * split) return;
     const int u = item / split, sub = item % split;
-    const int splitT = split >= 2 ? 2 : 1, splitJ = split / splitT;
-    const int jh = sub / splitT, th = sub % splitT;
+    const int splitJ = tt_split_j(split), splitT = split / splitJ;
+    const int jh = sub % splitJ, th = sub / splitJ;
     const int it = units[u].x, jt = units[u].y;
     const int sys = b.tile_sys[it];
     const int t0 = b.tile_off[sys];
@@ -289,17 +372,15 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     const R bet = R(d.bet), a1 = R(d.a1);
     const int zsi = DAMP == kZDamping ? b.zid[ic] : 0;
     const int nid = b.nid;
-    // i sums: FP32 partials over at most 128 terms (mixed form) added to the
-    // FP64 sums in shared memory; the FP64 form adds every term to its
-    // register sums and stores them at the end
+    // i sums: partials in R over the partners of one translation chunk (at
+    // most 32 additions), added to the FP64 sums in shared memory per chunk
     double (*acc)[32] = sacc[wid];
     for (int v = 0; v < kUnitI + kUnitJ; v++) acc[v][lane] = 0.0;
+    __syncwarp();
     R te = R(0), tde = R(0), tgx = R(0), tgy = R(0), tgz = R(0);
     R txx = R(0), tyy = R(0), tzz = R(0), txy = R(0), txz = R(0), tyz = R(0);
     R tp0 = R(0), tp1 = R(0), tp2 = R(0), tp3 = R(0);
-    int pending = 0;          // terms in the FP32 partials (warp-uniform)
-    unsigned long long nterm = 0;
-    double b_de = 0, b_gx = 0, b_gy = 0, b_gz = 0;   // j sums of the FP64 form (registers)
+    unsigned nterm = 0;
 
     auto flush = [&]() {
         acc[0][lane] += double(te); acc[1][lane] += double(tde);
@@ -315,7 +396,6 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
             acc[13][lane] += double(tp2); acc[14][lane] += double(tp3);
             tp0 = tp1 = tp2 = tp3 = R(0);
         }
-        pending = 0;
     };
 
     for (int tc = tt0; tc < tt1; tc += kTTChunk) {
@@ -323,29 +403,27 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
         // translations that can join the two tiles
         const int nreach = tt_reach<V>(b.img, tc, nt, dcx, dcy, dcz, lim, lane, sth[wid], stl[wid]);
         if (nreach == 0) continue;
-        // this item's half of the reachable translations
-        const int qhalf = (nreach + splitT - 1) / splitT;
-        const int qbeg = th * qhalf, qend = min(nreach, qbeg + qhalf);
+        // this item's part of the reachable translations
+        const int qpart = (nreach + splitT - 1) / splitT;
+        const int qbeg = th * qpart, qend = min(nreach, qbeg + qpart);
         if (qbeg >= qend) continue;
         const int jl0 = jh * (kTile / splitJ), jl1 = min(nj, jl0 + kTile / splitJ);
         for (int jl = jl0; jl < jl1; jl++) {
             const int j = ja0 + jl;
             const bool self = diag && jl == lane;
             bool valid = ivalid && (!diag || jl <= lane) && !gi;
-            const int lj = b.local[j];
-            if (valid && p.nparts > 1) valid = tt_owns(p, li, lj);
+            if (valid && p.nparts > 1) valid = tt_owns(p, li, b.local[j]);
             const int sj = b.sp[j];
             // C6 and its CN derivatives from the species vectors of j
             R c6 = R(0), dc6i = R(0), dc6j = R(0);
             if (valid) {
-                const R* uj = U + ((size_t)j * nid + si) * kMaxRef;
-                const R* duj = dU + ((size_t)j * nid + si) * kMaxRef;
+                R uj[kRefPad], duj[kRefPad];
+                tt_load_uv<R>(UV + ((size_t)j * nid + si) * (2 * kRefPad), uj, duj);
 #pragma unroll
                 for (int r = 0; r < kMaxRef; r++) {
-                    const R ur = __ldg(uj + r), dur = __ldg(duj + r);
-                    c6 += gwi[r] * ur;
-                    dc6i += dgwi[r] * ur;
-                    dc6j += gwi[r] * dur;
+                    c6 += gwi[r] * uj[r];
+                    dc6i += dgwi[r] * uj[r];
+                    dc6j += gwi[r] * duj[r];
                 }
                 valid = c6 != R(0);
             }
@@ -358,14 +436,17 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
                 dhx = hix - hj.x; dhy = hiy - hj.y; dhz = hiz - hj.z;
                 dlx = lix - lj4.x; dly = liy - lj4.y; dlz = liz - lj4.z;
             }
-            const double* pr = s.pair + kPairSlots * (si * nid + sj);
-            const R rrij = R(__ldg(pr + 0));
-            const R q1 = R(__ldg(pr + 1)), q2 = R(__ldg(pr + 2)), q3 = R(__ldg(pr + 3)), q4 = R(__ldg(pr + 4));
-            const R q5 = DAMP == kMZero ? R(__ldg(pr + 5)) : R(0);
+            const double2* pr = reinterpret_cast<const double2*>(s.pair + kPairSlots * (si * nid + sj));
+            const double2 p01 = __ldg(pr), p23 = __ldg(pr + 1), p45 = __ldg(pr + 2);
+            const R rrij = R(p01.x);
+            const R q1 = R(p01.y), q2 = R(p23.x), q3 = R(p23.y), q4 = R(p45.x);
+            const R q5 = DAMP == kMZero ? R(p45.y) : R(0);
             // Z damping: R0 C6 with R0 = a1 / (species index sum) (z.f90:413)
             const R zc = DAMP == kZDamping ? a1 / R(zsi + b.zid[j]) * c6 : R(0);
             // both halves of a pair go to i; a self pair (j = i, T != 0) is one half
             const R we = self ? R(0.5) : R(1);
+            // a lane outside the pair list accepts no term
+            const R cut2v = valid ? cut2 : R(-1);
             // sums over the translations of this (i, j); C6 and its derivatives,
             // which do not depend on T, multiply them afterwards
             R se = R(0), se6 = R(0), se8 = R(0), spa = R(0), spb = R(0);
@@ -373,78 +454,96 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
             R sgx = R(0), sgy = R(0), sgz = R(0);
             R sxx = R(0), syy = R(0), szz = R(0), sxy = R(0), sxz = R(0), syz = R(0);
             const R s8rr = s8 * rrij;
-            // translations of this half that can bring j within the cutoff of tile it
+            // One (i, j, T) term, without branches: a lane whose term lies
+            // outside the cutoff (or is the T = 0 self pair) evaluates it at
+            // r^2 = 1 with weight 0 and adds exact zeros (tt_geo).
+            auto geo = [&](int q, bool on) {
+                return tt_geo<R, V>(sth[wid], stl[wid], q, dhx, dhy, dhz, dlx, dly, dlz, cut2v, R(DBL_EPSILON), on);
+            };
+            auto term = [&](const TTGeo<R>& g) {
+                const R vx = g.vx, vy = g.vy, vz = g.vz, r2 = g.r2;
+                const bool ok = g.ok;
+                nterm += ok ? 1u : 0u;
+                R sw = ok ? R(1) : R(0), dswdr = R(0), r1 = R(1);
+                if (smooth_on) {
+                    r1 = tt_sqrt<R>(r2);
+                    R sw1, dsw1;
+                    tt_smooth<R>(r1, cutoff, width, sw1, dsw1);
+                    sw = ok ? sw1 : R(0);
+                    dswdr = ok ? dsw1 : R(0);
+                }
+                R edisp0, gdisp0, e6, e8, dpa = R(0), dpb = R(0), cdisp0 = R(0);
+                if constexpr (DAMP == kRational) {
+                    // rational.f90:462-497: q1 = R0^6, q2 = R0^8, q3 = R0, q4 = sqrt(rrij)
+                    const R r4 = r2 * r2;
+                    const R a6 = r4 * r2 + q1, a8 = r4 * r4 + q2;
+                    const R inv = tt_rcp<R>(a6 * a8);
+                    const R t6 = a8 * inv;
+                    const R t8 = a6 * inv;
+                    e6 = t6; e8 = rrij * t8;
+                    edisp0 = s6 * t6 + s8rr * t8;
+                    // s6 d6 + s8 rrij d8 with d6 = -6 r^4 t6^2, d8 = -8 r^6 t8^2
+                    gdisp0 = r4 * (R(-6) * s6 * t6 * t6 + R(-8) * s8rr * r2 * t8 * t8);
+                    if (PG) {
+                        const R dedr0 = s6 * R(-6) * (q1 / q3) * t6 * t6 + s8rr * R(-8) * (q2 / q3) * t8 * t8;
+                        dpa = dedr0 * q4;
+                        dpb = dedr0;
+                    }
+                } else if constexpr (DAMP == kZero) {
+                    // zero.f90:490-536: q1 = rs6 R0, q2 = rs8 R0
+                    if (!smooth_on) r1 = tt_sqrt<R>(r2);
+                    const R r6 = r2 * r2 * r2;
+                    const R r8 = r6 * r2;
+                    const R t6 = tt_pow<R>(q1 / r1, alp6);
+                    const R t8 = tt_pow<R>(q2 / r1, alp8);
+                    const R f6 = R(1) / (R(1) + R(6) * t6);
+                    const R f8 = R(1) / (R(1) + R(6) * t8);
+                    const R d6 = R(-6) * f6 / r2 + R(6) * alp6 * t6 * (f6 * f6) / r2;
+                    const R d8 = R(-8) * f8 / r2 + R(6) * alp8 * t8 * (f8 * f8) / r2;
+                    e6 = f6 / r6; e8 = rrij * f8 / r8;
+                    edisp0 = s6 * f6 / r6 + s8 * rrij * f8 / r8;
+                    gdisp0 = s6 * d6 / r6 + s8 * rrij * d8 / r8;
+                    if (PG) {
+                        dpa = d.rs6 != 0.0 ? s6 / r6 * R(-6) * f6 * f6 * alp6 * t6 / R(d.rs6) : R(0);
+                        dpb = d.rs8 != 0.0 ? s8 * rrij / r8 * R(-6) * f8 * f8 * alp8 * t8 / R(d.rs8) : R(0);
+                    }
+                } else {
+                    e6 = e8 = R(0);
+                    tt_family<R, DAMP>(r2, r1, smooth_on, rrij, q1, q2, q3, q4, q5, zc, s6, s8, alp6, alp8, bet, a1,
+                                       edisp0, gdisp0, cdisp0);
+                }
+                se += sw * edisp0;
+                if (DAMP == kZDamping) sc += sw * cdisp0;
+                if (PG) { se6 += sw * e6; se8 += sw * e8; spa += sw * dpa; spb += sw * dpb; }
+                if (GRAD) {
+                    R gdisp = sw * gdisp0;
+                    if (smooth_on) gdisp += dswdr * edisp0 / r1;
+                    const R gx = gdisp * vx, gy = gdisp * vy, gz = gdisp * vz;
+                    sgx += gx; sgy += gy; sgz += gz;
+                    sxx += gx * vx; syy += gy * vy; szz += gz * vz;
+                    sxy += gx * vy; sxz += gx * vz; syz += gy * vz;
+                }
+            };
+            // translations of this part that can bring j within the cutoff of tile it
             unsigned jm[kJMaskWords];
             const int nw = tt_jmask<V>(sth[wid], stl[wid], qbeg, qend, ci, xj, yj, zj, limj, lane, jm);
 #pragma unroll
             for (int h = 0; h < kJMaskWords; h++) {
                 if (h >= nw) break;
-                for (unsigned mm = jm[h]; mm; mm &= mm - 1) {
-                    const int q = qbeg + 32 * h + __ffs(mm) - 1;
-                    const V th = sth[wid][q];
-                    R vx, vy, vz;
-                    if constexpr (sizeof(R) == 8) { vx = dhx - th.x; vy = dhy - th.y; vz = dhz - th.z; }
-                    else {
-                        const V tl = stl[wid][q];
-                        vx = (dhx - th.x) + (dlx - tl.x);
-                        vy = (dhy - th.y) + (dly - tl.y);
-                        vz = (dhz - th.z) + (dlz - tl.z);
-                    }
-                    const R r2 = vx * vx + vy * vy + vz * vz;
-                    if (!valid || r2 > cut2 || r2 < R(DBL_EPSILON)) continue;
-                    nterm++;
-                    R sw = R(1), dswdr = R(0), r1 = R(0);
-                    if (smooth_on) { r1 = tt_sqrt<R>(r2); tt_smooth<R>(r1, cutoff, width, sw, dswdr); }
-                    R edisp0, gdisp0, e6, e8, dpa = R(0), dpb = R(0), cdisp0 = R(0);
-                    if constexpr (DAMP == kRational) {
-                        // rational.f90:462-497: q1 = R0^6, q2 = R0^8, q3 = R0, q4 = sqrt(rrij)
-                        const R r4 = r2 * r2;
-                        const R a6 = r4 * r2 + q1, a8 = r4 * r4 + q2;
-                        const R inv = tt_rcp<R>(a6 * a8);
-                        const R t6 = a8 * inv;
-                        const R t8 = a6 * inv;
-                        e6 = t6; e8 = rrij * t8;
-                        edisp0 = s6 * t6 + s8rr * t8;
-                        // s6 d6 + s8 rrij d8 with d6 = -6 r^4 t6^2, d8 = -8 r^6 t8^2
-                        gdisp0 = r4 * (R(-6) * s6 * t6 * t6 + R(-8) * s8rr * r2 * t8 * t8);
-                        if (PG) {
-                            const R dedr0 = s6 * R(-6) * (q1 / q3) * t6 * t6 + s8rr * R(-8) * (q2 / q3) * t8 * t8;
-                            dpa = dedr0 * q4;
-                            dpb = dedr0;
-                        }
-                    } else if constexpr (DAMP == kZero) {
-                        // zero.f90:490-536: q1 = rs6 R0, q2 = rs8 R0
-                        if (!smooth_on) r1 = tt_sqrt<R>(r2);
-                        const R r6 = r2 * r2 * r2;
-                        const R r8 = r6 * r2;
-                        const R t6 = tt_pow<R>(q1 / r1, alp6);
-                        const R t8 = tt_pow<R>(q2 / r1, alp8);
-                        const R f6 = R(1) / (R(1) + R(6) * t6);
-                        const R f8 = R(1) / (R(1) + R(6) * t8);
-                        const R d6 = R(-6) * f6 / r2 + R(6) * alp6 * t6 * (f6 * f6) / r2;
-                        const R d8 = R(-8) * f8 / r2 + R(6) * alp8 * t8 * (f8 * f8) / r2;
-                        e6 = f6 / r6; e8 = rrij * f8 / r8;
-                        edisp0 = s6 * f6 / r6 + s8 * rrij * f8 / r8;
-                        gdisp0 = s6 * d6 / r6 + s8 * rrij * d8 / r8;
-                        if (PG) {
-                            dpa = d.rs6 != 0.0 ? s6 / r6 * R(-6) * f6 * f6 * alp6 * t6 / R(d.rs6) : R(0);
-                            dpb = d.rs8 != 0.0 ? s8 * rrij / r8 * R(-6) * f8 * f8 * alp8 * t8 / R(d.rs8) : R(0);
-                        }
+                const int qh = qbeg + 32 * h - 1;
+                for (unsigned mm = jm[h]; mm;) {
+                    const int qa = qh + __ffs(mm);
+                    mm &= mm - 1;
+                    if constexpr (kPairStep<R>) {
+                        const bool two = mm != 0u;
+                        const int qb = two ? qh + __ffs(mm) : qa;
+                        mm &= mm - 1;
+                        const TTGeo<R> ga = geo(qa, true), gb = geo(qb, two);
+                        term(ga);
+                        term(gb);
                     } else {
-                        e6 = e8 = R(0);
-                        tt_family<R, DAMP>(r2, r1, smooth_on, rrij, q1, q2, q3, q4, q5, zc, s6, s8, alp6, alp8, bet, a1,
-                                           edisp0, gdisp0, cdisp0);
-                    }
-                    se += sw * edisp0;
-                    if (DAMP == kZDamping) sc += sw * cdisp0;
-                    if (PG) { se6 += sw * e6; se8 += sw * e8; spa += sw * dpa; spb += sw * dpb; }
-                    if (GRAD) {
-                        R gdisp = sw * gdisp0;
-                        if (smooth_on) gdisp += dswdr * edisp0 / r1;
-                        const R gx = gdisp * vx, gy = gdisp * vy, gz = gdisp * vz;
-                        sgx += gx; sgy += gy; sgz += gz;
-                        sxx += gx * vx; syy += gy * vy; szz += gz * vz;
-                        sxy += gx * vy; sxz += gx * vz; syz += gy * vz;
+                        const TTGeo<R> ga = geo(qa, true);
+                        if (ga.ok) term(ga);
                     }
                 }
             }
@@ -455,49 +554,35 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
             // dE/dCN = -dC6/dCN sum sw edisp; Z damping: dC6/dCN dE/dC6 (z.f90:431-445)
             const R sdc = DAMP == kZDamping ? sc : se;
             tde -= dc6i * sdc;
-            R jde = self ? R(0) : -dc6j * sdc, jgx = R(0), jgy = R(0), jgz = R(0);
+            const R jde = self ? R(0) : -dc6j * sdc;
             if (PG) { tp0 -= c6w * se6; tp1 -= c6w * se8; tp2 -= c6w * spa; tp3 -= c6w * spb; }
             if (GRAD) {
+                R jgx = R(0), jgy = R(0), jgz = R(0);
                 if (!self) {
                     tgx -= c6 * sgx; tgy -= c6 * sgy; tgz -= c6 * sgz;
                     jgx = c6 * sgx; jgy = c6 * sgy; jgz = c6 * sgz;
                 }
                 txx -= c6w * sxx; tyy -= c6w * syy; tzz -= c6w * szz;
                 txy -= c6w * sxy; txz -= c6w * sxz; tyz -= c6w * syz;
-            }
-            // j's share, summed over the warp's atoms i
-            jde = wsum_tt<R>(jde);
-            if (GRAD) { jgx = wsum_tt<R>(jgx); jgy = wsum_tt<R>(jgy); jgz = wsum_tt<R>(jgz); }
-            if (lane == jl) {
-                if constexpr (sizeof(R) == 4) {
-                    acc[kUnitI + 0][lane] += double(jde);
-                    if (GRAD) {
-                        acc[kUnitI + 1][lane] += double(jgx); acc[kUnitI + 2][lane] += double(jgy);
-                        acc[kUnitI + 3][lane] += double(jgz);
-                    }
-                } else {
-                    b_de += jde;
-                    if (GRAD) { b_gx += jgx; b_gy += jgy; b_gz += jgz; }
-                }
-            }
-            if constexpr (sizeof(R) == 4) {
-                pending += qend - qbeg;
-                if (pending >= 128) flush();
+                // j's share summed over the warp's atoms i: lane 8v holds value v
+                const R z = wsum4_tt<R>(jde, jgx, jgy, jgz, lane);
+                if ((lane & 7) == 0) acc[kUnitI + (lane >> 3)][jl] += double(z);
+            } else {
+                const R z = wsum_tt<R>(jde);
+                if (lane == 0) acc[kUnitI][jl] += double(z);
             }
         }
+        flush();
     }
-    flush();
-    if constexpr (sizeof(R) == 8) {
-        acc[kUnitI + 0][lane] = b_de; acc[kUnitI + 1][lane] = b_gx;
-        acc[kUnitI + 2][lane] = b_gy; acc[kUnitI + 3][lane] = b_gz;
-    }
+    __syncwarp();
     double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
     for (int v = 0; v < kUnitI; v++) oi[v] = acc[v][lane];
     double* oj = unit_j + ((size_t)item * kTile + lane) * kUnitJ;
     for (int v = 0; v < kUnitJ; v++) oj[v] = acc[kUnitI + v][lane];
     if (w.counts) {
-        for (int off = 16; off > 0; off >>= 1) nterm += __shfl_xor_sync(0xffffffffu, nterm, off);
-        if (lane == 0) atomicAdd(w.counts + 0, nterm);
+        unsigned long long n = nterm;
+        for (int off = 16; off > 0; off >>= 1) n += __shfl_xor_sync(0xffffffffu, n, off);
+        if (lane == 0) atomicAdd(w.counts + 0, n);
     }
 }
 
@@ -570,12 +655,15 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
     using V = typename T4<R>::type;
     __shared__ V sth[kTTWarps][kTTChunk];
     __shared__ V stl[kTTWarps][kTTChunk];
+    // FP64 j sums of the partner lanes: CN [cn], chain rule [g(3)]
+    __shared__ double sjs[kTTWarps][3][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int item = blockIdx.x * kTTWarps + wid;
     if (item >= nunits * split) return;
     const int u = item / split, sub = item % split;
-    const int splitT = split >= 2 ? 2 : 1, splitJ = split / splitT;
-    const int jh = sub / splitT, th = sub % splitT;
+    const int splitJ = tt_split_j(split), splitT = split / splitJ;
+    const int jh = sub % splitJ, th = sub / splitJ;
+    const int jslots = kTile / splitJ;
     const int it = units[u].x, jt = units[u].y;
     const int sys = b.tile_sys[it];
     const int t0 = b.tile_off[sys];
@@ -602,12 +690,14 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
     const double limj = c.cut_cn + ci.w + 1.0e-6 * c.cut_cn + 1.0e-6;
     const double dcx = ci.x - cj.x, dcy = ci.y - cj.y, dcz = ci.z - cj.z;
     const R cut2 = R(c.cut_cn * c.cut_cn);
-    // i sums: CN: a0 = cn; chain: a1..a3 gradient, a4..a8 virial xx yy zz xy xz, a0 virial yz
+    double (*sj)[32] = sjs[wid];
+    for (int v = 0; v < 3; v++) sj[v][lane] = 0.0;
+    __syncwarp();
+    // i sums: CN: a0 = cn; chain: a1..a3 gradient, a4..a8 virial xx yy zz xy xz, a0 virial yz;
+    // partials in R over the partners of one translation chunk
     double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0, a7 = 0, a8 = 0;
     R t0_ = R(0), t1_ = R(0), t2_ = R(0), t3_ = R(0), t4_ = R(0), t5_ = R(0), t6_ = R(0), t7_ = R(0), t8_ = R(0);
-    double b0 = 0, b1 = 0, b2 = 0;                                                   // cn | g(3) of j
-    int pending = 0;
-    unsigned long long nterm = 0;
+    unsigned nterm = 0;
     bool ran = false;          // STORE: this item evaluated its (single) chunk
     auto flush = [&]() {
         a0 += double(t0_); t0_ = R(0);
@@ -616,16 +706,15 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
             a6 += double(t6_); a7 += double(t7_); a8 += double(t8_);
             t1_ = t2_ = t3_ = t4_ = t5_ = t6_ = t7_ = t8_ = R(0);
         }
-        pending = 0;
     };
     for (int tc = tt0; tc < tt1; tc += kTTChunk) {
         const int nt = min(kTTChunk, tt1 - tc);
         const int nreach = tt_reach<V>(b.img, tc, nt, dcx, dcy, dcz, lim, lane, sth[wid], stl[wid]);
         if (nreach == 0) continue;
-        const int qhalf = (nreach + splitT - 1) / splitT;
-        const int qbeg = th * qhalf, qend = min(nreach, qbeg + qhalf);
+        const int qpart = (nreach + splitT - 1) / splitT;
+        const int qbeg = th * qpart, qend = min(nreach, qbeg + qpart);
         if (qbeg >= qend) continue;
-        const int jl0 = jh * (kTile / splitJ), jl1 = min(nj, jl0 + kTile / splitJ);
+        const int jl0 = jh * jslots, jl1 = min(nj, jl0 + jslots);
         ran = true;
         for (int jl = jl0; jl < jl1; jl++) {
             const int j = ja0 + jl;
@@ -645,114 +734,109 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
             // chain rule weight of the pair: dE/dCN_i + dE/dCN_j, or dE/dCN_i for j = i (ncoord.f90:205-213)
             const R dsum = CHAIN ? R(dei + w.dEdcn[j]) : R(0);
             const R dsig = CHAIN ? (self ? R(dei) : dsum) : R(0);
-            R j0 = R(0), j1 = R(0), j2 = R(0);
+            // a lane outside the pair list accepts no term
+            const R cut2v = valid ? cut2 : R(-1);
             // sums over the translations of this (i, j); the pair weights
             // dE/dCN_i + dE/dCN_j do not depend on T and multiply them afterwards
             R sc = R(0), scx = R(0), scy = R(0), scz = R(0);
             R sxx = R(0), syy = R(0), szz = R(0), sxy = R(0), sxz = R(0), syz = R(0);
+            // One (i, j, T) term without branches: a term outside the cutoff
+            // (or the T = 0 self pair) is evaluated at r^2 = 1 and adds zeros (tt_geo).
+            auto geo = [&](int q, bool on) {
+                return tt_geo<R, V>(sth[wid], stl[wid], q, dhx, dhy, dhz, dlx, dly, dlz, cut2v, R(1.0e-12), on);
+            };
+            auto term = [&](const TTGeo<R>& g) {
+                const R vx = g.vx, vy = g.vy, vz = g.vz, r2 = g.r2;
+                const bool ok = g.ok;
+                nterm += ok ? 1u : 0u;
+                if (STORE || CHAIN) {
+                    // the count and the chain rule's countd of the same term (ncoord.f90:198-206)
+                    R cf, f;
+                    if constexpr (sizeof(R) == 8) {
+                        const R r1 = sqrt(r2);
+                        cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / r1 - R(1))));
+                        f = -cf * (R(1) - cf) * R(kKcnTT) * rc / r2 / r1;
+                    } else {
+                        const R ir = rsqrtf(r2);
+                        cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * ir - R(1))));
+                        f = -cf * (R(1) - cf) * R(kKcnTT) * rc * (ir * ir * ir);
+                    }
+                    if (STORE) sc += ok ? cf : R(0);
+                    f = ok ? f : R(0);
+                    const R cx = f * vx, cy = f * vy, cz = f * vz;   // countd
+                    scx += cx; scy += cy; scz += cz;
+                    sxx += cx * vx; syy += cy * vy; szz += cz * vz;
+                    sxy += cx * vy; sxz += cx * vz; syz += cy * vz;
+                } else {
+                    R cf;
+                    if constexpr (sizeof(R) == 8) cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / sqrt(r2) - R(1))));
+                    else cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * rsqrtf(r2) - R(1))));
+                    sc += ok ? cf : R(0);
+                }
+            };
             unsigned jm[kJMaskWords];
             const int nw = tt_jmask<V>(sth[wid], stl[wid], qbeg, qend, ci, xj, yj, zj, limj, lane, jm);
 #pragma unroll
             for (int h = 0; h < kJMaskWords; h++) {
                 if (h >= nw) break;
-                for (unsigned mm = jm[h]; mm; mm &= mm - 1) {
-                    const int q = qbeg + 32 * h + __ffs(mm) - 1;
-                    const V thv = sth[wid][q];
-                    R vx, vy, vz;
-                    if constexpr (sizeof(R) == 8) { vx = dhx - thv.x; vy = dhy - thv.y; vz = dhz - thv.z; }
-                    else {
-                        const V tl = stl[wid][q];
-                        vx = (dhx - thv.x) + (dlx - tl.x);
-                        vy = (dhy - thv.y) + (dly - tl.y);
-                        vz = (dhz - thv.z) + (dlz - tl.z);
-                    }
-                    const R r2 = vx * vx + vy * vy + vz * vz;
-                    if (!valid || r2 > cut2 || r2 < R(1.0e-12)) continue;
-                    nterm++;
-                    if (STORE) {
-                        // the count and the chain rule's countd of the same term
-                        R cf, f;
-                        if constexpr (sizeof(R) == 8) {
-                            const R r1 = sqrt(r2);
-                            cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / r1 - R(1))));
-                            f = -cf * (R(1) - cf) * R(kKcnTT) * rc / r2 / r1;
-                        } else {
-                            const R ir = rsqrtf(r2);
-                            cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * ir - R(1))));
-                            f = -cf * (R(1) - cf) * R(kKcnTT) * rc * (ir * ir * ir);
-                        }
-                        sc += cf;
-                        const R cx = f * vx, cy = f * vy, cz = f * vz;
-                        scx += cx; scy += cy; scz += cz;
-                        sxx += cx * vx; syy += cy * vy; szz += cz * vz;
-                        sxy += cx * vy; sxz += cx * vz; syz += cy * vz;
-                    } else if (!CHAIN) {
-                        R cf;
-                        if constexpr (sizeof(R) == 8) cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / sqrt(r2) - R(1))));
-                        else cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * rsqrtf(r2) - R(1))));
-                        sc += cf;
+                const int qh = qbeg + 32 * h - 1;
+                for (unsigned mm = jm[h]; mm;) {
+                    const int qa = qh + __ffs(mm);
+                    mm &= mm - 1;
+                    if constexpr (kPairStep<R>) {
+                        const bool two = mm != 0u;
+                        const int qb = two ? qh + __ffs(mm) : qa;
+                        mm &= mm - 1;
+                        term(geo(qa, true));
+                        term(geo(qb, two));
                     } else {
-                        R f;
-                        if constexpr (sizeof(R) == 8) {
-                            // ncoord.f90:198-206
-                            const R r1 = sqrt(r2);
-                            const R cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / r1 - R(1))));
-                            const R dcf = -cf * (R(1) - cf) * R(kKcnTT) * rc / r2;
-                            f = dcf / r1;
-                        } else {
-                            const R ir = rsqrtf(r2);
-                            const R cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * ir - R(1))));
-                            f = -cf * (R(1) - cf) * R(kKcnTT) * rc * (ir * ir * ir);
-                        }
-                        const R cx = f * vx, cy = f * vy, cz = f * vz;   // countd
-                        scx += cx; scy += cy; scz += cz;
-                        sxx += cx * vx; syy += cy * vy; szz += cz * vz;
-                        sxy += cx * vy; sxz += cx * vz; syz += cy * vz;
+                        const TTGeo<R> ga = geo(qa, true);
+                        if (ga.ok) term(ga);
                     }
                 }
             }
             if (STORE) {
-                R* out = store + ((size_t)item * kTile + (jl - jl0)) * kCnStore * kTile + lane;
+                R* out = store + ((size_t)item * jslots + (jl - jl0)) * kCnStore * kTile + lane;
                 const R vals[kCnStore] = {scx, scy, scz, sxx, syy, szz, sxy, sxz, syz};
 #pragma unroll
                 for (int v = 0; v < kCnStore; v++) out[v * kTile] = vals[v];
             }
             if (!CHAIN) {
                 t0_ += sc;
-                if (!self) j0 = sc;
+                const R z = wsum_tt<R>(self ? R(0) : sc);
+                if (lane == 0) sj[0][jl] += double(z);
             } else {
+                R j0 = R(0), j1 = R(0), j2 = R(0);
                 if (!self) {
                     t1_ += scx * dsum; t2_ += scy * dsum; t3_ += scz * dsum;
                     j0 = -scx * dsum; j1 = -scy * dsum; j2 = -scz * dsum;
                 }
                 t4_ += sxx * dsig; t5_ += syy * dsig; t6_ += szz * dsig;
                 t7_ += sxy * dsig; t8_ += sxz * dsig; t0_ += syz * dsig;
-            }
-            j0 = wsum_tt<R>(j0);
-            if (CHAIN) { j1 = wsum_tt<R>(j1); j2 = wsum_tt<R>(j2); }
-            if (lane == jl) { b0 += double(j0); b1 += double(j1); b2 += double(j2); }
-            if constexpr (sizeof(R) == 4) {
-                pending += qend - qbeg;
-                if (pending >= 128) flush();
+                // lane 8v holds the warp sum of value v
+                const R z = wsum4_tt<R>(j0, j1, j2, R(0), lane);
+                if ((lane & 7) == 0 && lane < 24) sj[lane >> 3][jl] += double(z);
             }
         }
+        flush();
     }
-    flush();
+    __syncwarp();
     double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
     double* oj = unit_j + ((size_t)item * kTile + lane) * kUnitJ;
     if (!CHAIN) {
         oi[0] = a0;
-        oj[0] = b0;
+        oj[0] = sj[0][lane];
     } else {
         // g(3), sigma xx yy zz xy xz yz
         oi[0] = a1; oi[1] = a2; oi[2] = a3;
         oi[3] = a4; oi[4] = a5; oi[5] = a6; oi[6] = a7; oi[7] = a8; oi[8] = a0;
-        oj[0] = b0; oj[1] = b1; oj[2] = b2;
+        oj[0] = sj[0][lane]; oj[1] = sj[1][lane]; oj[2] = sj[2][lane];
     }
     if (STORE && lane == 0) store_ok[item] = ran ? 1 : 0;
     if (!CHAIN && w.counts) {
-        for (int off = 16; off > 0; off >>= 1) nterm += __shfl_xor_sync(0xffffffffu, nterm, off);
-        if (lane == 0) atomicAdd(w.counts + 2, nterm);
+        unsigned long long n = nterm;
+        for (int off = 16; off > 0; off >>= 1) n += __shfl_xor_sync(0xffffffffu, n, off);
+        if (lane == 0) atomicAdd(w.counts + 2, n);
     }
 }
 
@@ -764,12 +848,14 @@ __global__ void __launch_bounds__(kTTThreads)
 k_cn_chain_stored(Batch b, Config c, Partition p, Work w, const int2* units, int nunits, int split, const R* store,
                   const unsigned char* store_ok, double* unit_i, double* unit_j)
 {
+    __shared__ double sjs[kTTWarps][3][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int item = blockIdx.x * kTTWarps + wid;
     if (item >= nunits * split) return;
     const int u = item / split, sub = item % split;
-    const int splitT = split >= 2 ? 2 : 1, splitJ = split / splitT;
-    const int jh = sub / splitT;
+    const int splitJ = tt_split_j(split);
+    const int jh = sub % splitJ;
+    const int jslots = kTile / splitJ;
     const int it = units[u].x, jt = units[u].y;
     const int sys = b.tile_sys[it];
     const int t0 = b.tile_off[sys];
@@ -781,9 +867,12 @@ k_cn_chain_stored(Batch b, Config c, Partition p, Work w, const int2* units, int
     const int ic = ivalid ? ia0 + lane : ia0;
     const int li = b.local[ic];
     const double dei = w.dEdcn[ic];
-    double g[3] = {0, 0, 0}, sg[6] = {0, 0, 0, 0, 0, 0}, bj[3] = {0, 0, 0};
+    double (*sj)[32] = sjs[wid];
+    for (int v = 0; v < 3; v++) sj[v][lane] = 0.0;
+    __syncwarp();
+    double g[3] = {0, 0, 0}, sg[6] = {0, 0, 0, 0, 0, 0};
     if (store_ok[item]) {
-        const int jl0 = jh * (kTile / splitJ), jl1 = min(nj, jl0 + kTile / splitJ);
+        const int jl0 = jh * jslots, jl1 = min(nj, jl0 + jslots);
         // the sums of NQ partners are loaded together (memory-level parallelism);
         // sums of a partner that no lane of the item took were not stored and
         // are loaded but not used
@@ -792,7 +881,7 @@ k_cn_chain_stored(Batch b, Config c, Partition p, Work w, const int2* units, int
             R sv[NQ][kCnStore];
 #pragma unroll
             for (int q = 0; q < NQ; q++) {
-                const R* in = store + ((size_t)item * kTile + min(jg + q, jl1 - 1) - jl0) * kCnStore * kTile + lane;
+                const R* in = store + ((size_t)item * jslots + min(jg + q, jl1 - 1) - jl0) * kCnStore * kTile + lane;
 #pragma unroll
                 for (int v = 0; v < kCnStore; v++) sv[q][v] = in[v * kTile];
             }
@@ -815,17 +904,19 @@ k_cn_chain_stored(Batch b, Config c, Partition p, Work w, const int2* units, int
                 }
 #pragma unroll
                 for (int v = 0; v < 6; v++) sg[v] += double(sv[q][3 + v]) * dsig;
-                j0 = wsum_tt<double>(j0); j1 = wsum_tt<double>(j1); j2 = wsum_tt<double>(j2);
-                if (lane == jl) { bj[0] += j0; bj[1] += j1; bj[2] += j2; }
+                // lane 8v holds the warp sum of value v
+                const double z = wsum4_tt<double>(j0, j1, j2, 0.0, lane);
+                if ((lane & 7) == 0 && lane < 24) sj[lane >> 3][jl] += z;
             }
         }
     }
+    __syncwarp();
     double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
     double* oj = unit_j + ((size_t)item * kTile + lane) * kUnitJ;
     // g(3), sigma xx yy zz xy xz yz (the layout of k_cn_tt<R, 1>)
     oi[0] = g[0]; oi[1] = g[1]; oi[2] = g[2];
     oi[3] = sg[0]; oi[4] = sg[1]; oi[5] = sg[2]; oi[6] = sg[3]; oi[7] = sg[4]; oi[8] = sg[5];
-    oj[0] = bj[0]; oj[1] = bj[1]; oj[2] = bj[2];
+    oj[0] = sj[0][lane]; oj[1] = sj[1][lane]; oj[2] = sj[2][lane];
 }
 
 // Gather of the CN (assign) or chain-rule (add to gradient and virial) slots,
@@ -879,7 +970,7 @@ void launch_tt(const Batch& b, const Species& s, const Damp& d, const Config& c,
 {
     const int blocks = (pu.nunits * pu.split + kTTWarps - 1) / kTTWarps;
     k_two_body_tt<R, DAMP, GRAD, PG><<<blocks, kTTThreads, 0, stream>>>(
-        b, s, d, c, p, w, pu.units, pu.nunits, pu.split, (const R*)pu.U, (const R*)pu.dU, pu.unit_i, pu.unit_j);
+        b, s, d, c, p, w, pu.units, pu.nunits, pu.split, (const R*)pu.U, pu.unit_i, pu.unit_j);
 }
 
 // the families without damping-parameter derivatives (the engine refuses
@@ -944,22 +1035,24 @@ void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Pa
 
 size_t cn_store_bytes(const PairUnits& pu, bool mixed)
 {
-    return (size_t)pu.nunits * pu.split * kTile * kCnStore * kTile * (mixed ? sizeof(float) : sizeof(double));
+    return (size_t)pu.nunits * pu.split * (kTile / tt_split_j(pu.split)) * kCnStore * kTile *
+           (mixed ? sizeof(float) : sizeof(double));
 }
 
 size_t pair_unit_slot_doubles() { return (size_t)kSplitMax * kTile * (kUnitI + kUnitJ); }
 size_t pair_unit_i_doubles() { return (size_t)kSplitMax * kTile * kUnitI; }
+size_t species_vector_doubles(int natoms, int nid) { return (size_t)natoms * nid * 2 * kRefPad; }
 
 void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
                            const Work& w, const PairUnits& pu, cudaStream_t stream, cudaEvent_t ev_begin,
                            cudaEvent_t ev_end)
 {
     if (b.natoms <= 0) return;
-    const long long nsv = (long long)b.natoms * b.nid * kMaxRef;
+    const long long nsv = (long long)b.natoms * b.nid * kRefPad;
     if (c.mixed)
-        k_species_vectors<float><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (float*)pu.U, (float*)pu.dU);
+        k_species_vectors<float><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (float*)pu.U);
     else
-        k_species_vectors<double><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (double*)pu.U, (double*)pu.dU);
+        k_species_vectors<double><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (double*)pu.U);
     if (ev_begin) cudaEventRecord(ev_begin, stream);
     if (pu.nunits > 0) {
         switch (d.kind) {
