@@ -146,8 +146,9 @@ dftd3_b200_set_batch_graph(dftd3_error /* error */,
  * the default, Morton order with 3 Bohr cells for systems above 16384 atoms;
  * > 0: Morton order with keys quantised to cells of that many Bohr),
  * tuning[1] work items per tile pair of the pair sweeps (1, 2
- * or 4; 0 chooses 1 for batches of molecules, else 2 in the mixed and 4 in
- * the FP64 form), tuning[2] resident blocks per SM of the neighbour-list three-body
+ * or 4; 0 chooses 1 for batches of molecules, else 2, and 1 for the CN
+ * sweeps of the mixed form when the tile pairs give every SM eight warps),
+ * tuning[2] resident blocks per SM of the neighbour-list three-body
  * kernel (0 = occupancy limit), tuning[3] the block-per-molecule three-body
  * kernel for non-periodic systems of at most 256 atoms (0: when the batch has
  * at least one such molecule per SM, 1: always, 2: never). */

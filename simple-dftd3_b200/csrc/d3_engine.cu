@@ -652,7 +652,7 @@ void Engine::pairwise_host(const Damp& d, const double* positions, double* energ
     c.grad = false; c.mixed = false; c.param_grad = false; c.cn_partitioned = false;
     Work w = work_;
     w.counts = nullptr; w.e3_atom = nullptr; w.sig3_atom = nullptr; w.pg_atom = nullptr;
-    pu_.split = tune_.pair_split ? tune_.pair_split : (auto_split_ == 1 ? 1 : 4);
+    pu_.split = cn_split();
     pu_.cn_store = nullptr;
     pu_.cn_store_ok = nullptr;
     order_atoms(d, d_pos_in_, b, false, stream);
@@ -665,6 +665,22 @@ void Engine::pairwise_host(const Damp& d, const double* positions, double* energ
     check(cudaMemcpyAsync(energy3, d_pw_ + 2 * total, sizeof(double) * c6mat_total_, cudaMemcpyDeviceToHost, stream),
           "pairwise energy3");
     check(cudaStreamSynchronize(stream), "pairwise");
+}
+
+// Items per tile pair with tuning 0 (measured on B200): one for batches of
+// molecules; for periodic systems two, and for the CN sweeps of the mixed
+// form one once the units alone give every SM eight warps.
+int Engine::pair_split() const
+{
+    if (tune_.pair_split) return tune_.pair_split;
+    return auto_split_ == 1 ? 1 : 2;
+}
+
+int Engine::cn_split() const
+{
+    if (tune_.pair_split) return tune_.pair_split;
+    if (auto_split_ == 1) return 1;
+    return mixed_ && pu_.nunits >= 8 * sms_ ? 1 : 2;
 }
 
 void Engine::hessian_host(const Damp& d, const double* positions, double* hessian)
@@ -720,15 +736,16 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     c.cut_cn = cut_.cn; c.cut2 = cut_.disp2; c.cut3 = cut_.disp3;
     c.width2 = cut_.width2; c.width3 = cut_.width3;
     c.grad = grad; c.mixed = mixed_; c.param_grad = pg; c.cn_partitioned = cn_partitioned_;
-    // automatic split: one item per tile pair for molecules; for periodic
-    // systems two (mixed form) or four (FP64 form), measured on B200
-    pu_.split = tune_.pair_split ? tune_.pair_split : (auto_split_ == 1 ? 1 : (mixed_ ? 2 : 4));
+    // the CN sweeps and the two-body sweep split the tile pairs each their own way
+    pu_.split = pair_split();
+    PairUnits pcn = pu_;
+    pcn.split = cn_split();
     // the CN pass keeps the chain rule's per-pair sums when every system's CN
     // translations fit one chunk and the buffer stays below kCnStoreCap
-    pu_.cn_store = nullptr;
-    pu_.cn_store_ok = nullptr;
+    pcn.cn_store = nullptr;
+    pcn.cn_store_ok = nullptr;
     if (grad && cn_single_chunk()) {
-        const size_t bytes = cn_store_bytes(pu_, mixed_);
+        const size_t bytes = cn_store_bytes(pcn, mixed_);
         if (bytes <= kCnStoreCap && (bytes <= cn_store_cap_ || !capturing_)) {
             if (bytes > cn_store_cap_) {
                 free_block(d_cn_store_);
@@ -738,8 +755,8 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
                 d_cn_store_ok_ = dev_alloc<unsigned char>((size_t)pu_.nunits * 4);
                 cn_store_cap_ = bytes;
             }
-            pu_.cn_store = d_cn_store_;
-            pu_.cn_store_ok = d_cn_store_ok_;
+            pcn.cn_store = d_cn_store_;
+            pcn.cn_store_ok = d_cn_store_ok_;
         }
     }
     Work w = work_;
@@ -761,7 +778,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     mark(0);
     order_atoms(d, d_positions, b, mixed_, stream);
     mark(1);
-    launch_cn_units(b, s, c, part_, w, pu_, false, stream);
+    launch_cn_units(b, s, c, part_, w, pcn, false, stream);
     if (reducer_) reduce(w.cn, natoms_, stream);
     mark(2);
     launch_weights(b, s, c, w, stream);
@@ -797,7 +814,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     mark(5);
     if (grad) {
         if (reducer_) reduce(w.dEdcn, natoms_, stream);
-        launch_cn_units(b, s, c, part_, w, pu_, true, stream);
+        launch_cn_units(b, s, c, part_, w, pcn, true, stream);
     }
     mark(6);
     if (!reducer_) {
@@ -1143,9 +1160,8 @@ double Engine::autotune(const Damp& d, const double* d_positions, bool grad, cud
         };
         for (double cell : {0.0, 2.0, 3.0, 4.5, 6.0})
             if (cell != best.morton_cell) { Tuning t = best; t.morton_cell = cell; consider(t); }
-        const int cur_split = best.pair_split ? best.pair_split : (auto_split_ == 1 ? 1 : (mixed_ ? 2 : 4));
         for (int sp : {1, 2, 4})
-            if (sp != cur_split) { Tuning t = best; t.pair_split = sp; consider(t); }
+            if (sp != best.pair_split) { Tuning t = best; t.pair_split = sp; consider(t); }
         if (threebody) {
             // molecules: one block each, or the neighbour-list kernel
             bool any_mol = false;

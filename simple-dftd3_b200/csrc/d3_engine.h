@@ -184,6 +184,8 @@ private:
     int* d_mol_order_ = nullptr;
     std::vector<int> sys_natoms_;
     int auto_split_ = 1;                 // pair split of tuning 0
+    int pair_split() const;              // items per tile pair of the two-body sweep
+    int cn_split() const;                // items per tile pair of the CN sweeps
     bool any_periodic_ = false;          // a system has a periodic direction
     void configure_molecules();          // mol_order_ and root_atoms_ from tune_.atm_mol
     uint8_t* d_sys_mol_ = nullptr;       // [nsys] 1 for those systems

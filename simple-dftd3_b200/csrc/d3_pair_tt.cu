@@ -318,7 +318,9 @@ __device__ __forceinline__ void tt_family(R r2, R r1, bool have_r1, R rrij, R q1
     }
 }
 
-template <class R, int DAMP, bool GRAD, bool PG>
+// SMOOTH: the smooth cutoff of the two-body sum is on (0 < width < cutoff);
+// a compile-time switch keeps its sqrt and divisions out of the plain loop.
+template <class R, int DAMP, bool GRAD, bool PG, bool SMOOTH>
 __global__ void __launch_bounds__(kTTThreads, sizeof(R) == 4 ? 4 : 3)
 k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const int2* units, int nunits, int split,
               const R* UV, double* unit_i, double* unit_j)
@@ -366,7 +368,6 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     const double limj = c.cut2 + ci.w + 1.0e-6 * c.cut2 + 1.0e-6;   // one atom j against tile it
     const double dcx = ci.x - cj.x, dcy = ci.y - cj.y, dcz = ci.z - cj.z;
     const R cutoff = R(c.cut2), cut2 = R(c.cut2 * c.cut2), width = R(c.width2);
-    const bool smooth_on = c.width2 > 0.0 && c.width2 < c.cut2;
     const R s6 = R(d.s6), s8 = R(d.s8);
     const R alp6 = R(d.alp), alp8 = R(d.alp + 2.0);
     const R bet = R(d.bet), a1 = R(d.a1);
@@ -464,8 +465,10 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
                 const R vx = g.vx, vy = g.vy, vz = g.vz, r2 = g.r2;
                 const bool ok = g.ok;
                 nterm += ok ? 1u : 0u;
-                R sw = ok ? R(1) : R(0), dswdr = R(0), r1 = R(1);
-                if (smooth_on) {
+                // weight of the term; without the smooth cutoff the rational
+                // form zeroes a rejected term through its reciprocal instead
+                R sw = (SMOOTH || DAMP != kRational) ? (ok ? R(1) : R(0)) : R(1), dswdr = R(0), r1 = R(1);
+                if constexpr (SMOOTH) {
                     r1 = tt_sqrt<R>(r2);
                     R sw1, dsw1;
                     tt_smooth<R>(r1, cutoff, width, sw1, dsw1);
@@ -477,7 +480,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
                     // rational.f90:462-497: q1 = R0^6, q2 = R0^8, q3 = R0, q4 = sqrt(rrij)
                     const R r4 = r2 * r2;
                     const R a6 = r4 * r2 + q1, a8 = r4 * r4 + q2;
-                    const R inv = tt_rcp<R>(a6 * a8);
+                    const R inv = SMOOTH ? tt_rcp<R>(a6 * a8) : (ok ? tt_rcp<R>(a6 * a8) : R(0));
                     const R t6 = a8 * inv;
                     const R t8 = a6 * inv;
                     e6 = t6; e8 = rrij * t8;
@@ -491,7 +494,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
                     }
                 } else if constexpr (DAMP == kZero) {
                     // zero.f90:490-536: q1 = rs6 R0, q2 = rs8 R0
-                    if (!smooth_on) r1 = tt_sqrt<R>(r2);
+                    if (!SMOOTH) r1 = tt_sqrt<R>(r2);
                     const R r6 = r2 * r2 * r2;
                     const R r8 = r6 * r2;
                     const R t6 = tt_pow<R>(q1 / r1, alp6);
@@ -509,7 +512,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
                     }
                 } else {
                     e6 = e8 = R(0);
-                    tt_family<R, DAMP>(r2, r1, smooth_on, rrij, q1, q2, q3, q4, q5, zc, s6, s8, alp6, alp8, bet, a1,
+                    tt_family<R, DAMP>(r2, r1, SMOOTH, rrij, q1, q2, q3, q4, q5, zc, s6, s8, alp6, alp8, bet, a1,
                                        edisp0, gdisp0, cdisp0);
                 }
                 se += sw * edisp0;
@@ -517,7 +520,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
                 if (PG) { se6 += sw * e6; se8 += sw * e8; spa += sw * dpa; spb += sw * dpb; }
                 if (GRAD) {
                     R gdisp = sw * gdisp0;
-                    if (smooth_on) gdisp += dswdr * edisp0 / r1;
+                    if constexpr (SMOOTH) gdisp += dswdr * edisp0 / r1;
                     const R gx = gdisp * vx, gy = gdisp * vy, gz = gdisp * vz;
                     sgx += gx; sgy += gy; sgz += gz;
                     sxx += gx * vx; syy += gy * vy; szz += gz * vz;
@@ -969,8 +972,12 @@ void launch_tt(const Batch& b, const Species& s, const Damp& d, const Config& c,
                const PairUnits& pu, cudaStream_t stream)
 {
     const int blocks = (pu.nunits * pu.split + kTTWarps - 1) / kTTWarps;
-    k_two_body_tt<R, DAMP, GRAD, PG><<<blocks, kTTThreads, 0, stream>>>(
-        b, s, d, c, p, w, pu.units, pu.nunits, pu.split, (const R*)pu.U, pu.unit_i, pu.unit_j);
+    if (c.width2 > 0.0 && c.width2 < c.cut2)
+        k_two_body_tt<R, DAMP, GRAD, PG, true><<<blocks, kTTThreads, 0, stream>>>(
+            b, s, d, c, p, w, pu.units, pu.nunits, pu.split, (const R*)pu.U, pu.unit_i, pu.unit_j);
+    else
+        k_two_body_tt<R, DAMP, GRAD, PG, false><<<blocks, kTTThreads, 0, stream>>>(
+            b, s, d, c, p, w, pu.units, pu.nunits, pu.split, (const R*)pu.U, pu.unit_i, pu.unit_j);
 }
 
 // the families without damping-parameter derivatives (the engine refuses
