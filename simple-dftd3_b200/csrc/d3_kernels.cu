@@ -476,16 +476,17 @@ __global__ void __launch_bounds__(kThreads) k_cn_chain(Batch b, Species s, Confi
 
 // Per-system sums of the atom energies, virial shares and parameter
 // derivatives in a fixed order (one block per system).
-__global__ void k_reduce_systems(Batch b, Config c, Work w, double* energies, double* sigma9,
-                                 double* param_grad, double* grad_out)
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_reduce_systems(Batch b, Config c, Work w, double* energies, double* sigma9, double* param_grad, double* grad_out)
 {
     constexpr int kVals = 1 + kSigma + kParamGrad;
-    __shared__ double red[kVals][256];
+    __shared__ double red[kVals][BLOCK / 32];
     const int sys = blockIdx.x;
     const int a0 = b.atom_off[sys], a1 = b.atom_off[sys + 1];
     double v[kVals];
     for (int k = 0; k < kVals; k++) v[k] = 0.0;
-    for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+    for (int a = a0 + threadIdx.x; a < a1; a += BLOCK) {
         v[0] += w.e_atom[a] + (w.e3_atom ? w.e3_atom[a] : 0.0);
         if (c.grad)
             for (int k = 0; k < kSigma; k++)
@@ -498,25 +499,28 @@ __global__ void k_reduce_systems(Batch b, Config c, Work w, double* energies, do
             for (int k = 0; k < 3; k++) grad_out[3 * o + k] = w.grad[3 * a + k];
         }
     }
-    for (int k = 0; k < kVals; k++) red[k][threadIdx.x] = v[k];
+    // warp sums, then the warps' sums in warp order (a fixed order)
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int k = 0; k < kVals; k++) {
+        double x = v[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[k][wid] = x;
+    }
     __syncthreads();
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if (threadIdx.x < st)
-            for (int k = 0; k < kVals; k++) red[k][threadIdx.x] += red[k][threadIdx.x + st];
-        __syncthreads();
+    if (wid != 0) return;
+    double tot = 0.0;
+    if (lane < kVals)
+        for (int q = 0; q < BLOCK / 32; q++) tot += red[lane][q];
+    // lane k holds value k
+    if (lane == 0 && energies) energies[sys] = tot;
+    if (c.grad && sigma9 && lane >= 1 && lane <= kSigma) {
+        // Fortran sigma(3,3): element (a, b) at a + 3 b; symmetric; packed xx yy zz xy xz yz
+        constexpr int kAt[kSigma][2] = {{0, 0}, {4, 4}, {8, 8}, {1, 3}, {2, 6}, {5, 7}};
+        double* o = sigma9 + 9 * sys;
+        o[kAt[lane - 1][0]] = tot;
+        o[kAt[lane - 1][1]] = tot;
     }
-    if (threadIdx.x == 0) {
-        if (energies) energies[sys] = red[0][0];
-        if (c.grad && sigma9) {
-            // Fortran sigma(3,3): element (a, b) at a + 3 b; symmetric
-            const double sx = red[1][0], sy = red[2][0], sz = red[3][0];
-            const double xy = red[4][0], xz = red[5][0], yz = red[6][0];
-            double* o = sigma9 + 9 * sys;
-            o[0] = sx; o[1] = xy; o[2] = xz; o[3] = xy; o[4] = sy; o[5] = yz; o[6] = xz; o[7] = yz; o[8] = sz;
-        }
-        if (c.param_grad && param_grad)
-            for (int k = 0; k < kParamGrad; k++) param_grad[kParamGrad * sys + k] = red[1 + kSigma + k][0];
-    }
+    if (c.param_grad && param_grad && lane > kSigma && lane < kVals) param_grad[kParamGrad * sys + lane - 1 - kSigma] = tot;
 }
 
 // Dependent-FMA throughput probe: 8 independent chains per thread, used to
@@ -636,7 +640,11 @@ void launch_reduce_systems(const Batch& b, const Config& c, const Work& w, doubl
                            double* sigma9, double* param_grad, double* grad_out, cudaStream_t stream)
 {
     if (b.nsys <= 0) return;
-    k_reduce_systems<<<b.nsys, 256, 0, stream>>>(b, c, w, energies, sigma9, param_grad, grad_out);
+    // a block of 1024 threads where systems average above 512 atoms
+    if (b.natoms > 512LL * b.nsys)
+        k_reduce_systems<1024><<<b.nsys, 1024, 0, stream>>>(b, c, w, energies, sigma9, param_grad, grad_out);
+    else
+        k_reduce_systems<256><<<b.nsys, 256, 0, stream>>>(b, c, w, energies, sigma9, param_grad, grad_out);
 }
 
 }  // namespace d3

@@ -602,12 +602,14 @@ __device__ __forceinline__ unsigned long long order_word(unsigned long long grou
 }
 
 // Slabs and columns of every system from its bounding box, boxes of about
-// equal edge holding one tile each; one block per system, which also writes
-// the pass-0 words of its atoms.
-__global__ void k_rank_shape(const double* __restrict__ pos, const int* atom_off, const int* tile_off, int2* shape,
-                             unsigned long long* word)
+// equal edge holding one tile each; one block of BLOCK threads per system,
+// which also writes the pass-0 words of its atoms.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_rank_shape(const double* __restrict__ pos, const int* atom_off, const int* tile_off, int2* shape,
+             unsigned long long* word)
 {
-    __shared__ double red[6][kOrderThreads / 32];
+    __shared__ double red[6][BLOCK / 32];
     const int sys = blockIdx.x;
     const int a0 = atom_off[sys], a1 = atom_off[sys + 1];
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -629,7 +631,7 @@ __global__ void k_rank_shape(const double* __restrict__ pos, const int* atom_off
         for (int c = 0; c < 3; c++) { red[c][wid] = lo[c]; red[3 + c][wid] = hi[c]; }
     __syncthreads();
     if (threadIdx.x != 0) return;
-    for (int w = 1; w < kOrderThreads / 32; w++)
+    for (int w = 1; w < BLOCK / 32; w++)
         for (int c = 0; c < 3; c++) {
             lo[c] = fmin(lo[c], red[c][w]);
             hi[c] = fmax(hi[c], red[3 + c][w]);
@@ -647,13 +649,18 @@ __global__ void k_rank_shape(const double* __restrict__ pos, const int* atom_off
     shape[sys] = make_int2(nx, ny);
 }
 
+constexpr int kRankThreads = 256;        // threads of a rank-pass block
+constexpr int kRankChunk = 2048;         // words staged in shared memory at a time
+
 template <int PASS, int G>
-__global__ void k_rank_pass(const double* __restrict__ pos, int n, const int* sys_of_atom, const int* atom_off,
-                            const int* tile_off, const int2* shape, const unsigned long long* __restrict__ word,
-                            unsigned long long* next, const int* sp_in, const uint8_t* ghost_in, const int* zid_in,
-                            bool mixed, int* perm, double* x, double* y, double* z, float4* xhi, float4* xlo,
-                            int* sp, uint8_t* ghost, int* local, int* zid)
+__global__ void __launch_bounds__(kRankThreads)
+k_rank_pass(const double* __restrict__ pos, int n, const int* sys_of_atom, const int* atom_off,
+            const int* tile_off, const int2* shape, const unsigned long long* __restrict__ word,
+            unsigned long long* next, const int* sp_in, const uint8_t* ghost_in, const int* zid_in,
+            bool mixed, int* perm, double* x, double* y, double* z, float4* xhi, float4* xlo,
+            int* sp, uint8_t* ghost, int* local, int* zid)
 {
+    __shared__ unsigned long long sword[kRankChunk];
     // G lanes per atom a (G = 4, 8 or 32 by the largest system)
     const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int a = (int)(gt / G), lane = (int)(gt % G);
@@ -666,9 +673,20 @@ __global__ void k_rank_pass(const double* __restrict__ pos, int n, const int* sy
         a1 = atom_off[sys + 1];
         wa = word[a];
     }
-    // position of a inside its system: the words below its own
+    // position of a inside its system: the words below its own.  The words of
+    // the systems of the block's atoms are staged through shared memory.
+    const int afirst = blockIdx.x * (kRankThreads / G);
+    const int alast = min(n, afirst + kRankThreads / G) - 1;
+    const int r0 = atom_off[sys_of_atom[afirst]], r1 = atom_off[sys_of_atom[alast] + 1];
     int r = 0;
-    for (int j = a0 + lane; j < a1; j += G) r += (int)(word[j] < wa);
+    for (int c0 = r0; c0 < r1; c0 += kRankChunk) {
+        const int c1 = min(r1, c0 + kRankChunk);
+        __syncthreads();
+        for (int k = threadIdx.x; k < c1 - c0; k += kRankThreads) sword[k] = word[c0 + k];
+        __syncthreads();
+        const int lo = max(a0, c0), hi = min(a1, c1);
+        for (int j = lo + lane; j < hi; j += G) r += (int)(sword[j - c0] < wa);
+    }
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
     if (!valid || lane != 0) return;
@@ -769,16 +787,19 @@ void launch_rank_order(const double* pos, int natoms, int nsys, int max_atoms, c
                        int* local, int* zid, cudaStream_t stream)
 {
     if (natoms <= 0 || nsys <= 0) return;
-    k_rank_shape<<<nsys, kOrderThreads, 0, stream>>>(pos, atom_off, tile_off, shape, word_a);
+    // a block of 1024 threads for systems above 256 atoms (two atoms a thread
+    // for 2000 atoms instead of sixteen)
+    if (max_atoms > 256) k_rank_shape<1024><<<nsys, 1024, 0, stream>>>(pos, atom_off, tile_off, shape, word_a);
+    else k_rank_shape<kOrderThreads><<<nsys, kOrderThreads, 0, stream>>>(pos, atom_off, tile_off, shape, word_a);
     // lanes per atom: a whole warp for large systems, groups of 8 or 4 lanes
     // for batches of molecules (a warp would idle on a few dozen words)
     const int g = max_atoms > 512 ? 32 : (max_atoms > 64 ? 8 : 4);
-    const unsigned blocks = (unsigned)(((long long)natoms * g + 255) / 256);
+    const unsigned blocks = (unsigned)(((long long)natoms * g + kRankThreads - 1) / kRankThreads);
 #define D3_RANK_PASS(P, W_IN, W_OUT)                                                                          \
     do {                                                                                                     \
-        if (g == 32) k_rank_pass<P, 32><<<blocks, 256, 0, stream>>>RANK_ARGS(W_IN, W_OUT);                  \
-        else if (g == 8) k_rank_pass<P, 8><<<blocks, 256, 0, stream>>>RANK_ARGS(W_IN, W_OUT);               \
-        else k_rank_pass<P, 4><<<blocks, 256, 0, stream>>>RANK_ARGS(W_IN, W_OUT);                           \
+        if (g == 32) k_rank_pass<P, 32><<<blocks, kRankThreads, 0, stream>>>RANK_ARGS(W_IN, W_OUT);         \
+        else if (g == 8) k_rank_pass<P, 8><<<blocks, kRankThreads, 0, stream>>>RANK_ARGS(W_IN, W_OUT);      \
+        else k_rank_pass<P, 4><<<blocks, kRankThreads, 0, stream>>>RANK_ARGS(W_IN, W_OUT);                  \
     } while (0)
 #define RANK_ARGS(W_IN, W_OUT) (pos, natoms, sys_of_atom, atom_off, tile_off, shape, W_IN, W_OUT, sp_in, ghost_in, \
                                 zid_in, mixed, perm, x, y, z, xhi, xlo, sp, ghost, local, zid)

@@ -589,10 +589,49 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     }
 }
 
-// Per-atom sums of the unit slots in a fixed order: one warp per atom, the
-// lanes take the atom's slots (its i slots of the units (t, jt <= t), then
-// its j slots of the units (it >= t, t)) round robin and a fixed shuffle tree
-// adds the lane sums.
+// An atom's sums over the slots of the items that hold it, in a fixed order,
+// one warp per atom.  Lane l adds value l % VI of the atom's i slots (items
+// l / VI, l / VI + 32 / VI, ...) and value l % VJ of its j slots, VI and VJ
+// the powers of two >= KI and KJ, so that a warp load reads a few contiguous
+// slot rows; the i slots of an atom are the items of the units (tl, jt <= tl),
+// consecutive, its j slots those of the units (it >= tl, tl).  The j total of
+// value m is added to i value JOFF + m; lanes 0 .. KI - 1 return the totals.
+template <int KI, int KJ, int JOFF>
+__device__ __forceinline__ double tt_gather_atom(long long base, int tl, int nt, int sl, int split,
+                                                 const double* unit_i, const double* unit_j, int lane)
+{
+    constexpr int VI = KI <= 1 ? 1 : KI <= 2 ? 2 : KI <= 4 ? 4 : KI <= 8 ? 8 : 16;
+    constexpr int VJ = KJ <= 1 ? 1 : KJ <= 2 ? 2 : 4;
+    const int sh = split >> 1;   // log2 of the split (1, 2 or 4)
+    double si = 0.0, sj = 0.0;
+    if (lane % VI < KI) {
+        const long long i0 = (base + (long long)tl * (tl + 1) / 2) * split;
+        const double* p = unit_i + (i0 * kTile + sl) * kUnitI + lane % VI;
+        const int ni = (tl + 1) * split;
+#pragma unroll 8
+        for (int q = lane / VI; q < ni; q += 32 / VI) si += p[(long long)q * (kTile * kUnitI)];
+    }
+#pragma unroll
+    for (int o = VI; o < 32; o <<= 1) si += __shfl_xor_sync(0xffffffffu, si, o);
+    if (lane % VJ < KJ) {
+        const int nj = (nt - tl) * split;
+#pragma unroll 8
+        for (int q = lane / VJ; q < nj; q += 32 / VJ) {
+            const int it = tl + (q >> sh);
+            const long long item = (base + (long long)it * (it + 1) / 2 + tl) * split + (q & (split - 1));
+            sj += unit_j[(item * kTile + sl) * kUnitJ + lane % VJ];
+        }
+    }
+#pragma unroll
+    for (int o = VJ; o < 32; o <<= 1) sj += __shfl_xor_sync(0xffffffffu, sj, o);
+    const int m = lane - JOFF;
+    const double add = __shfl_sync(0xffffffffu, sj, m & (VJ - 1));
+    if (m >= 0 && m < KJ) si += add;
+    return si;
+}
+
+// Per-atom sums of the two-body unit slots: energy, dE/dCN, gradient,
+// virial and parameter derivatives (lanes 0 .. 14 of tt_gather_atom).
 __global__ void k_unit_gather(Batch b, Config c, const int* unit_base, int split, const double* unit_i,
                               const double* unit_j, Work w)
 {
@@ -604,39 +643,12 @@ __global__ void k_unit_gather(Batch b, Config c, const int* unit_base, int split
     const int t0 = b.tile_off[sys], t1 = b.tile_off[sys + 1];
     const int tl = (a - as) / kTile;              // tile of a, local to the system
     const int sl = (a - as) % kTile;              // slot lane
-    const int nt = t1 - t0;
-    const long long base = unit_base[sys];
-    double v[kUnitI];
-#pragma unroll
-    for (int k = 0; k < kUnitI; k++) v[k] = 0.0;
-    const int ni = (tl + 1) * split, nj = (nt - tl) * split;
-    for (int q = lane; q < ni; q += 32) {
-        const int jt = q / split, sb = q % split;
-        const long long item = (base + (long long)tl * (tl + 1) / 2 + jt) * split + sb;
-        const double* o = unit_i + (item * kTile + sl) * kUnitI;
-#pragma unroll
-        for (int k = 0; k < kUnitI; k++) v[k] += o[k];
-    }
-    for (int q = lane; q < nj; q += 32) {
-        const int it = tl + q / split, sb = q % split;
-        const long long item = (base + (long long)it * (it + 1) / 2 + tl) * split + sb;
-        const double* o = unit_j + (item * kTile + sl) * kUnitJ;
-        v[1] += o[0]; v[2] += o[1]; v[3] += o[2]; v[4] += o[3];
-    }
-#pragma unroll
-    for (int k = 0; k < kUnitI; k++) v[k] = wsum_tt<double>(v[k]);
-    if (lane != 0) return;
-    w.e_atom[a] = v[0];
-    if (w.dEdcn) w.dEdcn[a] = v[1];
-    if (c.grad) {
-        w.grad[3 * a + 0] = v[2]; w.grad[3 * a + 1] = v[3]; w.grad[3 * a + 2] = v[4];
-        double* sg = w.sig_atom + kSigma * a;
-        for (int k = 0; k < kSigma; k++) sg[k] = v[5 + k];
-    }
-    if (c.param_grad && w.pg_atom) {
-        double* pg = w.pg_atom + kParamGrad * a;
-        for (int k = 0; k < 4; k++) pg[k] = v[11 + k];
-    }
+    const double v = tt_gather_atom<kUnitI, kUnitJ, 1>(unit_base[sys], tl, t1 - t0, sl, split, unit_i, unit_j, lane);
+    if (lane == 0) w.e_atom[a] = v;
+    else if (lane == 1) { if (w.dEdcn) w.dEdcn[a] = v; }
+    else if (lane < 5) { if (c.grad) w.grad[3 * a + lane - 2] = v; }
+    else if (lane < 5 + kSigma) { if (c.grad) w.sig_atom[kSigma * a + lane - 5] = v; }
+    else if (lane < kUnitI) { if (c.param_grad && w.pg_atom) w.pg_atom[kParamGrad * a + lane - 11] = v; }
 }
 
 constexpr double kKcnTT = 16.0;   // ncoord.f90:31
@@ -923,7 +935,7 @@ k_cn_chain_stored(Batch b, Config c, Partition p, Work w, const int2* units, int
 }
 
 // Gather of the CN (assign) or chain-rule (add to gradient and virial) slots,
-// one warp per atom, in the fixed order of k_unit_gather.
+// one warp per atom, in the fixed order of tt_gather_atom.
 template <bool CHAIN>
 __global__ void k_cn_gather(Batch b, const int* unit_base, int split, const double* unit_i, const double* unit_j,
                             Work w)
@@ -935,35 +947,14 @@ __global__ void k_cn_gather(Batch b, const int* unit_base, int split, const doub
     const int as = b.atom_off[sys];
     const int t0 = b.tile_off[sys], t1 = b.tile_off[sys + 1];
     const int tl = (a - as) / kTile, sl = (a - as) % kTile;
-    const int nt = t1 - t0;
-    const long long base = unit_base[sys];
-    constexpr int kI = CHAIN ? 9 : 1, kJ = CHAIN ? 3 : 1;
-    double v[kI];
-#pragma unroll
-    for (int k = 0; k < kI; k++) v[k] = 0.0;
-    const int ni = (tl + 1) * split, nj = (nt - tl) * split;
-    for (int q = lane; q < ni; q += 32) {
-        const long long item = (base + (long long)tl * (tl + 1) / 2 + q / split) * split + q % split;
-        const double* o = unit_i + (item * kTile + sl) * kUnitI;
-#pragma unroll
-        for (int k = 0; k < kI; k++) v[k] += o[k];
-    }
-    for (int q = lane; q < nj; q += 32) {
-        const int itl = tl + q / split;
-        const long long item = (base + (long long)itl * (itl + 1) / 2 + tl) * split + q % split;
-        const double* o = unit_j + (item * kTile + sl) * kUnitJ;
-#pragma unroll
-        for (int k = 0; k < kJ; k++) v[k] += o[k];
-    }
-#pragma unroll
-    for (int k = 0; k < kI; k++) v[k] = wsum_tt<double>(v[k]);
-    if (lane != 0) return;
     if (!CHAIN) {
-        w.cn[a] = v[0];
+        const double v = tt_gather_atom<1, 1, 0>(unit_base[sys], tl, t1 - t0, sl, split, unit_i, unit_j, lane);
+        if (lane == 0) w.cn[a] = v;
     } else {
-        w.grad[3 * a + 0] += v[0]; w.grad[3 * a + 1] += v[1]; w.grad[3 * a + 2] += v[2];
-        double* sg = w.sig_atom + kSigma * a;
-        for (int k = 0; k < kSigma; k++) sg[k] += v[3 + k];
+        // g(3), sigma(6); j slots g(3)
+        const double v = tt_gather_atom<9, 3, 0>(unit_base[sys], tl, t1 - t0, sl, split, unit_i, unit_j, lane);
+        if (lane < 3) w.grad[3 * a + lane] += v;
+        else if (lane < 9) w.sig_atom[kSigma * a + lane - 3] += v;
     }
 }
 
