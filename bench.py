@@ -44,7 +44,7 @@ FLOPS_PER_TRIPLE = 220         # ATM term with gradient, virial and dE/dCN
 METRIC = "pair-terms/s, D3(BJ) two-body E+grad+virial (mixed FP32/FP64, <=1e-7 rel. E error)"
 # DRAM bytes (read + write) of one k_two_body_tt<float, rational> launch on cell2000, from
 # an ncu capture of that launch
-TWO_BODY_TRAFFIC_BYTES = 982784
+TWO_BODY_TRAFFIC_BYTES = 1065728
 
 
 def parse_args():
