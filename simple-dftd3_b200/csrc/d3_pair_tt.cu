@@ -330,6 +330,10 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     __shared__ V stl[kTTWarps][kTTChunk];
     // FP64 sums, [value][lane]: i sums of the lane's atom, j sums of partner lane
     __shared__ double sacc[kTTWarps][kUnitI + kUnitJ][32];
+    // FP32 form: the reference weights gw, dgw/dCN of the lane's atom, [ref][lane]
+    // (read once per partner; registers in the FP64 form)
+    constexpr bool kSharedWeights = sizeof(R) == 4;
+    __shared__ R swt[kSharedWeights ? kTTWarps : 1][2 * kMaxRef][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int item = blockIdx.x * kTTWarps + wid;
     if (item >= nunits * split) return;
@@ -356,11 +360,16 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
         hiy = __double2float_rn(yi); liy = __double2float_rn(yi - (double)hiy);
         hiz = __double2float_rn(zi); liz = __double2float_rn(zi - (double)hiz);
     }
-    R gwi[kMaxRef], dgwi[kMaxRef];
+    R gwi[kSharedWeights ? 1 : kMaxRef], dgwi[kSharedWeights ? 1 : kMaxRef];
+    if constexpr (kSharedWeights) {
 #pragma unroll
-    for (int r = 0; r < kMaxRef; r++) {
-        if constexpr (sizeof(R) == 8) { gwi[r] = w.gw[ic * kMaxRef + r]; dgwi[r] = w.dgw[ic * kMaxRef + r]; }
-        else { gwi[r] = w.gwf[ic * kMaxRef + r]; dgwi[r] = w.dgwf[ic * kMaxRef + r]; }
+        for (int r = 0; r < kMaxRef; r++) {
+            swt[wid][r][lane] = w.gwf[ic * kMaxRef + r];
+            swt[wid][kMaxRef + r][lane] = w.dgwf[ic * kMaxRef + r];
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < kMaxRef; r++) { gwi[r] = w.gw[ic * kMaxRef + r]; dgwi[r] = w.dgw[ic * kMaxRef + r]; }
     }
     const int tt0 = b.img_off[kImgDisp2 * (b.nsys + 1) + sys], tt1 = b.img_off[kImgDisp2 * (b.nsys + 1) + sys + 1];
     const double4 ci = b.tiles[it], cj = b.tiles[jt];
@@ -422,9 +431,12 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
                 tt_load_uv<R>(UV + ((size_t)j * nid + si) * (2 * kRefPad), uj, duj);
 #pragma unroll
                 for (int r = 0; r < kMaxRef; r++) {
-                    c6 += gwi[r] * uj[r];
-                    dc6i += dgwi[r] * uj[r];
-                    dc6j += gwi[r] * duj[r];
+                    R g, dg;
+                    if constexpr (kSharedWeights) { g = swt[wid][r][lane]; dg = swt[wid][kMaxRef + r][lane]; }
+                    else { g = gwi[r]; dg = dgwi[r]; }
+                    c6 += g * uj[r];
+                    dc6i += dg * uj[r];
+                    dc6j += g * duj[r];
                 }
                 valid = c6 != R(0);
             }
