@@ -214,17 +214,20 @@ void launch_cn_chain_rule_tiled(const Batch& b, const Species& s, const Config& 
 // gather (d3_pair_tt.cu); writes e_atom, dEdcn, grad, sig_atom, pg_atom.
 // Coordination number (chain = false, writes cn) or its chain rule (chain =
 // true, adds to grad and sig_atom) over the same units (d3_pair_tt.cu).
+// weights: the CN pass also writes the reference weights (as launch_weights)
+// and, when uv is given, the species vectors of PairUnits::U.
 size_t cn_store_bytes(const PairUnits& pu, bool mixed);   // d3_pair_tt.cu
 constexpr int kCnStoreChunk = 128; // translations of a system the stored chain rule covers
 void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Partition& p, const Work& w,
-                     const PairUnits& pu, bool chain, cudaStream_t stream);
+                     const PairUnits& pu, bool chain, cudaStream_t stream, bool weights = false, void* uv = nullptr);
 size_t pair_unit_slot_doubles();   // per unit: i and j slots
 size_t pair_unit_i_doubles();      // per unit: i slots
 size_t species_vector_doubles(int natoms, int nid);   // PairUnits::U (FP64 size)
-// ev_begin/ev_end (or null) are recorded around the tile-pair kernel alone.
+// ev_begin/ev_end (or null) are recorded around the tile-pair kernel alone;
+// species_ready: the CN pass wrote the species vectors.
 void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
                            const Work& w, const PairUnits& pu, cudaStream_t stream, cudaEvent_t ev_begin = nullptr,
-                           cudaEvent_t ev_end = nullptr);
+                           cudaEvent_t ev_end = nullptr, bool species_ready = false);
 
 // Three-body term (d3_atm.cu): C6 table, neighbour lists, triple sum.
 size_t atm_c6_entry_bytes(bool mixed);

@@ -778,13 +778,18 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     mark(0);
     order_atoms(d, d_positions, b, mixed_, stream);
     mark(1);
-    launch_cn_units(b, s, c, part_, w, pcn, false, stream);
+    // without a reducer the CN pass also writes the reference weights and the
+    // species vectors (one kernel after the sweep instead of three)
+    const bool two_body = two_body_active(d) || pg;
+    const bool fused = !reducer_;
+    launch_cn_units(b, s, c, part_, w, pcn, false, stream, fused, fused && two_body ? pu_.U : nullptr);
     if (reducer_) reduce(w.cn, natoms_, stream);
     mark(2);
-    launch_weights(b, s, c, w, stream);
+    if (!fused) launch_weights(b, s, c, w, stream);
     mark(3);
-    if (two_body_active(d) || pg) {
-        launch_two_body_units(b, s, d, c, part_, w, pu_, stream, timed ? kev_[0] : nullptr, timed ? kev_[1] : nullptr);
+    if (two_body) {
+        launch_two_body_units(b, s, d, c, part_, w, pu_, stream, timed ? kev_[0] : nullptr, timed ? kev_[1] : nullptr,
+                              fused);
     } else {
         check(cudaMemsetAsync(w.e_atom, 0, sizeof(double) * natoms_, stream), "memset");
         if (grad) {

@@ -970,6 +970,89 @@ __global__ void k_cn_gather(Batch b, const int* unit_base, int split, const doub
     }
 }
 
+constexpr double kWfTT = 4.0;   // model.f90:80
+
+// After the CN sweep, one warp per atom: the CN from the unit slots, the
+// Gaussian reference weights and their CN derivative with the reference's
+// NaN/Inf fallback (weight_references, model.f90:201-324; FP64, the
+// arithmetic of k_weights: lane r takes reference r, the sums run in
+// reference order) and, when UV is given, the atom's species vectors for
+// the two-body sweep (the entries of k_species_vectors).
+template <class R>
+__global__ void k_cn_weights(Batch b, Species s, Config c, const int* unit_base, int split, const double* unit_i,
+                             const double* unit_j, Work w, R* UV)
+{
+    const int lane = threadIdx.x & 31;
+    const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (a >= b.natoms) return;
+    const int sys = b.sys_of_atom[a];
+    const int as = b.atom_off[sys];
+    const int t0 = b.tile_off[sys], t1 = b.tile_off[sys + 1];
+    const int tl = (a - as) / kTile, sl = (a - as) % kTile;
+    const double cn = __shfl_sync(
+        0xffffffffu, tt_gather_atom<1, 1, 0>(unit_base[sys], tl, t1 - t0, sl, split, unit_i, unit_j, lane), 0);
+    if (lane == 0) w.cn[a] = cn;
+    const int sp = b.sp[a];
+    const int nref = s.nref[sp];
+    const double* cnref = s.refcn + sp * kMaxRef;
+    const double wf2 = 2 * kWfTT;
+    const double cr = lane < nref ? cnref[lane] : 0.0;
+    double g = 0.0;
+    if (lane < nref) {
+        const double d = cn - cr;
+        g = exp(-kWfTT * d * d);
+    }
+    double norm = 0.0, dnorm = 0.0, maxcn = cnref[0];
+    for (int r = 0; r < nref; r++) {
+        const double gr = __shfl_sync(0xffffffffu, g, r), crr = __shfl_sync(0xffffffffu, cr, r);
+        norm = norm + gr;
+        dnorm = dnorm + wf2 * (crr - cn) * gr;
+        maxcn = fmax(maxcn, crr);
+    }
+    norm = 1.0 / norm;
+    double gwk = 0.0, dgwk = 0.0;
+    if (lane < nref) {
+        const double expd = wf2 * (cr - cn) * g;
+        gwk = g * norm;
+        if (isnan(gwk) || isinf(gwk)) gwk = (maxcn == cr) ? 1.0 : 0.0;
+        dgwk = expd * norm - g * dnorm * (norm * norm);
+        if (isnan(dgwk) || isinf(dgwk)) dgwk = 0.0;
+    }
+    if (lane < kMaxRef) {
+        w.gw[a * kMaxRef + lane] = gwk;
+        w.dgw[a * kMaxRef + lane] = dgwk;
+        if (c.mixed) {
+            w.gwf[a * kMaxRef + lane] = float(gwk);
+            w.dgwf[a * kMaxRef + lane] = float(dgwk);
+        }
+    }
+    if (!UV) return;
+    double gq[kMaxRef], dq[kMaxRef];
+#pragma unroll
+    for (int q = 0; q < kMaxRef; q++) {
+        gq[q] = __shfl_sync(0xffffffffu, gwk, q);
+        dq[q] = __shfl_sync(0xffffffffu, dgwk, q);
+    }
+    const bool ghost = b.ghost && b.ghost[a];
+    const int nid = b.nid;
+    R* o = UV + (size_t)a * nid * (2 * kRefPad);
+    for (int e = lane; e < nid * kRefPad; e += 32) {
+        const int sx = e / kRefPad, r = e % kRefPad;
+        double u = 0.0, du = 0.0;
+        if (!ghost && r < s.nref[sx]) {
+            const double* ref = s.c6ref + ((size_t)(sx * nid + sp) * kMaxRef + r) * kMaxRef;
+#pragma unroll
+            for (int q = 0; q < kMaxRef; q++)
+                if (q < nref) {
+                    u += gq[q] * __ldg(ref + q);
+                    du += dq[q] * __ldg(ref + q);
+                }
+        }
+        o[sx * (2 * kRefPad) + r] = R(u);
+        o[sx * (2 * kRefPad) + kRefPad + r] = R(du);
+    }
+}
+
 template <class R, int DAMP, bool GRAD, bool PG>
 void launch_tt(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p, const Work& w,
                const PairUnits& pu, cudaStream_t stream)
@@ -1009,7 +1092,7 @@ void launch_tt_flags(const Batch& b, const Species& s, const Damp& d, const Conf
 }  // namespace
 
 void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Partition& p, const Work& w,
-                     const PairUnits& pu, bool chain, cudaStream_t stream)
+                     const PairUnits& pu, bool chain, cudaStream_t stream, bool weights, void* uv)
 {
     if (b.natoms <= 0) return;
     const int blocks = (pu.nunits * pu.split + kTTWarps - 1) / kTTWarps;
@@ -1039,8 +1122,15 @@ void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Pa
         }
     }
 #undef D3_CN
-    if (chain) k_cn_gather<true><<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
-    else k_cn_gather<false><<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
+    const unsigned gb = (unsigned)((b.natoms + 7) / 8);
+    if (chain) k_cn_gather<true><<<gb, 256, 0, stream>>>(b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
+    else if (!weights) k_cn_gather<false><<<gb, 256, 0, stream>>>(b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
+    else if (c.mixed)
+        k_cn_weights<float><<<gb, 256, 0, stream>>>(b, s, c, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w,
+                                                     (float*)uv);
+    else
+        k_cn_weights<double><<<gb, 256, 0, stream>>>(b, s, c, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w,
+                                                      (double*)uv);
 }
 
 size_t cn_store_bytes(const PairUnits& pu, bool mixed)
@@ -1055,11 +1145,13 @@ size_t species_vector_doubles(int natoms, int nid) { return (size_t)natoms * nid
 
 void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
                            const Work& w, const PairUnits& pu, cudaStream_t stream, cudaEvent_t ev_begin,
-                           cudaEvent_t ev_end)
+                           cudaEvent_t ev_end, bool species_ready)
 {
     if (b.natoms <= 0) return;
     const long long nsv = (long long)b.natoms * b.nid * kRefPad;
-    if (c.mixed)
+    if (species_ready) {
+        // k_cn_weights wrote the species vectors
+    } else if (c.mixed)
         k_species_vectors<float><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (float*)pu.U);
     else
         k_species_vectors<double><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (double*)pu.U);
