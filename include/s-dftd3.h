@@ -151,10 +151,11 @@ dftd3_set_model_mpi_comm(dftd3_error /* error */,
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_delete_model(dftd3_model* /* disp */) SDFTD3_API_SUFFIX__V_0_2;
 
-/* Damping parameters.  Zero (new_zero_damping_api :626-654) and rational
- * (new_rational_damping_api :558-586) are evaluated on the GPU; the
- * parameter-database loaders (load_*_api) and the other damping families
- * report "not supported". */
+/* Damping parameters.  Zero (new_zero_damping_api :626-654), rational
+ * (new_rational_damping_api :558-586) and the other families below
+ * (modified rational and zero, optimized power, CSO, Z; :658-1018) are
+ * evaluated on the GPU; the parameter-database loaders (load_*_api,
+ * e.g. :590-622) look up the reference's method table. */
 SDFTD3_API_ENTRY dftd3_param SDFTD3_API_CALL
 dftd3_new_zero_damping(dftd3_error /* error */,
                        double /* s6 */,
@@ -297,7 +298,8 @@ dftd3_get_dispersion(dftd3_error /* error */,
                      double* /* gradient[n][3] */,
                      double* /* sigma[3][3] */) SDFTD3_API_SUFFIX__V_0_2;
 
-/* Pairwise decomposition (get_pairwise_dispersion_api): not supported */
+/* Pairwise decomposition (get_pairwise_dispersion_api :1180-1233): FP64
+ * pair-energy matrices of the two- and three-body terms */
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_get_pairwise_dispersion(dftd3_error /* error */,
                               dftd3_structure /* mol */,
@@ -306,7 +308,8 @@ dftd3_get_pairwise_dispersion(dftd3_error /* error */,
                               double* /* pair_energy2[n][n] */,
                               double* /* pair_energy3[n][n] */) SDFTD3_API_SUFFIX__V_0_5;
 
-/* Analytical Hessian (get_dispersion_hessian_api): not supported */
+/* Analytical Hessian (get_dispersion_hessian_api :1115-1176): FP64 energy
+ * and Hessian of one structure */
 SDFTD3_API_ENTRY void SDFTD3_API_CALL
 dftd3_get_dispersion_hessian(dftd3_error /* error */,
                              dftd3_structure /* mol */,
