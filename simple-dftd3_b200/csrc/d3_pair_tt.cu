@@ -329,11 +329,12 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     __shared__ V sth[kTTWarps][kTTChunk];
     __shared__ V stl[kTTWarps][kTTChunk];
     // FP64 sums, [value][lane]: i sums of the lane's atom, j sums of partner lane
-    __shared__ double sacc[kTTWarps][kUnitI + kUnitJ][32];
-    // FP32 form: the reference weights gw, dgw/dCN of the lane's atom, [ref][lane]
-    // (read once per partner; registers in the FP64 form)
-    constexpr bool kSharedWeights = sizeof(R) == 4;
-    __shared__ R swt[kSharedWeights ? kTTWarps : 1][2 * kMaxRef][32];
+    // (the FP64 form keeps its i sums in FP64 registers: j sums only)
+    constexpr int kAccI = sizeof(R) == 4 ? kUnitI : 0;
+    __shared__ double sacc[kTTWarps][kAccI + kUnitJ][32];
+    // the reference weights gw, dgw/dCN of the lane's atom, [ref][lane]
+    // (read once per partner)
+    __shared__ R swt[kTTWarps][2 * kMaxRef][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int item = blockIdx.x * kTTWarps + wid;
     if (item >= nunits * split) return;
@@ -360,16 +361,15 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
         hiy = __double2float_rn(yi); liy = __double2float_rn(yi - (double)hiy);
         hiz = __double2float_rn(zi); liz = __double2float_rn(zi - (double)hiz);
     }
-    R gwi[kSharedWeights ? 1 : kMaxRef], dgwi[kSharedWeights ? 1 : kMaxRef];
-    if constexpr (kSharedWeights) {
 #pragma unroll
-        for (int r = 0; r < kMaxRef; r++) {
+    for (int r = 0; r < kMaxRef; r++) {
+        if constexpr (sizeof(R) == 8) {
+            swt[wid][r][lane] = w.gw[ic * kMaxRef + r];
+            swt[wid][kMaxRef + r][lane] = w.dgw[ic * kMaxRef + r];
+        } else {
             swt[wid][r][lane] = w.gwf[ic * kMaxRef + r];
             swt[wid][kMaxRef + r][lane] = w.dgwf[ic * kMaxRef + r];
         }
-    } else {
-#pragma unroll
-        for (int r = 0; r < kMaxRef; r++) { gwi[r] = w.gw[ic * kMaxRef + r]; dgwi[r] = w.dgw[ic * kMaxRef + r]; }
     }
     const int tt0 = b.img_off[kImgDisp2 * (b.nsys + 1) + sys], tt1 = b.img_off[kImgDisp2 * (b.nsys + 1) + sys + 1];
     const double4 ci = b.tiles[it], cj = b.tiles[jt];
@@ -382,10 +382,11 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     const R bet = R(d.bet), a1 = R(d.a1);
     const int zsi = DAMP == kZDamping ? b.zid[ic] : 0;
     const int nid = b.nid;
-    // i sums: partials in R over the partners of one translation chunk (at
-    // most 32 additions), added to the FP64 sums in shared memory per chunk
+    // i sums: FP32 form, partials in R over the partners of one translation
+    // chunk (at most 32 additions), added to the FP64 sums in shared memory
+    // per chunk; FP64 form, the register sums themselves
     double (*acc)[32] = sacc[wid];
-    for (int v = 0; v < kUnitI + kUnitJ; v++) acc[v][lane] = 0.0;
+    for (int v = 0; v < kAccI + kUnitJ; v++) acc[v][lane] = 0.0;
     __syncwarp();
     R te = R(0), tde = R(0), tgx = R(0), tgy = R(0), tgz = R(0);
     R txx = R(0), tyy = R(0), tzz = R(0), txy = R(0), txz = R(0), tyz = R(0);
@@ -393,6 +394,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     unsigned nterm = 0;
 
     auto flush = [&]() {
+        if constexpr (kAccI == 0) return;   // FP64 form: the register sums are the FP64 sums
         acc[0][lane] += double(te); acc[1][lane] += double(tde);
         te = tde = R(0);
         if (GRAD) {
@@ -431,9 +433,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
                 tt_load_uv<R>(UV + ((size_t)j * nid + si) * (2 * kRefPad), uj, duj);
 #pragma unroll
                 for (int r = 0; r < kMaxRef; r++) {
-                    R g, dg;
-                    if constexpr (kSharedWeights) { g = swt[wid][r][lane]; dg = swt[wid][kMaxRef + r][lane]; }
-                    else { g = gwi[r]; dg = dgwi[r]; }
+                    const R g = swt[wid][r][lane], dg = swt[wid][kMaxRef + r][lane];
                     c6 += g * uj[r];
                     dc6i += dg * uj[r];
                     dc6j += g * duj[r];
@@ -581,19 +581,27 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
                 txy -= c6w * sxy; txz -= c6w * sxz; tyz -= c6w * syz;
                 // j's share summed over the warp's atoms i: lane 8v holds value v
                 const R z = wsum4_tt<R>(jde, jgx, jgy, jgz, lane);
-                if ((lane & 7) == 0) acc[kUnitI + (lane >> 3)][jl] += double(z);
+                if ((lane & 7) == 0) acc[kAccI + (lane >> 3)][jl] += double(z);
             } else {
                 const R z = wsum_tt<R>(jde);
-                if (lane == 0) acc[kUnitI][jl] += double(z);
+                if (lane == 0) acc[kAccI][jl] += double(z);
             }
         }
         flush();
     }
     __syncwarp();
     double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
-    for (int v = 0; v < kUnitI; v++) oi[v] = acc[v][lane];
+    if constexpr (kAccI > 0) {
+        for (int v = 0; v < kUnitI; v++) oi[v] = acc[v][lane];
+    } else {
+        const double vi[kUnitI] = {double(te),  double(tde), double(tgx), double(tgy), double(tgz),
+                                   double(txx), double(tyy), double(tzz), double(txy), double(txz),
+                                   double(tyz), double(tp0), double(tp1), double(tp2), double(tp3)};
+#pragma unroll
+        for (int v = 0; v < kUnitI; v++) oi[v] = vi[v];
+    }
     double* oj = unit_j + ((size_t)item * kTile + lane) * kUnitJ;
-    for (int v = 0; v < kUnitJ; v++) oj[v] = acc[kUnitI + v][lane];
+    for (int v = 0; v < kUnitJ; v++) oj[v] = acc[kAccI + v][lane];
     if (w.counts) {
         unsigned long long n = nterm;
         for (int off = 16; off > 0; off >>= 1) n += __shfl_xor_sync(0xffffffffu, n, off);
