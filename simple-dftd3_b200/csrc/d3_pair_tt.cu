@@ -320,7 +320,8 @@ __device__ __forceinline__ void tt_family(R r2, R r1, bool have_r1, R rrij, R q1
 
 // SMOOTH: the smooth cutoff of the two-body sum is on (0 < width < cutoff);
 // a compile-time switch keeps its sqrt and divisions out of the plain loop.
-template <class R, int DAMP, bool GRAD, bool PG, bool SMOOTH>
+// COUNT: the accepted terms are counted into w.counts (work counters only).
+template <class R, int DAMP, bool GRAD, bool PG, bool SMOOTH, bool COUNT>
 __global__ void __launch_bounds__(kTTThreads, sizeof(R) == 4 ? 4 : 3)
 k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const int2* units, int nunits, int split,
               const R* UV, double* unit_i, double* unit_j)
@@ -476,7 +477,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
             auto term = [&](const TTGeo<R>& g) {
                 const R vx = g.vx, vy = g.vy, vz = g.vz, r2 = g.r2;
                 const bool ok = g.ok;
-                nterm += ok ? 1u : 0u;
+                if constexpr (COUNT) nterm += ok ? 1u : 0u;
                 // weight of the term; without the smooth cutoff the rational
                 // form zeroes a rejected term through its reciprocal instead
                 R sw = (SMOOTH || DAMP != kRational) ? (ok ? R(1) : R(0)) : R(1), dswdr = R(0), r1 = R(1);
@@ -602,7 +603,7 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     }
     double* oj = unit_j + ((size_t)item * kTile + lane) * kUnitJ;
     for (int v = 0; v < kUnitJ; v++) oj[v] = acc[kAccI + v][lane];
-    if (w.counts) {
+    if (COUNT && w.counts) {
         unsigned long long n = nterm;
         for (int off = 16; off > 0; off >>= 1) n += __shfl_xor_sync(0xffffffffu, n, off);
         if (lane == 0) atomicAdd(w.counts + 0, n);
@@ -1066,12 +1067,18 @@ void launch_tt(const Batch& b, const Species& s, const Damp& d, const Config& c,
                const PairUnits& pu, cudaStream_t stream)
 {
     const int blocks = (pu.nunits * pu.split + kTTWarps - 1) / kTTWarps;
-    if (c.width2 > 0.0 && c.width2 < c.cut2)
-        k_two_body_tt<R, DAMP, GRAD, PG, true><<<blocks, kTTThreads, 0, stream>>>(
-            b, s, d, c, p, w, pu.units, pu.nunits, pu.split, (const R*)pu.U, pu.unit_i, pu.unit_j);
-    else
-        k_two_body_tt<R, DAMP, GRAD, PG, false><<<blocks, kTTThreads, 0, stream>>>(
-            b, s, d, c, p, w, pu.units, pu.nunits, pu.split, (const R*)pu.U, pu.unit_i, pu.unit_j);
+    const bool smooth = c.width2 > 0.0 && c.width2 < c.cut2;
+#define D3_TT(SM, CO)                                                                                   \
+    k_two_body_tt<R, DAMP, GRAD, PG, SM, CO><<<blocks, kTTThreads, 0, stream>>>(                         \
+        b, s, d, c, p, w, pu.units, pu.nunits, pu.split, (const R*)pu.U, pu.unit_i, pu.unit_j)
+    if (w.counts) {
+        if (smooth) D3_TT(true, true);
+        else D3_TT(false, true);
+    } else {
+        if (smooth) D3_TT(true, false);
+        else D3_TT(false, false);
+    }
+#undef D3_TT
 }
 
 // the families without damping-parameter derivatives (the engine refuses
