@@ -446,14 +446,14 @@ def run_ours(args, rank, world, dist):
         line["mixed_speedup_vs_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
         line["mixed_vs_fp64_rel_energy_error"] = abs(res["mixed"]["energy"] - res["fp64"]["energy"]) / abs(
             res["fp64"]["energy"])
-    # kernels launched per step (counted in the ncu launch list of the headline): Morton
-    # keys, radix sort (one kernel up to a few thousand atoms; histogram, scan and one
-    # pass per key byte above), gather, tile bounds, CN tile pairs + gather, weights,
-    # species vectors, two-body tile pairs + gather, chain rule tile pairs + gather,
-    # reduction; ATM adds the C6 table, neighbour count, scan (2), capacity guard, fill
-    # and the triple kernel
-    natoms_total = int(run.natoms.sum())
-    per_step = 13 + (0 if natoms_total <= 4096 else 9) + (7 if atm else 0)
+    # kernels launched per step (counted in the ncu launch list of the headline): the
+    # column order (system shape and three rank passes; systems above 16384 atoms take
+    # Morton keys, a radix sort of about nine kernels and a gather instead), tile
+    # bounds, CN tile pairs + gather with weights and species vectors, two-body tile
+    # pairs + gather, chain rule + gather, reduction; ATM adds the C6 table, neighbour
+    # count, scan (2), capacity guard, fill and the triple kernel
+    order_kernels = 4 if int(run.natoms.max()) <= 16384 else 11
+    per_step = order_kernels + 8 + (7 if atm else 0)
     line["gpu_launches"] = per_step * args.steps * len(precs)
     rl = roofline(units, flops, res[head]["stage_ms"][stage], peak32 if head == "mixed" else peak64,
                   kern + ("<float>" if head == "mixed" else "<double>"), "fp32" if head == "mixed" else "fp64")
