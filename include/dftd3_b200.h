@@ -129,6 +129,13 @@ dftd3_b200_get_batch_stage_times(dftd3_error /* error */,
                                  dftd3_b200_batch /* batch */,
                                  double* /* ms[9] */);
 
+/* Kernel launches of one replay of the batch's captured CUDA graph: the
+ * kernel nodes of the graph (0 while no graph is captured). */
+SDFTD3_API_ENTRY void SDFTD3_API_CALL
+dftd3_b200_get_batch_graph_kernels(dftd3_error /* error */,
+                                   dftd3_b200_batch /* batch */,
+                                   long long* /* kernels */);
+
 /* Replay the whole pipeline of an evaluation as one captured CUDA graph
  * (enable != 0).  The first evaluation for a parameter set, derivative set
  * and launch shape runs the ordinary launch sequence and then captures it;
@@ -209,11 +216,15 @@ dftd3_b200_delete_batch(dftd3_b200_batch* /* batch */);
 /* Energy, gradient and virial of one system (two-body term, s9 = 0) without
  * allocating memory.  This entry point has no counterpart in the reference.
  * It serves callers that cannot allocate device memory while they run --
- * code executing under another framework's stream capture, integrators that
- * hand out all device memory from their own pool, latency-critical loops in
- * which cudaMalloc/cudaFree (which can synchronise the device) are not
- * allowed.  All work arrays come from a fixed __device__ array inside
- * the library (4 MiB), held by every GPU that loads it until exit.
+ * integrators and MD engines that hand out all device memory from their own
+ * pool, time-step loops in which cudaMalloc/cudaFree (which can synchronise
+ * the device) are not allowed.  All work arrays come from a fixed __device__
+ * array inside the library (4 MiB), held by every GPU that loads it until
+ * exit.  The call copies small per-call tables from static host buffers on
+ * `stream` and waits for that stream before returning (so it blocks the host
+ * until earlier work on `stream` is done); the kernels then run
+ * asynchronously.  A CUDA launch error pending from earlier work is reported
+ * and nothing is launched; periodic directions need a non-degenerate lattice.
  *   numbers[natoms], lattice[3][3], periodic[3] and cutoffs[5] (disp2, disp3,
  *   cn, width2, width3; NULL for the defaults) are host memory;
  *   d_positions[natoms][3], d_energy[1], d_gradient[natoms][3] and

@@ -834,6 +834,16 @@ void dftd3_b200_get_batch_stage_times(dftd3_error error, dftd3_b200_batch batch,
     guarded(error, [&] { batch->engine->stage_times(ms); });
 }
 
+void dftd3_b200_get_batch_graph_kernels(dftd3_error error, dftd3_b200_batch batch, long long* kernels)
+{
+    if (!error) return;
+    if (!batch || !kernels) {
+        fail(error, "Batch is missing");
+        return;
+    }
+    *kernels = batch->engine->graph_kernels();
+}
+
 void dftd3_b200_get_dispersion_noalloc(dftd3_error error, dftd3_param param, int natoms, const int* numbers,
                                        const double* d_positions, const double* lattice, const bool* periodic,
                                        const double* cutoffs, int precision, double* d_energy,

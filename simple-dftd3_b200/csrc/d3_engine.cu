@@ -1074,6 +1074,20 @@ void Engine::capture(const Damp& d, const GraphKey& key, bool grad, bool pg)
     }
     capturing_ = false;
     check(cudaStreamEndCapture(stream_, &g), "cudaStreamEndCapture");
+    // kernels one replay launches: the kernel nodes of the captured graph
+    {
+        size_t nn = 0;
+        graph_kernels_ = 0;
+        if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn > 0) {
+            std::vector<cudaGraphNode_t> nodes(nn);
+            if (cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess)
+                for (size_t k = 0; k < nn; k++) {
+                    cudaGraphNodeType t;
+                    if (cudaGraphNodeGetType(nodes[k], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+                        graph_kernels_++;
+                }
+        }
+    }
     bool updated = false;
     if (graph_exec_) {
         cudaGraphExecUpdateResultInfo info;

@@ -101,6 +101,8 @@ public:
     // again without the graph, and the graph is captured anew.
     void set_graph(bool on);
     bool graph() const { return graph_on_; }
+    // kernel launches of one replay of the captured graph (0 before the first capture)
+    long long graph_kernels() const { return graph_valid_ ? graph_kernels_ : 0; }
 
     // Partitioned evaluation over several processes (the reference's MPI
     // path, disp.f90:120-171 with a reducer, and mpi.f90): this engine
@@ -192,6 +194,7 @@ private:
     long long root_atoms_ = 0;           // atoms of the other systems
     bool graph_on_ = false, capturing_ = false, graph_valid_ = false;
     cudaGraphExec_t graph_exec_ = nullptr;
+    long long graph_kernels_ = 0;
     GraphKey graph_key_{};
     unsigned long long alloc_epoch_ = 0, graph_epoch_ = 0;
     int* d_guard_ = nullptr;

@@ -4,12 +4,19 @@
 // __device__ array instead of cudaMalloc'd workspace.
 //
 // Who needs it: callers that must not allocate device memory at call time --
-// code that runs while another framework's stream is being captured into a
-// CUDA graph, integrators that own every byte of device memory through their
-// own pool, and latency-critical loops in which cudaMalloc/cudaFree (which can
-// synchronise the whole device) are forbidden.  The caller passes device
-// input and output buffers; the library allocates nothing, on the device or on
-// the host heap (host-side tables live in fixed static buffers).
+// integrators and MD engines that own every byte of device memory through
+// their own pool allocator (a cudaMalloc behind the pool's back can fail or
+// fragment the pool), and time-step loops in which cudaMalloc/cudaFree are
+// not allowed because they can synchronise the whole device.  The caller
+// passes device input and output buffers; the library allocates nothing, on
+// the device or on the host heap (host-side tables live in fixed static
+// buffers).
+//
+// Host blocking: the per-call tables are copied from those static host
+// buffers on `stream`, and the call then waits for the stream
+// (cudaStreamSynchronize) before the buffers can be reused, so it returns
+// only after all work queued earlier on `stream` and its copies are done; the
+// kernels themselves run asynchronously after it returns.
 //
 // Limits and sharing:
 //   * at most kNoAllocMaxAtoms atoms, kNoAllocMaxSpecies distinct elements and
@@ -107,6 +114,12 @@ int lattice_points_into(const double* lattice, const bool* periodic, double rthr
         const double z = a[0] * b[1] - b[0] * a[1];
         c[0] = x; c[1] = y; c[2] = z;
     };
+    // repetitions ceil(x) of one direction; -1 for a degenerate lattice (a zero
+    // vector or normal gives x = inf or NaN) or more images than fit
+    auto reps = [&](double x) {
+        if (!(x >= 0.0) || x > (double)cap) return -1;
+        return (int)std::ceil(x);
+    };
     auto translations = [&](const double lat[3][3], int rep[3]) {
         double nrm[3][3];
         cross(lat[1], lat[2], nrm[0]);
@@ -118,7 +131,7 @@ int lattice_points_into(const double* lattice, const bool* periodic, double rthr
         }
         for (int k = 0; k < 3; k++) {
             const double cs = nrm[k][0] * lat[k][0] + nrm[k][1] * lat[k][1] + nrm[k][2] * lat[k][2];
-            rep[k] = (int)std::ceil(std::fabs(rthr / cs));
+            rep[k] = reps(std::fabs(rthr / cs));
         }
     };
     double lat[3][3];
@@ -130,7 +143,7 @@ int lattice_points_into(const double* lattice, const bool* periodic, double rthr
     } else if (np == 1) {
         for (int k = 0; k < 3; k++) {
             const double v = std::sqrt(lat[k][0] * lat[k][0] + lat[k][1] * lat[k][1] + lat[k][2] * lat[k][2]);
-            rep[k] = periodic[k] ? (int)std::ceil(rthr / v) : 0;
+            rep[k] = periodic[k] ? reps(rthr / v) : 0;
         }
     } else {
         double nrm[3][3];
@@ -142,6 +155,7 @@ int lattice_points_into(const double* lattice, const bool* periodic, double rthr
         for (int k = 0; k < 3; k++)
             if (!periodic[k]) rep[k] = 0;
     }
+    if (rep[0] < 0 || rep[1] < 0 || rep[2] < 0) return -1;
     const long long n = (long long)(2 * rep[0] + 1) * (2 * rep[1] + 1) * (2 * rep[2] + 1);
     if (n > cap) return -1;
     int t = 0;
@@ -194,6 +208,17 @@ bool noalloc_dispersion(const Damp& damp, int natoms, const int* numbers, const 
         return fail("The allocation-free evaluation supports the rational and zero damping");
     if (precision != DFTD3_B200_PRECISION_FP64 && precision != DFTD3_B200_PRECISION_MIXED)
         return fail("Invalid precision selector");
+    for (int k = 0; k < 3 && periodic; k++)
+        if (periodic[k] && !lattice) return fail("Periodic directions need a lattice");
+    // a launch error still pending from earlier work would otherwise be
+    // reported (and cleared) as this call's own at the end
+    {
+        const cudaError_t pending = cudaPeekAtLastError();
+        if (pending != cudaSuccess) {
+            std::snprintf(msg, 256, "CUDA error pending from earlier work: %s", cudaGetErrorString(pending));
+            return false;
+        }
+    }
 
     std::lock_guard<std::mutex> lock(g_mutex);
     HostStage& h = g_host;
@@ -268,8 +293,9 @@ bool noalloc_dispersion(const Damp& damp, int natoms, const int* numbers, const 
     for (int k = 0; k < kImageKinds; k++) {
         const int n = lattice_points_into(lat, per, rthr[k], h.img + 3 * nimg_total, kNoAllocMaxImages);
         if (n < 0) {
-            std::snprintf(msg, 256, "Allocation-free evaluation supports at most %d lattice translations per cutoff",
-                          kNoAllocMaxImages);
+            std::snprintf(msg, 256,
+                          "Allocation-free evaluation supports at most %d lattice translations per cutoff "
+                          "(and a non-degenerate lattice)", kNoAllocMaxImages);
             return false;
         }
         h.img_off[2 * k] = nimg_total;

@@ -28,7 +28,7 @@ occurs in the reference's own fixtures.
 All literals are written out with the decimal digits of the source, so the C
 compiler rounds them exactly as the Fortran compiler did.
 
-Usage: python gen_tables.py [REFERENCE_ROOT] > d3_tables.c
+Usage: python gen_tables.py REFERENCE_ROOT > d3_tables.c
 """
 import re
 import sys
@@ -100,7 +100,9 @@ def emit_array(out, ctype, name, vals, per_line=8):
 
 
 def main():
-    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit("usage: python gen_tables.py <reference root>")
+    root = Path(sys.argv[1])
     nref, refcn, c6 = parse_reference(root)
     r4r2 = parse_r4r2(root)
     vdw = parse_vdwrad(root)

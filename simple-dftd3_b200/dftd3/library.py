@@ -324,6 +324,13 @@ STAGES = ("split", "cn", "weights", "two_body", "three_body", "cn_chain", "reduc
           "three_body_kernel")
 
 
+def get_batch_graph_kernels(batch: BatchHandle) -> int:
+    """Kernel launches of one replay of the batch's captured CUDA graph (0 if none)."""
+    n = np.zeros(1, dtype=np.int64)
+    error_check(lib.dftd3_b200_get_batch_graph_kernels)(batch.handle, _cast("long long*", n))
+    return int(n[0])
+
+
 def get_batch_stage_times(batch: BatchHandle) -> dict:
     ms = np.zeros(len(STAGES))
     error_check(lib.dftd3_b200_get_batch_stage_times)(batch.handle, _cast("double*", ms))

@@ -128,3 +128,16 @@ def frames256(seed=0, nframes=256, natoms=512):
         lattices.append(lat)
     return dict(numbers=numbers, positions=positions, lattices=np.array(lattices),
                 periodic=np.ones((nframes, 3), dtype=bool), s9=1.0)
+
+
+def batch4096_sample(sizes, n=64, largest=8):
+    """Indices of a fixed sample of a molecule batch for parity checks against
+    the FP64 oracle: the `largest` biggest molecules and n - largest more
+    spread evenly over the rest of the batch (in batch order)."""
+    sizes = np.asarray(sizes)
+    order = np.argsort(-sizes, kind="stable")
+    big = set(int(k) for k in order[:largest])
+    rest = [k for k in range(len(sizes)) if k not in big]
+    step = max(len(rest) // max(n - largest, 1), 1)
+    pick = sorted(big) + rest[::step][: n - largest]
+    return sorted(pick)

@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Extract golden vectors from the reference's own test files.
 
-Reads the reference source tree (default /root/reference) as text and writes
+Reads the reference source tree (its root given on the command line) as text and writes
 small JSON fixtures next to this script.  Every fixture records the file it
 came from, the damping parameters the reference test used (with the
 parameter-table line they come from) and the tolerance the reference test
@@ -10,7 +10,7 @@ applies.  Geometries keep the units of their source files ("angstrom" or
 readers use.
 
 Run it only where the reference is present:
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT
 """
 import ast
 import json
@@ -373,7 +373,9 @@ def unit_tests(root):
 
 
 def main():
-    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit("usage: python make_golden.py <reference root>")
+    root = Path(sys.argv[1])
     fixtures = {"validation": validation(root), "python": python_tests(root), "unit": unit_tests(root)}
     for key, cases in fixtures.items():
         (HERE / f"{key}.json").write_text(json.dumps(cases, indent=1) + "\n")

@@ -26,3 +26,13 @@ def test_reference_arm_line():
     assert line["metric"].startswith("pair-terms/s")
     assert line["e2e"]["value"] == line["value"] and line["e2e"]["h2d_bytes_per_step"] == 0
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    # the CPU record names the threads used, the physical cores and the OpenMP settings
+    cpu = line["cpu_baseline"]["cpu"]
+    for k in ("threads", "physical_cores", "logical_cpus", "model", "OMP_NUM_THREADS", "OMP_SCHEDULE"):
+        assert k in cpu, k
+    assert cpu["threads"] == line["cpu_baseline"]["cores"]
+    # both arms print the same config for the same workload
+    sys.path.insert(0, str(ROOT))
+    import bench
+    systems, _ = bench.make_workload("cell2000", natoms=200)
+    assert line["config"] == bench.workload_config("cell2000", systems, 1)
