@@ -3,16 +3,25 @@
 // For a non-periodic system of at most kMolMax atoms every triple is
 // (i > j > k) in the sorted atom order (get_atm_dispersion_derivs,
 // atm.f90:625-825, with a single lattice point, so triple_scale is 1).  A
-// block takes the largest remaining molecule from a queue, stages its atoms
-// in shared memory and hands out work items (root i, chunk of 32 rows j < i)
-// to its warps.  A warp's lanes own one row j each; the warp sweeps the
-// partners k < j in blocks of 32, whose (i, k) pair records the lanes build
-// and share through shared memory.  Per triple the row keeps its j-role sums
-// in registers, the k-role sums of the partners are reduced over the warp in
-// groups of four with a reduce-scatter, and the root's sums stay in registers.  Per-atom
-// gradient and dE/dCN accumulate in shared memory (FP64) and are added to the
-// global arrays once per molecule; energy and virial are reduced per block
-// in a fixed order.  No block-wide barrier separates the work items.
+// block takes the largest remaining molecule from a queue and stages its
+// atoms in shared memory.  The work items (root i, chunk of 32 rows j < i)
+// are dealt to the warps round-robin in a fixed order.  A lane owns one row j
+// and keeps the row's sums in registers; the partners k < j come in blocks
+// of 32 whose (i, k) pair records the lanes build together.  Inside a block
+// the warp walks the 32 x 32 (row, partner) tile along its diagonals: at step
+// t lane l pairs row l with partner (l + t) mod 32, and the partner's five
+// sums travel with the partner, one lane down per step (five shuffles), so
+// that every lane ends the block holding one partner's complete sums.  In the
+// diagonal block (the partners are the rows' own chunk) steps 1..16 visit
+// every unordered pair once, which is enough because the triple term and its
+// derivatives are symmetric in j and k.  Candidates are evaluated without
+// branches: a term outside the cutoff gets weight zero.
+//
+// Per-atom gradient and dE/dCN go to per-warp FP64 accumulators in shared
+// memory, summed over the warps in warp order at the end of the molecule;
+// energy and virial are per-lane FP64 sums reduced in a fixed order.  With
+// the fixed item order the result is bit-reproducible.
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 
@@ -26,18 +35,30 @@ namespace {
 constexpr int kMolMax = 256;      // atoms of a system handled by one block
 constexpr int kMolWarps = 8;
 constexpr int kMolThreads = 32 * kMolWarps;
+#ifndef MOL_MINB
+#define MOL_MINB 2
+#endif
 
 template <class R> struct V4;
 template <> struct V4<float> { using type = float4; };
 template <> struct V4<double> { using type = double4; };
 
-// Record of the pair (root i, partner p).
+// Record of the pair (root i, partner p).  An invalid record (p not a
+// partner, or r_ip outside the cutoff) has sqrt(C6) = 0, valid = 0 and finite
+// values elsewhere, so that a term built from it is finite and zero.
 template <class R>
 struct PairRec {
     typename V4<R>::type h;   // absolute position of p (head in the mixed form), r_ip^2
     typename V4<R>::type l;   // tail of the position (mixed form), 1 / r_ip^2
     typename V4<R>::type c;   // sqrt(C6_ip), dC6_ip/dCN_i / C6_ip, dC6_ip/dCN_p / C6_ip, alp3 log(r0_ip / r_ip)
     typename V4<R>::type s;   // 1 / r_ip, switch, dsw/dr / r, valid (1 or 0)
+};
+
+// Partner records of one warp, one array per field (the rotated reads of the
+// lanes hit consecutive 16- or 32-byte slots).
+template <class R>
+struct MolTile {
+    typename V4<R>::type h[32], l[32], c[32], s[32];
 };
 
 template <class R>
@@ -48,10 +69,10 @@ __device__ __forceinline__ void split_pos(double x, R& h, R& l)
 }
 
 // Pair record of (i, p) from shared positions and the C6 row of i.
-template <class R>
+template <class R, bool SMOOTH>
 __device__ __forceinline__ PairRec<R> make_rec(const double* px, const double* py, const double* pz, int ii, int pp,
-                                               bool in, const C6Entry<R>* row_i, R alp3, double cut2,
-                                               bool smooth_on, R cutoff, R width)
+                                               bool in, const C6Entry<R>* row_i, R alp3, double cut2, R cutoff,
+                                               R width)
 {
     PairRec<R> r;
     const double x = px[pp], y = py[pp], z = pz[pp];
@@ -71,16 +92,16 @@ __device__ __forceinline__ PairRec<R> make_rec(const double* px, const double* p
     // alp3 log(r0_ip / r_ip) with the damping radius term of the C6 entry,
     // 1 / r^2 and 1 / r: FP64, or FP32 from the FP64 distance in the mixed form
     if constexpr (sizeof(R) == 8) {
-        r.c.w = e.lr0 - 0.5 * (double)alp3 * log(r2s);
+        r.c.w = ok ? e.lr0 - 0.5 * (double)alp3 * log(r2s) : 0.0;
         r.l.w = 1.0 / r2s;
         r.s.x = rsqrt(r2s);
     } else {
         const float r2f = (float)r2s;
-        r.c.w = e.lr0 - 0.5f * alp3 * __log2f(r2f);
+        r.c.w = ok ? e.lr0 - 0.5f * alp3 * __log2f(r2f) : 0.0f;
         r.l.w = 1.0f / r2f;
         r.s.x = rsqrtf(r2f);
     }
-    if (smooth_on && ok) {
+    if (SMOOTH && ok) {
         R sw, dsw;
         const R rr = R(sqrt(r2s));
         smooth<R>(rr, cutoff, width, sw, dsw);
@@ -104,38 +125,246 @@ __device__ __forceinline__ int items_upto(int x)
     return 32 * (q * (q + 1) / 2) + r * (q + 1);
 }
 
-template <class R, bool GRAD>
-__global__ void __launch_bounds__(kMolThreads, sizeof(R) == 4 ? 2 : 1)
+// Vector from the root to a record's position (head and tail differences).
+template <class R>
+__device__ __forceinline__ void root_vec(const typename V4<R>::type& h, const typename V4<R>::type& l, R rhx, R rhy,
+                                         R rhz, R rlx, R rly, R rlz, R& vx, R& vy, R& vz)
+{
+    if constexpr (sizeof(R) == 8) {
+        vx = h.x - rhx; vy = h.y - rhy; vz = h.z - rhz;
+    } else {
+        vx = (h.x - rhx) + (l.x - rlx);
+        vy = (h.y - rhy) + (l.y - rly);
+        vz = (h.z - rhz) + (l.z - rlz);
+    }
+}
+
+// One work item (root i, chunk of 32 rows) of a molecule, by one warp: the
+// triples (i, j, k) of the chunk's rows j with every k < j, added to the
+// warp's per-atom accumulators acc[n][4] and to the lane's energy, virial and
+// triple count.
+template <class R, bool GRAD, bool SMOOTH>
+__device__ __forceinline__ void mol_item(int t, int n, int nitems, const C6Entry<R>* m0, const double* px,
+                                         const double* py, const double* pz, const int* loc, double* acc,
+                                         MolTile<R>& tl, const Partition& part, R s9, R alp, R alp3, double cut2d,
+                                         R cut2, R cutoff, R width, int lane, double& e_l, double& sxx, double& syy,
+                                         double& szz, double& sxy, double& sxz, double& syz, int& ntrip)
+{
+        // item t -> root i (descending), chunk (descending within the root)
+        const int u = nitems - t;
+        int lo = 1, hi = n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (items_upto(mid) >= u) hi = mid; else lo = mid + 1;
+        }
+        const int i = lo;
+        const int nch = (i + 31) >> 5;
+        const int chunk = nch - 1 - (t - (nitems - items_upto(i)));
+        const C6Entry<R>* row_i = m0 + (size_t)i * n;
+        R rhx, rlx, rhy, rly, rhz, rlz;
+        split_pos<R>(px[i], rhx, rlx);
+        split_pos<R>(py[i], rhy, rly);
+        split_pos<R>(pz[i], rhz, rlz);
+        // this lane's row j
+        const int J0 = 32 * chunk;
+        const int j = J0 + lane;
+        const bool jin = j < i;
+        const int jj = jin ? j : 0;
+        const PairRec<R> A = make_rec<R, SMOOTH>(px, py, pz, i, jj, jin, row_i, alp3, cut2d, cutoff, width);
+        const bool jvalid = A.s.w != R(0);
+        if (!__any_sync(0xffffffffu, jvalid)) return;
+        const C6Entry<R>* row_j = m0 + (size_t)jj * n;
+        const int lj = loc[jj];
+        const int li = loc[i];
+        // row and root sums of this lane, FP64 across partner blocks
+        double jS = 0, jGx = 0, jGy = 0, jGz = 0, jD = 0, dei = 0, gix = 0, giy = 0, giz = 0;
+        for (int K0 = 0; K0 <= J0; K0 += 32) {
+            const bool diag = K0 == J0;
+            // partner records k = K0 + lane (the rows' own records in the diagonal block)
+            {
+                PairRec<R> Bown;
+                if (diag) Bown = A;
+                else Bown = make_rec<R, SMOOTH>(px, py, pz, i, K0 + lane, true, row_i, alp3, cut2d, cutoff, width);
+                __syncwarp();
+                tl.h[lane] = Bown.h; tl.l[lane] = Bown.l; tl.c[lane] = Bown.c; tl.s[lane] = Bown.s;
+            }
+            __syncwarp();
+            const int t0 = diag ? 1 : 0, t1 = diag ? 16 : 31;
+            R kS = R(0), kGx = R(0), kGy = R(0), kGz = R(0), kD = R(0);
+            R rS = R(0), rGx = R(0), rGy = R(0), rGz = R(0), rD = R(0), rde = R(0);
+            R te = R(0), txx = R(0), tyy = R(0), tzz = R(0), txy = R(0), txz = R(0), tyz = R(0);
+            // C6 of (j, k), in the FP32 form one step ahead of its use (the loads
+            // overlap the arithmetic; the FP64 form has no registers to spare)
+            auto c6_of = [&](int st) {
+                const int k = K0 + ((lane + st) & 31);
+                return row_j[k < n ? k : 0];
+            };
+            C6Entry<R> e_next = c6_of(t0);
+            constexpr bool kPrefetch = sizeof(R) == 4;
+            for (int st = t0; st <= t1; st++) {
+                const int m = (lane + st) & 31;
+                const typename V4<R>::type Bh = tl.h[m], Bl = tl.l[m], Bc = tl.c[m], Bs = tl.s[m];
+                const int k = K0 + m;
+                const int kc = k < n ? k : 0;
+                // C6 of (j, k): qrc = dC6/dCN_j / C6, qcr = dC6/dCN_k / C6
+                const C6Entry<R> ejk = kPrefetch ? e_next : c6_of(st);
+                if (kPrefetch && st < t1) e_next = c6_of(st + 1);
+                R vx, vy, vz;
+                if constexpr (sizeof(R) == 8) {
+                    vx = Bh.x - A.h.x; vy = Bh.y - A.h.y; vz = Bh.z - A.h.z;
+                } else {
+                    vx = (Bh.x - A.h.x) + (Bl.x - A.l.x);
+                    vy = (Bh.y - A.h.y) + (Bl.y - A.l.y);
+                    vz = (Bh.z - A.h.z) + (Bl.z - A.l.z);
+                }
+                const R rc0 = vx * vx + vy * vy + vz * vz;   // r_jk^2
+                bool valid = jvalid && Bs.w != R(0) && (!diag || st < 16 || lane < 16) &&
+                             !(rc0 > cut2 || rc0 < R(DBL_EPSILON));
+                if (part.nparts > 1) {
+                    // owner of the triple: the pair of its two largest input indices
+                    int o1 = li, o2 = lj, o3 = loc[kc], tmp;
+                    if (o2 > o1) { tmp = o1; o1 = o2; o2 = tmp; }
+                    if (o3 > o2) { tmp = o2; o2 = o3; o3 = tmp; }
+                    if (o2 > o1) { tmp = o1; o1 = o2; o2 = tmp; }
+                    valid = valid && owns_pair_atm(part, o1, o2);
+                }
+                ntrip += valid ? 1 : 0;
+                const R rc = valid ? rc0 : R(1);
+                const R ra = A.h.w, rb = Bh.w;               // r_ij^2, r_ik^2
+                const R rsc = rsqrt_r<R>(rc);
+                const R irc = rsc * rsc;
+                const R ir1 = A.s.x * Bs.x * rsc;            // 1 / (r_ij r_ik r_jk)
+                const R ir2 = ir1 * ir1;
+                const R ir3 = ir2 * ir1;
+                const R ir5 = ir3 * ir2;
+                // (r0/r1)^alp3 with r0 = r0ij r0ik r0jk, r1 = r_ij r_ik r_jk (atm.f90:744-749)
+                const R tq = rexp<R>(A.c.w + Bc.w + ejk.lr0 - R(0.5) * alp3 * rlog<R>(rc));
+                const R fdmp = rcp_r<R>(R(1) + R(6) * tq);
+                const R s1 = ra + rb + rc;
+                const R ang = R(0.375) * (s1 - R(2) * rb) * (s1 - R(2) * rc) * (s1 - R(2) * ra) * ir5 + ir3;
+                const R c9 = valid ? -s9 * A.c.x * Bc.x * ejk.sc6 : R(0);
+                R sw = R(1), swjk = R(1), dswjkr = R(0);
+                if (SMOOTH) {
+                    R dsw;
+                    const R rjk = rc * rsc;
+                    smooth<R>(rjk, cutoff, width, swjk, dsw);
+                    dswjkr = dsw * rsc;
+                    sw = A.s.y * Bs.y * swjk;
+                }
+                const R c9f = c9 * fdmp;
+                const R dE0 = ang * c9f;
+                const R dE = SMOOTH ? dE0 * sw : dE0;
+                te -= dE;
+                if (GRAD) {
+                    const R common = dE0 * (R(-2) * alp * tq * fdmp);
+                    const R kfac = R(0.375) * c9f * ir5;
+                    R sij = (common + kfac * ang_deriv<R>(ra, rc, rb, s1)) * A.l.w;
+                    R sik = (common + kfac * ang_deriv<R>(rb, rc, ra, s1)) * Bl.w;
+                    R sjk = (common + kfac * ang_deriv<R>(rc, rb, ra, s1)) * irc;
+                    if (SMOOTH) {
+                        sij = sij * sw - dE0 * A.s.z * Bs.y * swjk;
+                        sik = sik * sw - dE0 * Bs.z * A.s.y * swjk;
+                        sjk = sjk * sw - dE0 * dswjkr * A.s.y * Bs.y;
+                    }
+                    const R gx = sjk * vx, gy = sjk * vy, gz = sjk * vz;
+                    // dE/dCN shares of the root, the row and the partner
+                    const R hdE = R(0.5) * dE;
+                    rde -= hdE * (A.c.y + Bc.y);
+                    rS += sij; rGx -= gx; rGy -= gy; rGz -= gz;
+                    rD -= hdE * (A.c.z + ejk.qrc);
+                    kS += sik; kGx += gx; kGy += gy; kGz += gz;
+                    kD -= hdE * (Bc.z + ejk.qcr);
+                    txx += gx * vx; tyy += gy * vy; tzz += gz * vz;
+                    txy += gx * vy; txz += gx * vz; tyz += gy * vz;
+                    // the partner's sums move one lane down, with the partner
+                    const int src = (lane + 1) & 31;
+                    kS = __shfl_sync(0xffffffffu, kS, src);
+                    kGx = __shfl_sync(0xffffffffu, kGx, src);
+                    kGy = __shfl_sync(0xffffffffu, kGy, src);
+                    kGz = __shfl_sync(0xffffffffu, kGz, src);
+                    kD = __shfl_sync(0xffffffffu, kD, src);
+                }
+            }
+            e_l += double(te);
+            if (GRAD) {
+                sxx += double(txx); syy += double(tyy); szz += double(tzz);
+                sxy += double(txy); sxz += double(txz); syz += double(tyz);
+                jS += double(rS); jGx += double(rGx); jGy += double(rGy); jGz += double(rGz);
+                jD += double(rD); dei += double(rde);
+                // the lane now holds the sums of partner (lane + t1 + 1) mod 32:
+                // its pair (i, k) force along x_k - x_i, and its jk and dE/dCN shares
+                const int mf = (lane + t1 + 1) & 31;
+                const int kk = K0 + mf;
+                if (tl.s[mf].w != R(0)) {
+                    R vx, vy, vz;
+                    root_vec<R>(tl.h[mf], tl.l[mf], rhx, rhy, rhz, rlx, rly, rlz, vx, vy, vz);
+                    const double fx = double(kS) * double(vx), fy = double(kS) * double(vy),
+                                 fz = double(kS) * double(vz);
+                    double* ak = acc + 4 * kk;
+                    ak[0] += fx + double(kGx);
+                    ak[1] += fy + double(kGy);
+                    ak[2] += fz + double(kGz);
+                    ak[3] += double(kD);
+                    gix -= fx; giy -= fy; giz -= fz;
+                    sxx += fx * double(vx); syy += fy * double(vy); szz += fz * double(vz);
+                    sxy += fx * double(vy); sxz += fx * double(vz); syz += fy * double(vz);
+                }
+            }
+        }
+        if (GRAD) {
+            // row j: pair (i, j) force along x_j - x_i, and the row's other sums
+            if (jvalid) {
+                R vx, vy, vz;
+                root_vec<R>(A.h, A.l, rhx, rhy, rhz, rlx, rly, rlz, vx, vy, vz);
+                const double fx = jS * double(vx), fy = jS * double(vy), fz = jS * double(vz);
+                double* aj = acc + 4 * j;
+                aj[0] += fx + jGx;
+                aj[1] += fy + jGy;
+                aj[2] += fz + jGz;
+                aj[3] += jD;
+                gix -= fx; giy -= fy; giz -= fz;
+                sxx += fx * double(vx); syy += fy * double(vy); szz += fz * double(vz);
+                sxy += fx * double(vy); sxz += fx * double(vz); syz += fy * double(vz);
+            }
+            const double rgx = wsum64(gix), rgy = wsum64(giy), rgz = wsum64(giz), rde = wsum64(dei);
+            if (lane == 0) {
+                double* ai = acc + 4 * i;
+                ai[0] += rgx; ai[1] += rgy; ai[2] += rgz; ai[3] += rde;
+            }
+            __syncwarp();
+        }
+}
+
+template <class R, bool GRAD, bool SMOOTH>
+__global__ void __launch_bounds__(kMolThreads, sizeof(R) == 4 ? 2 : MOL_MINB)
 k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, const C6Entry<R>* mat,
               const long long* mat_off, const int* mol_order, int nmol, unsigned int* queue, double* e3,
               double* sig3)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    double* px = reinterpret_cast<double*>(smem);
+    MolTile<R>* tiles = reinterpret_cast<MolTile<R>*>(smem);                   // [warps]
+    double* accw = reinterpret_cast<double*>(tiles + kMolWarps);               // [warps][kMolMax][4]
+    double* px = accw + (size_t)kMolWarps * kMolMax * 4;
     double* py = px + kMolMax;
     double* pz = py + kMolMax;
-    double* acc = pz + kMolMax;                                   // [kMolMax][4] gradient, dE/dCN
-    PairRec<R>* recs = reinterpret_cast<PairRec<R>*>(acc + 4 * kMolMax);   // [warps][32]
-    int* spc = reinterpret_cast<int*>(recs + kMolWarps * 32);     // [kMolMax] species
-    int* loc = spc + kMolMax;                                     // [kMolMax] input index
+    int* loc = reinterpret_cast<int*>(pz + kMolMax);                           // [kMolMax] input index
     __shared__ double wred[kMolWarps][8];
-    __shared__ int s_mol, s_item;
+    __shared__ int s_mol;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const R s9 = R(d.s9);
     const R alp = R(d.alp + 2.0);        // ATM exponent alp + 2 (rational.f90:563)
     const R alp3 = alp / R(3);
     const double cut2d = c.cut3 * c.cut3;
     const R cut2 = R(cut2d);
-    const bool smooth_on = c.width3 > 0.0 && c.width3 < c.cut3;
     const R cutoff = R(c.cut3), width = R(c.width3);
-    PairRec<R>* wrec = recs + wid * 32;
+    MolTile<R>& tl = tiles[wid];
+    double* acc = accw + (size_t)wid * kMolMax * 4;
 
     for (;;) {
         __syncthreads();
         if (tid == 0) {
             const unsigned q = atomicAdd(queue, 1u);
             s_mol = q < (unsigned)nmol ? mol_order[q] : -1;
-            s_item = 0;
         }
         __syncthreads();
         const int sys = s_mol;
@@ -145,241 +374,23 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
         const C6Entry<R>* m0 = mat + mat_off[sys];
         for (int a = tid; a < n; a += kMolThreads) {
             px[a] = b.x[a0 + a]; py[a] = b.y[a0 + a]; pz[a] = b.z[a0 + a];
-            spc[a] = b.sp[a0 + a];
             loc[a] = b.local[a0 + a];
-            acc[4 * a + 0] = 0.0; acc[4 * a + 1] = 0.0; acc[4 * a + 2] = 0.0; acc[4 * a + 3] = 0.0;
         }
+        if (GRAD)
+            for (int a = tid; a < kMolWarps * n * 4; a += kMolThreads) {
+                const int q = a / (n * 4);
+                accw[(size_t)q * kMolMax * 4 + (a - q * n * 4)] = 0.0;
+            }
         __syncthreads();
         const int nitems = n > 1 ? items_upto(n - 1) : 0;
         // per-lane sums over the warp's items: energy, virial, accepted triples
         double e_l = 0.0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
         int ntrip = 0;
-        for (;;) {
-            int t = 0;
-            if (lane == 0) t = atomicAdd(&s_item, 1);
-            t = __shfl_sync(0xffffffffu, t, 0);
-            if (t >= nitems) break;
-            // item t -> root i (descending), chunk (descending within the root)
-            const int u = nitems - t;
-            int lo = 1, hi = n - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (items_upto(mid) >= u) hi = mid; else lo = mid + 1;
-            }
-            const int i = lo;
-            const int nch = (i + 31) >> 5;
-            const int chunk = nch - 1 - (t - (nitems - items_upto(i)));
-            const C6Entry<R>* row_i = m0 + (size_t)i * n;
-            // root position split (head, tail)
-            R rhx, rlx, rhy, rly, rhz, rlz;
-            split_pos<R>(px[i], rhx, rlx);
-            split_pos<R>(py[i], rhy, rly);
-            split_pos<R>(pz[i], rhz, rlz);
-            // this lane's row j
-            const int j = 32 * chunk + lane;
-            const bool jin = j < i;
-            const int jj = jin ? j : 0;
-            const PairRec<R> A = make_rec<R>(px, py, pz, i, jj, jin, row_i, alp3, cut2d, smooth_on, cutoff, width);
-            const bool jvalid = A.s.w != R(0);
-            if (!__any_sync(0xffffffffu, jvalid)) continue;
-            const int kend = min(i, 32 * chunk + 32) - 1;   // partners k < j <= kend
-            const int lj = loc[jj];
-            const int li = loc[i];
-            // j-role and root sums
-            R jS = R(0), jGx = R(0), jGy = R(0), jGz = R(0), jD = R(0);
-            R gix = R(0), giy = R(0), giz = R(0), dei = R(0);
-            for (int K0 = 0; K0 < kend; K0 += 32) {
-                const int kk = K0 + lane;
-                const bool kin = kk < kend;
-                const int kc = kin ? kk : 0;
-                {
-                    const PairRec<R> Bown = make_rec<R>(px, py, pz, i, kc, kin, row_i, alp3, cut2d, smooth_on, cutoff, width);
-                    __syncwarp();
-                    wrec[lane] = Bown;
-                }
-                __syncwarp();
-                R kS = R(0), kGx = R(0), kGy = R(0), kGz = R(0), kD = R(0);
-                R te = R(0), txx = R(0), tyy = R(0), tzz = R(0), txy = R(0), txz = R(0), tyz = R(0);
-                const int tn = min(32, kend - K0);
-                // one candidate (row j, partner K0 + tt): root, row and virial sums
-                // here, the partner's five sums returned in cv
-                auto candidate = [&](int tt, R* cv) {
-                    R& cS = cv[0]; R& cGx = cv[1]; R& cGy = cv[2]; R& cGz = cv[3]; R& cD = cv[4];
-                    const int k = K0 + tt;
-                    const PairRec<R>& B = wrec[tt];
-                    bool valid = jvalid && k < j && B.s.w != R(0);
-                    // j-k vector from the absolute positions (head and tail differences)
-                    R vx, vy, vz;
-                    if constexpr (sizeof(R) == 8) {
-                        vx = B.h.x - A.h.x; vy = B.h.y - A.h.y; vz = B.h.z - A.h.z;
-                    } else {
-                        vx = (B.h.x - A.h.x) + (B.l.x - A.l.x);
-                        vy = (B.h.y - A.h.y) + (B.l.y - A.l.y);
-                        vz = (B.h.z - A.h.z) + (B.l.z - A.l.z);
-                    }
-                    const R rc = vx * vx + vy * vy + vz * vz;
-                    valid = valid && !(rc > cut2 || rc < R(DBL_EPSILON));
-                    if (!__any_sync(0xffffffffu, valid)) return;
-                    // C6 of (k, j): row k, column j (consecutive over the lanes)
-                    const C6Entry<R> ekj = m0[(size_t)k * n + jj];
-                    // a ghost gives C6 = 0 and with it zero contributions
-                    if (valid && part.nparts > 1) {
-                        // owner of the triple: the pair of its two largest input indices
-                        int o1 = li, o2 = lj, o3 = loc[k], tmp;
-                        if (o2 > o1) { tmp = o1; o1 = o2; o2 = tmp; }
-                        if (o3 > o2) { tmp = o2; o2 = o3; o3 = tmp; }
-                        if (o2 > o1) { tmp = o1; o1 = o2; o2 = tmp; }
-                        valid = owns_pair_atm(part, o1, o2);
-                    }
-                    if (valid) {
-                        const R ra = A.h.w, rb = B.h.w;           // r_ij^2, r_ik^2
-                        const R rsc = rsqrt_r<R>(rc);
-                        const R irc = rsc * rsc;
-                        const R ir1 = A.s.x * B.s.x * rsc;        // 1 / (r_ij r_ik r_jk)
-                        const R ir2 = ir1 * ir1;
-                        const R ir3 = ir2 * ir1;
-                        const R ir5 = ir3 * ir2;
-                        // (r0/r1)^alp3 with r0 = r0ij r0ik r0jk, r1 = r_ij r_ik r_jk (atm.f90:744-749)
-                        const R tq = rexp<R>(A.c.w + B.c.w + ekj.lr0 - R(0.5) * alp3 * rlog<R>(rc));
-                        const R fdmp = rcp_r<R>(R(1) + R(6) * tq);
-                        const R s1 = ra + rb + rc;
-                        const R ang = R(0.375) * (s1 - R(2) * rb) * (s1 - R(2) * rc) * (s1 - R(2) * ra) * ir5 + ir3;
-                        const R c9 = -s9 * A.c.x * B.c.x * ekj.sc6;
-                        R sw = R(1), swjk = R(1), dswjkr = R(0);
-                        if (smooth_on) {
-                            R dsw;
-                            const R rjk = rc * rsc;
-                            smooth<R>(rjk, cutoff, width, swjk, dsw);
-                            dswjkr = dsw * rsc;
-                            sw = A.s.y * B.s.y * swjk;
-                        }
-                        const R dE0 = ang * fdmp * c9;
-                        const R dE = dE0 * sw;
-                        te -= dE;
-                        ntrip++;
-                        if (GRAD) {
-                            const R common = c9 * ang * (R(-2) * alp * tq * (fdmp * fdmp));
-                            const R kfac = R(0.375) * c9 * fdmp * ir5;
-                            R sij = sw * (common + kfac * ang_deriv<R>(ra, rc, rb, s1)) * A.l.w;
-                            R sik = sw * (common + kfac * ang_deriv<R>(rb, rc, ra, s1)) * B.l.w;
-                            R sjk = sw * (common + kfac * ang_deriv<R>(rc, rb, ra, s1)) * irc;
-                            if (smooth_on) {
-                                sij -= dE0 * A.s.z * B.s.y * swjk;
-                                sik -= dE0 * B.s.z * A.s.y * swjk;
-                                sjk -= dE0 * dswjkr * A.s.y * B.s.y;
-                            }
-                            const R gx = sjk * vx, gy = sjk * vy, gz = sjk * vz;
-                            // dE/dCN: root, row and partner shares (model.f90 dc6dcn / c6 ratios)
-                            dei -= R(0.5) * dE * (A.c.y + B.c.y);
-                            jS += sij; jGx -= gx; jGy -= gy; jGz -= gz;
-                            jD -= R(0.5) * dE * (A.c.z + ekj.qcr);
-                            cS = sik; cGx = gx; cGy = gy; cGz = gz;
-                            cD = -R(0.5) * dE * (B.c.z + ekj.qrc);
-                            txx += gx * vx; tyy += gy * vy; tzz += gz * vz;
-                            txy += gx * vy; txz += gx * vz; tyz += gy * vz;
-                        }
-                    }
-                };
-                // partners in groups of four; their sums are reduced over the
-                // warp with a reduce-scatter (10 + 5 + 3 x 5 shuffles for the
-                // group) and handed to the partner's own lane
-                for (int tg = 0; tg < tn; tg += 4) {
-                    R kv[4][5];
-#pragma unroll
-                    for (int g = 0; g < 4; g++) {
-#pragma unroll
-                        for (int v = 0; v < 5; v++) kv[g][v] = R(0);
-                        if (tg + g < tn) candidate(tg + g, kv[g]);
-                    }
-                    if (GRAD) {
-                        const bool up16 = (lane & 16) != 0, up8 = (lane & 8) != 0;
-                        R r2[2][5];
-#pragma unroll
-                        for (int h = 0; h < 2; h++)
-#pragma unroll
-                            for (int v = 0; v < 5; v++) {
-                                const R send = up16 ? kv[h][v] : kv[2 + h][v];
-                                const R keep = up16 ? kv[2 + h][v] : kv[h][v];
-                                r2[h][v] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-                            }
-                        R r1[5];
-#pragma unroll
-                        for (int v = 0; v < 5; v++) {
-                            const R send = up8 ? r2[0][v] : r2[1][v];
-                            const R keep = up8 ? r2[1][v] : r2[0][v];
-                            r1[v] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-                        }
-#pragma unroll
-                        for (int v = 0; v < 5; v++)
-#pragma unroll
-                            for (int o = 4; o > 0; o >>= 1) r1[v] += __shfl_xor_sync(0xffffffffu, r1[v], o);
-                        // lanes 16 b4 + 8 b3 + x now hold partner tg + 2 b4 + b3
-                        const int gl = lane - tg;
-                        const bool mine = gl >= 0 && gl < 4 && lane < tn;
-                        const int src = mine ? 16 * (gl >> 1) + 8 * (gl & 1) : 0;
-                        R got[5];
-#pragma unroll
-                        for (int v = 0; v < 5; v++) got[v] = __shfl_sync(0xffffffffu, r1[v], src);
-                        if (mine) { kS += got[0]; kGx += got[1]; kGy += got[2]; kGz += got[3]; kD += got[4]; }
-                    }
-                }
-                e_l += double(te);
-                if (GRAD) {
-                    sxx += double(txx); syy += double(tyy); szz += double(tzz);
-                    sxy += double(txy); sxz += double(txz); syz += double(tyz);
-                    // k-role of partner K0 + lane: pair (i, k) force along x_k - x_i
-                    if (kin && (kS != R(0) || kGx != R(0) || kGy != R(0) || kGz != R(0) || kD != R(0))) {
-                        const PairRec<R>& Bown = wrec[lane];
-                        R vx, vy, vz;
-                        if constexpr (sizeof(R) == 8) {
-                            vx = Bown.h.x - rhx; vy = Bown.h.y - rhy; vz = Bown.h.z - rhz;
-                        } else {
-                            vx = (Bown.h.x - rhx) + (Bown.l.x - rlx);
-                            vy = (Bown.h.y - rhy) + (Bown.l.y - rly);
-                            vz = (Bown.h.z - rhz) + (Bown.l.z - rlz);
-                        }
-                        const double fx = double(kS * vx), fy = double(kS * vy), fz = double(kS * vz);
-                        atomicAdd(acc + 4 * kk + 0, fx + double(kGx));
-                        atomicAdd(acc + 4 * kk + 1, fy + double(kGy));
-                        atomicAdd(acc + 4 * kk + 2, fz + double(kGz));
-                        atomicAdd(acc + 4 * kk + 3, double(kD));
-                        gix -= R(fx); giy -= R(fy); giz -= R(fz);
-                        sxx += fx * vx; syy += fy * vy; szz += fz * vz;
-                        sxy += fx * vy; sxz += fx * vz; syz += fy * vz;
-                    }
-                }
-            }
-            if (GRAD) {
-                // row j: pair (i, j) force along x_j - x_i, and its partner sums
-                if (jvalid) {
-                    R vx, vy, vz;
-                    if constexpr (sizeof(R) == 8) {
-                        vx = A.h.x - rhx; vy = A.h.y - rhy; vz = A.h.z - rhz;
-                    } else {
-                        vx = (A.h.x - rhx) + (A.l.x - rlx);
-                        vy = (A.h.y - rhy) + (A.l.y - rly);
-                        vz = (A.h.z - rhz) + (A.l.z - rlz);
-                    }
-                    const double fx = double(jS * vx), fy = double(jS * vy), fz = double(jS * vz);
-                    atomicAdd(acc + 4 * j + 0, fx + double(jGx));
-                    atomicAdd(acc + 4 * j + 1, fy + double(jGy));
-                    atomicAdd(acc + 4 * j + 2, fz + double(jGz));
-                    atomicAdd(acc + 4 * j + 3, double(jD));
-                    gix -= R(fx); giy -= R(fy); giz -= R(fz);
-                    sxx += fx * vx; syy += fy * vy; szz += fz * vz;
-                    sxy += fx * vy; sxz += fx * vz; syz += fy * vz;
-                }
-                const double rgx = wsum64(double(gix)), rgy = wsum64(double(giy)), rgz = wsum64(double(giz));
-                const double rde = wsum64(double(dei));
-                if (lane == 0) {
-                    atomicAdd(acc + 4 * i + 0, rgx);
-                    atomicAdd(acc + 4 * i + 1, rgy);
-                    atomicAdd(acc + 4 * i + 2, rgz);
-                    atomicAdd(acc + 4 * i + 3, rde);
-                }
-            }
-        }
-        // molecule totals: energy and virial in a fixed order, gradient and dE/dCN per atom
+        for (int t = wid; t < nitems; t += kMolWarps)
+            mol_item<R, GRAD, SMOOTH>(t, n, nitems, m0, px, py, pz, loc, acc, tl, part, s9, alp, alp3, cut2d, cut2,
+                                      cutoff, width, lane, e_l, sxx, syy, szz, sxy, sxz, syz, ntrip);
+        // molecule totals: energy and virial in a fixed order, gradient and
+        // dE/dCN per atom summed over the warps in warp order
         double r[8] = {e_l, sxx, syy, szz, sxy, sxz, syz, double(ntrip)};
         for (int v = 0; v < 8; v++) r[v] = wsum64(r[v]);
         if (lane == 0)
@@ -401,10 +412,15 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
                     for (int v = 0; v < 6; v++) sig3[kSigma * (a0 + a) + v] = 0.0;
             }
             if (GRAD) {
-                w.grad[3 * (a0 + a) + 0] += acc[4 * a + 0];
-                w.grad[3 * (a0 + a) + 1] += acc[4 * a + 1];
-                w.grad[3 * (a0 + a) + 2] += acc[4 * a + 2];
-                w.dEdcn[a0 + a] += acc[4 * a + 3];
+                double g0 = 0, g1 = 0, g2 = 0, g3 = 0;
+                for (int q = 0; q < kMolWarps; q++) {
+                    const double* aq = accw + ((size_t)q * kMolMax + a) * 4;
+                    g0 += aq[0]; g1 += aq[1]; g2 += aq[2]; g3 += aq[3];
+                }
+                w.grad[3 * (a0 + a) + 0] += g0;
+                w.grad[3 * (a0 + a) + 1] += g1;
+                w.grad[3 * (a0 + a) + 2] += g2;
+                w.dEdcn[a0 + a] += g3;
             }
         }
     }
@@ -413,18 +429,38 @@ k_triples_mol(Batch b, Species sp, Damp d, Config c, Partition part, Work w, con
 template <class R>
 size_t mol_smem()
 {
-    return sizeof(double) * 3 * kMolMax + sizeof(double) * 4 * kMolMax + sizeof(PairRec<R>) * kMolWarps * 32 +
-           sizeof(int) * 2 * kMolMax;
+    return sizeof(MolTile<R>) * kMolWarps + sizeof(double) * kMolWarps * kMolMax * 4 + sizeof(double) * 3 * kMolMax +
+           sizeof(int) * kMolMax;
 }
 
-template <class R, bool GRAD>
+template <class R, bool GRAD, bool SMOOTH>
 void mol_configure()
 {
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(k_triples_mol<R, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mol_smem<R>());
+        cudaFuncSetAttribute(k_triples_mol<R, GRAD, SMOOTH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)mol_smem<R>());
         configured = true;
     }
+}
+
+template <class R, bool GRAD, bool SMOOTH>
+int mol_occupancy()
+{
+    mol_configure<R, GRAD, SMOOTH>();
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_triples_mol<R, GRAD, SMOOTH>, kMolThreads, mol_smem<R>());
+    return n;
+}
+
+template <class R, bool GRAD, bool SMOOTH>
+void mol_launch(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p, const Work& w,
+                const void* mat, const long long* mat_off, const int* mol_order, int nmol, unsigned int* queue,
+                int blocks, double* e3, double* sig3, cudaStream_t stream)
+{
+    mol_configure<R, GRAD, SMOOTH>();
+    k_triples_mol<R, GRAD, SMOOTH><<<blocks, kMolThreads, mol_smem<R>(), stream>>>(
+        b, s, d, c, p, w, (const C6Entry<R>*)mat, mat_off, mol_order, nmol, queue, e3, sig3);
 }
 
 }  // namespace
@@ -433,13 +469,14 @@ int atm_mol_max_atoms() { return kMolMax; }
 
 int atm_mol_blocks_per_sm(bool mixed, bool grad)
 {
-    int n = 0;
+    // the smallest occupancy of the variants (the smooth-cutoff ones included)
+    int n;
     if (mixed) {
-        if (grad) { mol_configure<float, true>(); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_triples_mol<float, true>, kMolThreads, mol_smem<float>()); }
-        else { mol_configure<float, false>(); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_triples_mol<float, false>, kMolThreads, mol_smem<float>()); }
+        n = grad ? std::min(mol_occupancy<float, true, false>(), mol_occupancy<float, true, true>())
+                 : std::min(mol_occupancy<float, false, false>(), mol_occupancy<float, false, true>());
     } else {
-        if (grad) { mol_configure<double, true>(); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_triples_mol<double, true>, kMolThreads, mol_smem<double>()); }
-        else { mol_configure<double, false>(); cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_triples_mol<double, false>, kMolThreads, mol_smem<double>()); }
+        n = grad ? std::min(mol_occupancy<double, true, false>(), mol_occupancy<double, true, true>())
+                 : std::min(mol_occupancy<double, false, false>(), mol_occupancy<double, false, true>());
     }
     return n > 0 ? n : 1;
 }
@@ -449,25 +486,16 @@ void launch_triples_mol(const Batch& b, const Species& s, const Damp& d, const C
                         unsigned int* queue, int blocks, double* e3, double* sig3, cudaStream_t stream)
 {
     if (nmol <= 0) return;
+    const bool smooth_on = c.width3 > 0.0 && c.width3 < c.cut3;
+#define D3_MOL(R, G, S) mol_launch<R, G, S>(b, s, d, c, p, w, mat, mat_off, mol_order, nmol, queue, blocks, e3, sig3, stream)
     if (c.mixed) {
-        const auto* m = (const C6Entry<float>*)mat;
-        if (c.grad) {
-            mol_configure<float, true>();
-            k_triples_mol<float, true><<<blocks, kMolThreads, mol_smem<float>(), stream>>>(b, s, d, c, p, w, m, mat_off, mol_order, nmol, queue, e3, sig3);
-        } else {
-            mol_configure<float, false>();
-            k_triples_mol<float, false><<<blocks, kMolThreads, mol_smem<float>(), stream>>>(b, s, d, c, p, w, m, mat_off, mol_order, nmol, queue, e3, sig3);
-        }
+        if (c.grad) { if (smooth_on) D3_MOL(float, true, true); else D3_MOL(float, true, false); }
+        else { if (smooth_on) D3_MOL(float, false, true); else D3_MOL(float, false, false); }
     } else {
-        const auto* m = (const C6Entry<double>*)mat;
-        if (c.grad) {
-            mol_configure<double, true>();
-            k_triples_mol<double, true><<<blocks, kMolThreads, mol_smem<double>(), stream>>>(b, s, d, c, p, w, m, mat_off, mol_order, nmol, queue, e3, sig3);
-        } else {
-            mol_configure<double, false>();
-            k_triples_mol<double, false><<<blocks, kMolThreads, mol_smem<double>(), stream>>>(b, s, d, c, p, w, m, mat_off, mol_order, nmol, queue, e3, sig3);
-        }
+        if (c.grad) { if (smooth_on) D3_MOL(double, true, true); else D3_MOL(double, true, false); }
+        else { if (smooth_on) D3_MOL(double, false, true); else D3_MOL(double, false, false); }
     }
+#undef D3_MOL
 }
 
 }  // namespace d3

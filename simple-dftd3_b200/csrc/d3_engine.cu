@@ -485,6 +485,12 @@ void Engine::ensure_workspace(bool grad, bool param_grad, bool threebody)
         d_keys_out_ = dev_alloc<unsigned long long>(n);
         d_idx_in_ = dev_alloc<int>(n);
         d_perm_ = dev_alloc<int>(n);
+        d_identity_ = dev_alloc<int>(n);
+        {
+            std::vector<int> id(n);
+            std::iota(id.begin(), id.end(), 0);
+            check(cudaMemcpy(d_identity_, id.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "identity order");
+        }
         d_sp_sorted_ = dev_alloc<int>(n);
         d_local_sorted_ = dev_alloc<int>(n);
         d_zid_sorted_ = dev_alloc<int>(n);
@@ -718,6 +724,17 @@ void Engine::hessian_host(const Damp& d, const double* positions, double* hessia
     check(cudaStreamSynchronize(stream), "hessian");
 }
 
+// The direct path (d3_kernels.cu: one warp per atom over its partners, atoms
+// in input order) for batches of small systems, where the tile sweeps are
+// latency-bound: rational or zero damping, no work partition, reducer,
+// parameter derivatives or term counters.
+bool Engine::direct_pairs(const Damp& d, bool pg) const
+{
+    if (reducer_ || counting_ || pg || part_.nparts > 1) return false;
+    if (d.kind != kRational && d.kind != kZero) return false;
+    return max_sys_atoms_ <= kDirectMaxAtoms && natoms_ <= kDirectMaxTotal;
+}
+
 void Engine::run(const Damp& d, const double* d_positions, double* d_energies, double* d_gradient,
                  double* d_sigma9, double* d_param_grad, bool grad, cudaStream_t stream)
 {
@@ -776,18 +793,31 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     }
     kev3_recorded_ = false;
     mark(0);
-    order_atoms(d, d_positions, b, mixed_, stream);
+    // small systems: atoms in input order and the pair sums of each atom in one
+    // warp (no ordering, tiles or slot gathers; fewer and shorter launches)
+    const bool direct = direct_pairs(d, pg);
+    if (direct) {
+        check(cudaMemcpyAsync(d_perm_, d_identity_, sizeof(int) * natoms_, cudaMemcpyDeviceToDevice, stream), "order");
+        launch_gather_sorted(d_positions, d_perm_, d_sp_, d_ghost_, d_sys_of_atom_, d_atom_off_, natoms_, d_x_, d_y_,
+                             d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed_, stream);
+        b.tiles = nullptr;
+    } else {
+        order_atoms(d, d_positions, b, mixed_, stream);
+    }
     mark(1);
     // without a reducer the CN pass also writes the reference weights and the
     // species vectors (one kernel after the sweep instead of three)
     const bool two_body = two_body_active(d) || pg;
-    const bool fused = !reducer_;
-    launch_cn_units(b, s, c, part_, w, pcn, false, stream, fused, fused && two_body ? pu_.U : nullptr);
+    const bool fused = !reducer_ && !direct;
+    if (direct) launch_coordination_number(b, s, c, part_, w, stream);
+    else launch_cn_units(b, s, c, part_, w, pcn, false, stream, fused, fused && two_body ? pu_.U : nullptr);
     if (reducer_) reduce(w.cn, natoms_, stream);
     mark(2);
     if (!fused) launch_weights(b, s, c, w, stream);
     mark(3);
-    if (two_body) {
+    if (two_body && direct) {
+        launch_two_body(b, s, d, c, part_, w, stream);
+    } else if (two_body) {
         launch_two_body_units(b, s, d, c, part_, w, pu_, stream, timed ? kev_[0] : nullptr, timed ? kev_[1] : nullptr,
                               fused);
     } else {
@@ -799,6 +829,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
         }
     }
     mark(4);
+    species_ready_ = two_body && !direct;
     if (threebody) {
         run_three_body(b, s, d, c, w, stream);
         if (pg) {
@@ -819,7 +850,8 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     mark(5);
     if (grad) {
         if (reducer_) reduce(w.dEdcn, natoms_, stream);
-        launch_cn_units(b, s, c, part_, w, pcn, true, stream);
+        if (direct) launch_cn_chain_rule(b, s, c, part_, w, stream);
+        else launch_cn_units(b, s, c, part_, w, pcn, true, stream);
     }
     mark(6);
     if (!reducer_) {
@@ -873,6 +905,7 @@ void Engine::run_three_body(const Batch& b, const Species& s, const Damp& d, con
         d_queue_ = dev_alloc<unsigned int>(2);   // root queue, molecule queue
         d_e3_ = dev_alloc<double>(n);
         d_sig3_ = dev_alloc<double>((size_t)kSigma * n);
+        d_fxacc_ = dev_alloc<unsigned long long>((size_t)8 * n);
         scan_bytes_ = scan_temp_bytes(n);
         d_scan_temp_ = dev_alloc<unsigned char>(scan_bytes_);
         check(cudaMallocHost(&h_atm_counts_, 2 * sizeof(long long)), "cudaMallocHost");
@@ -880,7 +913,9 @@ void Engine::run_three_body(const Batch& b, const Species& s, const Damp& d, con
         check(cudaMemsetAsync(d_guard_, 0, sizeof(int), stream), "memset");
         atm_ready_ = true;
     }
-    launch_c6_matrix(b, s, w, (d.alp + 2.0) / 3.0, d_c6mat_off_, d_c6mat_, c6mat_total_, c.mixed, stream);
+    // the two-body pass computed the species vectors; without it they are computed here
+    if (!species_ready_) launch_species_vectors(b, s, c, w, pu_.U, stream);
+    launch_c6_matrix(b, s, w, pu_.U, (d.alp + 2.0) / 3.0, d_c6mat_off_, d_c6mat_, c6mat_total_, c.mixed, stream);
     if (root_atoms_ > 0) {
         check(cudaMemsetAsync(d_maxcnt_, 0, sizeof(int), stream), "memset");
         check(cudaMemsetAsync(d_cnt_ + n, 0, sizeof(int), stream), "memset");
@@ -927,12 +962,15 @@ void Engine::run_three_body(const Batch& b, const Species& s, const Damp& d, con
             }
         }
         launch_atm_guard(d_off_ + n, d_maxcnt_, nbr_cap_, stride, d_guard_, stream);
-        launch_nbr_fill(b, c, d_sys_mol_, d_off_, d_nbr_j_, d_nbr_gend_, d_nbr_v_, d_guard_, stream);
+        launch_nbr_fill(b, c, d_sys_mol_, d_off_, d_cnt_, d_nbr_j_, d_nbr_gend_, d_nbr_v_, d_guard_, stream);
         check(cudaMemsetAsync(d_queue_, 0, sizeof(unsigned int), stream), "memset");
         w.atm_guard = d_guard_;
         if (profiling_ && !capturing_) check(cudaEventRecord(kev_[2], stream), "cudaEventRecord");
+        if (c.grad) check(cudaMemsetAsync(d_fxacc_, 0, sizeof(unsigned long long) * 8 * n, stream), "memset");
         launch_triples(b, s, d, c, part_, w, d_c6mat_, d_c6mat_off_, d_off_, d_cnt_, d_nbr_j_, d_nbr_gend_, d_nbr_v_,
-                       d_queue_, d_slot_acc_, d_slot_scr_, stride, blocks, any_periodic_, d_e3_, d_sig3_, stream);
+                       d_queue_, d_slot_acc_, d_slot_scr_, stride, blocks, any_periodic_, d_e3_, d_sig3_, d_fxacc_,
+                       stream);
+        if (c.grad) launch_atm_fixed(n, d_fxacc_, d_guard_, w, stream);
     }
     if (!mol_order_.empty()) {
         // after the root kernel, which writes zeros for the molecules' atoms

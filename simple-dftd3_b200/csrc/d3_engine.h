@@ -12,6 +12,13 @@
 
 #include "d3_device.cuh"
 
+#ifndef DIRECT_MAX_ATOMS
+#define DIRECT_MAX_ATOMS 256
+#endif
+#ifndef DIRECT_MAX_TOTAL
+#define DIRECT_MAX_TOTAL 2048
+#endif
+
 namespace d3 {
 
 struct Cutoffs {
@@ -190,6 +197,10 @@ private:
     int cn_split() const;                // items per tile pair of the CN sweeps
     bool any_periodic_ = false;          // a system has a periodic direction
     void configure_molecules();          // mol_order_ and root_atoms_ from tune_.atm_mol
+    // systems small enough for the direct pair kernels (see direct_pairs)
+    static constexpr int kDirectMaxAtoms = DIRECT_MAX_ATOMS;
+    static constexpr int kDirectMaxTotal = DIRECT_MAX_TOTAL;
+    bool direct_pairs(const Damp& d, bool pg) const;
     uint8_t* d_sys_mol_ = nullptr;       // [nsys] 1 for those systems
     long long root_atoms_ = 0;           // atoms of the other systems
     bool graph_on_ = false, capturing_ = false, graph_valid_ = false;
@@ -246,6 +257,7 @@ private:
     int* d_tile_off_ = nullptr;
     unsigned long long *d_keys_in_ = nullptr, *d_keys_out_ = nullptr;
     int *d_idx_in_ = nullptr, *d_perm_ = nullptr;
+    int* d_identity_ = nullptr;           // 0 .. natoms - 1 (the order of the direct path)
     int *d_sp_sorted_ = nullptr, *d_local_sorted_ = nullptr, *d_zid_ = nullptr, *d_zid_sorted_ = nullptr;
     uint8_t* d_ghost_sorted_ = nullptr;
     double4* d_tiles_ = nullptr;
@@ -286,8 +298,10 @@ private:
     long long slot_scr_cap_ = 0;
     double* d_e3_ = nullptr;
     double* d_sig3_ = nullptr;
+    unsigned long long* d_fxacc_ = nullptr;   // [natoms][4][2] fixed-point three-body gradient, dE/dCN
     long long* h_atm_counts_ = nullptr;   // pinned: total entries, largest list
     bool atm_ready_ = false;
+    bool species_ready_ = false;   // PairUnits::U holds this evaluation's species vectors
     long long last_triples_entries_ = 0;
 };
 

@@ -120,6 +120,7 @@ __device__ __forceinline__ R rpow(R x, R a) { if constexpr (sizeof(R) == 8) retu
 __global__ void k_split_positions(const double* __restrict__ pos, int n, double* x, double* y,
                                   double* z, float4* xhi, float4* xlo, bool mixed)
 {
+    pdl_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double px = pos[3 * i + 0], py = pos[3 * i + 1], pz = pos[3 * i + 2];
@@ -139,6 +140,7 @@ template <class R>
 __global__ void __launch_bounds__(kThreads) k_coordination_number(Batch b, Species s, Config c,
                                                                   Partition p, Work w)
 {
+    pdl_wait();
     using Sh = typename ShiftOf<R>::type;
     __shared__ Sh sbuf[kWarpsPerBlock][kImgChunk];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -191,6 +193,7 @@ __global__ void __launch_bounds__(kThreads) k_coordination_number(Batch b, Speci
 // NaN/Inf fallback (weight_references, model.f90:201-324), always FP64.
 __global__ void k_weights(Batch b, Species s, Config c, Work w)
 {
+    pdl_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= b.natoms) return;
     const int sp = b.sp[i];
@@ -261,6 +264,7 @@ template <class R, int DAMP>
 __global__ void __launch_bounds__(kThreads) k_two_body(Batch b, Species s, Damp d, Config c,
                                                        Partition p, Work w)
 {
+    pdl_wait();
     using Sh = typename ShiftOf<R>::type;
     __shared__ Sh sbuf[kWarpsPerBlock][kImgChunk];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -415,6 +419,7 @@ __global__ void __launch_bounds__(kThreads) k_two_body(Batch b, Species s, Damp 
 template <class R>
 __global__ void __launch_bounds__(kThreads) k_cn_chain(Batch b, Species s, Config c, Partition p, Work w)
 {
+    pdl_wait();
     using Sh = typename ShiftOf<R>::type;
     __shared__ Sh sbuf[kWarpsPerBlock][kImgChunk];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -480,6 +485,7 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_reduce_systems(Batch b, Config c, Work w, double* energies, double* sigma9, double* param_grad, double* grad_out)
 {
+    pdl_wait();
     constexpr int kVals = 1 + kSigma + kParamGrad;
     __shared__ double red[kVals][BLOCK / 32];
     const int sys = blockIdx.x;
@@ -581,7 +587,7 @@ void launch_split_positions(const double* pos, int natoms, double* x, double* y,
                             float4* xhi, float4* xlo, bool mixed, cudaStream_t stream)
 {
     if (natoms <= 0) return;
-    k_split_positions<<<(natoms + 255) / 256, 256, 0, stream>>>(pos, natoms, x, y, z, xhi, xlo, mixed);
+    launch_pdl(k_split_positions, dim3((natoms + 255) / 256), dim3(256), 0, stream, pos, natoms, x, y, z, xhi, xlo, mixed);
 }
 
 void launch_coordination_number(const Batch& b, const Species& s, const Config& c,
@@ -593,15 +599,15 @@ void launch_coordination_number(const Batch& b, const Species& s, const Config& 
         return;
     }
     if (c.mixed)
-        k_coordination_number<float><<<blocks_for_atoms(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
+        launch_pdl(k_coordination_number<float>, dim3(blocks_for_atoms(b.natoms)), dim3(kThreads), 0, stream, b, s, c, p, w);
     else
-        k_coordination_number<double><<<blocks_for_atoms(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
+        launch_pdl(k_coordination_number<double>, dim3(blocks_for_atoms(b.natoms)), dim3(kThreads), 0, stream, b, s, c, p, w);
 }
 
 void launch_weights(const Batch& b, const Species& s, const Config& c, const Work& w, cudaStream_t stream)
 {
     if (b.natoms <= 0) return;
-    k_weights<<<(b.natoms + 127) / 128, 128, 0, stream>>>(b, s, c, w);
+    launch_pdl(k_weights, dim3((b.natoms + 127) / 128), dim3(128), 0, stream, b, s, c, w);
 }
 
 void launch_two_body(const Batch& b, const Species& s, const Damp& d, const Config& c,
@@ -614,11 +620,11 @@ void launch_two_body(const Batch& b, const Species& s, const Damp& d, const Conf
     }
     const int nb = blocks_for_atoms(b.natoms);
     if (d.kind == kRational) {
-        if (c.mixed) k_two_body<float, kRational><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
-        else k_two_body<double, kRational><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
+        if (c.mixed) launch_pdl(k_two_body<float, kRational>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w);
+        else launch_pdl(k_two_body<double, kRational>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w);
     } else {
-        if (c.mixed) k_two_body<float, kZero><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
-        else k_two_body<double, kZero><<<nb, kThreads, 0, stream>>>(b, s, d, c, p, w);
+        if (c.mixed) launch_pdl(k_two_body<float, kZero>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w);
+        else launch_pdl(k_two_body<double, kZero>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w);
     }
 }
 
@@ -631,9 +637,9 @@ void launch_cn_chain_rule(const Batch& b, const Species& s, const Config& c, con
         return;
     }
     if (c.mixed)
-        k_cn_chain<float><<<blocks_for_atoms(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
+        launch_pdl(k_cn_chain<float>, dim3(blocks_for_atoms(b.natoms)), dim3(kThreads), 0, stream, b, s, c, p, w);
     else
-        k_cn_chain<double><<<blocks_for_atoms(b.natoms), kThreads, 0, stream>>>(b, s, c, p, w);
+        launch_pdl(k_cn_chain<double>, dim3(blocks_for_atoms(b.natoms)), dim3(kThreads), 0, stream, b, s, c, p, w);
 }
 
 void launch_reduce_systems(const Batch& b, const Config& c, const Work& w, double* energies,
@@ -642,9 +648,9 @@ void launch_reduce_systems(const Batch& b, const Config& c, const Work& w, doubl
     if (b.nsys <= 0) return;
     // a block of 1024 threads where systems average above 512 atoms
     if (b.natoms > 512LL * b.nsys)
-        k_reduce_systems<1024><<<b.nsys, 1024, 0, stream>>>(b, c, w, energies, sigma9, param_grad, grad_out);
+        launch_pdl(k_reduce_systems<1024>, dim3(b.nsys), dim3(1024), 0, stream, b, c, w, energies, sigma9, param_grad, grad_out);
     else
-        k_reduce_systems<256><<<b.nsys, 256, 0, stream>>>(b, c, w, energies, sigma9, param_grad, grad_out);
+        launch_pdl(k_reduce_systems<256>, dim3(b.nsys), dim3(256), 0, stream, b, c, w, energies, sigma9, param_grad, grad_out);
 }
 
 }  // namespace d3

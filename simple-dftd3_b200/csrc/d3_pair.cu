@@ -609,6 +609,7 @@ __global__ void __launch_bounds__(BLOCK)
 k_rank_shape(const double* __restrict__ pos, const int* atom_off, const int* tile_off, int2* shape,
              unsigned long long* word)
 {
+    pdl_wait();
     __shared__ double red[6][BLOCK / 32];
     const int sys = blockIdx.x;
     const int a0 = atom_off[sys], a1 = atom_off[sys + 1];
@@ -660,6 +661,7 @@ k_rank_pass(const double* __restrict__ pos, int n, const int* sys_of_atom, const
             bool mixed, int* perm, double* x, double* y, double* z, float4* xhi, float4* xlo,
             int* sp, uint8_t* ghost, int* local, int* zid)
 {
+    pdl_wait();
     __shared__ unsigned long long sword[kRankChunk];
     // G lanes per atom a (G = 4, 8 or 32 by the largest system)
     const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -724,6 +726,7 @@ __global__ void k_gather_sorted(const double* __restrict__ pos, const int* perm,
                                 double* x, double* y, double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost,
                                 int* local, bool mixed, const int* zid_in, int* zid)
 {
+    pdl_wait();
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= n) return;
     const int o = perm[a];
@@ -743,6 +746,7 @@ __global__ void k_gather_sorted(const double* __restrict__ pos, const int* perm,
 // Bounding sphere (centroid, largest distance) of each tile; one warp per tile.
 __global__ void k_tile_bounds(Batch b, const int* tile_sys, int ntiles, double4* tiles)
 {
+    pdl_wait();
     const int lane = threadIdx.x & 31;
     const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (t >= ntiles) return;
@@ -789,20 +793,20 @@ void launch_rank_order(const double* pos, int natoms, int nsys, int max_atoms, c
     if (natoms <= 0 || nsys <= 0) return;
     // a block of 1024 threads for systems above 256 atoms (two atoms a thread
     // for 2000 atoms instead of sixteen)
-    if (max_atoms > 256) k_rank_shape<1024><<<nsys, 1024, 0, stream>>>(pos, atom_off, tile_off, shape, word_a);
-    else k_rank_shape<kOrderThreads><<<nsys, kOrderThreads, 0, stream>>>(pos, atom_off, tile_off, shape, word_a);
+    if (max_atoms > 256) launch_pdl(k_rank_shape<1024>, dim3(nsys), dim3(1024), 0, stream, pos, atom_off, tile_off, shape, word_a);
+    else launch_pdl(k_rank_shape<kOrderThreads>, dim3(nsys), dim3(kOrderThreads), 0, stream, pos, atom_off, tile_off, shape, word_a);
     // lanes per atom: a whole warp for large systems, groups of 8 or 4 lanes
     // for batches of molecules (a warp would idle on a few dozen words)
     const int g = max_atoms > 512 ? 32 : (max_atoms > 64 ? 8 : 4);
     const unsigned blocks = (unsigned)(((long long)natoms * g + kRankThreads - 1) / kRankThreads);
 #define D3_RANK_PASS(P, W_IN, W_OUT)                                                                          \
     do {                                                                                                     \
-        if (g == 32) k_rank_pass<P, 32><<<blocks, kRankThreads, 0, stream>>>RANK_ARGS(W_IN, W_OUT);         \
-        else if (g == 8) k_rank_pass<P, 8><<<blocks, kRankThreads, 0, stream>>>RANK_ARGS(W_IN, W_OUT);      \
-        else k_rank_pass<P, 4><<<blocks, kRankThreads, 0, stream>>>RANK_ARGS(W_IN, W_OUT);                  \
+        if (g == 32) launch_pdl(k_rank_pass<P, 32>, dim3(blocks), dim3(kRankThreads), 0, stream, RANK_ARGS(W_IN, W_OUT)); \
+        else if (g == 8) launch_pdl(k_rank_pass<P, 8>, dim3(blocks), dim3(kRankThreads), 0, stream, RANK_ARGS(W_IN, W_OUT)); \
+        else launch_pdl(k_rank_pass<P, 4>, dim3(blocks), dim3(kRankThreads), 0, stream, RANK_ARGS(W_IN, W_OUT));  \
     } while (0)
-#define RANK_ARGS(W_IN, W_OUT) (pos, natoms, sys_of_atom, atom_off, tile_off, shape, W_IN, W_OUT, sp_in, ghost_in, \
-                                zid_in, mixed, perm, x, y, z, xhi, xlo, sp, ghost, local, zid)
+#define RANK_ARGS(W_IN, W_OUT) pos, natoms, sys_of_atom, atom_off, tile_off, shape, W_IN, W_OUT, sp_in, ghost_in, \
+                                zid_in, mixed, perm, x, y, z, xhi, xlo, sp, ghost, local, zid
     D3_RANK_PASS(0, word_a, word_b);
     D3_RANK_PASS(1, word_b, word_a);
     D3_RANK_PASS(2, word_a, word_b);
@@ -816,7 +820,7 @@ void launch_gather_sorted(const double* pos, const int* perm, const int* sp_in, 
                           cudaStream_t stream, const int* zid_in, int* zid)
 {
     if (natoms <= 0) return;
-    k_gather_sorted<<<(natoms + 255) / 256, 256, 0, stream>>>(pos, perm, sp_in, ghost_in, sys_of_atom, atom_off,
+    launch_pdl(k_gather_sorted, dim3((natoms + 255) / 256), dim3(256), 0, stream, pos, perm, sp_in, ghost_in, sys_of_atom, atom_off,
                                                               natoms, x, y, z, xhi, xlo, sp, ghost, local, mixed,
                                                               zid_in, zid);
 }
@@ -824,7 +828,7 @@ void launch_gather_sorted(const double* pos, const int* perm, const int* sp_in, 
 void launch_tile_bounds(const Batch& b, const int* tile_sys, int ntiles, double4* tiles, cudaStream_t stream)
 {
     if (ntiles <= 0) return;
-    k_tile_bounds<<<(ntiles + 7) / 8, 256, 0, stream>>>(b, tile_sys, ntiles, tiles);
+    launch_pdl(k_tile_bounds, dim3((ntiles + 7) / 8), dim3(256), 0, stream, b, tile_sys, ntiles, tiles);
 }
 
 // Atoms per block of the pair sweeps: 4 or 8 warps (one atom per warp).

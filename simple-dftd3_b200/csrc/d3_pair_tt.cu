@@ -33,7 +33,6 @@ constexpr int kUnitJ = 4;         // per-lane j sums: dE/dCN, g(3)
 constexpr int kCnStore = 9;       // stored chain-rule sums per (i, j): countd (3), countd v^T (6)
 constexpr int kSplitMax = 4;      // a unit is evaluated as 1, 2 (j-tile halves) or 4 items
                                   // (and translation halves); slots are sized for the largest split
-constexpr int kRefPad = 8;        // species-vector stride: U[0..6], pad, dU[0..6], pad
 
 template <class R> struct T4;
 template <> struct T4<float> { using type = float4; };
@@ -228,6 +227,7 @@ __device__ __forceinline__ int tt_jmask(const V* sth, const V* stl, int qbeg, in
 template <class R>
 __global__ void k_species_vectors(Batch b, Species s, Work w, R* UV)
 {
+    pdl_wait();
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long total = (long long)b.natoms * b.nid * kRefPad;
     if (t >= total) return;
@@ -326,6 +326,7 @@ __global__ void __launch_bounds__(kTTThreads, sizeof(R) == 4 ? 4 : 3)
 k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const int2* units, int nunits, int split,
               const R* UV, double* unit_i, double* unit_j)
 {
+    pdl_wait();
     using V = typename T4<R>::type;
     __shared__ V sth[kTTWarps][kTTChunk];
     __shared__ V stl[kTTWarps][kTTChunk];
@@ -656,6 +657,7 @@ __device__ __forceinline__ double tt_gather_atom(long long base, int tl, int nt,
 __global__ void k_unit_gather(Batch b, Config c, const int* unit_base, int split, const double* unit_i,
                               const double* unit_j, Work w)
 {
+    pdl_wait();
     const int lane = threadIdx.x & 31;
     const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (a >= b.natoms) return;
@@ -687,6 +689,7 @@ __global__ void __launch_bounds__(kTTThreads)
 k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, int nunits, int split, double* unit_i,
         double* unit_j, R* store, unsigned char* store_ok)
 {
+    pdl_wait();
     constexpr bool CHAIN = MODE == 1, STORE = MODE == 2;
     using V = typename T4<R>::type;
     __shared__ V sth[kTTWarps][kTTChunk];
@@ -884,6 +887,7 @@ __global__ void __launch_bounds__(kTTThreads)
 k_cn_chain_stored(Batch b, Config c, Partition p, Work w, const int2* units, int nunits, int split, const R* store,
                   const unsigned char* store_ok, double* unit_i, double* unit_j)
 {
+    pdl_wait();
     __shared__ double sjs[kTTWarps][3][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int item = blockIdx.x * kTTWarps + wid;
@@ -961,6 +965,7 @@ template <bool CHAIN>
 __global__ void k_cn_gather(Batch b, const int* unit_base, int split, const double* unit_i, const double* unit_j,
                             Work w)
 {
+    pdl_wait();
     const int lane = threadIdx.x & 31;
     const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (a >= b.natoms) return;
@@ -991,6 +996,7 @@ template <class R>
 __global__ void k_cn_weights(Batch b, Species s, Config c, const int* unit_base, int split, const double* unit_i,
                              const double* unit_j, Work w, R* UV)
 {
+    pdl_wait();
     const int lane = threadIdx.x & 31;
     const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (a >= b.natoms) return;
@@ -1069,7 +1075,7 @@ void launch_tt(const Batch& b, const Species& s, const Damp& d, const Config& c,
     const int blocks = (pu.nunits * pu.split + kTTWarps - 1) / kTTWarps;
     const bool smooth = c.width2 > 0.0 && c.width2 < c.cut2;
 #define D3_TT(SM, CO)                                                                                   \
-    k_two_body_tt<R, DAMP, GRAD, PG, SM, CO><<<blocks, kTTThreads, 0, stream>>>(                         \
+    launch_pdl(k_two_body_tt<R, DAMP, GRAD, PG, SM, CO>, dim3(blocks), dim3(kTTThreads), 0, stream, \
         b, s, d, c, p, w, pu.units, pu.nunits, pu.split, (const R*)pu.U, pu.unit_i, pu.unit_j)
     if (w.counts) {
         if (smooth) D3_TT(true, true);
@@ -1113,17 +1119,15 @@ void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Pa
     const int blocks = (pu.nunits * pu.split + kTTWarps - 1) / kTTWarps;
     const bool stored = pu.cn_store != nullptr;
 #define D3_CN(R, MODE)                                                                                     \
-    k_cn_tt<R, MODE><<<blocks, kTTThreads, 0, stream>>>(b, s, c, p, w, pu.units, pu.nunits, pu.split,     \
+    launch_pdl(k_cn_tt<R, MODE>, dim3(blocks), dim3(kTTThreads), 0, stream, b, s, c, p, w, pu.units, pu.nunits, pu.split,     \
                                                         pu.unit_i, pu.unit_j, (R*)pu.cn_store, pu.cn_store_ok)
     if (pu.nunits > 0) {
         if (chain && stored) {
             if (c.mixed)
-                k_cn_chain_stored<float><<<blocks, kTTThreads, 0, stream>>>(
-                    b, c, p, w, pu.units, pu.nunits, pu.split, (const float*)pu.cn_store, pu.cn_store_ok, pu.unit_i,
+                launch_pdl(k_cn_chain_stored<float>, dim3(blocks), dim3(kTTThreads), 0, stream, b, c, p, w, pu.units, pu.nunits, pu.split, (const float*)pu.cn_store, pu.cn_store_ok, pu.unit_i,
                     pu.unit_j);
             else
-                k_cn_chain_stored<double><<<blocks, kTTThreads, 0, stream>>>(
-                    b, c, p, w, pu.units, pu.nunits, pu.split, (const double*)pu.cn_store, pu.cn_store_ok, pu.unit_i,
+                launch_pdl(k_cn_chain_stored<double>, dim3(blocks), dim3(kTTThreads), 0, stream, b, c, p, w, pu.units, pu.nunits, pu.split, (const double*)pu.cn_store, pu.cn_store_ok, pu.unit_i,
                     pu.unit_j);
         } else if (chain) {
             if (c.mixed) D3_CN(float, 1);
@@ -1138,13 +1142,13 @@ void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Pa
     }
 #undef D3_CN
     const unsigned gb = (unsigned)((b.natoms + 7) / 8);
-    if (chain) k_cn_gather<true><<<gb, 256, 0, stream>>>(b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
-    else if (!weights) k_cn_gather<false><<<gb, 256, 0, stream>>>(b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
+    if (chain) launch_pdl(k_cn_gather<true>, dim3(gb), dim3(256), 0, stream, b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
+    else if (!weights) launch_pdl(k_cn_gather<false>, dim3(gb), dim3(256), 0, stream, b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
     else if (c.mixed)
-        k_cn_weights<float><<<gb, 256, 0, stream>>>(b, s, c, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w,
+        launch_pdl(k_cn_weights<float>, dim3(gb), dim3(256), 0, stream, b, s, c, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w,
                                                      (float*)uv);
     else
-        k_cn_weights<double><<<gb, 256, 0, stream>>>(b, s, c, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w,
+        launch_pdl(k_cn_weights<double>, dim3(gb), dim3(256), 0, stream, b, s, c, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w,
                                                       (double*)uv);
 }
 
@@ -1158,6 +1162,17 @@ size_t pair_unit_slot_doubles() { return (size_t)kSplitMax * kTile * (kUnitI + k
 size_t pair_unit_i_doubles() { return (size_t)kSplitMax * kTile * kUnitI; }
 size_t species_vector_doubles(int natoms, int nid) { return (size_t)natoms * nid * 2 * kRefPad; }
 
+void launch_species_vectors(const Batch& b, const Species& s, const Config& c, const Work& w, void* U,
+                            cudaStream_t stream)
+{
+    if (b.natoms <= 0) return;
+    const long long nsv = (long long)b.natoms * b.nid * kRefPad;
+    if (c.mixed)
+        launch_pdl(k_species_vectors<float>, dim3((unsigned)((nsv + 255) / 256)), dim3(256), 0, stream, b, s, w, (float*)U);
+    else
+        launch_pdl(k_species_vectors<double>, dim3((unsigned)((nsv + 255) / 256)), dim3(256), 0, stream, b, s, w, (double*)U);
+}
+
 void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, const Config& c, const Partition& p,
                            const Work& w, const PairUnits& pu, cudaStream_t stream, cudaEvent_t ev_begin,
                            cudaEvent_t ev_end, bool species_ready)
@@ -1167,9 +1182,9 @@ void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, cons
     if (species_ready) {
         // k_cn_weights wrote the species vectors
     } else if (c.mixed)
-        k_species_vectors<float><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (float*)pu.U);
+        launch_pdl(k_species_vectors<float>, dim3((unsigned)((nsv + 255) / 256)), dim3(256), 0, stream, b, s, w, (float*)pu.U);
     else
-        k_species_vectors<double><<<(unsigned)((nsv + 255) / 256), 256, 0, stream>>>(b, s, w, (double*)pu.U);
+        launch_pdl(k_species_vectors<double>, dim3((unsigned)((nsv + 255) / 256)), dim3(256), 0, stream, b, s, w, (double*)pu.U);
     if (ev_begin) cudaEventRecord(ev_begin, stream);
     if (pu.nunits > 0) {
         switch (d.kind) {
@@ -1200,7 +1215,7 @@ void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, cons
         }
     }
     if (ev_end) cudaEventRecord(ev_end, stream);
-    k_unit_gather<<<(b.natoms + 7) / 8, 256, 0, stream>>>(b, c, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
+    launch_pdl(k_unit_gather, dim3((b.natoms + 7) / 8), dim3(256), 0, stream, b, c, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
 }
 
 }  // namespace d3

@@ -86,7 +86,9 @@ def test_c_host_evaluates_validation_set(tmp_path, name):
         pytest.skip("gcc not found")
     case = _case(name)
     numbers = np.array(case["numbers"], dtype=np.int32)
-    xyz = np.array(case["positions"], dtype=float) * oracle_ref.AATOAU   # Angstrom -> Bohr
+    xyz = np.array(case["positions"], dtype=float)
+    if case["unit"] == "angstrom":
+        xyz = xyz * oracle_ref.AATOAU
     par = case["param"]
     src = tmp_path / "host.c"
     src.write_text(_program(numbers, xyz, par))

@@ -8,7 +8,9 @@ dispersion of one system with all work arrays taken from a fixed array inside
 the library.  These tests call that entry point through the C ABI, twice in a
 row (the calls share the array), and check its energy, gradient and virial
 against the regular entry point (dftd3_get_dispersion) at the parity
-tolerances of the other tests: 1e-12 for FP64, 1e-7 for the mixed form.  The
+tolerances of the other tests: 1e-12 for FP64; for the mixed form 1e-7
+relative energy, 1e-7 Hartree/Bohr gradient and 1e-6 of the largest virial
+component.  The
 largest input it accepts (4096 atoms, periodic) is also checked against the
 FP64 oracle, and inputs beyond the limits must be rejected with a message.
 The file is named so that pytest collects it last.
@@ -18,9 +20,11 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
+# FP64: energy 1e-12 relative, gradient and virial 1e-12 of their largest
+# component.  Mixed: energy 1e-7 relative, gradient 1e-7 Hartree/Bohr, virial
+# 1e-6 of its largest component (the tolerances of the other parity tests).
 RTOL = {"fp64": 1.0e-12, "mixed": 1.0e-7}
-# the mixed virial of periodic cells is held to 1e-6 of its largest component,
-# as in the work-split tests of the regular entry point
+GRAD_ABS_MIXED = 1.0e-7
 VIRIAL_RTOL = {"fp64": 1.0e-12, "mixed": 1.0e-6}
 RATIONAL = dict(s6=1.0, s8=0.7875, a1=0.4289, a2=4.4407, alp=14.0, s9=0.0)   # PBE-D3(BJ)
 ZERO = dict(s6=1.0, s8=0.722, rs6=1.217, rs8=1.0, alp=14.0, s9=0.0)           # PBE-D3(0)
@@ -84,7 +88,11 @@ def _check(res, ref, precision):
     assert np.isfinite(res["energy"])
     assert abs(res["energy"] - float(ref["energy"])) <= rtol * abs(float(ref["energy"])), (res["energy"], ref["energy"])
     if "gradient" in res:
-        assert _close(res["gradient"], ref["gradient"], rtol)
+        if precision == "fp64":
+            assert _close(res["gradient"], ref["gradient"], rtol)
+        else:
+            assert np.all(np.isfinite(res["gradient"]))
+            assert float(np.abs(res["gradient"] - ref["gradient"]).max()) <= GRAD_ABS_MIXED
     if "virial" in res:
         assert _close(res["virial"], ref["virial"], VIRIAL_RTOL[precision])
 
