@@ -144,6 +144,8 @@ struct Work {
     double* e_atom = nullptr;    // [natoms]
     double* grad = nullptr;      // [natoms][3]
     double* sig_atom = nullptr;  // [natoms][kSigma]
+    double* cn_sig = nullptr;    // [natoms][kSigma] sum of the CN chain rule's countd v^T over the atom's
+                                 // pairs (the stored-sum CN pass; virial = sum dE/dCN_i cn_sig_i)
     double* pg_atom = nullptr;   // [natoms][kParamGrad] or null
     unsigned long long* counts = nullptr;  // [3] pair, triple, cn terms or null
     // three-body results per root atom (summed by the per-system reduction)
@@ -230,6 +232,15 @@ void launch_gather_sorted(const double* pos, const int* perm, const int* sp_in, 
                           double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost, int* local, bool mixed,
                           cudaStream_t stream, const int* zid_in = nullptr, int* zid = nullptr);
 void launch_tile_bounds(const Batch& b, const int* tile_sys, int ntiles, double4* tiles, cudaStream_t stream);
+// The same column order, sorted atom arrays and tile bounds by one block per
+// system (three bitonic sorts in shared memory, one launch) for batches of at
+// least kOrderBlockMinSystems systems of at most kOrderBlockMax atoms.
+constexpr int kOrderBlockMax = 4096;
+constexpr int kOrderBlockMinSystems = 32;
+void launch_order_block(const double* pos, int nsys, int max_atoms, const int* atom_off, const int* tile_off,
+                        const int* sp_in, const uint8_t* ghost_in, const int* zid_in, bool mixed, int* perm,
+                        double* x, double* y, double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost,
+                        int* local, int* zid, double4* tiles, cudaStream_t stream);
 // Culled pair sweeps over sorted atoms and tiles (d3_pair.cu); used by the
 // launchers below when b.tiles is set and nid <= kMaxSpeciesFast.
 void launch_coordination_number_tiled(const Batch& b, const Species& s, const Config& c, const Partition& p,

@@ -509,6 +509,7 @@ void Engine::ensure_workspace(bool grad, bool param_grad, bool threebody)
         work_.e_atom = dev_alloc<double>(n);
         work_.grad = dev_alloc<double>(3 * n);
         work_.sig_atom = dev_alloc<double>(kSigma * n);
+        work_.cn_sig = dev_alloc<double>(kSigma * n);
         d_pos_in_ = dev_alloc<double>(3 * n);
         d_energies_ = dev_alloc<double>(nsys_);
         d_grad_out_ = dev_alloc<double>(3 * n);
@@ -536,8 +537,10 @@ void Engine::upload_pair_table(const Damp& d, cudaStream_t stream)
     for (int a = 0; a < nid; a++)
         for (int b = 0; b < nid; b++) {
             double* p = &t[kPairSlots * (a * nid + b)];
-            // rrij = 3 r4r2_i r4r2_j (rational.f90:458, zero.f90:475)
-            const double rrij = 3 * tab_.r4r2[a] * tab_.r4r2[b];
+            // rrij = 3 r4r2_i r4r2_j (rational.f90:458, zero.f90:475), the product
+            // formed first so that the (a, b) and (b, a) entries are equal and a
+            // pair's value does not depend on which atom comes first
+            const double rrij = 3 * (tab_.r4r2[a] * tab_.r4r2[b]);
             p[0] = rrij;
             switch (d.kind) {
             case kRational: {
@@ -618,6 +621,14 @@ void Engine::make_views(Batch& b, Species& s) const
 void Engine::order_atoms(const Damp& d, const double* d_positions, const Batch& b, bool mixed, cudaStream_t stream)
 {
     const int* zid_in = d.kind == kZDamping ? d_zid_ : nullptr;
+    // one block per system pays off for many systems; a few large ones are
+    // ordered faster by the rank passes, which spread each system over all SMs
+    if (!(tune_.morton_cell > 0.0) && max_sys_atoms_ <= kOrderBlockMax && nsys_ >= kOrderBlockMinSystems) {
+        launch_order_block(d_positions, nsys_, max_sys_atoms_, d_atom_off_, d_tile_off_, d_sp_, d_ghost_, zid_in,
+                           mixed, d_perm_, d_x_, d_y_, d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_,
+                           d_local_sorted_, d_zid_sorted_, d_tiles_, stream);
+        return;
+    }
     if (!(tune_.morton_cell > 0.0) && max_sys_atoms_ <= kRankOrderMax) {
         launch_rank_order(d_positions, natoms_, nsys_, max_sys_atoms_, d_sys_of_atom_, d_atom_off_, d_tile_off_,
                           d_shape_, d_keys_in_, d_keys_out_, d_sp_, d_ghost_, zid_in, mixed, d_perm_, d_x_, d_y_,

@@ -270,7 +270,7 @@ bool noalloc_dispersion(const Damp& damp, int natoms, const int* numbers, const 
     for (int a = 0; a < nid; a++)
         for (int b = 0; b < nid; b++) {
             double* p = &h.pair[kPairSlots * (a * nid + b)];
-            const double rrij = 3 * h.r4r2[a] * h.r4r2[b];
+            const double rrij = 3 * (h.r4r2[a] * h.r4r2[b]);   // symmetric in (a, b)
             p[0] = rrij;
             if (damp.kind == kRational) {
                 const double r0 = damp.a1 * std::sqrt(rrij) + damp.a2;

@@ -17,6 +17,7 @@
 // (get_atomic_c6, model.f90:432-461).
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 
@@ -604,6 +605,32 @@ __device__ __forceinline__ unsigned long long order_word(unsigned long long grou
 // Slabs and columns of every system from its bounding box, boxes of about
 // equal edge holding one tile each; one block of BLOCK threads per system,
 // which also writes the pass-0 words of its atoms.
+__device__ __forceinline__ int2 system_shape(const double lo[3], const double hi[3], int nt)
+{
+    int nx = 1, ny = 1;
+    if (nt > 1) {
+        const double lx = fmax(hi[0] - lo[0], 1.0), ly = fmax(hi[1] - lo[1], 1.0), lz = fmax(hi[2] - lo[2], 1.0);
+        const double edge = cbrt(lx * ly * lz / nt);
+        nx = (int)fmin(fmax(rint(lx / edge), 1.0), (double)kMaxColumns);
+        nx = min(nx, nt);
+        ny = (int)fmin(fmax(rint(ly / edge), 1.0), (double)kMaxColumns);
+        ny = max(1, min(ny, nt / nx));
+    }
+    return make_int2(nx, ny);
+}
+
+// Group of the next pass's word for the atom at position r of its system
+// after pass PASS (0: slab, 1: slab * ny + column).
+template <int PASS>
+__device__ __forceinline__ unsigned long long order_group(int r, int nt, int2 sh)
+{
+    const int t = r / kTile;
+    const int slab = part_of(t, nt, sh.x);
+    if (PASS == 0) return (unsigned long long)slab;
+    const int s0 = (int)((long long)slab * nt / sh.x), s1 = (int)((long long)(slab + 1) * nt / sh.x);
+    return (unsigned long long)(slab * sh.y + part_of(t - s0, s1 - s0, sh.y));
+}
+
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_rank_shape(const double* __restrict__ pos, const int* atom_off, const int* tile_off, int2* shape,
@@ -637,17 +664,7 @@ k_rank_shape(const double* __restrict__ pos, const int* atom_off, const int* til
             lo[c] = fmin(lo[c], red[c][w]);
             hi[c] = fmax(hi[c], red[3 + c][w]);
         }
-    const int nt = tile_off[sys + 1] - tile_off[sys];
-    int nx = 1, ny = 1;
-    if (nt > 1) {
-        const double lx = fmax(hi[0] - lo[0], 1.0), ly = fmax(hi[1] - lo[1], 1.0), lz = fmax(hi[2] - lo[2], 1.0);
-        const double edge = cbrt(lx * ly * lz / nt);
-        nx = (int)fmin(fmax(rint(lx / edge), 1.0), (double)kMaxColumns);
-        nx = min(nx, nt);
-        ny = (int)fmin(fmax(rint(ly / edge), 1.0), (double)kMaxColumns);
-        ny = max(1, min(ny, nt / nx));
-    }
-    shape[sys] = make_int2(nx, ny);
+    shape[sys] = system_shape(lo, hi, tile_off[sys + 1] - tile_off[sys]);
 }
 
 constexpr int kRankThreads = 256;        // threads of a rank-pass block
@@ -694,15 +711,7 @@ k_rank_pass(const double* __restrict__ pos, int n, const int* sys_of_atom, const
     if (!valid || lane != 0) return;
     const int li = a - a0;
     if constexpr (PASS < 2) {
-        const int nt = tile_off[sys + 1] - tile_off[sys];
-        const int2 sh = shape[sys];
-        const int t = r / kTile;
-        const int slab = part_of(t, nt, sh.x);
-        unsigned long long group = (unsigned long long)slab;
-        if (PASS == 1) {
-            const int s0 = (int)((long long)slab * nt / sh.x), s1 = (int)((long long)(slab + 1) * nt / sh.x);
-            group = (unsigned long long)(slab * sh.y + part_of(t - s0, s1 - s0, sh.y));
-        }
+        const unsigned long long group = order_group<PASS>(r, tile_off[sys + 1] - tile_off[sys], shape[sys]);
         next[a] = order_word(group, pos[3 * a + PASS + 1], li);
     } else {
         const int d = a0 + r;
@@ -743,7 +752,22 @@ __global__ void k_gather_sorted(const double* __restrict__ pos, const int* perm,
     if (zid_in) zid[a] = zid_in[o];
 }
 
-// Bounding sphere (centroid, largest distance) of each tile; one warp per tile.
+// Bounding sphere (centroid, largest distance) of the tile of sorted atoms
+// a0 .. a1 - 1, by one warp.
+__device__ __forceinline__ double4 tile_sphere(const double* bx, const double* by, const double* bz, int a0, int a1,
+                                               int lane)
+{
+    const int a = a0 + lane;
+    const bool valid = a < a1;
+    const double x = valid ? bx[a] : 0.0, y = valid ? by[a] : 0.0, z = valid ? bz[a] : 0.0;
+    const double inv = 1.0 / double(a1 - a0);
+    const double cx = warp_sum(x) * inv, cy = warp_sum(y) * inv, cz = warp_sum(z) * inv;
+    double r = valid ? sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy) + (z - cz) * (z - cz)) : 0.0;
+    for (int off = 16; off > 0; off >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, off));
+    return make_double4(cx, cy, cz, r * (1.0 + 1.0e-12) + 1.0e-12);
+}
+
+// Bounding sphere of each tile; one warp per tile.
 __global__ void k_tile_bounds(Batch b, const int* tile_sys, int ntiles, double4* tiles)
 {
     pdl_wait();
@@ -753,14 +777,117 @@ __global__ void k_tile_bounds(Batch b, const int* tile_sys, int ntiles, double4*
     const int sys = tile_sys[t];
     const int a0 = b.atom_off[sys] + kTile * (t - b.tile_off[sys]);
     const int a1 = min(a0 + kTile, b.atom_off[sys + 1]);
-    const int a = a0 + lane;
-    const bool valid = a < a1;
-    const double x = valid ? b.x[a] : 0.0, y = valid ? b.y[a] : 0.0, z = valid ? b.z[a] : 0.0;
-    const double inv = 1.0 / double(a1 - a0);
-    const double cx = warp_sum(x) * inv, cy = warp_sum(y) * inv, cz = warp_sum(z) * inv;
-    double r = valid ? sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy) + (z - cz) * (z - cz)) : 0.0;
-    for (int off = 16; off > 0; off >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, off));
-    if (lane == 0) tiles[t] = make_double4(cx, cy, cz, r * (1.0 + 1.0e-12) + 1.0e-12);
+    const double4 sph = tile_sphere(b.x, b.y, b.z, a0, a1, lane);
+    if (lane == 0) tiles[t] = sph;
+}
+
+// Ascending bitonic sort of the np (a power of two) words in shared memory by
+// the whole block; ends with a barrier.
+__device__ __forceinline__ void bitonic_block(unsigned long long* key, int np)
+{
+    const int half = np >> 1;
+    for (int k = 2; k <= np; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int t = threadIdx.x; t < half; t += blockDim.x) {
+                const int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+                const unsigned long long u = key[i], v = key[i + j];
+                if ((u > v) == ((i & k) == 0)) { key[i] = v; key[i + j] = u; }
+            }
+            __syncthreads();
+        }
+}
+
+// The column order of k_rank_shape / k_rank_pass and the tile spheres of
+// k_tile_bounds for systems of at most kOrderBlockMax atoms, one block per
+// system and one launch in place of five: the three passes sort the same
+// 64-bit words, which are distinct (the local index is their low bits), so a
+// sort gives each atom the position its rank does and the results are the
+// same bit for bit.  Shared memory: the words of the largest system, padded
+// to a power of two.
+__global__ void __launch_bounds__(1024)
+k_order_block(const double* __restrict__ pos, const int* atom_off, const int* tile_off, const int* sp_in,
+              const uint8_t* ghost_in, const int* zid_in, bool mixed, int* perm, double* x, double* y, double* z,
+              float4* xhi, float4* xlo, int* sp, uint8_t* ghost, int* local, int* zid, double4* tiles)
+{
+    pdl_wait();
+    extern __shared__ unsigned long long key[];
+    __shared__ double red[6][32];
+    __shared__ int2 s_shape;
+    const int sys = blockIdx.x;
+    const int a0 = atom_off[sys], n = atom_off[sys + 1] - a0;
+    const int tf = tile_off[sys], nt = tile_off[sys + 1] - tf;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
+    int np = 1;
+    while (np < n) np <<= 1;
+    // bounding box and the pass-0 words (x), the pad words above all others
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int k = tid; k < np; k += blockDim.x) {
+        if (k < n) {
+            for (int c = 0; c < 3; c++) {
+                const double v = pos[3 * (a0 + k) + c];
+                lo[c] = fmin(lo[c], v);
+                hi[c] = fmax(hi[c], v);
+            }
+            key[k] = order_word(0, pos[3 * (a0 + k)], k);
+        } else {
+            key[k] = ~0ull;
+        }
+    }
+    for (int c = 0; c < 3; c++)
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[c] = fmin(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+            hi[c] = fmax(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+        }
+    if (lane == 0)
+        for (int c = 0; c < 3; c++) { red[c][wid] = lo[c]; red[3 + c][wid] = hi[c]; }
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 1; w < nwarps; w++)
+            for (int c = 0; c < 3; c++) {
+                lo[c] = fmin(lo[c], red[c][w]);
+                hi[c] = fmax(hi[c], red[3 + c][w]);
+            }
+        s_shape = system_shape(lo, hi, nt);
+    }
+    bitonic_block(key, np);
+    const int2 sh = s_shape;
+    constexpr unsigned long long kLocal = (1ull << 20) - 1;
+    // pass 0 -> words of pass 1 (slab, y); pass 1 -> words of pass 2 (column, z)
+    for (int k = tid; k < n; k += blockDim.x) {
+        const int li = (int)(key[k] & kLocal);
+        key[k] = order_word(order_group<0>(k, nt, sh), pos[3 * (a0 + li) + 1], li);
+    }
+    __syncthreads();
+    bitonic_block(key, np);
+    for (int k = tid; k < n; k += blockDim.x) {
+        const int li = (int)(key[k] & kLocal);
+        key[k] = order_word(order_group<1>(k, nt, sh), pos[3 * (a0 + li) + 2], li);
+    }
+    __syncthreads();
+    bitonic_block(key, np);
+    // the sorted atom arrays (the writes of k_rank_pass<2>)
+    for (int k = tid; k < n; k += blockDim.x) {
+        const int li = (int)(key[k] & kLocal);
+        const int a = a0 + li, d = a0 + k;
+        const double px = pos[3 * a], py = pos[3 * a + 1], pz = pos[3 * a + 2];
+        perm[d] = a;
+        x[d] = px; y[d] = py; z[d] = pz;
+        if (mixed) {
+            const Sh32 s = split3(px, py, pz);
+            xhi[d] = s.hi;
+            xlo[d] = s.lo;
+        }
+        sp[d] = sp_in[a];
+        ghost[d] = ghost_in ? ghost_in[a] : 0;
+        local[d] = li;
+        if (zid_in) zid[d] = zid_in[a];
+    }
+    __syncthreads();
+    for (int t = wid; t < nt; t += nwarps) {
+        const int b0 = a0 + kTile * t;
+        const double4 sph = tile_sphere(x, y, z, b0, min(b0 + kTile, a0 + n), lane);
+        if (lane == 0) tiles[tf + t] = sph;
+    }
 }
 
 int blocks_for(int n, int warps) { return (n + warps - 1) / warps; }
@@ -812,6 +939,19 @@ void launch_rank_order(const double* pos, int natoms, int nsys, int max_atoms, c
     D3_RANK_PASS(2, word_a, word_b);
 #undef RANK_ARGS
 #undef D3_RANK_PASS
+}
+
+void launch_order_block(const double* pos, int nsys, int max_atoms, const int* atom_off, const int* tile_off,
+                        const int* sp_in, const uint8_t* ghost_in, const int* zid_in, bool mixed, int* perm,
+                        double* x, double* y, double* z, float4* xhi, float4* xlo, int* sp, uint8_t* ghost,
+                        int* local, int* zid, double4* tiles, cudaStream_t stream)
+{
+    if (nsys <= 0 || max_atoms <= 0) return;
+    int np = 1;
+    while (np < max_atoms) np <<= 1;
+    const int threads = std::min(1024, std::max(32, np / 2));
+    launch_pdl(k_order_block, dim3(nsys), dim3(threads), sizeof(unsigned long long) * np, stream, pos, atom_off,
+               tile_off, sp_in, ghost_in, zid_in, mixed, perm, x, y, z, xhi, xlo, sp, ghost, local, zid, tiles);
 }
 
 void launch_gather_sorted(const double* pos, const int* perm, const int* sp_in, const uint8_t* ghost_in,

@@ -30,7 +30,9 @@ constexpr int kTTThreads = 32 * kTTWarps;
 constexpr int kTTChunk = 128;     // translations tested per pass
 constexpr int kUnitI = 15;        // per-lane i sums: E, dE/dCN, g(3), sigma(6), dE/dparam(4)
 constexpr int kUnitJ = 4;         // per-lane j sums: dE/dCN, g(3)
-constexpr int kCnStore = 9;       // stored chain-rule sums per (i, j): countd (3), countd v^T (6)
+constexpr int kCnStore = 3;       // stored chain-rule sums per (i, j): countd (3)
+constexpr int kCnSigJ = 8;        // stored-sum CN pass: unit_i slots 8 .. 14 hold the j sums
+                                  // (cn, countd v^T (6)) of the column atoms
 constexpr int kSplitMax = 4;      // a unit is evaluated as 1, 2 (j-tile halves) or 4 items
                                   // (and translation halves); slots are sized for the largest split
 
@@ -618,12 +620,12 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
 // slot rows; the i slots of an atom are the items of the units (tl, jt <= tl),
 // consecutive, its j slots those of the units (it >= tl, tl).  The j total of
 // value m is added to i value JOFF + m; lanes 0 .. KI - 1 return the totals.
-template <int KI, int KJ, int JOFF>
+template <int KI, int KJ, int JOFF, int SJ = kUnitJ>
 __device__ __forceinline__ double tt_gather_atom(long long base, int tl, int nt, int sl, int split,
                                                  const double* unit_i, const double* unit_j, int lane)
 {
     constexpr int VI = KI <= 1 ? 1 : KI <= 2 ? 2 : KI <= 4 ? 4 : KI <= 8 ? 8 : 16;
-    constexpr int VJ = KJ <= 1 ? 1 : KJ <= 2 ? 2 : 4;
+    constexpr int VJ = KJ <= 1 ? 1 : KJ <= 2 ? 2 : KJ <= 4 ? 4 : 8;
     const int sh = split >> 1;   // log2 of the split (1, 2 or 4)
     double si = 0.0, sj = 0.0;
     if (lane % VI < KI) {
@@ -641,7 +643,7 @@ __device__ __forceinline__ double tt_gather_atom(long long base, int tl, int nt,
         for (int q = lane / VJ; q < nj; q += 32 / VJ) {
             const int it = tl + (q >> sh);
             const long long item = (base + (long long)it * (it + 1) / 2 + tl) * split + (q & (split - 1));
-            sj += unit_j[(item * kTile + sl) * kUnitJ + lane % VJ];
+            sj += unit_j[(item * kTile + sl) * SJ + lane % VJ];
         }
     }
 #pragma unroll
@@ -681,21 +683,29 @@ constexpr double kKcnTT = 16.0;   // ncoord.f90:31
 // lattice points.  Slots: CN: i [cn], j [cn]; chain: i [g(3), sigma(6)],
 // j [g(3)].
 // MODE 0: coordination numbers; 1: CN chain rule; 2: coordination numbers
-// and, per (i, j) of the item, the translation sums of the chain rule's
-// countd = dcf v / r and countd v^T (ncoord.f90:198-206) into `store`, for
-// k_cn_chain_stored (systems of one translation chunk only).
+// and, per (i, j) of the item, the translation sum of the chain rule's
+// countd = dcf v / r (ncoord.f90:198-206) into `store`, for
+// k_cn_chain_stored (systems of one translation chunk only), and per atom
+// the sum of countd v^T over all its pairs and translations.  The chain
+// rule's virial is sum over pairs of (dE/dCN_i + dE/dCN_j) countd v^T, and
+// countd v^T is the same seen from i and from j, so it equals
+// sum_i dE/dCN_i S_i with S_i = sum_(j, T) countd v^T (the j = i pairs of
+// the T != 0 images once): six values per atom instead of six per pair.
+// Slots of MODE 2: i [cn, S(6)], j in unit_i slots kCnSigJ .. [cn, S(6)].
 template <class R, int MODE>
-__global__ void __launch_bounds__(kTTThreads)
-k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, int nunits, int split, double* unit_i,
-        double* unit_j, R* store, unsigned char* store_ok)
+__device__ __forceinline__ void cn_tt(const Batch& b, const Species& s, const Config& c, const Partition& p,
+                                      const Work& w, const int2* units, int nunits, int split, double* unit_i,
+                                      double* unit_j, R* store, unsigned char* store_ok)
 {
     pdl_wait();
     constexpr bool CHAIN = MODE == 1, STORE = MODE == 2;
+    constexpr int NJ = STORE ? 7 : 3;
     using V = typename T4<R>::type;
     __shared__ V sth[kTTWarps][kTTChunk];
     __shared__ V stl[kTTWarps][kTTChunk];
-    // FP64 j sums of the partner lanes: CN [cn], chain rule [g(3)]
-    __shared__ double sjs[kTTWarps][3][32];
+    // FP64 j sums of the partner lanes: CN [cn], chain rule [g(3)], CN with
+    // stored sums [cn, S(6)]
+    __shared__ double sjs[kTTWarps][NJ][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int item = blockIdx.x * kTTWarps + wid;
     if (item >= nunits * split) return;
@@ -730,9 +740,10 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
     const double dcx = ci.x - cj.x, dcy = ci.y - cj.y, dcz = ci.z - cj.z;
     const R cut2 = R(c.cut_cn * c.cut_cn);
     double (*sj)[32] = sjs[wid];
-    for (int v = 0; v < 3; v++) sj[v][lane] = 0.0;
+    for (int v = 0; v < NJ; v++) sj[v][lane] = 0.0;
     __syncwarp();
     // i sums: CN: a0 = cn; chain: a1..a3 gradient, a4..a8 virial xx yy zz xy xz, a0 virial yz;
+    // stored sums: a1..a6 S xx yy zz xy xz yz (FP64 per partner);
     // partials in R over the partners of one translation chunk
     double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0, a7 = 0, a8 = 0;
     R t0_ = R(0), t1_ = R(0), t2_ = R(0), t3_ = R(0), t4_ = R(0), t5_ = R(0), t6_ = R(0), t7_ = R(0), t8_ = R(0);
@@ -836,11 +847,21 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
             }
             if (STORE) {
                 R* out = store + ((size_t)item * jslots + (jl - jl0)) * kCnStore * kTile + lane;
-                const R vals[kCnStore] = {scx, scy, scz, sxx, syy, szz, sxy, sxz, syz};
+                const R vals[kCnStore] = {scx, scy, scz};
 #pragma unroll
                 for (int v = 0; v < kCnStore; v++) out[v * kTile] = vals[v];
-            }
-            if (!CHAIN) {
+                t0_ += sc;
+                a1 += double(sxx); a2 += double(syy); a3 += double(szz);
+                a4 += double(sxy); a5 += double(sxz); a6 += double(syz);
+                // the column atom's cn and S (the j = i image pairs count once, on the row side)
+                const R z0 = wsum4_tt<R>(self ? R(0) : sc, self ? R(0) : sxx, self ? R(0) : syy,
+                                         self ? R(0) : szz, lane);
+                const R z1 = wsum4_tt<R>(self ? R(0) : sxy, self ? R(0) : sxz, self ? R(0) : syz, R(0), lane);
+                if ((lane & 7) == 0) {
+                    sj[lane >> 3][jl] += double(z0);
+                    if (lane < 24) sj[4 + (lane >> 3)][jl] += double(z1);
+                }
+            } else if (!CHAIN) {
                 t0_ += sc;
                 const R z = wsum_tt<R>(self ? R(0) : sc);
                 if (lane == 0) sj[0][jl] += double(z);
@@ -862,7 +883,12 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
     __syncwarp();
     double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
     double* oj = unit_j + ((size_t)item * kTile + lane) * kUnitJ;
-    if (!CHAIN) {
+    if (STORE) {
+        oi[0] = a0;
+        oi[1] = a1; oi[2] = a2; oi[3] = a3; oi[4] = a4; oi[5] = a5; oi[6] = a6;
+#pragma unroll
+        for (int v = 0; v < 7; v++) oi[kCnSigJ + v] = sj[v][lane];
+    } else if (!CHAIN) {
         oi[0] = a0;
         oj[0] = sj[0][lane];
     } else {
@@ -879,9 +905,27 @@ k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, in
     }
 }
 
-// CN chain rule from the sums k_cn_tt<R, 2> stored: per (i, j) of the item
-// the weight dE/dCN_i + dE/dCN_j (dE/dCN_i for j = i) times the stored
-// countd sums (ncoord.f90:205-213), into the same slots as k_cn_tt<R, 1>.
+template <class R, int MODE>
+__global__ void __launch_bounds__(kTTThreads)
+k_cn_tt(Batch b, Species s, Config c, Partition p, Work w, const int2* units, int nunits, int split, double* unit_i,
+        double* unit_j, R* store, unsigned char* store_ok)
+{
+    cn_tt<R, MODE>(b, s, c, p, w, units, nunits, split, unit_i, unit_j, store, store_ok);
+}
+
+// The FP64 stored-sum pass held to 128 registers: four blocks per SM instead
+// of three (a few bytes of spills; 142 registers unbounded).
+__global__ void __launch_bounds__(kTTThreads, 4)
+k_cn_tt_store64(Batch b, Species s, Config c, Partition p, Work w, const int2* units, int nunits, int split,
+                double* unit_i, double* unit_j, double* store, unsigned char* store_ok)
+{
+    cn_tt<double, 2>(b, s, c, p, w, units, nunits, split, unit_i, unit_j, store, store_ok);
+}
+
+// CN chain rule gradient from the sums k_cn_tt<R, 2> stored: per (i, j) of
+// the item the weight dE/dCN_i + dE/dCN_j times the stored countd sums
+// (ncoord.f90:205-209); slots i [g(3)], j [g(3)].  The virial follows per
+// atom from the S sums of the CN pass (k_cn_gather<true, true>).
 template <class R>
 __global__ void __launch_bounds__(kTTThreads)
 k_cn_chain_stored(Batch b, Config c, Partition p, Work w, const int2* units, int nunits, int split, const R* store,
@@ -910,13 +954,13 @@ k_cn_chain_stored(Batch b, Config c, Partition p, Work w, const int2* units, int
     double (*sj)[32] = sjs[wid];
     for (int v = 0; v < 3; v++) sj[v][lane] = 0.0;
     __syncwarp();
-    double g[3] = {0, 0, 0}, sg[6] = {0, 0, 0, 0, 0, 0};
+    double g[3] = {0, 0, 0};
     if (store_ok[item]) {
         const int jl0 = jh * jslots, jl1 = min(nj, jl0 + jslots);
         // the sums of NQ partners are loaded together (memory-level parallelism);
         // sums of a partner that no lane of the item took were not stored and
         // are loaded but not used
-        constexpr int NQ = sizeof(R) == 4 ? 4 : 2;
+        constexpr int NQ = sizeof(R) == 4 ? 8 : 4;
         for (int jg = jl0; jg < jl1; jg += NQ) {
             R sv[NQ][kCnStore];
 #pragma unroll
@@ -935,15 +979,12 @@ k_cn_chain_stored(Batch b, Config c, Partition p, Work w, const int2* units, int
                 if (valid && c.cn_partitioned && p.nparts > 1) valid = tt_owns(p, li, b.local[j]);
                 if (!__any_sync(0xffffffffu, valid)) continue;
                 const double dsum = dei + w.dEdcn[j];
-                const double dsig = self ? dei : dsum;
                 double j0 = 0.0, j1 = 0.0, j2 = 0.0;
                 if (!self) {
                     const double sx = double(sv[q][0]), sy = double(sv[q][1]), sz = double(sv[q][2]);
                     g[0] += sx * dsum; g[1] += sy * dsum; g[2] += sz * dsum;
                     j0 = -sx * dsum; j1 = -sy * dsum; j2 = -sz * dsum;
                 }
-#pragma unroll
-                for (int v = 0; v < 6; v++) sg[v] += double(sv[q][3 + v]) * dsig;
                 // lane 8v holds the warp sum of value v
                 const double z = wsum4_tt<double>(j0, j1, j2, 0.0, lane);
                 if ((lane & 7) == 0 && lane < 24) sj[lane >> 3][jl] += z;
@@ -953,15 +994,15 @@ k_cn_chain_stored(Batch b, Config c, Partition p, Work w, const int2* units, int
     __syncwarp();
     double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
     double* oj = unit_j + ((size_t)item * kTile + lane) * kUnitJ;
-    // g(3), sigma xx yy zz xy xz yz (the layout of k_cn_tt<R, 1>)
     oi[0] = g[0]; oi[1] = g[1]; oi[2] = g[2];
-    oi[3] = sg[0]; oi[4] = sg[1]; oi[5] = sg[2]; oi[6] = sg[3]; oi[7] = sg[4]; oi[8] = sg[5];
     oj[0] = sj[0][lane]; oj[1] = sj[1][lane]; oj[2] = sj[2][lane];
 }
 
 // Gather of the CN (assign) or chain-rule (add to gradient and virial) slots,
-// one warp per atom, in the fixed order of tt_gather_atom.
-template <bool CHAIN>
+// one warp per atom, in the fixed order of tt_gather_atom.  STORED: the slots
+// of the stored-sum passes, with the atom's S sums (CN) and its chain-rule
+// virial dE/dCN_i S_i (chain rule).
+template <bool CHAIN, bool STORED>
 __global__ void k_cn_gather(Batch b, const int* unit_base, int split, const double* unit_i, const double* unit_j,
                             Work w)
 {
@@ -973,9 +1014,18 @@ __global__ void k_cn_gather(Batch b, const int* unit_base, int split, const doub
     const int as = b.atom_off[sys];
     const int t0 = b.tile_off[sys], t1 = b.tile_off[sys + 1];
     const int tl = (a - as) / kTile, sl = (a - as) % kTile;
-    if (!CHAIN) {
+    if (!CHAIN && STORED) {
+        const double v = tt_gather_atom<7, 7, 0, kUnitI>(unit_base[sys], tl, t1 - t0, sl, split, unit_i,
+                                                         unit_i + kCnSigJ, lane);
+        if (lane == 0) w.cn[a] = v;
+        else if (lane < 7) w.cn_sig[kSigma * a + lane - 1] = v;
+    } else if (!CHAIN) {
         const double v = tt_gather_atom<1, 1, 0>(unit_base[sys], tl, t1 - t0, sl, split, unit_i, unit_j, lane);
         if (lane == 0) w.cn[a] = v;
+    } else if (STORED) {
+        const double v = tt_gather_atom<3, 3, 0>(unit_base[sys], tl, t1 - t0, sl, split, unit_i, unit_j, lane);
+        if (lane < 3) w.grad[3 * a + lane] += v;
+        else if (lane < 9) w.sig_atom[kSigma * a + lane - 3] += w.dEdcn[a] * w.cn_sig[kSigma * a + lane - 3];
     } else {
         // g(3), sigma(6); j slots g(3)
         const double v = tt_gather_atom<9, 3, 0>(unit_base[sys], tl, t1 - t0, sl, split, unit_i, unit_j, lane);
@@ -994,7 +1044,7 @@ constexpr double kWfTT = 4.0;   // model.f90:80
 // the two-body sweep (the entries of k_species_vectors).
 template <class R>
 __global__ void k_cn_weights(Batch b, Species s, Config c, const int* unit_base, int split, const double* unit_i,
-                             const double* unit_j, Work w, R* UV)
+                             const double* unit_j, Work w, R* UV, bool stored)
 {
     pdl_wait();
     const int lane = threadIdx.x & 31;
@@ -1004,8 +1054,17 @@ __global__ void k_cn_weights(Batch b, Species s, Config c, const int* unit_base,
     const int as = b.atom_off[sys];
     const int t0 = b.tile_off[sys], t1 = b.tile_off[sys + 1];
     const int tl = (a - as) / kTile, sl = (a - as) % kTile;
-    const double cn = __shfl_sync(
-        0xffffffffu, tt_gather_atom<1, 1, 0>(unit_base[sys], tl, t1 - t0, sl, split, unit_i, unit_j, lane), 0);
+    double cn;
+    if (stored) {
+        // the CN and the atom's S sums of the stored-sum pass
+        const double v = tt_gather_atom<7, 7, 0, kUnitI>(unit_base[sys], tl, t1 - t0, sl, split, unit_i,
+                                                         unit_i + kCnSigJ, lane);
+        if (lane >= 1 && lane < 7) w.cn_sig[kSigma * a + lane - 1] = v;
+        cn = __shfl_sync(0xffffffffu, v, 0);
+    } else {
+        cn = __shfl_sync(0xffffffffu,
+                         tt_gather_atom<1, 1, 0>(unit_base[sys], tl, t1 - t0, sl, split, unit_i, unit_j, lane), 0);
+    }
     if (lane == 0) w.cn[a] = cn;
     const int sp = b.sp[a];
     const int nref = s.nref[sp];
@@ -1134,7 +1193,9 @@ void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Pa
             else D3_CN(double, 1);
         } else if (stored) {
             if (c.mixed) D3_CN(float, 2);
-            else D3_CN(double, 2);
+            else
+                launch_pdl(k_cn_tt_store64, dim3(blocks), dim3(kTTThreads), 0, stream, b, s, c, p, w, pu.units,
+                           pu.nunits, pu.split, pu.unit_i, pu.unit_j, (double*)pu.cn_store, pu.cn_store_ok);
         } else {
             if (c.mixed) D3_CN(float, 0);
             else D3_CN(double, 0);
@@ -1142,14 +1203,21 @@ void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Pa
     }
 #undef D3_CN
     const unsigned gb = (unsigned)((b.natoms + 7) / 8);
-    if (chain) launch_pdl(k_cn_gather<true>, dim3(gb), dim3(256), 0, stream, b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
-    else if (!weights) launch_pdl(k_cn_gather<false>, dim3(gb), dim3(256), 0, stream, b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w);
-    else if (c.mixed)
+#define D3_GATHER(CH, ST) \
+    launch_pdl(k_cn_gather<CH, ST>, dim3(gb), dim3(256), 0, stream, b, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w)
+    if (chain) {
+        if (stored) D3_GATHER(true, true);
+        else D3_GATHER(true, false);
+    } else if (!weights) {
+        if (stored) D3_GATHER(false, true);
+        else D3_GATHER(false, false);
+    } else if (c.mixed)
         launch_pdl(k_cn_weights<float>, dim3(gb), dim3(256), 0, stream, b, s, c, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w,
-                                                     (float*)uv);
+                                                     (float*)uv, stored);
     else
         launch_pdl(k_cn_weights<double>, dim3(gb), dim3(256), 0, stream, b, s, c, pu.unit_base, pu.split, pu.unit_i, pu.unit_j, w,
-                                                      (double*)uv);
+                                                      (double*)uv, stored);
+#undef D3_GATHER
 }
 
 size_t cn_store_bytes(const PairUnits& pu, bool mixed)
