@@ -817,9 +817,11 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     }
     mark(1);
     // without a reducer the CN pass also writes the reference weights and the
-    // species vectors (one kernel after the sweep instead of three)
+    // species vectors (one kernel after the sweep instead of three); above
+    // kFusedWeightsMaxAtoms atoms the separate weight and species-vector
+    // kernels, with a thread per atom and per vector entry, are faster
     const bool two_body = two_body_active(d) || pg;
-    const bool fused = !reducer_ && !direct;
+    const bool fused = !reducer_ && !direct && natoms_ <= kFusedWeightsMaxAtoms;
     if (direct) launch_coordination_number(b, s, c, part_, w, stream);
     else launch_cn_units(b, s, c, part_, w, pcn, false, stream, fused, fused && two_body ? pu_.U : nullptr);
     if (reducer_) reduce(w.cn, natoms_, stream);

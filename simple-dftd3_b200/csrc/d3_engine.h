@@ -151,6 +151,7 @@ private:
     void make_views(Batch& b, Species& s) const;
     bool cn_single_chunk() const;
     static constexpr size_t kCnStoreCap = size_t(768) << 20;   // bytes of stored chain-rule sums at most
+    static constexpr int kFusedWeightsMaxAtoms = 65536;          // CN gather fused with weights and species vectors
     void* d_cn_store_ = nullptr;
     unsigned char* d_cn_store_ok_ = nullptr;
     size_t cn_store_cap_ = 0;
