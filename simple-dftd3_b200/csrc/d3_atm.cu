@@ -93,7 +93,12 @@ __global__ void k_c6_matrix(Batch b, Species s, Work w, const R* UV, double alp3
         g[ir] = ir < nr ? double(gw[ir]) : 0.0;
         dg[ir] = ir < nr ? double(dgw[ir]) : 0.0;
     }
-    for (int cl = lane; cl < n; cl += 32) {
+    // the lower triangle (c <= r) and its mirror: C6 is symmetric and the entry
+    // (c, r) swaps the two CN-derivative ratios (the damping radius table is
+    // symmetric), so every product is formed once
+    const int rl = r - a0;
+    C6Entry<R>* mat_sys = mat + mat_off[sys];
+    for (int cl = lane; cl <= rl; cl += 32) {
         const int c = a0 + cl;
         const int sc = b.sp[c];
         const R lr0 = table ? slr0[wid][sc] : lr0_of(sc);
@@ -129,6 +134,7 @@ __global__ void k_c6_matrix(Batch b, Species s, Work w, const R* UV, double alp3
             }
         }
         row[cl] = out;
+        if (cl < rl) mat_sys[(long long)cl * n + rl] = C6Entry<R>{out.sc6, out.qcr, out.qrc, out.lr0};
     }
 }
 
