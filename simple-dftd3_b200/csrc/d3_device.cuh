@@ -204,12 +204,16 @@ double measure_fma_peak(bool fp64);
 // Launchers (d3_kernels.cu); all asynchronous on `stream`.
 void launch_split_positions(const double* pos, int natoms, double* x, double* y, double* z,
                             float4* xhi, float4* xlo, bool mixed, cudaStream_t stream);
+// weights: the CN kernel goes on with the reference weights and, into uv
+// (natoms x nid x 2 x kRefPad of the form's type), the species vectors.
 void launch_coordination_number(const Batch& b, const Species& s, const Config& c,
-                                const Partition& p, const Work& w, cudaStream_t stream);
+                                const Partition& p, const Work& w, cudaStream_t stream, bool weights = false,
+                                void* uv = nullptr);
 void launch_weights(const Batch& b, const Species& s, const Config& c, const Work& w,
                     cudaStream_t stream);
 void launch_two_body(const Batch& b, const Species& s, const Damp& d, const Config& c,
-                     const Partition& p, const Work& w, cudaStream_t stream);
+                     const Partition& p, const Work& w, cudaStream_t stream,
+                     const void* uv = nullptr);
 // Spatial ordering and tile bounds (d3_pair.cu).
 size_t sort_temp_bytes(int natoms);
 void launch_spatial_sort(const double* pos, int natoms, const int* sys_of_atom, double cell,

@@ -511,9 +511,10 @@ void Engine::ensure_workspace(bool grad, bool param_grad, bool threebody)
         work_.sig_atom = dev_alloc<double>(kSigma * n);
         work_.cn_sig = dev_alloc<double>(kSigma * n);
         d_pos_in_ = dev_alloc<double>(3 * n);
-        d_energies_ = dev_alloc<double>(nsys_);
-        d_grad_out_ = dev_alloc<double>(3 * n);
-        d_sigma_ = dev_alloc<double>(9 * (size_t)nsys_);
+        // energies, gradient and virials side by side: one copy to the host
+        d_energies_ = dev_alloc<double>(nsys_ + 3 * n + 9 * (size_t)nsys_);
+        d_grad_out_ = d_energies_ + nsys_;
+        d_sigma_ = d_grad_out_ + 3 * n;
         ws_ready_ = true;
     }
     if (param_grad && !ws_pg_) {
@@ -808,9 +809,9 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     // warp (no ordering, tiles or slot gathers; fewer and shorter launches)
     const bool direct = direct_pairs(d, pg);
     if (direct) {
-        check(cudaMemcpyAsync(d_perm_, d_identity_, sizeof(int) * natoms_, cudaMemcpyDeviceToDevice, stream), "order");
-        launch_gather_sorted(d_positions, d_perm_, d_sp_, d_ghost_, d_sys_of_atom_, d_atom_off_, natoms_, d_x_, d_y_,
-                             d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed_, stream);
+        launch_gather_sorted(d_positions, d_identity_, d_sp_, d_ghost_, d_sys_of_atom_, d_atom_off_, natoms_, d_x_,
+                             d_y_, d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed_, stream);
+        b.perm = d_identity_;
         b.tiles = nullptr;
     } else {
         order_atoms(d, d_positions, b, mixed_, stream);
@@ -820,16 +821,17 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     // species vectors (one kernel after the sweep instead of three); above
     // kFusedWeightsMaxAtoms atoms the separate weight and species-vector
     // kernels, with a thread per atom and per vector entry, are faster
+    // (the direct path: the CN kernel itself, one warp per atom)
     const bool two_body = two_body_active(d) || pg;
-    const bool fused = !reducer_ && !direct && natoms_ <= kFusedWeightsMaxAtoms;
-    if (direct) launch_coordination_number(b, s, c, part_, w, stream);
+    const bool fused = !reducer_ && (direct || natoms_ <= kFusedWeightsMaxAtoms);
+    if (direct) launch_coordination_number(b, s, c, part_, w, stream, true, pu_.U);
     else launch_cn_units(b, s, c, part_, w, pcn, false, stream, fused, fused && two_body ? pu_.U : nullptr);
     if (reducer_) reduce(w.cn, natoms_, stream);
     mark(2);
     if (!fused) launch_weights(b, s, c, w, stream);
     mark(3);
     if (two_body && direct) {
-        launch_two_body(b, s, d, c, part_, w, stream);
+        launch_two_body(b, s, d, c, part_, w, stream, pu_.U);
     } else if (two_body) {
         launch_two_body_units(b, s, d, c, part_, w, pu_, stream, timed ? kev_[0] : nullptr, timed ? kev_[1] : nullptr,
                               fused);
@@ -842,7 +844,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
         }
     }
     mark(4);
-    species_ready_ = two_body && !direct;
+    species_ready_ = direct || two_body;
     if (threebody) {
         run_three_body(b, s, d, c, w, stream);
         if (pg) {
@@ -1293,11 +1295,9 @@ void Engine::evaluate_host(const Damp& d, const double* positions, double* energ
     check(cudaMemcpyAsync(d_pos_in_, hin, sizeof(double) * nin, cudaMemcpyHostToDevice, stream_), "positions");
     if (graph_on_) run_graphed(d, grad, false, stream_);
     else run(d, d_pos_in_, d_energies_, grad ? d_grad_out_ : nullptr, grad ? d_sigma_ : nullptr, nullptr, grad, stream_);
-    check(cudaMemcpyAsync(he, d_energies_, sizeof(double) * nsys_, cudaMemcpyDeviceToHost, stream_), "energies");
-    if (grad) {
-        check(cudaMemcpyAsync(hg, d_grad_out_, sizeof(double) * 3 * natoms_, cudaMemcpyDeviceToHost, stream_), "gradient");
-        check(cudaMemcpyAsync(hs, d_sigma_, sizeof(double) * 9 * nsys_, cudaMemcpyDeviceToHost, stream_), "sigma");
-    }
+    // the staging layout [energies | gradient | virials] is the device one
+    check(cudaMemcpyAsync(he, d_energies_, sizeof(double) * (grad ? nout : nsys_), cudaMemcpyDeviceToHost, stream_),
+          "results");
     check(cudaStreamSynchronize(stream_), "evaluate");
     std::memcpy(energies, he, sizeof(double) * nsys_);
     if (gradient) std::memcpy(gradient, hg, sizeof(double) * 3 * natoms_);

@@ -16,6 +16,7 @@
 #include <cstdint>
 
 #include "d3_device.cuh"
+#include "d3_weights.cuh"
 
 namespace d3 {
 
@@ -135,10 +136,12 @@ __global__ void k_split_positions(const double* __restrict__ pos, int n, double*
 // ----------------------------------------------------- coordination number --
 
 // CN_i = sum_{j,T} 1/(1 + exp(-kcn (rc/r - 1))) for 1e-12 <= r^2 <= cutoff^2
-// (get_partitioned_coordination_number, ncoord.f90:86-144).
-template <class R>
+// (get_partitioned_coordination_number, ncoord.f90:86-144).  W: the warp goes
+// on with the atom's reference weights and, into UV, its species vectors
+// (atom_weights), in place of separate weight and vector kernels.
+template <class R, bool W>
 __global__ void __launch_bounds__(kThreads) k_coordination_number(Batch b, Species s, Config c,
-                                                                  Partition p, Work w)
+                                                                  Partition p, Work w, R* UV)
 {
     pdl_wait();
     using Sh = typename ShiftOf<R>::type;
@@ -185,6 +188,7 @@ __global__ void __launch_bounds__(kThreads) k_coordination_number(Batch b, Speci
         for (int off = 16; off > 0; off >>= 1) nterm += __shfl_xor_sync(0xffffffffu, nterm, off);
         if (lane == 0) atomicAdd(w.counts + 2, nterm);
     }
+    if (W) atom_weights<R>(b, s, c, w, i, acc, lane, UV);
 }
 
 // ---------------------------------------------------------------- weights --
@@ -262,7 +266,7 @@ __device__ __forceinline__ void atomic_c6(const Species& s, int nid, int si, int
 // with energy, dE/dCN, gradient, virial and optional parameter derivatives.
 template <class R, int DAMP>
 __global__ void __launch_bounds__(kThreads) k_two_body(Batch b, Species s, Damp d, Config c,
-                                                       Partition p, Work w)
+                                                       Partition p, Work w, const R* UV)
 {
     pdl_wait();
     using Sh = typename ShiftOf<R>::type;
@@ -305,7 +309,17 @@ __global__ void __launch_bounds__(kThreads) k_two_body(Batch b, Species s, Damp 
             const int sj = b.sp[jj];
             const int nrj = s.nref[sj];
             R c6 = R(0), dc6i = R(0), dc6j = R(0);
-            if (valid && !gi && !(b.ghost && b.ghost[jj])) {
+            if (UV && valid && !gi) {
+                // from the species vectors of j for i's species (zero for a ghost j)
+                const R* u = UV + ((size_t)jj * nid + si) * (2 * kRefPad);
+#pragma unroll
+                for (int r = 0; r < kMaxRef; r++) {
+                    const R ur = __ldg(u + r), dur = __ldg(u + kRefPad + r);
+                    c6 += gwi[r] * ur;
+                    dc6i += dgwi[r] * ur;
+                    dc6j += gwi[r] * dur;
+                }
+            } else if (valid && !gi && !(b.ghost && b.ghost[jj])) {
                 R gwj[kMaxRef], dgwj[kMaxRef];
                 for (int r = 0; r < kMaxRef; r++) {
                     if constexpr (sizeof(R) == 8) { gwj[r] = w.gw[jj * kMaxRef + r]; dgwj[r] = w.dgw[jj * kMaxRef + r]; }
@@ -591,17 +605,21 @@ void launch_split_positions(const double* pos, int natoms, double* x, double* y,
 }
 
 void launch_coordination_number(const Batch& b, const Species& s, const Config& c,
-                                const Partition& p, const Work& w, cudaStream_t stream)
+                                const Partition& p, const Work& w, cudaStream_t stream, bool weights, void* uv)
 {
     if (b.natoms <= 0) return;
-    if (b.tiles && b.nid <= kMaxSpeciesFast) {
+    if (!weights && b.tiles && b.nid <= kMaxSpeciesFast) {
         launch_coordination_number_tiled(b, s, c, p, w, stream);
         return;
     }
-    if (c.mixed)
-        launch_pdl(k_coordination_number<float>, dim3(blocks_for_atoms(b.natoms)), dim3(kThreads), 0, stream, b, s, c, p, w);
-    else
-        launch_pdl(k_coordination_number<double>, dim3(blocks_for_atoms(b.natoms)), dim3(kThreads), 0, stream, b, s, c, p, w);
+    const dim3 grid(blocks_for_atoms(b.natoms)), block(kThreads);
+    if (c.mixed) {
+        if (weights) launch_pdl(k_coordination_number<float, true>, grid, block, 0, stream, b, s, c, p, w, (float*)uv);
+        else launch_pdl(k_coordination_number<float, false>, grid, block, 0, stream, b, s, c, p, w, (float*)nullptr);
+    } else {
+        if (weights) launch_pdl(k_coordination_number<double, true>, grid, block, 0, stream, b, s, c, p, w, (double*)uv);
+        else launch_pdl(k_coordination_number<double, false>, grid, block, 0, stream, b, s, c, p, w, (double*)nullptr);
+    }
 }
 
 void launch_weights(const Batch& b, const Species& s, const Config& c, const Work& w, cudaStream_t stream)
@@ -611,20 +629,22 @@ void launch_weights(const Batch& b, const Species& s, const Config& c, const Wor
 }
 
 void launch_two_body(const Batch& b, const Species& s, const Damp& d, const Config& c,
-                     const Partition& p, const Work& w, cudaStream_t stream)
+                     const Partition& p, const Work& w, cudaStream_t stream, const void* uv)
 {
     if (b.natoms <= 0) return;
-    if (b.tiles && b.nid <= kMaxSpeciesFast) {
+    if (!uv && b.tiles && b.nid <= kMaxSpeciesFast) {
         launch_two_body_tiled(b, s, d, c, p, w, stream);
         return;
     }
     const int nb = blocks_for_atoms(b.natoms);
+    const float* uf = (const float*)uv;
+    const double* ud = (const double*)uv;
     if (d.kind == kRational) {
-        if (c.mixed) launch_pdl(k_two_body<float, kRational>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w);
-        else launch_pdl(k_two_body<double, kRational>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w);
+        if (c.mixed) launch_pdl(k_two_body<float, kRational>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w, uf);
+        else launch_pdl(k_two_body<double, kRational>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w, ud);
     } else {
-        if (c.mixed) launch_pdl(k_two_body<float, kZero>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w);
-        else launch_pdl(k_two_body<double, kZero>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w);
+        if (c.mixed) launch_pdl(k_two_body<float, kZero>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w, uf);
+        else launch_pdl(k_two_body<double, kZero>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w, ud);
     }
 }
 

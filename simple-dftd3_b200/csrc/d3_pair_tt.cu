@@ -20,6 +20,7 @@
 #include <cstdint>
 
 #include "d3_device.cuh"
+#include "d3_weights.cuh"
 
 namespace d3 {
 
@@ -1034,7 +1035,6 @@ __global__ void k_cn_gather(Batch b, const int* unit_base, int split, const doub
     }
 }
 
-constexpr double kWfTT = 4.0;   // model.f90:80
 
 // After the CN sweep, one warp per atom: the CN from the unit slots, the
 // Gaussian reference weights and their CN derivative with the reference's
@@ -1066,65 +1066,7 @@ __global__ void k_cn_weights(Batch b, Species s, Config c, const int* unit_base,
                          tt_gather_atom<1, 1, 0>(unit_base[sys], tl, t1 - t0, sl, split, unit_i, unit_j, lane), 0);
     }
     if (lane == 0) w.cn[a] = cn;
-    const int sp = b.sp[a];
-    const int nref = s.nref[sp];
-    const double* cnref = s.refcn + sp * kMaxRef;
-    const double wf2 = 2 * kWfTT;
-    const double cr = lane < nref ? cnref[lane] : 0.0;
-    double g = 0.0;
-    if (lane < nref) {
-        const double d = cn - cr;
-        g = exp(-kWfTT * d * d);
-    }
-    double norm = 0.0, dnorm = 0.0, maxcn = cnref[0];
-    for (int r = 0; r < nref; r++) {
-        const double gr = __shfl_sync(0xffffffffu, g, r), crr = __shfl_sync(0xffffffffu, cr, r);
-        norm = norm + gr;
-        dnorm = dnorm + wf2 * (crr - cn) * gr;
-        maxcn = fmax(maxcn, crr);
-    }
-    norm = 1.0 / norm;
-    double gwk = 0.0, dgwk = 0.0;
-    if (lane < nref) {
-        const double expd = wf2 * (cr - cn) * g;
-        gwk = g * norm;
-        if (isnan(gwk) || isinf(gwk)) gwk = (maxcn == cr) ? 1.0 : 0.0;
-        dgwk = expd * norm - g * dnorm * (norm * norm);
-        if (isnan(dgwk) || isinf(dgwk)) dgwk = 0.0;
-    }
-    if (lane < kMaxRef) {
-        w.gw[a * kMaxRef + lane] = gwk;
-        w.dgw[a * kMaxRef + lane] = dgwk;
-        if (c.mixed) {
-            w.gwf[a * kMaxRef + lane] = float(gwk);
-            w.dgwf[a * kMaxRef + lane] = float(dgwk);
-        }
-    }
-    if (!UV) return;
-    double gq[kMaxRef], dq[kMaxRef];
-#pragma unroll
-    for (int q = 0; q < kMaxRef; q++) {
-        gq[q] = __shfl_sync(0xffffffffu, gwk, q);
-        dq[q] = __shfl_sync(0xffffffffu, dgwk, q);
-    }
-    const bool ghost = b.ghost && b.ghost[a];
-    const int nid = b.nid;
-    R* o = UV + (size_t)a * nid * (2 * kRefPad);
-    for (int e = lane; e < nid * kRefPad; e += 32) {
-        const int sx = e / kRefPad, r = e % kRefPad;
-        double u = 0.0, du = 0.0;
-        if (!ghost && r < s.nref[sx]) {
-            const double* ref = s.c6ref + ((size_t)(sx * nid + sp) * kMaxRef + r) * kMaxRef;
-#pragma unroll
-            for (int q = 0; q < kMaxRef; q++)
-                if (q < nref) {
-                    u += gq[q] * __ldg(ref + q);
-                    du += dq[q] * __ldg(ref + q);
-                }
-        }
-        o[sx * (2 * kRefPad) + r] = R(u);
-        o[sx * (2 * kRefPad) + kRefPad + r] = R(du);
-    }
+    atom_weights<R>(b, s, c, w, a, cn, lane, UV);
 }
 
 template <class R, int DAMP, bool GRAD, bool PG>
