@@ -204,11 +204,22 @@ double measure_fma_peak(bool fp64);
 // Launchers (d3_kernels.cu); all asynchronous on `stream`.
 void launch_split_positions(const double* pos, int natoms, double* x, double* y, double* z,
                             float4* xhi, float4* xlo, bool mixed, cudaStream_t stream);
-// weights: the CN kernel goes on with the reference weights and, into uv
-// (natoms x nid x 2 x kRefPad of the form's type), the species vectors.
+// Atoms in input order (small systems): the CN kernel reads the positions
+// from the input array, writes the batch's position arrays (x, y, z and, in
+// the mixed form, the FP32 head and tail) and goes on with the reference
+// weights and, into uv (natoms x nid x 2 x kRefPad of the form's type), the
+// species vectors.
+struct InputPositions {
+    const double* pos = nullptr;   // [natoms][3]
+    double* x = nullptr;
+    double* y = nullptr;
+    double* z = nullptr;
+    float4* xhi = nullptr;
+    float4* xlo = nullptr;
+};
 void launch_coordination_number(const Batch& b, const Species& s, const Config& c,
-                                const Partition& p, const Work& w, cudaStream_t stream, bool weights = false,
-                                void* uv = nullptr);
+                                const Partition& p, const Work& w, cudaStream_t stream,
+                                const InputPositions* in = nullptr, void* uv = nullptr);
 void launch_weights(const Batch& b, const Species& s, const Config& c, const Work& w,
                     cudaStream_t stream);
 void launch_two_body(const Batch& b, const Species& s, const Damp& d, const Config& c,
@@ -316,7 +327,8 @@ void launch_triples_mol(const Batch& b, const Species& s, const Damp& d, const C
                         const Work& w, const void* mat, const long long* mat_off, const int* mol_order, int nmol,
                         unsigned int* queue, int blocks, double* e3, double* sig3, cudaStream_t stream);
 void launch_cn_chain_rule(const Batch& b, const Species& s, const Config& c, const Partition& p,
-                          const Work& w, cudaStream_t stream);
+                          const Work& w, cudaStream_t stream,
+                          bool direct = false);
 void launch_reduce_systems(const Batch& b, const Config& c, const Work& w, double* energies,
                            double* sigma9, double* param_grad, double* grad_out,
                            cudaStream_t stream);

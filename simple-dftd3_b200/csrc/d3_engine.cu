@@ -809,8 +809,10 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     // warp (no ordering, tiles or slot gathers; fewer and shorter launches)
     const bool direct = direct_pairs(d, pg);
     if (direct) {
-        launch_gather_sorted(d_positions, d_identity_, d_sp_, d_ghost_, d_sys_of_atom_, d_atom_off_, natoms_, d_x_,
-                             d_y_, d_z_, d_xhi_, d_xlo_, d_sp_sorted_, d_ghost_sorted_, d_local_sorted_, mixed_, stream);
+        // the input arrays are the atom arrays; the CN kernel writes the positions
+        b.sp = d_sp_;
+        b.ghost = d_ghost_;
+        b.local = d_local_;
         b.perm = d_identity_;
         b.tiles = nullptr;
     } else {
@@ -824,7 +826,10 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     // (the direct path: the CN kernel itself, one warp per atom)
     const bool two_body = two_body_active(d) || pg;
     const bool fused = !reducer_ && (direct || natoms_ <= kFusedWeightsMaxAtoms);
-    if (direct) launch_coordination_number(b, s, c, part_, w, stream, true, pu_.U);
+    if (direct) {
+        const InputPositions in{d_positions, d_x_, d_y_, d_z_, d_xhi_, d_xlo_};
+        launch_coordination_number(b, s, c, part_, w, stream, &in, pu_.U);
+    }
     else launch_cn_units(b, s, c, part_, w, pcn, false, stream, fused, fused && two_body ? pu_.U : nullptr);
     if (reducer_) reduce(w.cn, natoms_, stream);
     mark(2);
@@ -865,7 +870,7 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     mark(5);
     if (grad) {
         if (reducer_) reduce(w.dEdcn, natoms_, stream);
-        if (direct) launch_cn_chain_rule(b, s, c, part_, w, stream);
+        if (direct) launch_cn_chain_rule(b, s, c, part_, w, stream, true);
         else launch_cn_units(b, s, c, part_, w, pcn, true, stream);
     }
     mark(6);

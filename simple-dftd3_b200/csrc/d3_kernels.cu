@@ -23,6 +23,7 @@ namespace d3 {
 namespace {
 
 constexpr int kWarpsPerBlock = 8;
+constexpr int kDirectWarps = 4;       // warps per atom of the small-system (input order) kernels
 constexpr int kThreads = 32 * kWarpsPerBlock;
 constexpr int kImgChunk = 128;        // images staged per warp and pass
 constexpr double kKcn = 16.0;         // ncoord.f90:31
@@ -133,26 +134,54 @@ __global__ void k_split_positions(const double* __restrict__ pos, int n, double*
     }
 }
 
+// Warps per atom of the warp-per-atom kernels: warp g of an atom takes its
+// partner blocks g, g + G, ...; the warps' sums meet in shared memory and the
+// atom's first warp adds them in warp order (a fixed order).  Returns whether
+// this warp holds the atom's totals in v (all lanes).
+template <int G, int NV>
+__device__ __forceinline__ bool combine_warps(double (&v)[NV], double (*part)[16], int wib, int lane, bool active)
+{
+    static_assert(NV <= 16, "values per atom");
+    if constexpr (G == 1) {
+        return active;
+    } else {
+        if (lane == 0)
+            for (int k = 0; k < NV; k++) part[wib][k] = v[k];
+        __syncthreads();
+        if (!active || wib % G != 0) return false;
+        for (int k = 0; k < NV; k++) {
+            double t = 0.0;
+            for (int q = 0; q < G; q++) t += part[wib + q][k];
+            v[k] = t;
+        }
+        return true;
+    }
+}
+
 // ----------------------------------------------------- coordination number --
 
 // CN_i = sum_{j,T} 1/(1 + exp(-kcn (rc/r - 1))) for 1e-12 <= r^2 <= cutoff^2
-// (get_partitioned_coordination_number, ncoord.f90:86-144).  W: the warp goes
-// on with the atom's reference weights and, into UV, its species vectors
-// (atom_weights), in place of separate weight and vector kernels.
-template <class R, bool W>
+// (get_partitioned_coordination_number, ncoord.f90:86-144).  W (atoms in
+// input order): the positions come from the input array and the warp writes
+// its atom's position arrays for the later kernels, then goes on with the
+// atom's reference weights and, into UV, its species vectors (atom_weights),
+// in place of separate gather, weight and vector kernels.
+template <class R, bool W, int G>
 __global__ void __launch_bounds__(kThreads) k_coordination_number(Batch b, Species s, Config c,
-                                                                  Partition p, Work w, R* UV)
+                                                                  Partition p, Work w, R* UV, InputPositions in)
 {
     pdl_wait();
     using Sh = typename ShiftOf<R>::type;
     __shared__ Sh sbuf[kWarpsPerBlock][kImgChunk];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int i = blockIdx.x * kWarpsPerBlock + wib;
-    if (i >= b.natoms) return;
+    __shared__ double part[kWarpsPerBlock][16];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, g = wib % G;
+    const int i0 = blockIdx.x * (kWarpsPerBlock / G) + wib / G;
+    const bool active = i0 < b.natoms;
+    const int i = active ? i0 : b.natoms - 1;
     const int sys = b.sys_of_atom[i];
     const int j0 = b.atom_off[sys], j1 = b.atom_off[sys + 1];
     const int t0 = b.img_off[kImgCN * (b.nsys + 1) + sys], t1 = b.img_off[kImgCN * (b.nsys + 1) + sys + 1];
-    const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
+    const double xi = W ? in.pos[3 * i] : b.x[i], yi = W ? in.pos[3 * i + 1] : b.y[i], zi = W ? in.pos[3 * i + 2] : b.z[i];
     const double rci = s.rcov[b.sp[i]];
     const int li = b.local[i];
     const R cut2 = R(c.cut_cn * c.cut_cn);
@@ -161,13 +190,22 @@ __global__ void __launch_bounds__(kThreads) k_coordination_number(Batch b, Speci
     for (int tc = t0; tc < t1; tc += kImgChunk) {
         const int nt = min(kImgChunk, t1 - tc);
         stage_images<R>(sbuf[wib], b.img, tc, nt, xi, yi, zi, lane);
-        for (int jb = j0; jb < j1; jb += 32) {
+        for (int jb = j0 + 32 * g; active && jb < j1; jb += 32 * G) {
             const int j = jb + lane;
             const bool valid = j < j1 && (!c.cn_partitioned || owns_pair(p, li, j - j0));
             const int jj = valid ? j : j0;
-            const double xj = b.x[jj], yj = b.y[jj], zj = b.z[jj];
+            double xj, yj, zj;
             float4 hj = make_float4(0, 0, 0, 0), lj = hj;
-            if constexpr (sizeof(R) == 4) { hj = b.xhi[jj]; lj = b.xlo[jj]; }
+            if constexpr (W) {
+                xj = in.pos[3 * jj]; yj = in.pos[3 * jj + 1]; zj = in.pos[3 * jj + 2];
+                if constexpr (sizeof(R) == 4) {
+                    const Shift32 sj = split_shift(xj, yj, zj);
+                    hj = sj.hi; lj = sj.lo;
+                }
+            } else {
+                xj = b.x[jj]; yj = b.y[jj]; zj = b.z[jj];
+                if constexpr (sizeof(R) == 4) { hj = b.xhi[jj]; lj = b.xlo[jj]; }
+            }
             const R rc = R(rci + s.rcov[b.sp[jj]]);
             for (int k = 0; k < nt; k++) {
                 R vx, vy, vz;
@@ -183,12 +221,25 @@ __global__ void __launch_bounds__(kThreads) k_coordination_number(Batch b, Speci
         __syncwarp();
     }
     acc = warp_sum(acc);
-    if (lane == 0) w.cn[i] = acc;
-    if (w.counts) {
+    if (w.counts && active) {
         for (int off = 16; off > 0; off >>= 1) nterm += __shfl_xor_sync(0xffffffffu, nterm, off);
         if (lane == 0) atomicAdd(w.counts + 2, nterm);
     }
-    if (W) atom_weights<R>(b, s, c, w, i, acc, lane, UV);
+    double v[1] = {acc};
+    if (!combine_warps<G, 1>(v, part, wib, lane, active)) return;
+    acc = v[0];
+    if (lane == 0) w.cn[i] = acc;
+    if (W) {
+        if (lane == 0) {
+            in.x[i] = xi; in.y[i] = yi; in.z[i] = zi;
+            if (c.mixed) {
+                const Shift32 si = split_shift(xi, yi, zi);
+                in.xhi[i] = si.hi;
+                in.xlo[i] = si.lo;
+            }
+        }
+        atom_weights<R>(b, s, c, w, i, acc, lane, UV);
+    }
 }
 
 // ---------------------------------------------------------------- weights --
@@ -264,16 +315,18 @@ __device__ __forceinline__ void atomic_c6(const Species& s, int nid, int si, int
 
 // Rational (rational.f90:378-514) and zero (zero.f90:409-553) damped pair sum
 // with energy, dE/dCN, gradient, virial and optional parameter derivatives.
-template <class R, int DAMP>
+template <class R, int DAMP, int G>
 __global__ void __launch_bounds__(kThreads) k_two_body(Batch b, Species s, Damp d, Config c,
                                                        Partition p, Work w, const R* UV)
 {
     pdl_wait();
     using Sh = typename ShiftOf<R>::type;
     __shared__ Sh sbuf[kWarpsPerBlock][kImgChunk];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int i = blockIdx.x * kWarpsPerBlock + wib;
-    if (i >= b.natoms) return;
+    __shared__ double part[kWarpsPerBlock][16];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, g = wib % G;
+    const int i0 = blockIdx.x * (kWarpsPerBlock / G) + wib / G;
+    const bool active = i0 < b.natoms;
+    const int i = active ? i0 : b.natoms - 1;
     const int sys = b.sys_of_atom[i];
     const int j0 = b.atom_off[sys], j1 = b.atom_off[sys + 1];
     const int t0 = b.img_off[kImgDisp2 * (b.nsys + 1) + sys];
@@ -299,7 +352,7 @@ __global__ void __launch_bounds__(kThreads) k_two_body(Batch b, Species s, Damp 
     for (int tc = t0; tc < t1; tc += kImgChunk) {
         const int nt = min(kImgChunk, t1 - tc);
         stage_images<R>(sbuf[wib], b.img, tc, nt, xi, yi, zi, lane);
-        for (int jb = j0; jb < j1; jb += 32) {
+        for (int jb = j0 + 32 * g; active && jb < j1; jb += 32 * G) {
             const int j = jb + lane;
             const bool valid = j < j1 && owns_pair(p, li, j - j0);
             const int jj = j < j1 ? j : j0;
@@ -400,12 +453,18 @@ __global__ void __launch_bounds__(kThreads) k_two_body(Batch b, Species s, Damp 
         }
         __syncwarp();
     }
-    e = warp_sum(e);
+    if (w.counts && active) {
+        for (int off = 16; off > 0; off >>= 1) nterm += __shfl_xor_sync(0xffffffffu, nterm, off);
+        if (lane == 0) atomicAdd(w.counts + 0, nterm);
+    }
+    double v[15] = {e, de, gx, gy, gz, sxx, syy, szz, sxy, sxz, syz, pg0, pg1, pg2, pg3};
+    for (int k = 0; k < 15; k++) v[k] = warp_sum(v[k]);
+    if (!combine_warps<G, 15>(v, part, wib, lane, active)) return;
+    e = v[0]; de = v[1]; gx = v[2]; gy = v[3]; gz = v[4];
+    sxx = v[5]; syy = v[6]; szz = v[7]; sxy = v[8]; sxz = v[9]; syz = v[10];
+    pg0 = v[11]; pg1 = v[12]; pg2 = v[13]; pg3 = v[14];
     if (lane == 0) w.e_atom[i] = e;
     if (c.grad) {
-        de = warp_sum(de); gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz);
-        sxx = warp_sum(sxx); syy = warp_sum(syy); szz = warp_sum(szz);
-        sxy = warp_sum(sxy); sxz = warp_sum(sxz); syz = warp_sum(syz);
         if (lane == 0) {
             w.dEdcn[i] = de;
             w.grad[3 * i + 0] = gx; w.grad[3 * i + 1] = gy; w.grad[3 * i + 2] = gz;
@@ -414,15 +473,10 @@ __global__ void __launch_bounds__(kThreads) k_two_body(Batch b, Species s, Damp 
         }
     }
     if (c.param_grad) {
-        pg0 = warp_sum(pg0); pg1 = warp_sum(pg1); pg2 = warp_sum(pg2); pg3 = warp_sum(pg3);
         if (lane == 0) {
             double* pg = w.pg_atom + kParamGrad * i;
             pg[0] = pg0; pg[1] = pg1; pg[2] = pg2; pg[3] = pg3;
         }
-    }
-    if (w.counts) {
-        for (int off = 16; off > 0; off >>= 1) nterm += __shfl_xor_sync(0xffffffffu, nterm, off);
-        if (lane == 0) atomicAdd(w.counts + 0, nterm);
     }
 }
 
@@ -430,15 +484,17 @@ __global__ void __launch_bounds__(kThreads) k_two_body(Batch b, Species s, Damp 
 
 // gradient += dE/dCN dCN/dR, sigma += dE/dCN dCN/deps
 // (add_coordination_number_derivs, ncoord.f90:152-228).
-template <class R>
+template <class R, int G>
 __global__ void __launch_bounds__(kThreads) k_cn_chain(Batch b, Species s, Config c, Partition p, Work w)
 {
     pdl_wait();
     using Sh = typename ShiftOf<R>::type;
     __shared__ Sh sbuf[kWarpsPerBlock][kImgChunk];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int i = blockIdx.x * kWarpsPerBlock + wib;
-    if (i >= b.natoms) return;
+    __shared__ double part[kWarpsPerBlock][16];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, g = wib % G;
+    const int i0 = blockIdx.x * (kWarpsPerBlock / G) + wib / G;
+    const bool active = i0 < b.natoms;
+    const int i = active ? i0 : b.natoms - 1;
     const int sys = b.sys_of_atom[i];
     const int j0 = b.atom_off[sys], j1 = b.atom_off[sys + 1];
     const int t0 = b.img_off[kImgCN * (b.nsys + 1) + sys], t1 = b.img_off[kImgCN * (b.nsys + 1) + sys + 1];
@@ -451,7 +507,7 @@ __global__ void __launch_bounds__(kThreads) k_cn_chain(Batch b, Species s, Confi
     for (int tc = t0; tc < t1; tc += kImgChunk) {
         const int nt = min(kImgChunk, t1 - tc);
         stage_images<R>(sbuf[wib], b.img, tc, nt, xi, yi, zi, lane);
-        for (int jb = j0; jb < j1; jb += 32) {
+        for (int jb = j0 + 32 * g; active && jb < j1; jb += 32 * G) {
             const int j = jb + lane;
             const bool valid = j < j1 && (!c.cn_partitioned || owns_pair(p, li, j - j0));
             const int jj = j < j1 ? j : j0;
@@ -481,9 +537,10 @@ __global__ void __launch_bounds__(kThreads) k_cn_chain(Batch b, Species s, Confi
         }
         __syncwarp();
     }
-    gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz);
-    sxx = warp_sum(sxx); syy = warp_sum(syy); szz = warp_sum(szz);
-    sxy = warp_sum(sxy); sxz = warp_sum(sxz); syz = warp_sum(syz);
+    double v[9] = {gx, gy, gz, sxx, syy, szz, sxy, sxz, syz};
+    for (int k = 0; k < 9; k++) v[k] = warp_sum(v[k]);
+    if (!combine_warps<G, 9>(v, part, wib, lane, active)) return;
+    gx = v[0]; gy = v[1]; gz = v[2]; sxx = v[3]; syy = v[4]; szz = v[5]; sxy = v[6]; sxz = v[7]; syz = v[8];
     if (lane == 0) {
         w.grad[3 * i + 0] += gx; w.grad[3 * i + 1] += gy; w.grad[3 * i + 2] += gz;
         double* sg = w.sig_atom + kSigma * i;
@@ -562,7 +619,11 @@ __global__ void __launch_bounds__(256) k_fma_peak(T* out, int iters)
     if (sum == T(-1)) out[blockIdx.x] = sum;  // never true; keeps the chains live
 }
 
-int blocks_for_atoms(int n) { return (n + kWarpsPerBlock - 1) / kWarpsPerBlock; }
+int blocks_for_atoms(int n, int warps_per_atom = 1)
+{
+    const int per_block = kWarpsPerBlock / warps_per_atom;
+    return (n + per_block - 1) / per_block;
+}
 
 }  // namespace
 
@@ -605,20 +666,31 @@ void launch_split_positions(const double* pos, int natoms, double* x, double* y,
 }
 
 void launch_coordination_number(const Batch& b, const Species& s, const Config& c,
-                                const Partition& p, const Work& w, cudaStream_t stream, bool weights, void* uv)
+                                const Partition& p, const Work& w, cudaStream_t stream, const InputPositions* in,
+                                void* uv)
 {
     if (b.natoms <= 0) return;
-    if (!weights && b.tiles && b.nid <= kMaxSpeciesFast) {
+    if (!in && b.tiles && b.nid <= kMaxSpeciesFast) {
         launch_coordination_number_tiled(b, s, c, p, w, stream);
         return;
     }
-    const dim3 grid(blocks_for_atoms(b.natoms)), block(kThreads);
+    // small systems in input order: kDirectWarps warps per atom
+    const dim3 grid(in ? blocks_for_atoms(b.natoms, kDirectWarps) : blocks_for_atoms(b.natoms)), block(kThreads);
+    const InputPositions none{};
     if (c.mixed) {
-        if (weights) launch_pdl(k_coordination_number<float, true>, grid, block, 0, stream, b, s, c, p, w, (float*)uv);
-        else launch_pdl(k_coordination_number<float, false>, grid, block, 0, stream, b, s, c, p, w, (float*)nullptr);
+        if (in)
+            launch_pdl(k_coordination_number<float, true, kDirectWarps>, grid, block, 0, stream, b, s, c, p, w,
+                       (float*)uv, *in);
+        else
+            launch_pdl(k_coordination_number<float, false, 1>, grid, block, 0, stream, b, s, c, p, w, (float*)nullptr,
+                       none);
     } else {
-        if (weights) launch_pdl(k_coordination_number<double, true>, grid, block, 0, stream, b, s, c, p, w, (double*)uv);
-        else launch_pdl(k_coordination_number<double, false>, grid, block, 0, stream, b, s, c, p, w, (double*)nullptr);
+        if (in)
+            launch_pdl(k_coordination_number<double, true, kDirectWarps>, grid, block, 0, stream, b, s, c, p, w,
+                       (double*)uv, *in);
+        else
+            launch_pdl(k_coordination_number<double, false, 1>, grid, block, 0, stream, b, s, c, p, w,
+                       (double*)nullptr, none);
     }
 }
 
@@ -636,30 +708,40 @@ void launch_two_body(const Batch& b, const Species& s, const Damp& d, const Conf
         launch_two_body_tiled(b, s, d, c, p, w, stream);
         return;
     }
-    const int nb = blocks_for_atoms(b.natoms);
     const float* uf = (const float*)uv;
     const double* ud = (const double*)uv;
+    // with the species vectors (small systems in input order): kDirectWarps warps per atom
+#define D3_TB(R, DAMP, G, U)                                                                                  \
+    launch_pdl(k_two_body<R, DAMP, G>, dim3(blocks_for_atoms(b.natoms, G)), dim3(kThreads), 0, stream, b, s, d, c, p, \
+               w, U)
     if (d.kind == kRational) {
-        if (c.mixed) launch_pdl(k_two_body<float, kRational>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w, uf);
-        else launch_pdl(k_two_body<double, kRational>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w, ud);
+        if (c.mixed) { if (uv) D3_TB(float, kRational, kDirectWarps, uf); else D3_TB(float, kRational, 1, uf); }
+        else { if (uv) D3_TB(double, kRational, kDirectWarps, ud); else D3_TB(double, kRational, 1, ud); }
     } else {
-        if (c.mixed) launch_pdl(k_two_body<float, kZero>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w, uf);
-        else launch_pdl(k_two_body<double, kZero>, dim3(nb), dim3(kThreads), 0, stream, b, s, d, c, p, w, ud);
+        if (c.mixed) { if (uv) D3_TB(float, kZero, kDirectWarps, uf); else D3_TB(float, kZero, 1, uf); }
+        else { if (uv) D3_TB(double, kZero, kDirectWarps, ud); else D3_TB(double, kZero, 1, ud); }
     }
+#undef D3_TB
 }
 
 void launch_cn_chain_rule(const Batch& b, const Species& s, const Config& c, const Partition& p,
-                          const Work& w, cudaStream_t stream)
+                          const Work& w, cudaStream_t stream, bool direct)
 {
     if (b.natoms <= 0) return;
-    if (b.tiles && b.nid <= kMaxSpeciesFast) {
+    if (!direct && b.tiles && b.nid <= kMaxSpeciesFast) {
         launch_cn_chain_rule_tiled(b, s, c, p, w, stream);
         return;
     }
-    if (c.mixed)
-        launch_pdl(k_cn_chain<float>, dim3(blocks_for_atoms(b.natoms)), dim3(kThreads), 0, stream, b, s, c, p, w);
-    else
-        launch_pdl(k_cn_chain<double>, dim3(blocks_for_atoms(b.natoms)), dim3(kThreads), 0, stream, b, s, c, p, w);
+    const dim3 block(kThreads);
+    if (direct) {
+        const dim3 grid(blocks_for_atoms(b.natoms, kDirectWarps));
+        if (c.mixed) launch_pdl(k_cn_chain<float, kDirectWarps>, grid, block, 0, stream, b, s, c, p, w);
+        else launch_pdl(k_cn_chain<double, kDirectWarps>, grid, block, 0, stream, b, s, c, p, w);
+    } else {
+        const dim3 grid(blocks_for_atoms(b.natoms));
+        if (c.mixed) launch_pdl(k_cn_chain<float, 1>, grid, block, 0, stream, b, s, c, p, w);
+        else launch_pdl(k_cn_chain<double, 1>, grid, block, 0, stream, b, s, c, p, w);
+    }
 }
 
 void launch_reduce_systems(const Batch& b, const Config& c, const Work& w, double* energies,
