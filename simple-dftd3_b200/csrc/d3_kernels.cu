@@ -115,6 +115,8 @@ __device__ __forceinline__ R rexp(R x) { if constexpr (sizeof(R) == 8) return ex
 template <class R>
 __device__ __forceinline__ R rsqrt_(R x) { if constexpr (sizeof(R) == 8) return sqrt(x); else return sqrtf(x); }
 template <class R>
+__device__ __forceinline__ R rinv_sqrt(R x) { if constexpr (sizeof(R) == 8) return rsqrt(x); else return rsqrtf(x); }
+template <class R>
 __device__ __forceinline__ R rpow(R x, R a) { if constexpr (sizeof(R) == 8) return pow(x, a); else return powf(x, a); }
 
 // ------------------------------------------------------------ positions ----
@@ -212,8 +214,7 @@ __global__ void __launch_bounds__(kThreads) k_coordination_number(Batch b, Speci
                 displacement(sbuf[wib][k], xj, yj, zj, hj, lj, vx, vy, vz);
                 const R r2 = vx * vx + vy * vy + vz * vz;
                 if (!valid || r2 > cut2 || r2 < R(1.0e-12)) continue;
-                const R r1 = rsqrt_(r2);
-                const R cf = R(1) / (R(1) + rexp(-R(kKcn) * (rc / r1 - R(1))));
+                const R cf = R(1) / (R(1) + rexp(-R(kKcn) * (rc * rinv_sqrt(r2) - R(1))));
                 acc += double(cf);
                 nterm += (jj <= i);
             }
@@ -396,8 +397,11 @@ __global__ void __launch_bounds__(kThreads) k_two_body(Batch b, Species s, Damp 
                 if constexpr (DAMP == kRational) {
                     // q1 = R0^6, q2 = R0^8, q3 = R0 = a1 sqrt(rrij) + a2, q4 = sqrt(rrij)
                     const R r4 = r2 * r2;
-                    const R t6 = R(1) / (r4 * r2 + q1);
-                    const R t8 = R(1) / (r4 * r4 + q2);
+                    // one reciprocal for both denominators
+                    const R a6 = r4 * r2 + q1, a8 = r4 * r4 + q2;
+                    const R inv = R(1) / (a6 * a8);
+                    const R t6 = a8 * inv;
+                    const R t8 = a6 * inv;
                     const R d6 = R(-6) * r4 * t6 * t6;
                     const R d8 = R(-8) * r4 * r2 * t8 * t8;
                     e6 = t6; e8 = rrij * t8;
@@ -523,11 +527,11 @@ __global__ void __launch_bounds__(kThreads) k_cn_chain(Batch b, Species s, Confi
                 displacement(sbuf[wib][k], xj, yj, zj, hj, lj, vx, vy, vz);
                 const R r2 = vx * vx + vy * vy + vz * vz;
                 if (!valid || r2 > cut2 || r2 < R(1.0e-12)) continue;
-                const R r1 = rsqrt_(r2);
-                const R expterm = rexp(-R(kKcn) * (rc / r1 - R(1)));
+                const R ir = rinv_sqrt(r2);
+                const R expterm = rexp(-R(kKcn) * (rc * ir - R(1)));
                 const R cf = R(1) / (R(1) + expterm);
-                const R dcf = -cf * (R(1) - cf) * R(kKcn) * rc / r2;
-                const R f = dcf / r1 * dsum;
+                // dcf / r with dcf = -cf (1 - cf) kcn rc / r^2 (ncoord.f90:198-201)
+                const R f = -cf * (R(1) - cf) * R(kKcn) * rc * (ir * ir * ir) * dsum;
                 const R cx = f * vx, cy = f * vy, cz = f * vz;
                 if (jj != i) { gx += double(cx); gy += double(cy); gz += double(cz); }
                 sxx += double(R(0.5) * cx * vx); syy += double(R(0.5) * cy * vy);
