@@ -364,14 +364,27 @@ __global__ void __launch_bounds__(kThreads) k_two_body(Batch b, Species s, Damp 
             const int nrj = s.nref[sj];
             R c6 = R(0), dc6i = R(0), dc6j = R(0);
             if (UV && valid && !gi) {
-                // from the species vectors of j for i's species (zero for a ghost j)
-                const R* u = UV + ((size_t)jj * nid + si) * (2 * kRefPad);
+                // from the species vectors of j for i's species (zero for a ghost j), vector loads
+                R u[2 * kRefPad];
+                const R* up = UV + ((size_t)jj * nid + si) * (2 * kRefPad);
+                if constexpr (sizeof(R) == 4) {
+#pragma unroll
+                    for (int q = 0; q < kRefPad / 2; q++) {
+                        const float4 v4 = __ldg(reinterpret_cast<const float4*>(up) + q);
+                        u[4 * q] = v4.x; u[4 * q + 1] = v4.y; u[4 * q + 2] = v4.z; u[4 * q + 3] = v4.w;
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < kRefPad; q++) {
+                        const double2 v2 = __ldg(reinterpret_cast<const double2*>(up) + q);
+                        u[2 * q] = v2.x; u[2 * q + 1] = v2.y;
+                    }
+                }
 #pragma unroll
                 for (int r = 0; r < kMaxRef; r++) {
-                    const R ur = __ldg(u + r), dur = __ldg(u + kRefPad + r);
-                    c6 += gwi[r] * ur;
-                    dc6i += dgwi[r] * ur;
-                    dc6j += gwi[r] * dur;
+                    c6 += gwi[r] * u[r];
+                    dc6i += dgwi[r] * u[r];
+                    dc6j += gwi[r] * u[kRefPad + r];
                 }
             } else if (valid && !gi && !(b.ghost && b.ghost[jj])) {
                 R gwj[kMaxRef], dgwj[kMaxRef];
@@ -381,10 +394,11 @@ __global__ void __launch_bounds__(kThreads) k_two_body(Batch b, Species s, Damp 
                 }
                 atomic_c6<R>(s, nid, si, sj, nri, nrj, gwi, dgwi, gwj, dgwj, c6, dc6i, dc6j);
             }
-            const double* pr = s.pair + kPairSlots * (si * nid + sj);
-            const R rrij = R(__ldg(pr + 0));
-            const R q1 = R(__ldg(pr + 1)), q2 = R(__ldg(pr + 2)), q3 = R(__ldg(pr + 3));
-            const R q4 = R(__ldg(pr + 4));
+            const double2* pr = reinterpret_cast<const double2*>(s.pair + kPairSlots * (si * nid + sj));
+            const double2 p01 = __ldg(pr), p23 = __ldg(pr + 1), p45 = __ldg(pr + 2);
+            const R rrij = R(p01.x);
+            const R q1 = R(p01.y), q2 = R(p23.x), q3 = R(p23.y);
+            const R q4 = R(p45.x);
             for (int k = 0; k < nt; k++) {
                 R vx, vy, vz;
                 displacement(sbuf[wib][k], xj, yj, zj, hj, lj, vx, vy, vz);
