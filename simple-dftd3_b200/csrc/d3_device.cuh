@@ -88,13 +88,15 @@ struct PairUnits {
     int nunits = 0;
     const int* unit_base = nullptr;      // [nsys]
     int split = 4;                       // items per unit: 1, 2 (j-tile halves), 4 (and translation halves)
+    bool single_image = false;           // every system has the lattice point T = 0 only (molecules) and
+                                         // the two-body sum takes the diagonal walk (k_two_body_rot)
     void* U = nullptr;                   // [natoms][nid][16] species vectors U (7 + pad) and dU (7 + pad) (R)
     double* unit_i = nullptr;            // [nunits][kTile][15]
     double* unit_j = nullptr;            // [nunits][kTile][4]
     // chain-rule sums of the CN pass per (item, j, lane), or null: the CN
     // pass stores them and the chain rule reads them instead of evaluating
     // the terms again (systems of one translation chunk, cn_store_bytes)
-    void* cn_store = nullptr;            // [items][kTile / splitJ][9][kTile] (R)
+    void* cn_store = nullptr;            // [items][kTile / splitJ][3][kTile] (R)
     unsigned char* cn_store_ok = nullptr;   // [items]: the item stored its sums
 };
 

@@ -767,6 +767,9 @@ void Engine::run(const Damp& d, const double* d_positions, double* d_energies, d
     c.grad = grad; c.mixed = mixed_; c.param_grad = pg; c.cn_partitioned = cn_partitioned_;
     // the CN sweeps and the two-body sweep split the tile pairs each their own way
     pu_.split = pair_split();
+    // molecules: the two-body diagonal walk (FP64 only for systems of at most
+    // 256 atoms, where few tile pairs lie beyond the cutoff)
+    pu_.single_image = !any_periodic_ && (mixed_ || max_sys_atoms_ <= 256);
     PairUnits pcn = pu_;
     pcn.split = cn_split();
     // the CN pass keeps the chain rule's per-pair sums when every system's CN

@@ -614,6 +614,194 @@ k_two_body_tt(Batch b, Species s, Damp d, Config c, Partition p, Work w, const i
     }
 }
 
+// Two-body tile pairs of systems with the single lattice point T = 0
+// (molecules), rational or zero damping with energy, dE/dCN, gradient and
+// virial: one item per tile pair and no translation lists.  A warp walks the
+// 32 x 32 (i, j) pairs along the diagonals: at step t lane l pairs atom
+// ia0 + l with partner ja0 + (l + t) mod 32; the partner's dE/dCN and
+// gradient sums move one lane down per step with the partner (four
+// shuffles), so every lane ends the item holding one partner's sums.  The
+// diagonal tile takes steps 1..16 (each unordered pair once; the i side takes
+// the pair's energy and virial).  The slots are those of k_two_body_tt with
+// one item per unit, so k_unit_gather adds them unchanged.  Compared with the
+// general kernel, which runs each partner's translation list (one entry here),
+// a step does one term without the per-partner reach mask and warp sums.
+template <class R, int DAMP>
+__global__ void __launch_bounds__(kTTThreads, sizeof(R) == 4 ? 4 : 3)
+k_two_body_rot(Batch b, Species s, Damp d, Config c, Work w, const int2* units, int nunits, const R* UV,
+               double* unit_i, double* unit_j)
+{
+    pdl_wait();
+    using V = typename T4<R>::type;
+    // per warp: the partner tile's positions (head, tail) and species
+    __shared__ V sph[kTTWarps][kTile];
+    __shared__ V spl[kTTWarps][kTile];
+    __shared__ int ssp[kTTWarps][kTile];
+    // pair constants per species pair: rrij, q1, q2, q3 (rational: R0^6, R0^8, R0;
+    // zero: rs6 R0, rs8 R0, R0)
+    __shared__ V spc[kMaxSpeciesFast * kMaxSpeciesFast];
+    const int nid = b.nid;
+    for (int k = threadIdx.x; k < nid * nid; k += kTTThreads) {
+        const double* pr = s.pair + kPairSlots * k;
+        if constexpr (sizeof(R) == 8) spc[k] = make_double4(pr[0], pr[1], pr[2], pr[3]);
+        else spc[k] = make_float4(float(pr[0]), float(pr[1]), float(pr[2]), float(pr[3]));
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int item = blockIdx.x * kTTWarps + wid;
+    if (item >= nunits) return;
+    const int it = units[item].x, jt = units[item].y;
+    const int sys = b.tile_sys[it];
+    const int t0 = b.tile_off[sys];
+    const int as = b.atom_off[sys], ae = b.atom_off[sys + 1];
+    const int ia0 = as + kTile * (it - t0), ja0 = as + kTile * (jt - t0);
+    const int ni = min(kTile, ae - ia0), nj = min(kTile, ae - ja0);
+    const bool diag = it == jt;
+    double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
+    {
+        // tile spheres farther apart than the cutoff: no pair, zero slots
+        const double4 ci = b.tiles[it], cj = b.tiles[jt];
+        const double dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
+        const double lim = c.cut2 + ci.w + cj.w + 1.0e-6 * c.cut2 + 1.0e-6;
+        if (dx * dx + dy * dy + dz * dz > lim * lim) {
+#pragma unroll
+            for (int v = 0; v < kUnitI; v++) oi[v] = 0.0;
+            double* oj = unit_j + ((size_t)item * kTile + lane) * kUnitJ;
+#pragma unroll
+            for (int v = 0; v < kUnitJ; v++) oj[v] = 0.0;
+            return;
+        }
+    }
+    const bool ivalid = lane < ni;
+    const int ic = ivalid ? ia0 + lane : ia0;
+    const int si = b.sp[ic];
+    const bool gi = b.ghost && b.ghost[ic];
+    const double xi = b.x[ic], yi = b.y[ic], zi = b.z[ic];
+    R hix, hiy, hiz, lix = R(0), liy = R(0), liz = R(0);
+    if constexpr (sizeof(R) == 8) { hix = xi; hiy = yi; hiz = zi; }
+    else {
+        hix = __double2float_rn(xi); lix = __double2float_rn(xi - (double)hix);
+        hiy = __double2float_rn(yi); liy = __double2float_rn(yi - (double)hiy);
+        hiz = __double2float_rn(zi); liz = __double2float_rn(zi - (double)hiz);
+    }
+    // the lane's reference weights
+    R gwi[kMaxRef], dgwi[kMaxRef];
+#pragma unroll
+    for (int r = 0; r < kMaxRef; r++) {
+        if constexpr (sizeof(R) == 8) { gwi[r] = w.gw[ic * kMaxRef + r]; dgwi[r] = w.dgw[ic * kMaxRef + r]; }
+        else { gwi[r] = w.gwf[ic * kMaxRef + r]; dgwi[r] = w.dgwf[ic * kMaxRef + r]; }
+    }
+    // the partner tile: a partner outside the system (or a ghost) gets species -1
+    {
+        const bool jv = lane < nj;
+        const int jc = jv ? ja0 + lane : ja0;
+        if constexpr (sizeof(R) == 8) {
+            sph[wid][lane] = make_double4(b.x[jc], b.y[jc], b.z[jc], 0.0);
+        } else {
+            sph[wid][lane] = b.xhi[jc];
+            spl[wid][lane] = b.xlo[jc];
+        }
+        ssp[wid][lane] = (jv && !(b.ghost && b.ghost[jc])) ? b.sp[jc] : -1;
+    }
+    __syncwarp();
+    const R cut2 = R(c.cut2 * c.cut2);
+    const R s6 = R(d.s6), s8 = R(d.s8);
+    const R alp6 = R(d.alp), alp8 = R(d.alp + 2.0);
+    const bool iok = ivalid && !gi;
+    const bool half = diag && lane >= 16;
+    const int st0 = diag ? 1 : 0, st1 = diag ? 16 : 31;
+    // i sums of the lane (FP32 partials in the mixed form), j sums travelling with the partner
+    R te = R(0), tde = R(0), tgx = R(0), tgy = R(0), tgz = R(0);
+    R txx = R(0), tyy = R(0), tzz = R(0), txy = R(0), txz = R(0), tyz = R(0);
+    R jde = R(0), jgx = R(0), jgy = R(0), jgz = R(0);
+    for (int st = st0; st <= st1; st++) {
+        const int m = (lane + st) & 31;
+        const V ph = sph[wid][m];
+        const int sj = ssp[wid][m];
+        R vx, vy, vz;
+        if constexpr (sizeof(R) == 8) { vx = hix - ph.x; vy = hiy - ph.y; vz = hiz - ph.z; }
+        else {
+            const V pl = spl[wid][m];
+            vx = (hix - ph.x) + (lix - pl.x);
+            vy = (hiy - ph.y) + (liy - pl.y);
+            vz = (hiz - ph.z) + (liz - pl.z);
+        }
+        const R r2raw = vx * vx + vy * vy + vz * vz;
+        const bool ok = iok && sj >= 0 && !(half && st == 16) && r2raw <= cut2 && r2raw >= R(DBL_EPSILON);
+        // the FP32 form evaluates every lane (branch-free, a rejected term adds
+        // zeros); the FP64 form only the lanes with a term (its library
+        // division, sqrt and pow cost more than the divergence)
+        if (sizeof(R) == 4 || ok) {
+            const int sjc = sj >= 0 ? sj : 0;
+            // C6 and its CN derivatives from the partner's species vectors for species si
+            R u[kRefPad], du[kRefPad];
+            tt_load_uv<R>(UV + ((size_t)(ja0 + (m < nj ? m : 0)) * nid + si) * (2 * kRefPad), u, du);
+            R c6 = R(0), dc6i = R(0), dc6j = R(0);
+#pragma unroll
+            for (int r = 0; r < kMaxRef; r++) {
+                c6 += gwi[r] * u[r];
+                dc6i += dgwi[r] * u[r];
+                dc6j += gwi[r] * du[r];
+            }
+            const V pc = spc[si * nid + sjc];
+            const R rrij = pc.x, q1 = pc.y, q2 = pc.z;
+            R edisp0, gdisp0;
+            if constexpr (DAMP == kRational) {
+                const R r2 = r2raw;
+                const R r4 = r2 * r2;
+                const R a6 = r4 * r2 + q1, a8 = r4 * r4 + q2;
+                const R inv = ok ? tt_rcp<R>(a6 * a8) : R(0);
+                const R t6 = a8 * inv;
+                const R t8 = a6 * inv;
+                const R s8rr = s8 * rrij;
+                edisp0 = s6 * t6 + s8rr * t8;
+                gdisp0 = r4 * (R(-6) * s6 * t6 * t6 + R(-8) * s8rr * r2 * t8 * t8);
+            } else {
+                // zero.f90:490-536 with q1 = rs6 R0, q2 = rs8 R0 (a rejected term at r^2 = 1, weight 0)
+                const R r2 = ok ? r2raw : R(1);
+                const R r1 = tt_sqrt<R>(r2);
+                const R r6 = r2 * r2 * r2;
+                const R r8 = r6 * r2;
+                const R t6 = tt_pow<R>(q1 / r1, alp6);
+                const R t8 = tt_pow<R>(q2 / r1, alp8);
+                const R f6 = R(1) / (R(1) + R(6) * t6);
+                const R f8 = R(1) / (R(1) + R(6) * t8);
+                const R d6 = R(-6) * f6 / r2 + R(6) * alp6 * t6 * (f6 * f6) / r2;
+                const R d8 = R(-8) * f8 / r2 + R(6) * alp8 * t8 * (f8 * f8) / r2;
+                const R sw = ok ? R(1) : R(0);
+                edisp0 = sw * (s6 * f6 / r6 + s8 * rrij * f8 / r8);
+                gdisp0 = sw * (s6 * d6 / r6 + s8 * rrij * d8 / r8);
+            }
+            // E_pair = -C6 edisp (both halves to i), dE/dCN = -dC6/dCN edisp, gradient -C6 gdisp v
+            // (rational.f90:488-497)
+            te -= c6 * edisp0;
+            tde -= dc6i * edisp0;
+            jde -= dc6j * edisp0;
+            const R f = c6 * gdisp0;
+            const R gx = f * vx, gy = f * vy, gz = f * vz;
+            tgx -= gx; tgy -= gy; tgz -= gz;
+            jgx += gx; jgy += gy; jgz += gz;
+            txx -= gx * vx; tyy -= gy * vy; tzz -= gz * vz;
+            txy -= gx * vy; txz -= gx * vz; tyz -= gy * vz;
+        }
+        // the partner's sums move one lane down, with the partner
+        const int src = (lane + 1) & 31;
+        jde = __shfl_sync(0xffffffffu, jde, src);
+        jgx = __shfl_sync(0xffffffffu, jgx, src);
+        jgy = __shfl_sync(0xffffffffu, jgy, src);
+        jgz = __shfl_sync(0xffffffffu, jgz, src);
+    }
+    const double vi[kUnitI] = {double(te),  double(tde), double(tgx), double(tgy), double(tgz),
+                               double(txx), double(tyy), double(tzz), double(txy), double(txz),
+                               double(tyz), 0.0,         0.0,         0.0,         0.0};
+#pragma unroll
+    for (int v = 0; v < kUnitI; v++) oi[v] = vi[v];
+    // this lane holds the sums of partner (lane + st1 + 1) mod 32
+    const int mf = (lane + st1 + 1) & 31;
+    double* oj = unit_j + ((size_t)item * kTile + mf) * kUnitJ;
+    oj[0] = double(jde); oj[1] = double(jgx); oj[2] = double(jgy); oj[3] = double(jgz);
+}
+
 // An atom's sums over the slots of the items that hold it, in a fixed order,
 // one warp per atom.  Lane l adds value l % VI of the atom's i slots (items
 // l / VI, l / VI + 32 / VI, ...) and value l % VJ of its j slots, VI and VJ
@@ -1196,7 +1384,21 @@ void launch_two_body_units(const Batch& b, const Species& s, const Damp& d, cons
     else
         launch_pdl(k_species_vectors<double>, dim3((unsigned)((nsv + 255) / 256)), dim3(256), 0, stream, b, s, w, (double*)pu.U);
     if (ev_begin) cudaEventRecord(ev_begin, stream);
-    if (pu.nunits > 0) {
+    // molecules only (one lattice point), rational or zero damping, gradient,
+    // no parameter derivatives, smooth cutoff, counters or partition: the
+    // diagonal walk without translation lists
+    const bool smooth = c.width2 > 0.0 && c.width2 < c.cut2;
+    const bool rot = pu.single_image && pu.split == 1 && c.grad && !c.param_grad && !smooth && !w.counts &&
+                     p.nparts <= 1 && b.nid <= kMaxSpeciesFast && (d.kind == kRational || d.kind == kZero);
+    if (rot && pu.nunits > 0) {
+        const dim3 grid((pu.nunits + kTTWarps - 1) / kTTWarps), block(kTTThreads);
+#define D3_ROT(R, DK) \
+    launch_pdl(k_two_body_rot<R, DK>, grid, block, 0, stream, b, s, d, c, w, pu.units, pu.nunits, (const R*)pu.U, \
+               pu.unit_i, pu.unit_j)
+        if (d.kind == kRational) { if (c.mixed) D3_ROT(float, kRational); else D3_ROT(double, kRational); }
+        else { if (c.mixed) D3_ROT(float, kZero); else D3_ROT(double, kZero); }
+#undef D3_ROT
+    } else if (pu.nunits > 0) {
         switch (d.kind) {
         case kRational:
             if (c.mixed) launch_tt_flags<float, kRational>(b, s, d, c, p, w, pu, stream);
