@@ -32,6 +32,7 @@ constexpr int kTTChunk = 128;     // translations tested per pass
 constexpr int kUnitI = 15;        // per-lane i sums: E, dE/dCN, g(3), sigma(6), dE/dparam(4)
 constexpr int kUnitJ = 4;         // per-lane j sums: dE/dCN, g(3)
 constexpr int kCnStore = 3;       // stored chain-rule sums per (i, j): countd (3)
+constexpr double kKcnTT = 16.0;   // ncoord.f90:31
 constexpr int kCnSigJ = 8;        // stored-sum CN pass: unit_i slots 8 .. 14 hold the j sums
                                   // (cn, countd v^T (6)) of the column atoms
 constexpr int kSplitMax = 4;      // a unit is evaluated as 1, 2 (j-tile halves) or 4 items
@@ -713,7 +714,8 @@ k_two_body_rot(Batch b, Species s, Damp d, Config c, Work w, const int2* units, 
     // i sums of the lane (FP32 partials in the mixed form), j sums travelling with the partner
     R te = R(0), tde = R(0), tgx = R(0), tgy = R(0), tgz = R(0);
     R txx = R(0), tyy = R(0), tzz = R(0), txy = R(0), txz = R(0), tyz = R(0);
-    R jde = R(0), jgx = R(0), jgy = R(0), jgz = R(0);
+    // the partner's sums travel in FP64 (a sum over the steps in order)
+    double jde = 0.0, jgx = 0.0, jgy = 0.0, jgz = 0.0;
     for (int st = st0; st <= st1; st++) {
         const int m = (lane + st) & 31;
         const V ph = sph[wid][m];
@@ -776,11 +778,11 @@ k_two_body_rot(Batch b, Species s, Damp d, Config c, Work w, const int2* units, 
             // (rational.f90:488-497)
             te -= c6 * edisp0;
             tde -= dc6i * edisp0;
-            jde -= dc6j * edisp0;
+            jde -= double(dc6j * edisp0);
             const R f = c6 * gdisp0;
             const R gx = f * vx, gy = f * vy, gz = f * vz;
             tgx -= gx; tgy -= gy; tgz -= gz;
-            jgx += gx; jgy += gy; jgz += gz;
+            jgx += double(gx); jgy += double(gy); jgz += double(gz);
             txx -= gx * vx; tyy -= gy * vy; tzz -= gz * vz;
             txy -= gx * vy; txz -= gx * vz; tyz -= gy * vz;
         }
@@ -799,7 +801,202 @@ k_two_body_rot(Batch b, Species s, Damp d, Config c, Work w, const int2* units, 
     // this lane holds the sums of partner (lane + st1 + 1) mod 32
     const int mf = (lane + st1 + 1) & 31;
     double* oj = unit_j + ((size_t)item * kTile + mf) * kUnitJ;
-    oj[0] = double(jde); oj[1] = double(jgx); oj[2] = double(jgy); oj[3] = double(jgz);
+    oj[0] = jde; oj[1] = jgx; oj[2] = jgy; oj[3] = jgz;
+}
+
+// Coordination numbers of molecule tile pairs (the single lattice point
+// T = 0; ncoord.f90:86-144) by the diagonal walk of k_two_body_rot, one item
+// per tile pair.  STORE: also the chain rule's countd = dcf v / r of every
+// (lane, step) into `store` (the slot of partner index st in the general
+// kernel's layout) and the per-atom sums S of countd v^T on both sides; the
+// partner's CN (and S) travel with the partner, in FP64 (a sum over the
+// steps in order, not a tree, would lose more in FP32 than the terms do).
+// Slots as k_cn_tt<R, 0 or 2>.
+template <class R, bool STORE>
+__global__ void __launch_bounds__(kTTThreads)
+k_cn_rot(Batch b, Species s, Config c, Work w, const int2* units, int nunits, double* unit_i, double* unit_j,
+         R* store, unsigned char* store_ok)
+{
+    pdl_wait();
+    using V = typename T4<R>::type;
+    __shared__ V sph[kTTWarps][kTile];
+    __shared__ V spl[kTTWarps][kTile];
+    __shared__ double srj[kTTWarps][kTile];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int item = blockIdx.x * kTTWarps + wid;
+    if (item >= nunits) return;
+    const int it = units[item].x, jt = units[item].y;
+    const int sys = b.tile_sys[it];
+    const int t0 = b.tile_off[sys];
+    const int as = b.atom_off[sys], ae = b.atom_off[sys + 1];
+    const int ia0 = as + kTile * (it - t0), ja0 = as + kTile * (jt - t0);
+    const int ni = min(kTile, ae - ia0), nj = min(kTile, ae - ja0);
+    const bool diag = it == jt;
+    double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
+    {
+        // tile spheres farther apart than the cutoff: no term, zero slots
+        const double4 ci = b.tiles[it], cj = b.tiles[jt];
+        const double dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
+        const double lim = c.cut_cn + ci.w + cj.w + 1.0e-6 * c.cut_cn + 1.0e-6;
+        if (dx * dx + dy * dy + dz * dz > lim * lim) {
+            if (STORE) {
+#pragma unroll
+                for (int v = 0; v < 7; v++) { oi[v] = 0.0; oi[kCnSigJ + v] = 0.0; }
+                if (lane == 0) store_ok[item] = 0;
+            } else {
+                oi[0] = 0.0;
+                unit_j[((size_t)item * kTile + lane) * kUnitJ] = 0.0;
+            }
+            return;
+        }
+    }
+    const bool ivalid = lane < ni;
+    const int ic = ivalid ? ia0 + lane : ia0;
+    const double rci = s.rcov[b.sp[ic]];
+    const double xi = b.x[ic], yi = b.y[ic], zi = b.z[ic];
+    R hix, hiy, hiz, lix = R(0), liy = R(0), liz = R(0);
+    if constexpr (sizeof(R) == 8) { hix = xi; hiy = yi; hiz = zi; }
+    else {
+        hix = __double2float_rn(xi); lix = __double2float_rn(xi - (double)hix);
+        hiy = __double2float_rn(yi); liy = __double2float_rn(yi - (double)hiy);
+        hiz = __double2float_rn(zi); liz = __double2float_rn(zi - (double)hiz);
+    }
+    {
+        // the partner tile: positions, covalent radius (a partner outside the system: -1)
+        const bool jv = lane < nj;
+        const int jc = jv ? ja0 + lane : ja0;
+        srj[wid][lane] = jv ? s.rcov[b.sp[jc]] : -1.0;
+        if constexpr (sizeof(R) == 8) {
+            sph[wid][lane] = make_double4(b.x[jc], b.y[jc], b.z[jc], 0.0);
+        } else {
+            sph[wid][lane] = b.xhi[jc];
+            spl[wid][lane] = b.xlo[jc];
+        }
+    }
+    __syncwarp();
+    const R cut2 = R(c.cut_cn * c.cut_cn);
+    const bool half = diag && lane >= 16;
+    const int st0 = diag ? 1 : 0, st1 = diag ? 16 : 31;
+    double cn_i = 0.0;
+    double sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+    double cn_j = 0.0, jxx = 0, jyy = 0, jzz = 0, jxy = 0, jxz = 0, jyz = 0;
+    for (int st = st0; st <= st1; st++) {
+        const int m = (lane + st) & 31;
+        const V ph = sph[wid][m];
+        R vx, vy, vz;
+        if constexpr (sizeof(R) == 8) { vx = hix - ph.x; vy = hiy - ph.y; vz = hiz - ph.z; }
+        else {
+            const V pl = spl[wid][m];
+            vx = (hix - ph.x) + (lix - pl.x);
+            vy = (hiy - ph.y) + (liy - pl.y);
+            vz = (hiz - ph.z) + (liz - pl.z);
+        }
+        const R r2 = vx * vx + vy * vy + vz * vz;
+        const double rcj = srj[wid][m];
+        const bool ok = ivalid && rcj >= 0.0 && !(half && st == 16) && r2 <= cut2 && r2 >= R(1.0e-12);
+        R cf = R(0), f = R(0);
+        // the FP32 form evaluates every lane (a rejected term adds zeros); the
+        // FP64 form only the lanes with a term
+        if (sizeof(R) == 4 || ok) {
+            const R rc = R(rci + rcj);
+            const R rr = ok ? r2 : R(1);
+            if constexpr (sizeof(R) == 8) {
+                const R r1 = sqrt(rr);
+                cf = R(1) / (R(1) + exp(-R(kKcnTT) * (rc / r1 - R(1))));
+                f = -cf * (R(1) - cf) * R(kKcnTT) * rc / rr / r1;
+            } else {
+                const R ir = rsqrtf(rr);
+                cf = __fdividef(1.0f, 1.0f + expf(-R(kKcnTT) * (rc * ir - R(1))));
+                f = -cf * (R(1) - cf) * R(kKcnTT) * rc * (ir * ir * ir);
+            }
+            cf = ok ? cf : R(0);
+            f = ok ? f : R(0);
+        }
+        cn_i += double(cf);
+        cn_j += double(cf);
+        if (STORE) {
+            const R cx = f * vx, cy = f * vy, cz = f * vz;   // countd
+            R* out = store + ((size_t)item * kTile + st) * kCnStore * kTile + lane;
+            out[0] = cx; out[kTile] = cy; out[2 * kTile] = cz;
+            const double qxx = double(cx * vx), qyy = double(cy * vy), qzz = double(cz * vz);
+            const double qxy = double(cx * vy), qxz = double(cx * vz), qyz = double(cy * vz);
+            sxx += qxx; syy += qyy; szz += qzz; sxy += qxy; sxz += qxz; syz += qyz;
+            jxx += qxx; jyy += qyy; jzz += qzz; jxy += qxy; jxz += qxz; jyz += qyz;
+        }
+        // the partner's sums move one lane down, with the partner
+        const int src = (lane + 1) & 31;
+        cn_j = __shfl_sync(0xffffffffu, cn_j, src);
+        if (STORE) {
+            jxx = __shfl_sync(0xffffffffu, jxx, src); jyy = __shfl_sync(0xffffffffu, jyy, src);
+            jzz = __shfl_sync(0xffffffffu, jzz, src); jxy = __shfl_sync(0xffffffffu, jxy, src);
+            jxz = __shfl_sync(0xffffffffu, jxz, src); jyz = __shfl_sync(0xffffffffu, jyz, src);
+        }
+    }
+    // this lane holds the sums of partner (lane + st1 + 1) mod 32
+    const int mf = (lane + st1 + 1) & 31;
+    if (STORE) {
+        // (k_cn_chain_rot reads the steps the walk took only)
+        oi[0] = cn_i;
+        oi[1] = sxx; oi[2] = syy; oi[3] = szz; oi[4] = sxy; oi[5] = sxz; oi[6] = syz;
+        double* oj = unit_i + ((size_t)item * kTile + mf) * kUnitI + kCnSigJ;
+        oj[0] = cn_j;
+        oj[1] = jxx; oj[2] = jyy; oj[3] = jzz;
+        oj[4] = jxy; oj[5] = jxz; oj[6] = jyz;
+        if (lane == 0) store_ok[item] = 1;
+    } else {
+        oi[0] = cn_i;
+        unit_j[((size_t)item * kTile + mf) * kUnitJ] = cn_j;
+    }
+}
+
+// CN chain rule gradient of molecule tile pairs from the sums k_cn_rot<R, true>
+// stored, by the same walk: per (lane, step) the weight dE/dCN_i + dE/dCN_j
+// times the stored countd (ncoord.f90:205-209); the partner's gradient sums
+// travel with the partner.  Slots as k_cn_chain_stored.
+template <class R>
+__global__ void __launch_bounds__(kTTThreads)
+k_cn_chain_rot(Batch b, Work w, const int2* units, int nunits, const R* store, const unsigned char* store_ok,
+               double* unit_i, double* unit_j)
+{
+    pdl_wait();
+    __shared__ double sde[kTTWarps][kTile];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int item = blockIdx.x * kTTWarps + wid;
+    if (item >= nunits) return;
+    const int it = units[item].x, jt = units[item].y;
+    const int sys = b.tile_sys[it];
+    const int t0 = b.tile_off[sys];
+    const int as = b.atom_off[sys], ae = b.atom_off[sys + 1];
+    const int ia0 = as + kTile * (it - t0), ja0 = as + kTile * (jt - t0);
+    const int ni = min(kTile, ae - ia0), nj = min(kTile, ae - ja0);
+    const bool diag = it == jt;
+    double* oi = unit_i + ((size_t)item * kTile + lane) * kUnitI;
+    const int st0 = diag ? 1 : 0, st1 = diag ? 16 : 31;
+    const int mf = (lane + st1 + 1) & 31;
+    double* oj = unit_j + ((size_t)item * kTile + mf) * kUnitJ;
+    if (!store_ok[item]) {
+        oi[0] = 0.0; oi[1] = 0.0; oi[2] = 0.0;
+        oj[0] = 0.0; oj[1] = 0.0; oj[2] = 0.0;
+        return;
+    }
+    const double dei = lane < ni ? w.dEdcn[ia0 + lane] : 0.0;
+    sde[wid][lane] = lane < nj ? w.dEdcn[ja0 + lane] : 0.0;
+    __syncwarp();
+    double gx = 0, gy = 0, gz = 0, jx = 0, jy = 0, jz = 0;
+    for (int st = st0; st <= st1; st++) {
+        const int m = (lane + st) & 31;
+        const R* in = store + ((size_t)item * kTile + st) * kCnStore * kTile + lane;
+        const double dsum = dei + sde[wid][m];
+        const double sx = double(in[0]) * dsum, sy = double(in[kTile]) * dsum, sz = double(in[2 * kTile]) * dsum;
+        gx += sx; gy += sy; gz += sz;
+        jx -= sx; jy -= sy; jz -= sz;
+        const int src = (lane + 1) & 31;
+        jx = __shfl_sync(0xffffffffu, jx, src);
+        jy = __shfl_sync(0xffffffffu, jy, src);
+        jz = __shfl_sync(0xffffffffu, jz, src);
+    }
+    oi[0] = gx; oi[1] = gy; oi[2] = gz;
+    oj[0] = jx; oj[1] = jy; oj[2] = jz;
 }
 
 // An atom's sums over the slots of the items that hold it, in a fixed order,
@@ -864,8 +1061,6 @@ __global__ void k_unit_gather(Batch b, Config c, const int* unit_base, int split
     else if (lane < 5 + kSigma) { if (c.grad) w.sig_atom[kSigma * a + lane - 5] = v; }
     else if (lane < kUnitI) { if (c.param_grad && w.pg_atom) w.pg_atom[kParamGrad * a + lane - 11] = v; }
 }
-
-constexpr double kKcnTT = 16.0;   // ncoord.f90:31
 
 // Coordination number (CHAIN = false, ncoord.f90:86-144) or its chain rule
 // (CHAIN = true, ncoord.f90:152-228) over the tile-pair units with the CN
@@ -1310,7 +1505,34 @@ void launch_cn_units(const Batch& b, const Species& s, const Config& c, const Pa
 #define D3_CN(R, MODE)                                                                                     \
     launch_pdl(k_cn_tt<R, MODE>, dim3(blocks), dim3(kTTThreads), 0, stream, b, s, c, p, w, pu.units, pu.nunits, pu.split,     \
                                                         pu.unit_i, pu.unit_j, (R*)pu.cn_store, pu.cn_store_ok)
-    if (pu.nunits > 0) {
+    // molecules: the diagonal walk (CN with stored sums or alone, chain rule from the stored sums)
+    const bool rot = pu.single_image && pu.split == 1 && p.nparts <= 1 && !c.cn_partitioned && !w.counts &&
+                     (stored || !chain);
+    if (rot && pu.nunits > 0) {
+        const dim3 grid(blocks), block(kTTThreads);
+        if (chain) {
+            if (c.mixed)
+                launch_pdl(k_cn_chain_rot<float>, grid, block, 0, stream, b, w, pu.units, pu.nunits,
+                           (const float*)pu.cn_store, pu.cn_store_ok, pu.unit_i, pu.unit_j);
+            else
+                launch_pdl(k_cn_chain_rot<double>, grid, block, 0, stream, b, w, pu.units, pu.nunits,
+                           (const double*)pu.cn_store, pu.cn_store_ok, pu.unit_i, pu.unit_j);
+        } else if (stored) {
+            if (c.mixed)
+                launch_pdl(k_cn_rot<float, true>, grid, block, 0, stream, b, s, c, w, pu.units, pu.nunits, pu.unit_i,
+                           pu.unit_j, (float*)pu.cn_store, pu.cn_store_ok);
+            else
+                launch_pdl(k_cn_rot<double, true>, grid, block, 0, stream, b, s, c, w, pu.units, pu.nunits, pu.unit_i,
+                           pu.unit_j, (double*)pu.cn_store, pu.cn_store_ok);
+        } else {
+            if (c.mixed)
+                launch_pdl(k_cn_rot<float, false>, grid, block, 0, stream, b, s, c, w, pu.units, pu.nunits, pu.unit_i,
+                           pu.unit_j, (float*)nullptr, pu.cn_store_ok);
+            else
+                launch_pdl(k_cn_rot<double, false>, grid, block, 0, stream, b, s, c, w, pu.units, pu.nunits,
+                           pu.unit_i, pu.unit_j, (double*)nullptr, pu.cn_store_ok);
+        }
+    } else if (pu.nunits > 0) {
         if (chain && stored) {
             if (c.mixed)
                 launch_pdl(k_cn_chain_stored<float>, dim3(blocks), dim3(kTTThreads), 0, stream, b, c, p, w, pu.units, pu.nunits, pu.split, (const float*)pu.cn_store, pu.cn_store_ok, pu.unit_i,
