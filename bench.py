@@ -279,8 +279,9 @@ def batched_launch_modes(run, systems, par, flush, dist, sample=256):
 
 
 def autograd_step(systems, par, flush, steps=2):
-    """Periodic frames through the torch.autograd wrapper: mixed forward (energies)
-    and recomputing backward for positions, cell strain and (s6, s8, a1, a2, s9)."""
+    """Periodic frames through the torch.autograd wrapper: mixed forward (energies
+    with the analytic derivatives of the same pass) and backward for positions,
+    cell strain and (s6, s8, a1, a2, s9)."""
     import torch
     from dftd3.torch_api import D3Batch
     nums = [np.asarray(sy[0]) for sy in systems]

@@ -1,10 +1,10 @@
 """PyTorch autograd wrapper of the batched GPU evaluation.
 
-``DispersionEnergy`` is a ``torch.autograd.Function``: the forward pass
-evaluates the per-system dispersion energies only, the backward pass
-re-evaluates the pipeline with the analytic gradient, virial and damping
-parameter derivatives (it recomputes the pair and triple quantities instead of
-storing them) and applies the chain rule to
+``DispersionEnergy`` is a ``torch.autograd.Function``: when an input requires
+a gradient, the forward pass evaluates the energies together with the analytic
+gradient, virial and damping parameter derivatives in one pass (keeping those
+O(natoms) results, not the pair and triple quantities); otherwise it evaluates
+the energies only.  The backward pass applies the chain rule to
 
 * the Cartesian positions (Bohr),
 * a per-system strain tensor eps: positions x' = x (I + eps)^T and lattice
@@ -103,20 +103,21 @@ def _evaluate(model: D3Batch, positions, params, strain, derivatives: bool):
 
 
 class DispersionEnergy(torch.autograd.Function):
-    """Per-system D3 energies with a recomputing analytic backward pass."""
+    """Per-system D3 energies with the analytic derivatives of the same pass."""
 
     @staticmethod
     def forward(ctx, positions, params, strain, model):
-        energies, _, _, _ = _evaluate(model, positions, params, strain, derivatives=False)
+        derivatives = any(ctx.needs_input_grad[:3])
+        energies, grad, sigma, pgrad = _evaluate(model, positions, params, strain, derivatives=derivatives)
         ctx.model = model
-        ctx.save_for_backward(positions, params, strain)
+        if derivatives:
+            ctx.save_for_backward(positions, params, strain, grad, sigma, pgrad)
         return energies
 
     @staticmethod
     def backward(ctx, grad_e):
-        positions, params, strain = ctx.saved_tensors
+        positions, params, strain, grad, sigma, pgrad = ctx.saved_tensors
         model = ctx.model
-        _, grad, sigma, pgrad = _evaluate(model, positions, params, strain, derivatives=True)
         idx = model._sys_index.to(positions.device)
         ge = grad_e.to(torch.float64)
         deform = torch.eye(3, dtype=torch.float64, device=positions.device) + strain.detach()

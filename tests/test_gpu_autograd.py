@@ -1,5 +1,5 @@
-"""GPU tests of the torch.autograd wrapper: forward energies and the recomputing
-analytic backward pass w.r.t. positions, cell strain and damping parameters,
+"""GPU tests of the torch.autograd wrapper: forward energies and the analytic
+backward pass w.r.t. positions, cell strain and damping parameters,
 against the FP64 oracle (its energies, gradient and virial) and central finite
 differences."""
 import numpy as np
@@ -101,7 +101,7 @@ def test_parameter_and_strain_gradients_fp64():
 
 
 def test_mixed_forward_backward_finite_differences():
-    """Mixed forward + recomputing backward, central differences with h = 1e-4 Bohr."""
+    """Mixed forward + analytic backward, central differences with h = 1e-4 Bohr."""
     import torch
     nums, pos, lats = _frames(nframes=2, natoms=32, seed=8)
     model = _model(nums, lats, "mixed")
