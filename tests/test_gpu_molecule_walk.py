@@ -91,3 +91,27 @@ def test_walks_match_general_sweeps(batch, name):
         assert np.abs(gw - gg).max() <= RTOL64 * max(np.abs(gg).max(), 1e-300)
         vw, vg = np.asarray(walk["virial"][k]), np.asarray(general["virial"][k])
         assert np.abs(vw - vg).max() <= RTOL64 * max(np.abs(vg).max(), 1e-300)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_walks_with_ghost_atoms(precision):
+    """A 300-atom molecule (tile path: the mixed form takes the walks, FP64 the
+    general sweeps above 256 atoms) with ghost atoms, which keep their CN
+    share but have no C6 (model.f90:166-174, 398-401)."""
+    from dftd3 import synthetic as S
+    from dftd3.interface import DispersionModel
+    c = S.cluster5000(seed=43, natoms=300)
+    par = PARAMS["rational"]
+    ghost = [0, 17, 64, 150, 299]
+    ref = O.dispersion(c["numbers"], c["positions"], par, ghost=ghost)
+    model = DispersionModel(c["numbers"], c["positions"])
+    model.set_precision(precision)
+    model.set_ghost_atoms(ghost)
+    res = model.get_dispersion(_param(par), grad=True)
+    e, g = float(res["energy"]), np.asarray(res["gradient"])
+    if precision == "fp64":
+        assert abs(e - ref["energy"]) <= RTOL64 * abs(ref["energy"])
+        assert np.abs(g - ref["gradient"]).max() <= RTOL64 * np.abs(ref["gradient"]).max()
+    else:
+        assert abs(e - ref["energy"]) <= ETOL_MIXED * abs(ref["energy"])
+        assert np.abs(g - ref["gradient"]).max() <= GTOL_MIXED
