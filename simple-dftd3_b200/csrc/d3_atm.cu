@@ -120,17 +120,32 @@ __global__ void k_c6_matrix(Batch b, Species s, Work w, const R* UV, double alp3
                     u[2 * q] = v.x; u[2 * q + 1] = v.y;
                 }
             }
-            double c6 = 0.0, dr = 0.0, dc = 0.0;
+            if constexpr (sizeof(R) == 4) {
+                // the FP32 entries of the mixed form from FP32 operands: FP32 arithmetic
+                float c6 = 0.f, dr = 0.f, dc = 0.f;
 #pragma unroll
-            for (int ir = 0; ir < kMaxRef; ir++) {
-                const double uv = double(u[ir]), du = double(u[kRefPad + ir]);
-                c6 += g[ir] * uv;
-                dr += dg[ir] * uv;
-                dc += g[ir] * du;
-            }
-            if (c6 != 0.0) {
-                const double inv = 1.0 / c6;
-                out = C6Entry<R>{R(sqrt(c6)), R(dr * inv), R(dc * inv), lr0};
+                for (int ir = 0; ir < kMaxRef; ir++) {
+                    c6 += float(g[ir]) * u[ir];
+                    dr += float(dg[ir]) * u[ir];
+                    dc += float(g[ir]) * u[kRefPad + ir];
+                }
+                if (c6 != 0.f) {
+                    const float inv = 1.0f / c6;
+                    out = C6Entry<R>{sqrtf(c6), dr * inv, dc * inv, lr0};
+                }
+            } else {
+                double c6 = 0.0, dr = 0.0, dc = 0.0;
+#pragma unroll
+                for (int ir = 0; ir < kMaxRef; ir++) {
+                    const double uv = double(u[ir]), du = double(u[kRefPad + ir]);
+                    c6 += g[ir] * uv;
+                    dr += dg[ir] * uv;
+                    dc += g[ir] * du;
+                }
+                if (c6 != 0.0) {
+                    const double inv = 1.0 / c6;
+                    out = C6Entry<R>{R(sqrt(c6)), R(dr * inv), R(dc * inv), lr0};
+                }
             }
         }
         row[cl] = out;
